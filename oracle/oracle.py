@@ -1,0 +1,329 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings for the CPU FP64 oracle.
+
+The oracle (pq_oracle.cpp) is a line-by-line C++ restatement of PEQUOD's
+serial QG time-step path.  Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg import this module, and only as the checker; the
+pequod_b200 product never imports it.
+
+Arrays follow the reference's Fortran conventions: numpy arrays in Fortran
+(column-major) order, i fastest; sdata (ii, jj, L), full data arrays
+(ii+2, jj+2, L), FLUX_II (ii+3, jj+2, L), FLUX_JJ (ii+2, jj+3, L).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "_build", "libpq_oracle.so")
+
+BC_PARTIAL_SLIP, BC_NO_SLIP, BC_FREE_SLIP = 1, 2, 3
+
+_dp = C.POINTER(C.c_double)
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc, no fast-math, no FMA)."""
+    src = os.path.join(_HERE, "pq_oracle.cpp")
+    if force or not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", _HERE, "-s"], check=True)
+    return _SO
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(_SO)
+        L.or_helm_create.restype = C.c_void_p
+        L.or_helm_create.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_int]
+        L.or_helm_destroy.argtypes = [C.c_void_p]
+        L.or_helm.argtypes = [C.c_void_p, _dp]
+        L.or_sint.argtypes = [C.c_void_p, _dp]
+        L.or_add_laplace_bc_rhs.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _dp]
+        L.or_apply_dirichlet_bc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _dp]
+        L.or_mean.restype = C.c_double
+        L.or_mean.argtypes = [C.c_int, C.c_int, C.c_int, _dp]
+        L.or_energy.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.or_strat_l2.argtypes = [C.c_double] * 3 + [_dp, _dp]
+        L.or_strat_l3.argtypes = [C.c_double] * 5 + [_dp] * 4
+        L.or_strat_from_parameters.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double] + [_dp] * 6
+        L.or_strat_from_rd.argtypes = [C.c_int, _dp, _dp, C.c_double] + [_dp] * 6
+        L.or_eigen_real_tridiag.argtypes = [C.c_int, _dp, _dp, _dp]
+        L.or_inverse.argtypes = [C.c_int, _dp, _dp]
+        L.or_solve.argtypes = [C.c_int, _dp, _dp, _dp]
+        L.or_determinant.restype = C.c_double
+        L.or_determinant.argtypes = [C.c_int, _dp]
+        L.or_model_create.restype = C.c_void_p
+        L.or_model_create.argtypes = [C.c_void_p]
+        L.or_model_destroy.argtypes = [C.c_void_p]
+        L.or_model_init.argtypes = [C.c_void_p, _dp]
+        L.or_model_step.argtypes = [C.c_void_p, C.c_int]
+        L.or_model_get.restype = C.c_long
+        L.or_model_get.argtypes = [C.c_void_p, C.c_char_p, _dp]
+        L.or_model_set.restype = C.c_long
+        L.or_model_set.argtypes = [C.c_void_p, C.c_char_p, _dp]
+        L.or_model_scalars.argtypes = [C.c_void_p, _dp]
+        L.or_model_energy.argtypes = [C.c_void_p, _dp, _dp]
+        L.or_model_cfl.restype = C.c_double
+        L.or_model_cfl.argtypes = [C.c_void_p]
+        L.or_pv_inversion.argtypes = [C.c_void_p, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim <= 1)
+    return a.ctypes.data_as(_dp)
+
+
+def farray(shape, fill=0.0):
+    return np.full(shape, fill, dtype=np.float64, order="F")
+
+
+class Helm:
+    """helm_cache + helm (qg3p_helmholtz.F90:292-386, 614-769)."""
+
+    def __init__(self, ii, jj, layers, ss, periodic_j=False):
+        ss = np.ascontiguousarray(np.asarray(ss, dtype=np.float64).reshape(layers))
+        self.ii, self.jj, self.layers = ii, jj, layers
+        self.h = lib().or_helm_create(ii, jj, layers, _p(ss), int(periodic_j))
+        if not self.h:
+            raise ValueError("or_helm_create failed")
+
+    def __call__(self, zeta: np.ndarray) -> np.ndarray:
+        z = np.asfortranarray(zeta, dtype=np.float64).reshape((self.ii, self.jj, self.layers), order="F").copy(order="F")
+        rc = lib().or_helm(self.h, _p(z))
+        if rc:
+            raise RuntimeError(f"or_helm rc={rc}")
+        return z
+
+    def sint(self, x: np.ndarray) -> np.ndarray:
+        x = np.array(x, dtype=np.float64)
+        assert x.size == self.ii - 1
+        rc = lib().or_sint(self.h, _p(x))
+        if rc:
+            raise RuntimeError(f"or_sint rc={rc}")
+        return x
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_helm_destroy(self.h)
+            self.h = None
+
+
+def add_laplace_bc_rhs(rhs, bc, bc_d=None, periodic_j=False):
+    r = np.asfortranarray(rhs, dtype=np.float64).copy(order="F")
+    ii, jj = r.shape[0], r.shape[1]
+    L = 1 if r.ndim == 2 else r.shape[2]
+    lib().or_add_laplace_bc_rhs(ii, jj, L, int(periodic_j), bc, bc if bc_d is None else bc_d, _p(r))
+    return r
+
+
+def apply_dirichlet_bc(z, bc, bc_d=None, periodic_j=False):
+    r = np.asfortranarray(z, dtype=np.float64).copy(order="F")
+    ii, jj = r.shape[0], r.shape[1]
+    L = 1 if r.ndim == 2 else r.shape[2]
+    lib().or_apply_dirichlet_bc(ii, jj, L, int(periodic_j), bc, bc if bc_d is None else bc_d, _p(r))
+    return r
+
+
+def mean(psi, periodic_j=False):
+    p = np.asfortranarray(psi, dtype=np.float64)
+    return lib().or_mean(p.shape[0], p.shape[1], int(periodic_j), _p(p))
+
+
+def energy(psi_data, h, s2, periodic_j=False):
+    p = np.asfortranarray(psi_data, dtype=np.float64)
+    ii, jj, L = p.shape[0] - 2, p.shape[1] - 2, p.shape[2]
+    ekin = np.zeros(L)
+    epot = np.zeros(1)
+    lib().or_energy(ii, jj, L, int(periodic_j), _p(np.ascontiguousarray(h, dtype=np.float64)),
+                    _p(np.ascontiguousarray(s2, dtype=np.float64)), _p(p), _p(ekin), _p(epot))
+    return ekin, float(epot[0])
+
+
+def strat_from_parameters(h, s1, s2, l_scale=1.0):
+    """allocate_stratification_parameters: h[L], s1[L-1] (=s1(2:L)), s2[L-1]."""
+    L = len(h)
+    out = [np.zeros(L) for _ in range(4)] + [np.zeros((L, L), order="F") for _ in range(2)]
+    s1a = np.ascontiguousarray(s1 if L > 1 else [0.0], dtype=np.float64)
+    s2a = np.ascontiguousarray(s2 if L > 1 else [0.0], dtype=np.float64)
+    rc = lib().or_strat_from_parameters(L, _p(np.ascontiguousarray(h, dtype=np.float64)), _p(s1a), _p(s2a),
+                                        l_scale, *[_p(o) for o in out])
+    if rc:
+        raise RuntimeError(f"or_strat_from_parameters rc={rc}")
+    keys = ["h", "s1", "s2", "ss", "m2z", "z2m"]
+    return dict(zip(keys, out))
+
+
+def strat_from_rd(rd, h, l_scale=1.0):
+    L = len(h)
+    out = [np.zeros(L) for _ in range(4)] + [np.zeros((L, L), order="F") for _ in range(2)]
+    rda = np.ascontiguousarray(list(rd) + [0.0], dtype=np.float64)
+    rc = lib().or_strat_from_rd(L, _p(rda), _p(np.ascontiguousarray(h, dtype=np.float64)), l_scale,
+                                *[_p(o) for o in out])
+    if rc:
+        raise RuntimeError(f"or_strat_from_rd rc={rc}")
+    return dict(zip(["h", "s1", "s2", "ss", "m2z", "z2m"], out))
+
+
+def eigen(a):
+    a = np.asfortranarray(a, dtype=np.float64)
+    n = a.shape[0]
+    w = np.zeros(n)
+    v = np.zeros((n, n), order="F")
+    rc = lib().or_eigen_real_tridiag(n, _p(a), _p(w), _p(v))
+    if rc:
+        raise RuntimeError("eigen failed")
+    return w, v
+
+
+def inverse(a):
+    a = np.asfortranarray(a, dtype=np.float64)
+    out = np.zeros_like(a, order="F")
+    if lib().or_inverse(a.shape[0], _p(a), _p(out)):
+        raise RuntimeError("singular")
+    return out
+
+
+def solve(a, rhs):
+    a = np.asfortranarray(a, dtype=np.float64)
+    x = np.zeros(a.shape[0])
+    lib().or_solve(a.shape[0], _p(a), _p(np.ascontiguousarray(rhs, dtype=np.float64)), _p(x))
+    return x
+
+
+def determinant(a):
+    a = np.asfortranarray(a, dtype=np.float64)
+    return lib().or_determinant(a.shape[0], _p(a))
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("ii", C.c_int), ("jj", C.c_int), ("layers", C.c_int),
+        ("periodic_j", C.c_int), ("scheme", C.c_int), ("limiter", C.c_int), ("bc_type", C.c_int),
+        ("alpha", C.c_double), ("dt", C.c_double), ("viscosity", C.c_double), ("visc_bot", C.c_double),
+        ("adapt_dt", C.c_int),
+        ("target_cfl", C.c_double), ("max_dt", C.c_double), ("max_dt_increase", C.c_double),
+        ("ra_nu", C.c_double), ("ra_alpha", C.c_double),
+        ("beta", _dp), ("h", _dp), ("s1", _dp), ("s2", _dp), ("ss", _dp), ("m2z", _dp), ("z2m", _dp),
+        ("force_wind", _dp),
+    ]
+
+
+class Model:
+    """The serial qg3 time loop (qg3.F90:590-967) on reference-layout state.
+
+    ``cfg`` is the non-dimensional configuration dictionary produced by
+    pequod_b200.setup (keys: ii, jj, layers, dt, beta, h, s1, s2, ss, m2z,
+    z2m, viscosity, visc_bot, bc_type, alpha, force_wind, scheme, ...).
+    """
+
+    def __init__(self, cfg: dict):
+        self.cfg = cfg
+        L = cfg["layers"]
+        self._keep = {}
+
+        def arr(name, shape=None):
+            a = np.ascontiguousarray(np.asarray(cfg[name], dtype=np.float64).ravel(order="F"))
+            self._keep[name] = a
+            return _p(a)
+
+        P = _Params()
+        P.ii, P.jj, P.layers = cfg["ii"], cfg["jj"], L
+        P.periodic_j = 0
+        P.scheme = cfg.get("scheme", 0)
+        P.limiter = cfg.get("limiter", 1)
+        P.bc_type = cfg.get("bc_type", BC_PARTIAL_SLIP)
+        P.alpha = cfg.get("alpha", 0.0)
+        P.dt = cfg["dt"]
+        P.viscosity = cfg["viscosity"]
+        P.visc_bot = cfg["visc_bot"]
+        P.adapt_dt = cfg.get("adapt_dt", 0)
+        P.target_cfl = cfg.get("target_cfl", 0.1)
+        P.max_dt = cfg.get("max_dt", 1e300)
+        P.max_dt_increase = cfg.get("max_dt_increase", 1.5)
+        P.ra_nu = cfg.get("ra_nu", 0.02)
+        P.ra_alpha = cfg.get("ra_alpha", 0.5)
+        for k in ["beta", "h", "s1", "s2", "ss", "m2z", "z2m"]:
+            setattr(P, k, arr(k))
+        if cfg.get("force_wind") is not None:
+            P.force_wind = arr("force_wind")
+        self._P = P
+        self.m = lib().or_model_create(C.byref(P))
+        if not self.m:
+            raise ValueError("or_model_create failed")
+
+    def init(self, zeta_ic: np.ndarray) -> None:
+        z = np.asfortranarray(zeta_ic, dtype=np.float64)
+        rc = lib().or_model_init(self.m, _p(z))
+        if rc:
+            raise RuntimeError(f"or_model_init rc={rc}")
+
+    def step(self, n: int = 1) -> None:
+        rc = lib().or_model_step(self.m, n)
+        if rc:
+            raise RuntimeError(f"or_model_step rc={rc}")
+
+    def shape_of(self, name):
+        ii, jj, L = self.cfg["ii"], self.cfg["jj"], self.cfg["layers"]
+        if name in ("ui", "uimo", "zeta_fi", "flux_i"):
+            return (ii + 3, jj + 2, L)
+        if name in ("uj", "ujmo", "zeta_fj", "flux_j"):
+            return (ii + 2, jj + 3, L)
+        if name in ("res", "res_beta", "corr"):
+            return (ii, jj, L)
+        return (ii + 2, jj + 2, L)
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.zeros(self.shape_of(name), order="F")
+        n = lib().or_model_get(self.m, name.encode(), _p(out))
+        if n < 0:
+            raise KeyError(name)
+        return out
+
+    def set(self, name: str, value: np.ndarray) -> None:
+        v = np.asfortranarray(value, dtype=np.float64).reshape(self.shape_of(name), order="F")
+        if lib().or_model_set(self.m, name.encode(), _p(v)) < 0:
+            raise KeyError(name)
+
+    def sdata(self, name: str) -> np.ndarray:
+        a = self.get(name)
+        return np.asfortranarray(a[1:-1, 1:-1, :])
+
+    def scalars(self):
+        out = np.zeros(4)
+        lib().or_model_scalars(self.m, _p(out))
+        return dict(dt=out[0], tweight_a=out[1], tweight_u=out[2], model_time=out[3])
+
+    def energy(self):
+        L = self.cfg["layers"]
+        ekin = np.zeros(L)
+        epot = np.zeros(1)
+        rc = lib().or_model_energy(self.m, _p(ekin), _p(epot))
+        if rc:
+            raise RuntimeError("NaN value encountered")
+        return ekin, float(epot[0])
+
+    def cfl(self) -> float:
+        return lib().or_model_cfl(self.m)
+
+    def pv_inversion(self, zeta_data: np.ndarray) -> np.ndarray:
+        z = np.asfortranarray(zeta_data, dtype=np.float64)
+        psi = np.zeros_like(z, order="F")
+        rc = lib().or_pv_inversion(self.m, _p(z), _p(psi))
+        if rc:
+            raise RuntimeError(f"pv_inversion rc={rc}")
+        return psi
+
+    def __del__(self):
+        if getattr(self, "m", None):
+            lib().or_model_destroy(self.m)
+            self.m = None
