@@ -1,0 +1,371 @@
+#!/usr/bin/env python3
+"""Benchmark: CABARET QG time steps of the 3-layer 513 x 513 double gyre.
+
+Workload (the single-GPU configuration the headline metric is quoted on):
+3-layer closed-basin wind-driven double gyre, 513 x 513 nodes (dx = 7.5 km),
+layer depths 300/700/3000 m, reduced gravities 0.015/0.0075 m s^-2,
+f0 = 9.4e-5 s^-1, beta = 1.8e-11 m^-1 s^-1, tau0 = 0.08 N m^-2, bottom drag
+1e-7 s^-1, viscosity 100 m^2 s^-1, partial slip (alpha = 120 km), CABARET with
+the limiter, dt = 900 s.  Initial PV: seeded 1e-7 s^-1 N(0,1) white noise
+smoothed by a Gaussian of 3 cells (synthetic; no dataset exists).
+
+A step is one iteration of the reference's time loop (qg3.F90:590-957) over
+the whole grid.  Metric: cell-layer-steps/s = ii * jj * L * steps / time.
+
+  value  device time of exactly K steps, state resident in HBM; the L2 cache is
+         flushed (a 256 MiB memset) before every timed step and the step is
+         bracketed by CUDA events on the model's stream.
+  e2e    the same K steps through the public C ABI with host buffers:
+         every step copies zeta (ii*jj*L doubles) from pinned host memory to
+         the device, steps, and copies psi back (pq_step_exchange).
+
+--impl reference times the CPU restatement of the reference (the oracle; the
+Fortran/MPI reference cannot be built here) with one process per host core,
+the K steps divided among them.
+
+Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun): one independent replica per GPU ("replicas only": a
+single domain does not shard without an exchange step), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-layer-steps/s"
+UNIT = "cell-layer-steps/s"
+
+
+def workload_args(a):
+    return dict(ii=a.size, layers=a.layers, dt=a.dt)
+
+
+def make_config(ii, layers, dt, precision=0):
+    import pequod_b200 as pq
+
+    H = {3: (3.0e4, 7.0e4, 3.0e5), 5: (2.5e4, 5.0e4, 7.5e4, 1.0e5, 1.5e5)}[layers]
+    gp = {3: (1.5, 0.75), 5: (1.5, 0.75, 0.375, 0.1875)}[layers]
+    dx = 3.84e8 / (ii - 1)
+    p = pq.double_gyre_physical(ii, layers=layers, dt=dt, dx=dx, H=H, gprime=gp, precision=precision)
+    return pq.Config.from_physical(p)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append(out.stdout.strip().splitlines()[0])
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            f = [x.strip() for x in s.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(f) > 5 + k and f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def kernel_bytes_per_cell_layer(L, elem=8):
+    """Algorithmic bytes per cell-layer of each kernel of the FP64 step."""
+    return {
+        # zeta_old, res, ui, res_beta in; zeta, res_beta, spectral rows out
+        "dst_forward": 7 * elem,
+        # spectral rows in and out
+        "tridiag": 2 * elem,
+        # spectral rows in, corr for the baroclinic modes, psi out
+        "dst_inverse_backproject": (2 + (L - 1) / L) * elem,
+        # psi, zeta, zeta_old, uimo, ujmo, zeta_fi, zeta_fj, wind/L in;
+        # zeta_old, res, ui, uj, uimo, ujmo, zeta_fi, zeta_fj out
+        "cabaret_fused": (15 + 1.0 / L) * elem,
+    }
+
+
+def load_traffic(workload):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(workload, {})
+    except Exception:
+        return {}
+
+
+def cpu_baseline_sample(cfg, seconds=10.0):
+    """The oracle (single core) on a bounded sample of the same workload."""
+    from oracle import oracle as O
+    import pequod_b200 as pq
+
+    o = O.Model(cfg.oracle_cfg())
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=1, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    o.init(ic)
+    o.step(1)
+    n = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        o.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    return cfg.ii * cfg.jj * cfg.layers * n / dt, n, dt
+
+
+def _ref_worker(args):
+    ii, layers, dt, steps, seed = args
+    sys.path.insert(0, ROOT)
+    cfg = make_config(ii, layers, dt)
+    from oracle import oracle as O
+    import pequod_b200 as pq
+
+    o = O.Model(cfg.oracle_cfg())
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    o.init(ic)
+    t0 = time.perf_counter()
+    o.step(steps)
+    return time.perf_counter() - t0
+
+
+def run_reference(a, rank, world):
+    """CPU restatement of the reference, all host cores, K steps divided among them."""
+    import multiprocessing as mp
+
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    cfg_units = a.size * a.size * a.layers
+    # Warm-up: W steps on one process (bounded), untimed.
+    procs = max(1, min(cores, a.steps))
+    per = [a.steps // procs + (1 if r < a.steps % procs else 0) for r in range(procs)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        pool.map(_ref_worker, [(a.size, a.layers, a.dt, max(1, min(a.warmup, 3)), r) for r in range(procs)])
+        t0 = time.perf_counter()
+        times = pool.map(_ref_worker, [(a.size, a.layers, a.dt, per[r], 100 + r) for r in range(procs)])
+        wall = time.perf_counter() - t0
+    value = cfg_units * a.steps / wall
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": wall * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"double_gyre_{a.size}x{a.size}x{a.layers}_dt{int(a.dt)}s_cabaret",
+                   "ii": a.size, "jj": a.size, "layers": a.layers},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": f"{a.steps} oracle steps split over {procs} processes "
+                                   f"(C++ restatement of the reference; the Fortran/MPI reference cannot be built)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(a, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import pequod_b200 as pq
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    cfg = make_config(a.size, a.layers, a.dt, precision=0 if a.precision == "fp64" else 1)
+    units = cfg.ii * cfg.jj * cfg.layers
+    m = pq.Model(cfg, device=dev)
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=1 + rank, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    m.init_perturb(ic)
+    m.step(max(3, a.warmup))
+    stream = torch.cuda.ExternalStream(m.stream, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    K = a.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- timed region: K steps, L2 flushed before each ----------------------
+    m.kernel_timing(True)
+    barrier()
+    with ClockSampler(dev) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(K):
+                flush.zero_()
+                ev[k][0].record(stream)
+                m.step_async(1)
+                ev[k][1].record(stream)
+        stream.synchronize()
+    barrier()
+    m.check()
+    m.kernel_timing(False)
+    step_ms = [s.elapsed_time(e) for s, e in ev]
+    total_ms = float(sum(step_ms))
+    kt = m.kernel_times()
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * units * K / (total_ms * 1e-3)
+
+    # ---- back-to-back steps (CUDA graphs, L2 warm), informational -----------
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        m.step_async(K)
+        e1.record(stream)
+    stream.synchronize()
+    m.check()
+    b2b_ms = e0.elapsed_time(e1)
+
+    # ---- e2e: host buffers through the public C ABI ---------------------------
+    zin = torch.empty(units, dtype=torch.float64, pin_memory=True)
+    pout = torch.empty(units, dtype=torch.float64, pin_memory=True)
+    zin.numpy()[:] = np.asfortranarray(m.sdata("zeta")).ravel(order="F")
+    ee = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    barrier()
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.zero_()
+            ee[k][0].record(stream)
+            m.step_exchange(zin.data_ptr(), pout.data_ptr(), pq.PTR_HOST)
+            ee[k][1].record(stream)
+    stream.synchronize()
+    m.check()
+    e2e_ms = float(sum(s.elapsed_time(e) for s, e in ee))
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * units * K / (e2e_ms * 1e-3)
+
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel --------------------------------------
+    peak, peak_kind = peaks()
+    bpc = kernel_bytes_per_cell_layer(cfg.layers)
+    dom = max(kt, key=lambda k: kt[k][0])
+    dom_ms = kt[dom][0] / max(1, kt[dom][1])
+    alg = bpc[dom] * units
+    achieved = alg / (dom_ms * 1e-3) / 1e9
+    workload = f"double_gyre_{cfg.ii}x{cfg.jj}x{cfg.layers}_dt{int(a.dt)}s_cabaret"
+    traffic = load_traffic(workload).get(dom)
+    step_alg = 8 * (22 + 1.0 / cfg.layers) * units  # SURVEY 8(d) B_alg(FP64) per step
+    shares = {k: round(v[0] / max(1e-30, sum(x[0] for x in kt.values())), 4) for k, v in kt.items()}
+    clocks = clk.summary()
+
+    cpu = None
+    if world == 1 and not a.no_cpu_baseline:
+        v, n, secs = cpu_baseline_sample(cfg, seconds=a.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{n} steps of the same {cfg.ii}x{cfg.jj}x{cfg.layers} workload in {secs:.1f} s "
+                         f"(C++ restatement of the reference, one core)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": a.warmup,
+        "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if a.precision == "fp64" else "f32/f64", "data": "synthetic",
+        "config": {"workload": workload, "ii": cfg.ii, "jj": cfg.jj, "layers": cfg.layers, "dt_s": a.dt,
+                   "precision": a.precision, "l2": "flushed before every timed step (256 MiB memset)",
+                   "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "alg_bytes_per_launch": alg, "ms_per_launch": dom_ms},
+        "step_roofline": {"alg_bytes_per_step": step_alg, "achieved_gbs": step_alg / (total_ms / K * 1e-3) / 1e9,
+                          "frac": step_alg / (total_ms / K * 1e-3) / 1e9 / peak},
+        "kernel_shares": shares,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": units * 8, "d2h_bytes_per_step": units * 8},
+        "gpu_launches": 4 * K,
+        "back_to_back": {"value": world * units * K / (b2b_ms * 1e-3), "ms_per_step": b2b_ms / K,
+                         "note": "CUDA-graph replay, L2 not flushed"},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=513)
+    ap.add_argument("--layers", type=int, default=3)
+    ap.add_argument("--dt", type=float, default=900.0)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+    else:
+        run_ours(a, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

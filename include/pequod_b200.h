@@ -1,0 +1,236 @@
+/*
+ * pequod_b200.h -- C ABI of the B200-native PEQUOD QG time-step hot path.
+ *
+ * The reference (PEQUOD, Fortran 2003 + MPI) has no C or FFI plugin API; its
+ * swap point for the elliptic solver is the module alias in qg3p_aux.F90:10-17
+ *     use qg_helmholtz, only : solve_helmholtz => helm, helmholtz_solver_cache => helm_cache
+ * and the advection routines are qg_aux's public list (qg3p_aux.F90:33-43),
+ * called positionally from qg3.F90:598-807,952.  Every entry point below is
+ * the C side of a bind(C) interface that replaces one of those Fortran
+ * routines; INTEGRATION.md shows the Fortran interface module.
+ *
+ * Conventions
+ *  - Arrays are Fortran column-major, i (first index) fastest, REAL(8).
+ *    sdata-shaped arrays are (ii, jj, L); "reference layout" arrays in
+ *    pq_get_field / pq_set_field are the reference's own shapes:
+ *      full data (ii+2, jj+2, L), FLUX_II (ii+3, jj+2, L),
+ *      FLUX_JJ (ii+2, jj+3, L), residuals (ii, jj, L)
+ *    (qg3p_base.F90:1322-1323, 2808-2818; qg3.F90:84).
+ *  - ptr_kind: PQ_PTR_HOST (pointer into host memory, copied) or
+ *    PQ_PTR_DEVICE (dense device array on the context's device).
+ *  - Every call returns PQ_OK (0) or a PQ_ERR_* code and never aborts the
+ *    process (the reference calls mpi_abort, qg3p_base.F90:383-403);
+ *    pq_last_error() gives the message.
+ *  - One context per caller thread; calls on different contexts are
+ *    independent.  A context's device state persists between calls.
+ *  - All quantities are in the reference's non-dimensional units
+ *    (qg3.F90:152-168): grid spacing 1, t_scale = l_scale / u_scale.
+ */
+#ifndef PEQUOD_B200_H
+#define PEQUOD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PQ_API __attribute__((visibility("default")))
+#else
+#define PQ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PQ_OK 0
+#define PQ_ERR_ARG 1         /* invalid argument / unsupported size */
+#define PQ_ERR_CUDA 2        /* CUDA runtime error */
+#define PQ_ERR_NAN 3         /* NaN psiC or energy (the reference aborts) */
+#define PQ_ERR_NOMEM 4       /* device allocation failed */
+#define PQ_ERR_UNSUPPORTED 5 /* feature not available in this build */
+#define PQ_ERR_STATE 6       /* call out of order (e.g. step before init) */
+#define PQ_ERR_BUDGET 7      /* request exceeds the server's HBM budget */
+#define PQ_ERR_NOTFOUND 8    /* unknown request id */
+
+#define PQ_PTR_HOST 0
+#define PQ_PTR_DEVICE 1
+
+#define PQ_SCHEME_CABARET 0  /* config.h: #define CABARET, CABARET_LIMITER */
+#define PQ_SCHEME_LEAPFROG 1 /* config.h: #undef CABARET (centred + RAW filter) */
+
+#define PQ_PREC_FP64 0       /* plain form: FP64 throughout */
+#define PQ_PREC_MIXED 1      /* FP32 storage/transforms, FP64 barotropic solve, projection and reductions */
+
+/* Velocity boundary conditions, qg3p_diagnostics.F90:57-58. */
+#define PQ_BC_PARTIAL_SLIP 1
+#define PQ_BC_NO_SLIP 2
+#define PQ_BC_FREE_SLIP 3
+
+#define PQ_MAX_LAYERS 8
+
+/* Fields of the model state, for pq_get_field / pq_set_field. */
+#define PQ_F_PSI 0       /* psi%data       (ii+2, jj+2, L) */
+#define PQ_F_ZETA 1      /* zeta%data      (ii+2, jj+2, L) */
+#define PQ_F_REL 2       /* rel%data       (ii+2, jj+2, L) */
+#define PQ_F_ZETA_OLD 3  /* zeta_old       (ii+2, jj+2, L) */
+#define PQ_F_UI 4        /* ui%data        (ii+3, jj+2, L) */
+#define PQ_F_UJ 5        /* uj%data        (ii+2, jj+3, L) */
+#define PQ_F_UIMO 6      /* uimo%data      (ii+3, jj+2, L) */
+#define PQ_F_UJMO 7      /* ujmo%data      (ii+2, jj+3, L) */
+#define PQ_F_ZETA_FI 8   /* zeta_fi%data   (ii+3, jj+2, L) */
+#define PQ_F_ZETA_FJ 9   /* zeta_fj%data   (ii+2, jj+3, L) */
+#define PQ_F_RES 10      /* res            (ii, jj, L) */
+#define PQ_F_RES_BETA 11 /* res_beta       (ii, jj, L) */
+#define PQ_F_CORR 12     /* hcache%corr    (ii, jj, L), read only */
+
+/* Model description in non-dimensional units.  Matrices are column-major
+ * with leading dimension `layers` (the Fortran strat%modes_to_z layout). */
+typedef struct pq_model_desc {
+    int ii, jj, layers;   /* nodes including the boundary; ii - 1 = 2^p, p >= 2 */
+    int periodic_j;       /* must be 0: closed basin */
+    int scheme;           /* PQ_SCHEME_* */
+    int limiter;          /* CABARET_LIMITER (1 = on) */
+    int bc_type;          /* PQ_BC_* */
+    int precision;        /* PQ_PREC_* */
+    int adapt_dt;         /* cabaret_adapt_dt each step */
+    double alpha;         /* partial-slip parameter l_scale / alpha_dim */
+    double dt;            /* time step */
+    double viscosity;     /* lateral viscosity */
+    double visc_bot;      /* bottom drag */
+    double target_cfl, max_dt, max_dt_increase;  /* adaptive time step */
+    double ra_nu, ra_alpha;                      /* leapfrog RAW filter */
+    double beta[PQ_MAX_LAYERS];   /* beta per layer */
+    double h[PQ_MAX_LAYERS];      /* layer thicknesses */
+    double s1[PQ_MAX_LAYERS];     /* strat%s1 (s1[0] unused) */
+    double s2[PQ_MAX_LAYERS];     /* strat%s2 (s2[L-1] unused) */
+    double ss[PQ_MAX_LAYERS];     /* strat%ss, ss[0] = 0 (barotropic) */
+    double m2z[PQ_MAX_LAYERS * PQ_MAX_LAYERS];  /* strat%modes_to_z */
+    double z2m[PQ_MAX_LAYERS * PQ_MAX_LAYERS];  /* strat%z_to_modes */
+    const double* force_wind;     /* (ii, jj) layer-1 wind forcing, or NULL */
+} pq_model_desc;
+
+/* Physical (cgs) description of a wind-driven double gyre; converted to a
+ * pq_model_desc by pq_setup_double_gyre the way qg3.F90:150-307 does. */
+typedef struct pq_physical {
+    int ii, jj, layers;
+    double basinscale;      /* cm: (ii - 1) * dx (qg3p_params.F90:47) */
+    double dt;              /* s */
+    double f0;              /* s^-1 */
+    double beta;            /* cm^-1 s^-1 */
+    double H[PQ_MAX_LAYERS];       /* cm */
+    double gprime[PQ_MAX_LAYERS];  /* cm s^-2, interfaces 1..L-1 */
+    double tau;             /* cm^2 s^-2: wind stress / rho */
+    double wind_asym, wind_tilt, wind_shift;
+    double visc;            /* cm^2 s^-1 */
+    double visc_bot;        /* s^-1 */
+    double alpha;           /* cm; >= 1e100 selects free slip */
+    int partial_slip;       /* 0: no slip */
+    int scheme, limiter, precision, adapt_dt;
+    double target_cfl, max_dt, max_dt_increase;  /* max_dt in s */
+    double u_scale;         /* cm s^-1 (qg3p_params.F90:105) */
+} pq_physical;
+
+typedef struct pq_ctx pq_ctx;
+
+/* ---- set-up (host) ------------------------------------------------------ */
+
+/* Stratification from layer thicknesses and s1(2:L), s2(1:L-1) in cgs
+ * (allocate_stratification_parameters + s_conversion_matrices,
+ * qg3p_diagnostics.F90:210-236, 372-422): fills h, s1, s2, ss, m2z, z2m of
+ * `d` scaled by l_scale. */
+PQ_API int pq_stratification(pq_model_desc* d, int layers, const double* H, const double* s1_in,
+                      const double* s2_in, double l_scale);
+
+/* Non-dimensionalisation, stratification, wind forcing and beta of
+ * qg3.F90:150-307.  wind_out: caller buffer of ii*jj doubles that d->force_wind
+ * will point to. */
+PQ_API int pq_setup_double_gyre(const pq_physical* p, pq_model_desc* d, double* wind_out, double* t_scale_out);
+
+/* Seeded synthetic initial PV: amplitude * (N(0,1) white noise smoothed by a
+ * separable Gaussian of standard deviation sigma cells), sdata (ii, jj, L). */
+PQ_API int pq_make_ic(int ii, int jj, int layers, uint64_t seed, double amplitude, double sigma, double* out);
+
+/* ---- context ------------------------------------------------------------ */
+
+/* helm_cache + helmholtz_cache allocation (qg3p_aux.F90:152-193,
+ * qg3p_helmholtz.F90:292-386) plus the device model state. */
+PQ_API int pq_create(pq_ctx** out, const pq_model_desc* d, int device);
+PQ_API void pq_destroy(pq_ctx* ctx);
+PQ_API const char* pq_last_error(const pq_ctx* ctx);
+PQ_API size_t pq_device_bytes(const pq_ctx* ctx);
+
+/* ---- drop-in elliptic entry points --------------------------------------- */
+
+/* helm(helm_c, zeta), qg3p_helmholtz.F90:614-769: zeta (ii, jj, L) holds the
+ * right-hand side on entry and the solution on exit, with helm's in-place
+ * semantics (boundary entries untouched except row ii and column 1, which
+ * are zeroed).  The layers of the context are the modes, ss = d->ss. */
+PQ_API int pq_helm(pq_ctx* ctx, double* zeta, int ptr_kind);
+
+/* pv_inversion(strat, vbc, zeta, hcache, psi), qg3p_aux.F90:452-479:
+ * zeta sdata (ii, jj, L) in, psi sdata (ii, jj, L) out.  Returns PQ_ERR_NAN
+ * where the reference aborts on a NaN psiC. */
+PQ_API int pq_pv_inversion(pq_ctx* ctx, const double* zeta_sdata, double* psi_sdata, int ptr_kind);
+
+/* ---- model state and time stepping -------------------------------------- */
+
+/* START_PERTURB initialisation, qg3.F90:365-404 and :450-459: zeta sdata
+ * (ii, jj, L) initial PV; Dirichlet 0, inversion, rel and boundary PV, zeroed
+ * CABARET fields, zeta_old = zeta, tweights 0.5. */
+PQ_API int pq_init_perturb(pq_ctx* ctx, const double* zeta_ic, int ptr_kind);
+
+/* nsteps iterations of the CABARET timestep_loop body (qg3.F90:590-957):
+ * adapt_dt, predictor, beta, pv_inversion, rel, boundary PV, forcing, cell
+ * boundaries, extrapolator, flux, corrector, zeta_old = zeta.  Runs as
+ * captured CUDA graphs on the context's stream. */
+PQ_API int pq_step(pq_ctx* ctx, int nsteps);
+
+/* pq_step without the final wait: enqueues the steps on the context's stream
+ * and returns.  pq_check waits for the stream and reports a NaN psiC or
+ * energy (PQ_ERR_NAN) raised by the device since initialisation. */
+PQ_API int pq_step_async(pq_ctx* ctx, int nsteps);
+PQ_API int pq_check(pq_ctx* ctx);
+
+/* One step with the prognostic state exchanged through caller buffers, the
+ * way a host-side driver that owns its arrays would call the solver: if
+ * zeta_in is not NULL it replaces zeta (sdata (ii, jj, L)) before the step;
+ * if psi_out is not NULL it receives the step's psi (sdata).  Asynchronous:
+ * host buffers should be pinned; pq_check or pq_sync completes the copies. */
+PQ_API int pq_step_exchange(pq_ctx* ctx, const double* zeta_in, double* psi_out, int ptr_kind);
+
+/* energy(strat, psi, ekin, epot), qg3p_diagnostics.F90:778-863, on the
+ * current psi.  ekin: L doubles. */
+PQ_API int pq_energy(pq_ctx* ctx, double* ekin, double* epot);
+
+/* cabaret_cfl, qg3p_aux.F90:920-942, of the last step's face velocities. */
+PQ_API int pq_cfl(pq_ctx* ctx, double* cfl);
+
+/* Copy a state field (PQ_F_*) out of / into the context, reference layout,
+ * host memory. */
+PQ_API int pq_get_field(pq_ctx* ctx, int field, double* out);
+PQ_API int pq_set_field(pq_ctx* ctx, int field, const double* in);
+
+/* dt, tweight_a, tweight_u, model_time (non-dimensional). */
+PQ_API int pq_get_scalars(pq_ctx* ctx, double* out4);
+
+/* Block until the context's queued device work is complete. */
+PQ_API int pq_sync(pq_ctx* ctx);
+
+/* The CUDA stream the context's work is ordered on (a cudaStream_t). */
+PQ_API void* pq_stream(pq_ctx* ctx);
+
+/* Per-kernel CUDA-event timing of steps launched outside CUDA graphs (an odd
+ * single step, or every step of pq_step_async(ctx, 1)).  pq_kernel_times
+ * waits for the stream and returns, for the four kernels of a step
+ * (forward DST, tridiagonal, inverse DST + back-projection, fused CABARET),
+ * the summed milliseconds and launch counts since the last call. */
+PQ_API int pq_kernel_timing(pq_ctx* ctx, int enable);
+PQ_API int pq_kernel_times(pq_ctx* ctx, double* ms4, long* launches4);
+
+/* Number of kernel launches the last pq_step enqueued. */
+PQ_API long pq_last_launch_count(const pq_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PEQUOD_B200_H */

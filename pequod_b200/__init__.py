@@ -1,0 +1,341 @@
+"""pequod_b200: B200-native (sm_100a) QG time-step hot path of PEQUOD.
+
+Python mirror of the C ABI in include/pequod_b200.h.  The compute path is the
+CUDA library pequod_b200/_lib/libpequod_b200.so; this module only marshals
+arguments.  There is no CPU fallback: if the library is missing or cannot be
+loaded the import of the native handle raises.
+
+The interface follows the reference's routines (qg3p_helmholtz.F90 helm,
+qg3p_aux.F90 pv_inversion / cabaret_*, qg3p_diagnostics.F90 energy) with
+Fortran-ordered numpy arrays in the reference's layouts.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "_lib", "libpequod_b200.so")
+
+PQ_OK = 0
+PQ_ERR_ARG, PQ_ERR_CUDA, PQ_ERR_NAN, PQ_ERR_NOMEM, PQ_ERR_UNSUPPORTED, PQ_ERR_STATE, PQ_ERR_BUDGET, PQ_ERR_NOTFOUND = (
+    1, 2, 3, 4, 5, 6, 7, 8)
+PTR_HOST, PTR_DEVICE = 0, 1
+SCHEME_CABARET, SCHEME_LEAPFROG = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+BC_PARTIAL_SLIP, BC_NO_SLIP, BC_FREE_SLIP = 1, 2, 3
+MAX_LAYERS = 8
+
+FIELDS = {
+    "psi": 0, "zeta": 1, "rel": 2, "zeta_old": 3, "ui": 4, "uj": 5, "uimo": 6, "ujmo": 7,
+    "zeta_fi": 8, "zeta_fj": 9, "res": 10, "res_beta": 11, "corr": 12,
+}
+
+_dp = C.POINTER(C.c_double)
+
+
+class PQError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pequod_b200 error {code}: {msg}")
+        self.code = code
+
+
+class ModelDesc(C.Structure):
+    _fields_ = [
+        ("ii", C.c_int), ("jj", C.c_int), ("layers", C.c_int), ("periodic_j", C.c_int),
+        ("scheme", C.c_int), ("limiter", C.c_int), ("bc_type", C.c_int), ("precision", C.c_int),
+        ("adapt_dt", C.c_int),
+        ("alpha", C.c_double), ("dt", C.c_double), ("viscosity", C.c_double), ("visc_bot", C.c_double),
+        ("target_cfl", C.c_double), ("max_dt", C.c_double), ("max_dt_increase", C.c_double),
+        ("ra_nu", C.c_double), ("ra_alpha", C.c_double),
+        ("beta", C.c_double * MAX_LAYERS), ("h", C.c_double * MAX_LAYERS),
+        ("s1", C.c_double * MAX_LAYERS), ("s2", C.c_double * MAX_LAYERS), ("ss", C.c_double * MAX_LAYERS),
+        ("m2z", C.c_double * (MAX_LAYERS * MAX_LAYERS)), ("z2m", C.c_double * (MAX_LAYERS * MAX_LAYERS)),
+        ("force_wind", _dp),
+    ]
+
+
+class Physical(C.Structure):
+    _fields_ = [
+        ("ii", C.c_int), ("jj", C.c_int), ("layers", C.c_int),
+        ("basinscale", C.c_double), ("dt", C.c_double), ("f0", C.c_double), ("beta", C.c_double),
+        ("H", C.c_double * MAX_LAYERS), ("gprime", C.c_double * MAX_LAYERS),
+        ("tau", C.c_double), ("wind_asym", C.c_double), ("wind_tilt", C.c_double), ("wind_shift", C.c_double),
+        ("visc", C.c_double), ("visc_bot", C.c_double), ("alpha", C.c_double), ("partial_slip", C.c_int),
+        ("scheme", C.c_int), ("limiter", C.c_int), ("precision", C.c_int), ("adapt_dt", C.c_int),
+        ("target_cfl", C.c_double), ("max_dt", C.c_double), ("max_dt_increase", C.c_double),
+        ("u_scale", C.c_double),
+    ]
+
+
+# Every function the C ABI exports, with its ctypes signature.
+SIGNATURES = {
+    "pq_stratification": (C.c_int, [C.POINTER(ModelDesc), C.c_int, _dp, _dp, _dp, C.c_double]),
+    "pq_setup_double_gyre": (C.c_int, [C.POINTER(Physical), C.POINTER(ModelDesc), _dp, _dp]),
+    "pq_make_ic": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_double, _dp]),
+    "pq_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelDesc), C.c_int]),
+    "pq_destroy": (None, [C.c_void_p]),
+    "pq_last_error": (C.c_char_p, [C.c_void_p]),
+    "pq_device_bytes": (C.c_size_t, [C.c_void_p]),
+    "pq_helm": (C.c_int, [C.c_void_p, _dp, C.c_int]),
+    "pq_pv_inversion": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    "pq_init_perturb": (C.c_int, [C.c_void_p, _dp, C.c_int]),
+    "pq_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "pq_step_async": (C.c_int, [C.c_void_p, C.c_int]),
+    "pq_check": (C.c_int, [C.c_void_p]),
+    "pq_step_exchange": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    "pq_energy": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "pq_cfl": (C.c_int, [C.c_void_p, _dp]),
+    "pq_get_field": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "pq_set_field": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "pq_get_scalars": (C.c_int, [C.c_void_p, _dp]),
+    "pq_sync": (C.c_int, [C.c_void_p]),
+    "pq_stream": (C.c_void_p, [C.c_void_p]),
+    "pq_last_launch_count": (C.c_long, [C.c_void_p]),
+    "pq_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "pq_kernel_times": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_long)]),
+}
+
+KERNELS = ("dst_forward", "tridiag", "dst_inverse_backproject", "cabaret_fused")
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library.  Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"pequod_b200 native library not built: {LIB_PATH} (run pequod_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _check(rc, ctx=None):
+    if rc != PQ_OK:
+        msg = lib().pq_last_error(ctx).decode() if ctx else ""
+        raise PQError(rc, msg)
+
+
+# ---------------------------------------------------------------------------
+# Configurations
+
+
+def double_gyre_physical(ii, jj=None, layers=3, dt=1800.0, dx=30.0e5, H=(3.0e4, 7.0e4, 3.0e5),
+                         gprime=(1.5, 0.75), f0=9.4e-5, beta=1.8e-13, tau=0.8, visc=1.0e6, visc_bot=1.0e-7,
+                         alpha=120.0e5, partial_slip=True, wind_asym=1.0, wind_tilt=0.0, wind_shift=0.0,
+                         scheme=SCHEME_CABARET, limiter=1, precision=PREC_FP64, adapt_dt=0,
+                         target_cfl=0.1, max_dt=86400.0, max_dt_increase=1.5) -> Physical:
+    """Wind-driven closed-basin double gyre in cgs units.
+
+    Defaults are the 3-layer 129 x 129, dx = 30 km configuration: layer depths
+    300/700/3000 m, reduced gravities 0.015/0.0075 m s^-2, f0 = 9.4e-5 s^-1,
+    beta = 1.8e-11 m^-1 s^-1, tau0 = 0.08 N m^-2 (0.8 cm^2 s^-2 over
+    rho0 = 1000 kg m^-3) with a -cos(2 pi y / L) profile, bottom drag 1e-7 s^-1,
+    lateral viscosity 100 m^2 s^-1, partial slip with alpha = 120 km.
+    """
+    jj = ii if jj is None else jj
+    p = Physical()
+    p.ii, p.jj, p.layers = ii, jj, layers
+    p.basinscale = (ii - 1) * dx
+    p.dt, p.f0, p.beta = dt, f0, beta
+    H = list(H)
+    if len(H) != layers:
+        raise ValueError("len(H) != layers")
+    for k in range(layers):
+        p.H[k] = H[k]
+    for k in range(layers - 1):
+        p.gprime[k] = gprime[k]
+    p.tau, p.wind_asym, p.wind_tilt, p.wind_shift = tau, wind_asym, wind_tilt, wind_shift
+    p.visc, p.visc_bot, p.alpha, p.partial_slip = visc, visc_bot, alpha, int(partial_slip)
+    p.scheme, p.limiter, p.precision, p.adapt_dt = scheme, limiter, precision, adapt_dt
+    p.target_cfl, p.max_dt, p.max_dt_increase = target_cfl, max_dt, max_dt_increase
+    p.u_scale = 1.0
+    return p
+
+
+class Config:
+    """A non-dimensional model description plus its wind-forcing buffer."""
+
+    def __init__(self, desc: ModelDesc, wind: np.ndarray | None, t_scale: float):
+        self.desc = desc
+        self.wind = wind
+        self.t_scale = t_scale
+        if wind is not None:
+            self.desc.force_wind = _p(self.wind)
+
+    @classmethod
+    def from_physical(cls, p: Physical) -> "Config":
+        d = ModelDesc()
+        wind = np.zeros((p.ii, p.jj), order="F")
+        ts = np.zeros(1)
+        _check(lib().pq_setup_double_gyre(C.byref(p), C.byref(d), _p(wind), _p(ts)))
+        return cls(d, wind, float(ts[0]))
+
+    @property
+    def ii(self):
+        return self.desc.ii
+
+    @property
+    def jj(self):
+        return self.desc.jj
+
+    @property
+    def layers(self):
+        return self.desc.layers
+
+    def modal(self):
+        L = self.layers
+        m2z = np.array(self.desc.m2z[: L * L]).reshape((L, L), order="F")
+        z2m = np.array(self.desc.z2m[: L * L]).reshape((L, L), order="F")
+        return np.array(self.desc.ss[:L]), m2z, z2m
+
+    def oracle_cfg(self) -> dict:
+        """The same configuration as a dictionary for the CPU oracle."""
+        L = self.layers
+        ss, m2z, z2m = self.modal()
+        d = self.desc
+        return dict(
+            ii=d.ii, jj=d.jj, layers=L, dt=d.dt, beta=list(d.beta[:L]), h=list(d.h[:L]), s1=list(d.s1[:L]),
+            s2=list(d.s2[:L]), ss=ss, m2z=m2z, z2m=z2m, viscosity=d.viscosity, visc_bot=d.visc_bot,
+            bc_type=d.bc_type, alpha=d.alpha, force_wind=self.wind, scheme=d.scheme, limiter=d.limiter,
+            adapt_dt=d.adapt_dt, target_cfl=d.target_cfl, max_dt=d.max_dt, max_dt_increase=d.max_dt_increase,
+            ra_nu=d.ra_nu, ra_alpha=d.ra_alpha,
+        )
+
+
+def make_ic(ii, jj, layers, seed=0, amplitude=1.0, sigma=3.0) -> np.ndarray:
+    """Seeded synthetic initial PV (N(0,1) noise smoothed by a Gaussian of sigma cells)."""
+    out = np.zeros((ii, jj, layers), order="F")
+    _check(lib().pq_make_ic(ii, jj, layers, seed, amplitude, sigma, _p(out)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+
+
+class Model:
+    """One device context: helm / pv_inversion drop-ins and the CABARET loop."""
+
+    def __init__(self, cfg: Config, device: int = 0):
+        self.cfg = cfg
+        self.ctx = C.c_void_p()
+        rc = lib().pq_create(C.byref(self.ctx), C.byref(cfg.desc), device)
+        if rc != PQ_OK:
+            msg = lib().pq_last_error(self.ctx).decode() if self.ctx else ""
+            if self.ctx:
+                lib().pq_destroy(self.ctx)
+                self.ctx = None
+            raise PQError(rc, msg)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            lib().pq_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def shape(self):
+        return (self.cfg.ii, self.cfg.jj, self.cfg.layers)
+
+    def helm(self, zeta: np.ndarray) -> np.ndarray:
+        z = np.array(zeta, dtype=np.float64, order="F").reshape(self.shape, order="F")
+        _check(lib().pq_helm(self.ctx, _p(z), PTR_HOST), self.ctx)
+        return z
+
+    def pv_inversion(self, zeta_sdata: np.ndarray) -> np.ndarray:
+        z = np.asfortranarray(zeta_sdata, dtype=np.float64).reshape(self.shape, order="F")
+        psi = np.zeros(self.shape, order="F")
+        _check(lib().pq_pv_inversion(self.ctx, _p(z), _p(psi), PTR_HOST), self.ctx)
+        return psi
+
+    def init_perturb(self, zeta_ic: np.ndarray) -> None:
+        z = np.asfortranarray(zeta_ic, dtype=np.float64).reshape(self.shape, order="F")
+        _check(lib().pq_init_perturb(self.ctx, _p(z), PTR_HOST), self.ctx)
+
+    def step(self, n: int = 1) -> None:
+        _check(lib().pq_step(self.ctx, n), self.ctx)
+
+    def step_async(self, n: int = 1) -> None:
+        _check(lib().pq_step_async(self.ctx, n), self.ctx)
+
+    def check(self) -> None:
+        _check(lib().pq_check(self.ctx), self.ctx)
+
+    def step_exchange(self, zeta_in_ptr, psi_out_ptr, ptr_kind=PTR_HOST) -> None:
+        """One step exchanging zeta in / psi out through raw pointers (pinned host or device)."""
+        _check(lib().pq_step_exchange(self.ctx, C.cast(zeta_in_ptr, _dp) if zeta_in_ptr else None,
+                                      C.cast(psi_out_ptr, _dp) if psi_out_ptr else None, ptr_kind), self.ctx)
+
+    @property
+    def stream(self) -> int:
+        return int(lib().pq_stream(self.ctx) or 0)
+
+    def sync(self) -> None:
+        _check(lib().pq_sync(self.ctx), self.ctx)
+
+    def energy(self):
+        ekin = np.zeros(self.cfg.layers)
+        epot = np.zeros(1)
+        _check(lib().pq_energy(self.ctx, _p(ekin), _p(epot)), self.ctx)
+        return ekin, float(epot[0])
+
+    def cfl(self) -> float:
+        out = np.zeros(1)
+        _check(lib().pq_cfl(self.ctx, _p(out)), self.ctx)
+        return float(out[0])
+
+    def field_shape(self, name):
+        ii, jj, L = self.shape
+        if name in ("ui", "uimo", "zeta_fi"):
+            return (ii + 3, jj + 2, L)
+        if name in ("uj", "ujmo", "zeta_fj"):
+            return (ii + 2, jj + 3, L)
+        if name in ("res", "res_beta", "corr"):
+            return (ii, jj, L)
+        return (ii + 2, jj + 2, L)
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.zeros(self.field_shape(name), order="F")
+        _check(lib().pq_get_field(self.ctx, FIELDS[name], _p(out)), self.ctx)
+        return out
+
+    def set(self, name: str, value: np.ndarray) -> None:
+        v = np.asfortranarray(value, dtype=np.float64).reshape(self.field_shape(name), order="F")
+        _check(lib().pq_set_field(self.ctx, FIELDS[name], _p(v)), self.ctx)
+
+    def sdata(self, name: str) -> np.ndarray:
+        return np.asfortranarray(self.get(name)[1:-1, 1:-1, :])
+
+    def scalars(self):
+        out = np.zeros(4)
+        _check(lib().pq_get_scalars(self.ctx, _p(out)), self.ctx)
+        return dict(dt=out[0], tweight_a=out[1], tweight_u=out[2], model_time=out[3])
+
+    def device_bytes(self) -> int:
+        return int(lib().pq_device_bytes(self.ctx))
+
+    def last_launch_count(self) -> int:
+        return int(lib().pq_last_launch_count(self.ctx))
+
+    def kernel_timing(self, enable: bool) -> None:
+        _check(lib().pq_kernel_timing(self.ctx, int(enable)), self.ctx)
+
+    def kernel_times(self) -> dict:
+        ms = np.zeros(4)
+        n = (C.c_long * 4)()
+        _check(lib().pq_kernel_times(self.ctx, _p(ms), n), self.ctx)
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNELS)}

@@ -1,0 +1,737 @@
+// pq_api.cu -- the C ABI: contexts, device state, tables and the time loop.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pequod_b200.h"
+#include "pq_common.cuh"
+#include "pq_kernels.h"
+
+namespace pq {
+cudaError_t launch_init_finish(const LaunchSet& ls, cudaStream_t st);
+}
+
+using namespace pq;
+
+namespace {
+
+enum { PRO_PLAIN = 0, PRO_MODAL = 1, PRO_STEP = 2 };
+enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
+
+}  // namespace
+
+struct pq_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    pq_model_desc desc{};
+    std::vector<double> wind;
+    Member hm[2];               // host copies of the two parity descriptors
+    Member* d_members = nullptr;  // device: [2]
+    int* d_prefix = nullptr;      // device: {0}
+    LaunchSet ls[2];
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    Scalars* d_sc = nullptr;
+    int* d_status = nullptr;
+    int cur = 0;
+    bool initialized = false;
+    cudaGraphExec_t graph2 = nullptr;
+    std::string err;
+    long last_launches = 0;
+    // Per-kernel CUDA-event timing of eagerly launched steps.
+    struct StepEvents {
+        cudaEvent_t e[5];
+    };
+    bool timing = false;
+    std::vector<StepEvents> events;
+    // host copies of layout facts
+    int ii = 0, jj = 0, L = 0, pitch = 0;
+    size_t field_bytes = 0;  // bytes of one L-layer field
+};
+
+namespace {
+
+int fail(pq_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(pq_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, PQ_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                           \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+    } while (0)
+
+// Pivots of the tridiagonal j-solves, exactly as allocate_h1d_c computes
+// ge_fact (qg3p_helmholtz.F90:794-809), compressed: for each (mode, k) the
+// reciprocal pivots g_p, p = 1..jj-2, are stored until the pivot recurrence
+// reaches a bitwise fixed point; the fixed point is stored once.
+struct PivotTables {
+    std::vector<int> off, len;
+    std::vector<double> piv, fix;
+};
+
+PivotTables build_pivots(int ii, int jj, int L, const double* ss) {
+    PivotTables t;
+    const int n = ii - 2, Mr = jj - 2;
+    t.off.resize((size_t)L * n);
+    t.len.resize((size_t)L * n);
+    t.fix.resize((size_t)L * n);
+    const double norm_fact = 3.14159265358979323846 / (2.0 * (double)(ii - 1));
+    std::vector<double> raw(Mr + 1);
+    for (int m = 0; m < L; ++m)
+        for (int k = 1; k <= n; ++k) {
+            const double s = std::sin((double)k * norm_fact);
+            const double diag = -2.0 - ss[m] - 4.0 * (s * s);
+            raw[1] = diag;
+            int conv = 0;  // first p with raw[p] == raw[p-1]
+            for (int p = 2; p <= Mr; ++p) {
+                raw[p] = diag - 1.0 / raw[p - 1];
+                if (raw[p] == raw[p - 1]) {
+                    conv = p;
+                    break;
+                }
+            }
+            const size_t mk = (size_t)m * n + (k - 1);
+            t.off[mk] = (int)t.piv.size();
+            if (conv) {
+                for (int p = 1; p <= conv - 2; ++p) t.piv.push_back(1.0 / raw[p]);
+                t.len[mk] = conv - 2;
+                t.fix[mk] = 1.0 / raw[conv - 1];
+            } else {
+                for (int p = 1; p <= Mr; ++p) t.piv.push_back(1.0 / raw[p]);
+                t.len[mk] = Mr;
+                t.fix[mk] = 1.0 / raw[Mr];
+            }
+        }
+    if (t.piv.empty()) t.piv.push_back(0.0);
+    return t;
+}
+
+// Copy between a dense (ii, jj, L) host/device array and a pitched field.
+int copy_in(pq_ctx* c, void* dst, const double* src, int kind) {
+    const size_t w = (size_t)c->ii * sizeof(double);
+    CK(cudaMemcpy2DAsync(dst, (size_t)c->pitch * sizeof(double), src, w, w, (size_t)c->jj * c->L,
+                         kind == PQ_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+    return PQ_OK;
+}
+
+int copy_out(pq_ctx* c, double* dst, const void* src, int kind) {
+    const size_t w = (size_t)c->ii * sizeof(double);
+    CK(cudaMemcpy2DAsync(dst, w, src, (size_t)c->pitch * sizeof(double), w, (size_t)c->jj * c->L,
+                         kind == PQ_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+    return PQ_OK;
+}
+
+int check_status(pq_ctx* c) {
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (st & (ST_NAN_PSIC)) return fail(c, PQ_ERR_NAN, "NaN psiC encountered");
+    if (st & (ST_NAN_ENERGY)) return fail(c, PQ_ERR_NAN, "NaN value encountered in energy");
+    return PQ_OK;
+}
+
+int upload_members(pq_ctx* c) {
+    CK(cudaMemcpyAsync(c->d_members, c->hm, 2 * sizeof(Member), cudaMemcpyHostToDevice, c->stream));
+    return PQ_OK;
+}
+
+// The three Helmholtz kernels.
+int run_helm(pq_ctx* c, int par, int prologue, int epilogue, int mean) {
+    CK(launch_dst_forward(c->ls[par], prologue, c->stream));
+    CK(launch_tridiag(c->ls[par], mean, c->stream));
+    CK(launch_dst_inverse(c->ls[par], epilogue, c->stream));
+    return PQ_OK;
+}
+
+int run_step(pq_ctx* c, int par) {
+    cudaEvent_t* ev = nullptr;
+    if (c->timing) {
+        c->events.emplace_back();
+        ev = c->events.back().e;
+        for (int k = 0; k < 5; ++k) CK(cudaEventCreate(&ev[k]));
+        CK(cudaEventRecord(ev[0], c->stream));
+    }
+    CK(launch_dst_forward(c->ls[par], PRO_STEP, c->stream));
+    if (ev) CK(cudaEventRecord(ev[1], c->stream));
+    CK(launch_tridiag(c->ls[par], 1, c->stream));
+    if (ev) CK(cudaEventRecord(ev[2], c->stream));
+    CK(launch_dst_inverse(c->ls[par], EPI_PV, c->stream));
+    if (ev) CK(cudaEventRecord(ev[3], c->stream));
+    CK(launch_cabaret_fused(c->ls[par], c->stream));
+    if (ev) CK(cudaEventRecord(ev[4], c->stream));
+    return PQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pq_last_error(const pq_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+size_t pq_device_bytes(const pq_ctx* c) { return c ? c->arena_bytes : 0; }
+
+void* pq_stream(pq_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+long pq_last_launch_count(const pq_ctx* c) { return c ? c->last_launches : 0; }
+
+void pq_destroy(pq_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph2) cudaGraphExecDestroy(c->graph2);
+    if (c->arena) cudaFree(c->arena);
+    if (c->d_members) cudaFree(c->d_members);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
+    if (!out || !d) return PQ_ERR_ARG;
+    *out = nullptr;
+    const int ii = d->ii, jj = d->jj, L = d->layers;
+    if (ii < 5 || jj < 5 || !is_pow2(ii - 1) || L < 1 || L > PQ_MAX_LAYERS || d->periodic_j) return PQ_ERR_ARG;
+    if (d->scheme != PQ_SCHEME_CABARET) return PQ_ERR_UNSUPPORTED;
+    if (d->precision != PQ_PREC_FP64) return PQ_ERR_UNSUPPORTED;
+    pq_ctx* c = new pq_ctx;
+    c->device = device;
+    c->desc = *d;
+    c->ii = ii;
+    c->jj = jj;
+    c->L = L;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(c, e, "cudaSetDevice");
+        *out = c;
+        return rc;
+    }
+    *out = c;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    if (d->force_wind) c->wind.assign(d->force_wind, d->force_wind + (size_t)ii * jj);
+    c->desc.force_wind = nullptr;
+
+    const int n = ii - 2, N = ii - 1, M = N / 2;
+    int logM = 0;
+    while ((1 << logM) < M) ++logM;
+    c->pitch = (ii + 31) & ~31;
+    const size_t lstride = (size_t)c->pitch * jj;
+    c->field_bytes = lstride * L * sizeof(double);
+    const int ntiles_tri = L * ((n + 7) / 8);
+    const int ntx = (ii + CAB_TX - 1) / CAB_TX, nty = (jj + CAB_TY - 1) / CAB_TY;
+    const int ntiles_cab = ntx * nty;
+
+    // Tables.
+    std::vector<double2> tw(M), wsplit(M);
+    for (int t = 0; t < M; ++t) {
+        const long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)M;
+        tw[t] = make_double2((double)cosl(a), (double)-sinl(a));
+        const long double b = 2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)N;
+        wsplit[t] = make_double2((double)cosl(b), (double)-sinl(b));
+    }
+    std::vector<double> was(N / 2 + 1, 0.0), wmean(n, 0.0);
+    for (int k = 1; k <= N / 2; ++k)
+        was[k] = (double)(2.0L * sinl(3.141592653589793238462643383279502884L * (long double)k / (long double)N));
+    for (int k = 1; k <= n; ++k)
+        if (k & 1)
+            wmean[k - 1] = (double)(2.0L / tanl(3.141592653589793238462643383279502884L * (long double)k /
+                                                (2.0L * (long double)N)));
+    PivotTables pv = build_pivots(ii, jj, L, d->ss);
+
+    // Arena layout.
+    const int nfields = 2 /*zeta_old*/ + 1 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 1 /*res_beta*/ + 1 /*ui*/ + 1 /*uj*/ +
+                        2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ + 1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ +
+                        1 /*corr*/;
+    const size_t fb = align256(c->field_bytes);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += align256(bytes);
+        return o;
+    };
+    const size_t o_fields = take(fb * nfields);
+    const size_t o_wind = take(lstride * sizeof(double));
+    const size_t o_tw = take(M * sizeof(double2));
+    const size_t o_ws = take(M * sizeof(double2));
+    const size_t o_was = take(was.size() * sizeof(double));
+    const size_t o_wm = take(wmean.size() * sizeof(double));
+    const size_t o_poff = take(pv.off.size() * sizeof(int));
+    const size_t o_plen = take(pv.len.size() * sizeof(int));
+    const size_t o_piv = take(pv.piv.size() * sizeof(double));
+    const size_t o_pfix = take(pv.fix.size() * sizeof(double));
+    const size_t npart = std::max((size_t)ntiles_tri, (size_t)jj * (PQ_MAXL + 1));
+    const size_t o_part = take(npart * sizeof(double));
+    const size_t o_maxu = take(ntiles_cab * sizeof(double));
+    const size_t o_cnt = take(4 * sizeof(unsigned));
+    const size_t o_sc = take(sizeof(Scalars));
+    const size_t o_st = take(sizeof(int));
+    c->arena_bytes = off;
+    e = cudaMalloc(&c->arena, off);
+    if (e != cudaSuccess) return fail(c, PQ_ERR_NOMEM, "device allocation failed");
+    CK(cudaMemsetAsync(c->arena, 0, off, c->stream));
+    char* A = c->arena;
+    CK(cudaMemcpyAsync(A + o_tw, tw.data(), M * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_ws, wsplit.data(), M * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_was, was.data(), was.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_wm, wmean.data(), wmean.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_poff, pv.off.data(), pv.off.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_plen, pv.len.data(), pv.len.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_piv, pv.piv.data(), pv.piv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_pfix, pv.fix.data(), pv.fix.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (!c->wind.empty())
+        CK(cudaMemcpy2DAsync(A + o_wind, (size_t)c->pitch * sizeof(double), c->wind.data(), (size_t)ii * sizeof(double),
+                             (size_t)ii * sizeof(double), jj, cudaMemcpyHostToDevice, c->stream));
+
+    Member m;
+    std::memset(&m, 0, sizeof(m));
+    m.ii = ii;
+    m.jj = jj;
+    m.L = L;
+    m.pitch = c->pitch;
+    m.n = n;
+    m.N = N;
+    m.M = M;
+    m.logM = logM;
+    m.lstride = (long long)lstride;
+    m.bc_type = d->bc_type;
+    m.limiter = d->limiter;
+    m.alpha = d->alpha;
+    m.viscosity = d->viscosity;
+    m.visc_bot = d->visc_bot;
+    for (int a = 0; a < L; ++a) {
+        for (int b = 0; b < L; ++b) {
+            m.z2m[a * PQ_MAXL + b] = d->z2m[a + L * b];  // z2m(m=a, l=b)
+            m.m2z[a * PQ_MAXL + b] = d->m2z[a + L * b];  // m2z(l=a, m=b)
+        }
+        m.ss[a] = d->ss[a];
+        m.s1[a] = d->s1[a];
+        m.s2[a] = d->s2[a];
+        m.beta[a] = d->beta[a];
+        m.h[a] = d->h[a];
+        m.htot += d->h[a];
+    }
+    m.mean_scale = 1.0 / ((double)(ii - 1) * (double)(jj - 1));
+    m.tw = reinterpret_cast<const double2*>(A + o_tw);
+    m.wsplit = reinterpret_cast<const double2*>(A + o_ws);
+    m.was = reinterpret_cast<const double*>(A + o_was);
+    m.wmean = reinterpret_cast<const double*>(A + o_wm);
+    m.piv_off = reinterpret_cast<const int*>(A + o_poff);
+    m.piv_len = reinterpret_cast<const int*>(A + o_plen);
+    m.piv = reinterpret_cast<const double*>(A + o_piv);
+    m.piv_fix = reinterpret_cast<const double*>(A + o_pfix);
+    char* F = A + o_fields;
+    int fi = 0;
+    auto fld = [&]() { return (void*)(F + fb * (fi++)); };
+    m.zeta_old[0] = fld();
+    m.zeta_old[1] = fld();
+    m.zeta = fld();
+    m.psi = (double*)fld();
+    m.res = fld();
+    m.res_beta = fld();
+    m.ui = fld();
+    m.uj = fld();
+    m.uimo[0] = fld();
+    m.uimo[1] = fld();
+    m.ujmo[0] = fld();
+    m.ujmo[1] = fld();
+    m.zfi[0] = fld();
+    m.zfi[1] = fld();
+    m.zfj[0] = fld();
+    m.zfj[1] = fld();
+    m.rel = fld();
+    m.helm_io = fld();
+    m.spec = fld();
+    m.corr = (const double*)fld();
+    m.wind = c->wind.empty() ? nullptr : reinterpret_cast<const double*>(A + o_wind);
+    m.partials = reinterpret_cast<double*>(A + o_part);
+    m.maxu_part = reinterpret_cast<double*>(A + o_maxu);
+    m.counters = reinterpret_cast<unsigned*>(A + o_cnt);
+    m.sc = reinterpret_cast<Scalars*>(A + o_sc);
+    m.status = reinterpret_cast<int*>(A + o_st);
+    m.ntiles_tri = ntiles_tri;
+    m.ntiles_cab = ntiles_cab;
+    m.adapt_dt = d->adapt_dt;
+    m.target_cfl = d->target_cfl;
+    m.max_dt = d->max_dt;
+    m.max_dt_increase = d->max_dt_increase;
+    c->d_sc = m.sc;
+    c->d_status = m.status;
+    c->hm[0] = m;
+    c->hm[1] = m;
+    c->hm[0].cur = 0;
+    c->hm[1].cur = 1;
+
+    e = cudaMalloc(&c->d_members, 2 * sizeof(Member) + 256);
+    if (e != cudaSuccess) return fail(c, PQ_ERR_NOMEM, "device allocation failed");
+    c->d_prefix = reinterpret_cast<int*>(reinterpret_cast<char*>(c->d_members) + 2 * sizeof(Member));
+    CK(cudaMemsetAsync(c->d_prefix, 0, 256, c->stream));
+    int rc = upload_members(c);
+    if (rc) return rc;
+    for (int p = 0; p < 2; ++p) {
+        LaunchSet& s = c->ls[p];
+        s.members = c->d_members + p;
+        s.nmem = 1;
+        s.maxL = L;
+        s.maxN = N;
+        s.maxJ = jj;
+        s.maxI = ii;
+        s.prefix_rows_interior = s.prefix_rows_all = s.prefix_tri = s.prefix_cab = c->d_prefix;
+        s.ctas_rows_interior = jj - 2;
+        s.ctas_rows_all = jj;
+        s.ctas_tri = ntiles_tri;
+        s.ctas_cab = ntiles_cab;
+    }
+    // Scalars: dt and the initial time weights.
+    Scalars sc;
+    std::memset(&sc, 0, sizeof(sc));
+    sc.dt = d->dt;
+    sc.tweight_a = 0.5;
+    sc.tweight_u = 0.5;
+    CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
+
+    // Correction function for mass conservation, correction_function_mass
+    // (qg3p_aux.F90:196-230): solve with a unit right-hand side, Dirichlet 0,
+    // then corr = (1 + ss psi) / (1 + ss mean(psi)) with the plain interior
+    // mean the reference uses there.
+    {
+        std::vector<double> ones((size_t)ii * jj * L, 1.0);
+        rc = copy_in(c, m.helm_io, ones.data(), PQ_PTR_HOST);
+        if (rc) return rc;
+        rc = run_helm(c, 0, PRO_PLAIN, EPI_HELM, 0);
+        if (rc) return rc;
+        std::vector<double> h((size_t)ii * jj * L);
+        rc = copy_out(c, h.data(), m.helm_io, PQ_PTR_HOST);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(c->stream));
+        for (int l = 0; l < L; ++l) {
+            double* p = h.data() + (size_t)ii * jj * l;
+            for (int i = 0; i < ii; ++i) p[i] = p[i + (size_t)ii * (jj - 1)] = 0.0;
+            for (int j = 0; j < jj; ++j) p[(size_t)ii * j] = p[(size_t)ii * j + ii - 1] = 0.0;
+            double s = 0.0;
+            for (int j = 1; j < jj - 1; ++j)
+                for (int i = 1; i < ii - 1; ++i) s += p[i + (size_t)ii * j];
+            const double mean = s / ((double)(ii - 1) * (double)(jj - 1));
+            const double den = 1.0 + d->ss[l] * mean;
+            for (size_t k = 0; k < (size_t)ii * jj; ++k) p[k] = (1.0 + d->ss[l] * p[k]) / den;
+        }
+        rc = copy_in(c, (void*)m.corr, h.data(), PQ_PTR_HOST);
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return PQ_OK;
+}
+
+int pq_helm(pq_ctx* c, double* zeta, int ptr_kind) {
+    if (!c || !zeta) return PQ_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    int rc = copy_in(c, c->hm[0].helm_io, zeta, ptr_kind);
+    if (rc) return rc;
+    rc = run_helm(c, c->cur, PRO_PLAIN, EPI_HELM, 0);
+    if (rc) return rc;
+    rc = copy_out(c, zeta, c->hm[0].helm_io, ptr_kind);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->last_launches = 3;
+    return PQ_OK;
+}
+
+int pq_pv_inversion(pq_ctx* c, const double* zeta, double* psi, int ptr_kind) {
+    if (!c || !zeta || !psi) return PQ_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    int rc = copy_in(c, c->hm[0].zeta, zeta, ptr_kind);
+    if (rc) return rc;
+    rc = run_helm(c, c->cur, PRO_MODAL, EPI_PV, 1);
+    if (rc) return rc;
+    rc = copy_out(c, psi, c->hm[0].psi, ptr_kind);
+    if (rc) return rc;
+    c->last_launches = 3;
+    return check_status(c);
+}
+
+int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
+    if (!c || !zeta_ic) return PQ_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    const int ii = c->ii, jj = c->jj, L = c->L;
+    std::vector<double> z((size_t)ii * jj * L);
+    if (ptr_kind == PQ_PTR_DEVICE)
+        CK(cudaMemcpy(z.data(), zeta_ic, z.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    else
+        std::memcpy(z.data(), zeta_ic, z.size() * sizeof(double));
+    // apply_dirichlet_bc(0, zeta), qg3.F90:383.
+    for (int l = 0; l < L; ++l) {
+        double* p = z.data() + (size_t)ii * jj * l;
+        for (int i = 0; i < ii; ++i) p[i] = p[i + (size_t)ii * (jj - 1)] = 0.0;
+        for (int j = 0; j < jj; ++j) p[(size_t)ii * j] = p[(size_t)ii * j + ii - 1] = 0.0;
+    }
+    const Member& m = c->hm[0];
+    // Zero all CABARET fields and both parities (qg3.F90:393-404).
+    const size_t fb = align256(c->field_bytes);
+    // Fields 0..15 of the arena: zeta_old[2], zeta, psi, res, res_beta, ui,
+    // uj, uimo[2], ujmo[2], zeta_fi[2], zeta_fj[2] (corr is kept).
+    CK(cudaMemsetAsync(m.zeta_old[0], 0, fb * 16, c->stream));
+    int rc = copy_in(c, m.zeta, z.data(), PQ_PTR_HOST);
+    if (rc) return rc;
+    Scalars sc;
+    std::memset(&sc, 0, sizeof(sc));
+    sc.dt = c->desc.dt;
+    sc.tweight_a = 0.5;
+    sc.tweight_u = 0.5;
+    sc.model_time = c->desc.dt / 2.0;
+    CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    // zeta was cleared together with the other fields; upload it again.
+    rc = copy_in(c, m.zeta, z.data(), PQ_PTR_HOST);
+    if (rc) return rc;
+    c->cur = 0;
+    rc = run_helm(c, 0, PRO_MODAL, EPI_PV, 1);
+    if (rc) return rc;
+    CK(launch_init_finish(c->ls[0], c->stream));
+    c->initialized = true;
+    return check_status(c);
+}
+
+int pq_step(pq_ctx* c, int nsteps) {
+    int rc = pq_step_async(c, nsteps);
+    if (rc) return rc;
+    return check_status(c);
+}
+
+int pq_check(pq_ctx* c) {
+    if (!c) return PQ_ERR_ARG;
+    return check_status(c);
+}
+
+int pq_step_exchange(pq_ctx* c, const double* zeta_in, double* psi_out, int ptr_kind) {
+    if (!c) return PQ_ERR_ARG;
+    if (!c->initialized) return fail(c, PQ_ERR_STATE, "pq_step_exchange before pq_init_perturb");
+    CK(cudaSetDevice(c->device));
+    if (zeta_in) {
+        int rc = copy_in(c, c->hm[c->cur].zeta_old[c->cur], zeta_in, ptr_kind);
+        if (rc) return rc;
+    }
+    int rc = pq_step_async(c, 1);
+    if (rc) return rc;
+    if (psi_out) {
+        rc = copy_out(c, psi_out, c->hm[0].psi, ptr_kind);
+        if (rc) return rc;
+    }
+    return PQ_OK;
+}
+
+int pq_step_async(pq_ctx* c, int nsteps) {
+    if (!c || nsteps < 0) return PQ_ERR_ARG;
+    if (!c->initialized) return fail(c, PQ_ERR_STATE, "pq_step before pq_init_perturb");
+    CK(cudaSetDevice(c->device));
+    int done = 0;
+    long launches = 0;
+    // An odd step first so that the graph always starts at parity 0.
+    if (c->cur == 1 && nsteps > 0) {
+        int rc = run_step(c, 1);
+        if (rc) return rc;
+        c->cur = 0;
+        ++done;
+        launches += 4;
+    }
+    if (nsteps - done >= 2) {
+        if (!c->graph2) {
+            cudaGraph_t g;
+            const bool timing = c->timing;
+            c->timing = false;  // no per-kernel events inside the graph
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+            int rc = run_step(c, 0);
+            if (rc == PQ_OK) rc = run_step(c, 1);
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            c->timing = timing;
+            if (rc) return rc;
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&c->graph2, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+        }
+        while (nsteps - done >= 2) {
+            CK(cudaGraphLaunch(c->graph2, c->stream));
+            done += 2;
+            launches += 8;
+        }
+    }
+    if (done < nsteps) {
+        int rc = run_step(c, 0);
+        if (rc) return rc;
+        c->cur = 1;
+        ++done;
+        launches += 4;
+    }
+    c->last_launches = launches;
+    return PQ_OK;
+}
+
+int pq_sync(pq_ctx* c) {
+    if (!c) return PQ_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return PQ_OK;
+}
+
+int pq_kernel_timing(pq_ctx* c, int enable) {
+    if (!c) return PQ_ERR_ARG;
+    c->timing = enable != 0;
+    return PQ_OK;
+}
+
+int pq_kernel_times(pq_ctx* c, double* ms, long* launches) {
+    if (!c || !ms || !launches) return PQ_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 4; ++k) {
+        ms[k] = 0.0;
+        launches[k] = 0;
+    }
+    for (auto& s : c->events) {
+        for (int k = 0; k < 4; ++k) {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, s.e[k], s.e[k + 1]));
+            ms[k] += t;
+            launches[k] += 1;
+        }
+        for (int k = 0; k < 5; ++k) cudaEventDestroy(s.e[k]);
+    }
+    c->events.clear();
+    return PQ_OK;
+}
+
+int pq_energy(pq_ctx* c, double* ekin, double* epot) {
+    if (!c || !ekin || !epot) return PQ_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(launch_energy(c->ls[c->cur], c->stream));
+    Scalars sc;
+    CK(cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    int rc = check_status(c);
+    for (int k = 0; k < c->L; ++k) ekin[k] = sc.ekin[k];
+    *epot = sc.epot;
+    return rc;
+}
+
+int pq_cfl(pq_ctx* c, double* cfl) {
+    if (!c || !cfl) return PQ_ERR_ARG;
+    Scalars sc;
+    CK(cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *cfl = sc.max_u * sc.dt;
+    return PQ_OK;
+}
+
+int pq_get_scalars(pq_ctx* c, double* out4) {
+    if (!c || !out4) return PQ_ERR_ARG;
+    Scalars sc;
+    CK(cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out4[0] = sc.dt;
+    out4[1] = sc.tweight_a;
+    out4[2] = sc.tweight_u;
+    out4[3] = sc.model_time;
+    return PQ_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Reference-layout geometry of a field: leading dims and the offset of the
+// device node (0, 0) inside it.
+struct RefShape {
+    int n1, n2;  // leading dims
+    int oi, oj;  // reference (0-based) index of device node/face (0, 0)
+};
+
+bool ref_shape(int field, int ii, int jj, RefShape* s) {
+    switch (field) {
+        case PQ_F_PSI:
+        case PQ_F_ZETA:
+        case PQ_F_REL:
+        case PQ_F_ZETA_OLD: *s = {ii + 2, jj + 2, 1, 1}; return true;
+        case PQ_F_UI:
+        case PQ_F_UIMO:
+        case PQ_F_ZETA_FI: *s = {ii + 3, jj + 2, 1, 1}; return true;
+        case PQ_F_UJ:
+        case PQ_F_UJMO:
+        case PQ_F_ZETA_FJ: *s = {ii + 2, jj + 3, 1, 1}; return true;
+        case PQ_F_RES:
+        case PQ_F_RES_BETA:
+        case PQ_F_CORR: *s = {ii, jj, 0, 0}; return true;
+    }
+    return false;
+}
+
+void* field_ptr(pq_ctx* c, int field) {
+    const Member& m = c->hm[c->cur];
+    const int cur = c->cur;
+    switch (field) {
+        case PQ_F_PSI: return m.psi;
+        case PQ_F_ZETA:
+        case PQ_F_ZETA_OLD: return m.zeta_old[cur];
+        case PQ_F_REL: return m.rel;
+        case PQ_F_UI: return m.ui;
+        case PQ_F_UJ: return m.uj;
+        case PQ_F_UIMO: return m.uimo[cur];
+        case PQ_F_UJMO: return m.ujmo[cur];
+        case PQ_F_ZETA_FI: return m.zfi[cur];
+        case PQ_F_ZETA_FJ: return m.zfj[cur];
+        case PQ_F_RES: return m.res;
+        case PQ_F_RES_BETA: return m.res_beta;
+        case PQ_F_CORR: return (void*)m.corr;
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pq_get_field(pq_ctx* c, int field, double* out) {
+    if (!c || !out) return PQ_ERR_ARG;
+    RefShape s;
+    if (!ref_shape(field, c->ii, c->jj, &s)) return fail(c, PQ_ERR_ARG, "unknown field");
+    CK(cudaSetDevice(c->device));
+    if (field == PQ_F_REL) CK(launch_rel(c->ls[c->cur], c->stream));
+    std::vector<double> dense((size_t)c->ii * c->jj * c->L);
+    int rc = copy_out(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)s.n1 * s.n2 * c->L;
+    std::memset(out, 0, n * sizeof(double));
+    for (int l = 0; l < c->L; ++l)
+        for (int j = 0; j < c->jj; ++j)
+            for (int i = 0; i < c->ii; ++i)
+                out[(size_t)(i + s.oi) + (size_t)s.n1 * ((j + s.oj) + (size_t)s.n2 * l)] =
+                    dense[(size_t)i + (size_t)c->ii * (j + (size_t)c->jj * l)];
+    return PQ_OK;
+}
+
+int pq_set_field(pq_ctx* c, int field, const double* in) {
+    if (!c || !in) return PQ_ERR_ARG;
+    RefShape s;
+    if (!ref_shape(field, c->ii, c->jj, &s) || field == PQ_F_CORR) return fail(c, PQ_ERR_ARG, "unknown field");
+    CK(cudaSetDevice(c->device));
+    std::vector<double> dense((size_t)c->ii * c->jj * c->L);
+    for (int l = 0; l < c->L; ++l)
+        for (int j = 0; j < c->jj; ++j)
+            for (int i = 0; i < c->ii; ++i)
+                dense[(size_t)i + (size_t)c->ii * (j + (size_t)c->jj * l)] =
+                    in[(size_t)(i + s.oi) + (size_t)s.n1 * ((j + s.oj) + (size_t)s.n2 * l)];
+    int rc = copy_in(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST);
+    if (rc) return rc;
+    if (field == PQ_F_ZETA) rc = copy_in(c, c->hm[0].zeta, dense.data(), PQ_PTR_HOST);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->initialized = true;
+    return PQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+// pq_common.cuh -- shared device-side definitions for the pequod_b200 kernels.
+//
+// Device layout (one ensemble member): every field is node-shaped,
+// [layer][j][i] with i fastest, i in [0, ii), j in [0, jj), a row pitch of
+// `pitch` elements (a multiple of 32, so every row starts on a 256-byte
+// boundary for doubles).  The reference's one-node halos are never read on a
+// single rank (every stencil in qg3p_aux.F90 stays inside fa_*), so the
+// device arrays hold the nodes only; host-side copies convert to and from the
+// reference's (ii+2, jj+2, L) / FLUX_II / FLUX_JJ layouts.
+//
+// Face arrays use the same node shape:
+//   ui, uimo, zeta_fi  at [l][j][a], a in [1, ii-1]: the face between nodes
+//                      (a-1, j) and (a, j)  (reference FLUX_II index a+2)
+//   uj, ujmo, zeta_fj  at [l][b][i], b in [1, jj-1]: the face between nodes
+//                      (i, b-1) and (i, b)  (reference FLUX_JJ index b+2)
+//
+// The spectral scratch `spec` holds, for mode m and interior row j, the DST
+// coefficient of wavenumber k (1..n, n = ii-2) at [m][j][k-1].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define PQ_MAXL 8
+
+namespace pq {
+
+// Scalars that change during a run live on the device so that a captured
+// CUDA graph can replay steps with an adaptive time step.
+struct Scalars {
+    double dt;         // current non-dimensional time step
+    double tweight_a;  // CABARET time weights (qg3.F90:457-459)
+    double tweight_u;
+    double max_u;      // max |u| over the faces, from the last fused step
+    double cfl;        // max_u * dt
+    double psiC[PQ_MAXL];
+    double ekin[PQ_MAXL];
+    double epot;
+    double model_time;  // advanced by dt at the end of every fused step
+    double pad[2];
+};
+
+// Device status bits (read by the host after a step).
+enum StatusBits : int {
+    ST_NAN_PSIC = 1,      // NaN psiC: the reference aborts (qg3p_aux.F90:504-510)
+    ST_LARGE_PSIC = 2,    // |psiC| > 1e100: the reference warns (:511-517)
+    ST_NAN_ENERGY = 4,    // NaN energy: the reference aborts (qg3p_diagnostics.F90:858-861)
+    ST_SMALL_DT = 8,      // dt < 1e-6 after adaptation: the reference warns (qg3p_aux.F90:982-986)
+};
+
+// Per-member device descriptor.  Lives in device global memory (an array of
+// these for a batch); kernels find their member from the CTA index.
+struct Member {
+    int ii, jj, L, pitch;
+    int n;       // DST length, ii - 2
+    int N;       // ii - 1, a power of two
+    int M;       // N / 2, the complex FFT length
+    int logM;
+    long long lstride;  // elements per layer (pitch * jj)
+    int bc_type;        // 1 partial slip, 2 no slip, 3 free slip
+    int limiter;
+    double alpha;       // partial-slip alpha (non-dimensional)
+    double viscosity, visc_bot;
+    double z2m[PQ_MAXL * PQ_MAXL];  // row-major [m][l]
+    double m2z[PQ_MAXL * PQ_MAXL];  // row-major [l][m]
+    double ss[PQ_MAXL], s1[PQ_MAXL], s2[PQ_MAXL], beta[PQ_MAXL];
+    double h[PQ_MAXL];  // non-dimensional layer thicknesses
+    double htot;
+    double mean_scale;  // 1 / (g_ii_int * g_jj_int)
+    // Helmholtz tables (shared between members of the same size)
+    const double2* tw;      // [M]  exp(-2 pi i t / M)
+    const double* was;      // [N/2] 2 sin(k pi / N), index k (0 unused)
+    const double2* wsplit;  // [M]  exp(-2 pi i q / N)
+    const double* wmean;    // [n]  2 * sum_i sin(i k pi / N), index k-1
+    // Compressed tridiagonal pivots, per (mode, k): piv[off + p - 1] for
+    // p < len, then the fixed point piv_fix.
+    const int* piv_off;     // [L * n]
+    const int* piv_len;     // [L * n]
+    const double* piv;
+    const double* piv_fix;  // [L * n]
+    // Fields (FP64 path; the mixed path reinterprets the storage pointers).
+    // Fields that the fused step reads at neighbour nodes or faces owned by
+    // another CTA are ping-ponged: [cur] is read, [cur ^ 1] written.
+    void* zeta_old[2];
+    void* zeta;       // zeta after predictor and beta (input of the inversion)
+    double* psi;
+    void* res;
+    void* res_beta;
+    void* ui;         // written by the fused step, read by the next step's beta term
+    void* uj;
+    void* uimo[2];
+    void* ujmo[2];
+    void* zfi[2];
+    void* zfj[2];
+    void* rel;
+    void* helm_io;    // in/out buffer of the stand-alone helm() entry point
+    void* flux_i;
+    void* flux_j;
+    void* spec;
+    double* spec64;   // barotropic-mode spectral scratch of the mixed path
+    const double* corr;
+    const double* wind;
+    double* partials;     // [L * ntiles_tri]
+    double* maxu_part;    // [ntiles_cab]
+    unsigned int* counters;  // [4] last-block counters
+    Scalars* sc;
+    int* status;
+    int ntiles_tri;       // L * ceil(n / 8)
+    int ntiles_cab;
+    int cur;              // ping-pong parity for ui / zfi / zfj (host-managed)
+    int adapt_dt;
+    double target_cfl, max_dt, max_dt_increase;
+};
+
+// Map a flat CTA index to (member, local CTA) given prefix sums.
+__device__ __forceinline__ int find_member(const int* __restrict__ prefix, int nmem, int cta, int* local) {
+    int lo = 0, hi = nmem - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= cta)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    *local = cta - prefix[lo];
+    return lo;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<double> {
+    typedef double2 type;
+    __device__ static double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct Cplx<float> {
+    typedef float2 type;
+    __device__ static float2 make(float a, float b) { return make_float2(a, b); }
+};
+
+// Warp-level inclusive prefix sum.
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+}  // namespace pq

@@ -1,0 +1,520 @@
+// pq_helm.cu -- the Helmholtz (PV-inversion) kernels.
+//
+// The reference solves, per vertical mode, (d_xx + d_yy - ss) psi = zeta by a
+// DST-I along i (FFTPACK sint, qg3p_helmholtz.F90:1370-1591), a tridiagonal
+// solve along j with precomputed reciprocal pivots (ge_local, :1028-1059),
+// and the inverse DST (helm, :614-769).  Here that is three kernels:
+//
+//   k_dst_rows<FWD>  one CTA per interior row j: load (optionally apply the
+//                    CABARET predictor + beta step and the z_to_modes
+//                    projection), scale by 0.5/(ii-1), DST every mode row in
+//                    shared memory, write the spectral rows.
+//   k_tridiag        one CTA per (mode, 8 consecutive wavenumbers): the whole
+//                    column strip is staged in shared memory; each warp owns
+//                    one wavenumber, each lane a chunk of rows, and the
+//                    forward / backward Thomas recurrences are solved as
+//                    chunked first-order linear recurrences (local sweep,
+//                    warp scan of the affine chunk maps, fix-up sweep).  The
+//                    same CTA accumulates the domain mean of the solution in
+//                    spectral space; the last CTA of a member finishes psiC.
+//   k_dst_rows<INV>  one CTA per row j: inverse DST of every mode row, then
+//                    the mass-corrected back-projection (modes_to_z_btcu,
+//                    qg3p_diagnostics.F90:615-635) straight into psi.
+//
+// DST-I of length n = N - 1 (N = ii - 1 = 2^p), FFTPACK convention
+// X_k = 2 sum_m x_m sin(m k pi / N): the sequence is pre-twiddled into a real
+// sequence c of length N (as sint1 does), c is packed into N/2 complex points
+// and transformed by a radix-4/2 Stockham FFT in shared memory, the real-FFT
+// split gives C_q = R_q + i I_q, and X_2q = -I_q, X_2q+1 = R_0/2 + sum_{p<=q} R_p
+// (the odd outputs are a prefix sum, done as a block scan).
+#include "pq_common.cuh"
+#include "pq_kernels.h"
+
+namespace pq {
+
+enum { PRO_PLAIN = 0, PRO_MODAL = 1, PRO_STEP = 2 };
+enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
+
+constexpr int DST_THREADS = 256;
+constexpr int TRI_THREADS = 256;
+constexpr int TRI_KT = 8;   // wavenumbers per tridiagonal CTA (one per warp)
+constexpr int TRI_PAD = 9;  // padded row stride of the staged strip
+
+__device__ __forceinline__ void load_member(Member& dst, const Member* src) {
+    const int n = sizeof(Member) / 4;
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
+}
+
+// Block-wide inclusive scan of v over the CTA (blockDim.x a multiple of 32,
+// at most 1024).  wsum: shared scratch of 32 doubles.
+__device__ __forceinline__ double block_inclusive_scan(double v, double* wsum) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double s = warp_inclusive_scan(v);
+    if (lane == 31) wsum[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        double t = lane < nw ? wsum[lane] : 0.0;
+        t = warp_inclusive_scan(t);
+        if (lane < nw) wsum[lane] = t;
+    }
+    __syncthreads();
+    double off = warp > 0 ? wsum[warp - 1] : 0.0;
+    __syncthreads();
+    return s + off;
+}
+
+// Radix-4/2 Stockham FFT of G complex rows of length M (a power of two) in
+// shared memory, forward sign.  Rows g at a + g*M.  Returns the buffer that
+// holds the result (a or b).
+__device__ double2* fft_stockham(double2* a, double2* b, int G, int M, const double2* __restrict__ tw) {
+    int Ns = 1;
+    const int M4 = M >> 2;
+    while (Ns * 4 <= M) {
+        const int st = M / (4 * Ns);
+        for (int w = threadIdx.x; w < G * M4; w += blockDim.x) {
+            const int g = w / M4, jj = w - g * M4;
+            const double2* ag = a + g * M;
+            double2* bg = b + g * M;
+            double2 v0 = ag[jj], v1 = ag[jj + M4], v2 = ag[jj + 2 * M4], v3 = ag[jj + 3 * M4];
+            const int k = jj % Ns;
+            if (k) {
+                v1 = cmul(v1, __ldg(&tw[k * st]));
+                v2 = cmul(v2, __ldg(&tw[2 * k * st]));
+                v3 = cmul(v3, __ldg(&tw[3 * k * st]));
+            }
+            double2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), d3 = csub(v1, v3);
+            double2 t3 = make_double2(d3.y, -d3.x);  // (v1 - v3) * (-i)
+            const int idx = (jj / Ns) * Ns * 4 + k;
+            bg[idx] = cadd(t0, t2);
+            bg[idx + Ns] = cadd(t1, t3);
+            bg[idx + 2 * Ns] = csub(t0, t2);
+            bg[idx + 3 * Ns] = csub(t1, t3);
+        }
+        __syncthreads();
+        double2* t = a;
+        a = b;
+        b = t;
+        Ns *= 4;
+    }
+    if (Ns < M) {
+        const int M2 = M >> 1;
+        const int st = M / (2 * Ns);
+        for (int w = threadIdx.x; w < G * M2; w += blockDim.x) {
+            const int g = w / M2, jj = w - g * M2;
+            const double2* ag = a + g * M;
+            double2* bg = b + g * M;
+            double2 v0 = ag[jj], v1 = ag[jj + M2];
+            const int k = jj % Ns;
+            if (k) v1 = cmul(v1, __ldg(&tw[k * st]));
+            const int idx = (jj / Ns) * Ns * 2 + k;
+            bg[idx] = cadd(v0, v1);
+            bg[idx + Ns] = csub(v0, v1);
+        }
+        __syncthreads();
+        double2* t = a;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// In-place DST-I (FFTPACK sint convention) of G real rows held in shared
+// memory at xr + g*xs, entries 1..n (entries 0 and N are scratch).
+// za, zb: shared complex scratch of G*M each.  wsum: 32 doubles.
+__device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, double* wsum, const Member& Mb) {
+    const int N = Mb.N, M = Mb.M, N2 = N >> 1;
+    const double* __restrict__ was = Mb.was;
+    // Pre-twiddle (sint1, qg3p_helmholtz.F90:1404-1413) and pack.
+    for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
+        const int g = w / M, t = w - g * M;
+        const double* x = xr + g * xs;
+        double c[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int k = 2 * t + e;
+            double v;
+            if (k == 0) {
+                v = 0.0;
+            } else if (k == N2) {
+                v = 4.0 * x[N2];
+            } else if (k < N2) {
+                const double xa = x[k], xb = x[N - k];
+                v = (xa - xb) + __ldg(&was[k]) * (xa + xb);
+            } else {
+                const int kk = N - k;
+                const double xa = x[kk], xb = x[k];
+                v = __ldg(&was[kk]) * (xa + xb) - (xa - xb);
+            }
+            c[e] = v;
+        }
+        za[w] = make_double2(c[0], c[1]);
+    }
+    __syncthreads();
+    double2* Z = fft_stockham(za, zb, G, M, Mb.tw);
+    double2* other = (Z == za) ? zb : za;
+    double* R = reinterpret_cast<double*>(other);  // G*M reals of scratch
+    // Real-FFT split; even outputs directly, R_q to scratch for the scan.
+    for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
+        const int g = w / M, q = w - g * M;
+        const double2* Zg = Z + g * M;
+        const double2 zq = Zg[q];
+        const double2 zr = Zg[(M - q) & (M - 1)];
+        const double2 zc = make_double2(zr.x, -zr.y);
+        const double2 E = make_double2(0.5 * (zq.x + zc.x), 0.5 * (zq.y + zc.y));
+        const double2 d = csub(zq, zc);
+        const double2 O = make_double2(0.5 * d.y, -0.5 * d.x);
+        const double2 C = cadd(E, cmul(__ldg(&Mb.wsplit[q]), O));
+        R[w] = (q == 0) ? 0.5 * C.x : C.x;
+        if (q >= 1) xr[g * xs + 2 * q] = -C.y;
+    }
+    __syncthreads();
+    // X_{2q+1} = inclusive prefix sum of R over q, one row at a time.
+    const int per = (M + blockDim.x - 1) / blockDim.x;
+    for (int g = 0; g < G; ++g) {
+        const double* Rg = R + g * M;
+        const int q0 = threadIdx.x * per;
+        double loc = 0.0;
+        for (int e = 0; e < per; ++e) {
+            const int q = q0 + e;
+            if (q < M) loc += Rg[q];
+        }
+        const double incl = block_inclusive_scan(loc, wsum);
+        double run = incl - loc;
+        double* x = xr + g * xs;
+        for (int e = 0; e < per; ++e) {
+            const int q = q0 + e;
+            if (q < M) {
+                run += Rg[q];
+                x[2 * q + 1] = run;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Shared memory plan of k_dst_rows for G modes at a time.
+__host__ __device__ inline size_t dst_smem_bytes(int L, int G, int N, int M) {
+    size_t xr = (size_t)L * (N + 2) * sizeof(double);
+    size_t z = 2 * (size_t)G * M * sizeof(double2);
+    return xr + z + 32 * sizeof(double);
+}
+
+template <int PRO, int EPI>
+__global__ void __launch_bounds__(DST_THREADS) k_dst_rows(const Member* __restrict__ mems,
+                                                            const int* __restrict__ prefix, int nmem, int G,
+                                                            int row_offset) {
+    __shared__ Member Mb;
+    extern __shared__ __align__(16) double sm[];
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
+    load_member(Mb, mems + mi);
+    __syncthreads();
+    const int j = local + row_offset;  // FWD: interior rows (offset 1); INV: all rows (offset 0)
+    const int L = Mb.L, N = Mb.N, n = Mb.n, ii = Mb.ii, jj = Mb.jj, pitch = Mb.pitch;
+    const long long ls = Mb.lstride;
+    const int xs = N + 2;
+    double* xr = sm;                                    // [L][N+2]
+    double2* za = reinterpret_cast<double2*>(xr + (size_t)L * xs);
+    double2* zb = za + (size_t)G * Mb.M;
+    double* wsum = reinterpret_cast<double*>(zb + (size_t)G * Mb.M);
+
+    const bool interior_row = (j >= 1 && j <= jj - 2);
+
+    if (EPI == EPI_SPEC) {
+        // ---------------- forward: load + prologue -------------------------
+        const double cff = 0.5 / (double)(ii - 1);
+        const double dt = Mb.sc->dt, ta = Mb.sc->tweight_a;
+        for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
+            const long long o = (long long)j * pitch + k;
+            double v[PQ_MAXL];
+            if (PRO == PRO_PLAIN) {
+                const double* src = reinterpret_cast<const double*>(Mb.helm_io);
+                for (int l = 0; l < L; ++l) v[l] = src[o + l * ls];
+            } else {
+                double z[PQ_MAXL];
+                if (PRO == PRO_STEP) {
+                    const double* zo = reinterpret_cast<const double*>(Mb.zeta_old[Mb.cur]);
+                    const double* rs = reinterpret_cast<const double*>(Mb.res);
+                    double* rb = reinterpret_cast<double*>(Mb.res_beta);
+                    const double* ui = reinterpret_cast<const double*>(Mb.ui);
+                    double* zp = reinterpret_cast<double*>(Mb.zeta);
+                    for (int l = 0; l < L; ++l) {
+                        const long long ol = o + l * ls;
+                        // cabaret_predictor, qg3p_aux.F90:1012-1018
+                        double zz = zo[ol] + 0.5 * dt * rs[ol];
+                        // cabaret_beta, qg3p_aux.F90:1051-1059
+                        const double rbn = dt * (0.5 * (ui[ol + 1] + ui[ol]) * Mb.beta[l]);
+                        zz = zz + (1.0 + ta) * rbn - ta * rb[ol];
+                        rb[ol] = rbn;
+                        zp[ol] = zz;
+                        z[l] = zz;
+                    }
+                } else {
+                    const double* zsrc = reinterpret_cast<const double*>(Mb.zeta);
+                    for (int l = 0; l < L; ++l) z[l] = zsrc[o + l * ls];
+                }
+                // z_to_modes, qg3p_diagnostics.F90:545-549
+                for (int m = 0; m < L; ++m) {
+                    double s = 0.0;
+                    for (int l = 0; l < L; ++l) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
+                    v[m] = s;
+                }
+            }
+            for (int m = 0; m < L; ++m) xr[m * xs + k] = cff * v[m];
+        }
+        __syncthreads();
+        for (int m0 = 0; m0 < L; m0 += G) {
+            const int g = min(G, L - m0);
+            dst_rows(xr + m0 * xs, xs, g, za, zb, wsum, Mb);
+        }
+        double* spec = reinterpret_cast<double*>(Mb.spec);
+        for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
+            const long long o = (long long)j * pitch + (k - 1);
+            for (int m = 0; m < L; ++m) spec[o + m * ls] = xr[m * xs + k];
+        }
+        return;
+    }
+
+    // ---------------- inverse: DST of the solved spectral rows --------------
+    if (interior_row) {
+        const double* spec = reinterpret_cast<const double*>(Mb.spec);
+        for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
+            const long long o = (long long)j * pitch + (k - 1);
+            for (int m = 0; m < L; ++m) xr[m * xs + k] = spec[o + m * ls];
+        }
+        __syncthreads();
+        for (int m0 = 0; m0 < L; m0 += G) {
+            const int g = min(G, L - m0);
+            dst_rows(xr + m0 * xs, xs, g, za, zb, wsum, Mb);
+        }
+    }
+    if (EPI == EPI_HELM) {
+        // helm's in-place output: interior entries of interior rows, row
+        // i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1) (:1055-1057).
+        double* io = reinterpret_cast<double*>(Mb.helm_io);
+        if (interior_row) {
+            for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
+                for (int m = 0; m < L; ++m) io[(long long)j * pitch + k + m * ls] = xr[m * xs + k];
+            if (threadIdx.x == 0)
+                for (int m = 0; m < L; ++m) io[(long long)j * pitch + (ii - 1) + m * ls] = 0.0;
+        } else if (j == 0) {
+            for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
+                for (int m = 0; m < L; ++m) io[k + m * ls] = 0.0;
+        }
+        return;
+    }
+    // EPI_PV: psi_l = phi_1 - psiC_1 + sum_{m>=2} m2z(l,m) (phi_m - psiC_m corr_m)
+    // (modes_to_z_btcu) on every node of row j; phi is zero on the boundary
+    // (apply_dirichlet_bc(0), qg3p_aux.F90:470).
+    const double* psiC = Mb.sc->psiC;
+    const double* corr = Mb.corr;
+    double* psi = Mb.psi;
+    for (int i = threadIdx.x; i < ii; i += blockDim.x) {
+        const bool inner = interior_row && i >= 1 && i <= n;
+        const long long o = (long long)j * pitch + i;
+        double ph[PQ_MAXL];
+        for (int m = 0; m < L; ++m) ph[m] = inner ? xr[m * xs + i] : 0.0;
+        for (int l = 0; l < L; ++l) {
+            double dot = 0.0;
+            for (int m = 1; m < L; ++m) dot += Mb.m2z[l * PQ_MAXL + m] * (ph[m] - psiC[m] * corr[o + m * ls]);
+            psi[o + l * ls] = (ph[0] - psiC[0]) + dot;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tridiagonal solves along j for 8 wavenumbers of one mode.
+__device__ __forceinline__ double pivot(const Member& Mb, int mk, int p) {
+    const int len = __ldg(&Mb.piv_len[mk]);
+    return p <= len ? __ldg(&Mb.piv[__ldg(&Mb.piv_off[mk]) + p - 1]) : __ldg(&Mb.piv_fix[mk]);
+}
+
+__global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restrict__ mems,
+                                                          const int* __restrict__ prefix, int nmem, int do_mean) {
+    __shared__ Member Mb;
+    __shared__ double wpart[TRI_KT];
+    __shared__ int is_last;
+    extern __shared__ __align__(16) double strip[];  // [Mr][TRI_PAD]
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
+    load_member(Mb, mems + mi);
+    __syncthreads();
+    const int n = Mb.n, jj = Mb.jj, pitch = Mb.pitch;
+    const int tiles_per_mode = (n + TRI_KT - 1) / TRI_KT;
+    const int m = local / tiles_per_mode;
+    const int tile = local - m * tiles_per_mode;
+    const int k0 = tile * TRI_KT;  // 0-based column (wavenumber k0+1)
+    const int Mr = jj - 2;
+    double* spec = reinterpret_cast<double*>(Mb.spec) + (long long)m * Mb.lstride;
+
+    for (int idx = threadIdx.x; idx < Mr * TRI_KT; idx += blockDim.x) {
+        const int p = idx / TRI_KT, c = idx - p * TRI_KT;
+        strip[p * TRI_PAD + c] = (k0 + c < n) ? spec[(long long)(p + 1) * pitch + k0 + c] : 0.0;
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = warp;
+    const int kk = k0 + c;  // 0-based wavenumber index
+    double colsum = 0.0;
+    if (kk < n) {
+        const int mk = m * n + kk;
+        const int C = (Mr + 31) / 32;
+        const int a = lane * C + 1, b = min(Mr, (lane + 1) * C);
+        double* s = strip + c;  // s[(p-1)*TRI_PAD] is row position p
+        // Forward elimination, local pass: y~_a = f_a, y~_p = f_p - g_{p-1} y~_{p-1}.
+        double A = 1.0, cend = 0.0;
+        if (a <= b) {
+            double y = s[(a - 1) * TRI_PAD];
+            A = (a > 1) ? -pivot(Mb, mk, a - 1) : 0.0;
+            double gprev = pivot(Mb, mk, a);
+            for (int p = a + 1; p <= b; ++p) {
+                y = s[(p - 1) * TRI_PAD] - gprev * y;
+                s[(p - 1) * TRI_PAD] = y;
+                A = -gprev * A;
+                gprev = pivot(Mb, mk, p);
+            }
+            cend = y;
+        }
+        // Inclusive scan of the affine chunk maps y_out = c + A y_in.
+        double sA = A, sc = cend;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double pA = __shfl_up_sync(0xffffffffu, sA, o);
+            const double pc = __shfl_up_sync(0xffffffffu, sc, o);
+            if (lane >= o) {
+                sc = sc + sA * pc;
+                sA = sA * pA;
+            }
+        }
+        double yin = __shfl_up_sync(0xffffffffu, sc, 1);
+        if (lane == 0) yin = 0.0;
+        if (a <= b) {
+            double Ap = (a > 1) ? -pivot(Mb, mk, a - 1) : 0.0;
+            s[(a - 1) * TRI_PAD] = s[(a - 1) * TRI_PAD] + Ap * yin;
+            for (int p = a + 1; p <= b; ++p) {
+                Ap = -pivot(Mb, mk, p - 1) * Ap;
+                s[(p - 1) * TRI_PAD] = s[(p - 1) * TRI_PAD] + Ap * yin;
+            }
+        }
+        // Back substitution, local pass: x~_b = y_b g_b, x~_p = (y_p - x~_{p+1}) g_p.
+        double B = 1.0, cstart = 0.0;
+        if (a <= b) {
+            double gb = pivot(Mb, mk, b);
+            double x = s[(b - 1) * TRI_PAD] * gb;
+            s[(b - 1) * TRI_PAD] = x;
+            B = -gb;
+            for (int p = b - 1; p >= a; --p) {
+                const double gp = pivot(Mb, mk, p);
+                x = (s[(p - 1) * TRI_PAD] - x) * gp;
+                s[(p - 1) * TRI_PAD] = x;
+                B = -gp * B;
+            }
+            cstart = x;
+        }
+        // Reverse inclusive scan of x_start = c + B x_next.
+        double rB = B, rc = cstart;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double nB = __shfl_down_sync(0xffffffffu, rB, o);
+            const double nc = __shfl_down_sync(0xffffffffu, rc, o);
+            if (lane + o < 32) {
+                rc = rc + rB * nc;
+                rB = rB * nB;
+            }
+        }
+        double xin = __shfl_down_sync(0xffffffffu, rc, 1);
+        if (lane == 31) xin = 0.0;
+        double lsum = 0.0;
+        if (a <= b) {
+            double Bp = -pivot(Mb, mk, b);
+            double v = s[(b - 1) * TRI_PAD] + Bp * xin;
+            s[(b - 1) * TRI_PAD] = v;
+            lsum += v;
+            for (int p = b - 1; p >= a; --p) {
+                Bp = -pivot(Mb, mk, p) * Bp;
+                v = s[(p - 1) * TRI_PAD] + Bp * xin;
+                s[(p - 1) * TRI_PAD] = v;
+                lsum += v;
+            }
+        }
+        if (do_mean) colsum = warp_sum(lsum) * __ldg(&Mb.wmean[kk]);
+    }
+    if (lane == 0) wpart[warp] = colsum;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < Mr * TRI_KT; idx += blockDim.x) {
+        const int p = idx / TRI_KT, cc = idx - p * TRI_KT;
+        if (k0 + cc < n) spec[(long long)(p + 1) * pitch + k0 + cc] = strip[p * TRI_PAD + cc];
+    }
+    if (!do_mean) return;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < TRI_KT; ++w) t += wpart[w];
+        Mb.partials[local] = t;
+        __threadfence();
+        const unsigned prev = atomicAdd(&Mb.counters[0], 1u);
+        is_last = (prev == (unsigned)(Mb.ntiles_tri - 1));
+    }
+    __syncthreads();
+    if (!is_last) return;
+    // Last CTA of this member: psiC_m = (sum of partials) / (g_ii_int g_jj_int),
+    // summed in a fixed order so that the result is independent of CTA timing.
+    if (threadIdx.x < Mb.L) {
+        __threadfence();
+        const int mm = threadIdx.x;
+        const volatile double* part = Mb.partials;
+        double t = 0.0;
+        for (int q = 0; q < tiles_per_mode; ++q) t += part[mm * tiles_per_mode + q];
+        const double pc = t * Mb.mean_scale;
+        Mb.sc->psiC[mm] = pc;
+        if (pc != pc) atomicOr(Mb.status, (int)ST_NAN_PSIC);
+        else if (fabs(pc) > 1.0e100) atomicOr(Mb.status, (int)ST_LARGE_PSIC);
+    }
+    if (threadIdx.x == 0) Mb.counters[0] = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers.
+static int pick_group(int L, int N, int M, size_t* bytes) {
+    int G = L;
+    while (G > 1 && dst_smem_bytes(L, G, N, M) > 112 * 1024) --G;
+    *bytes = dst_smem_bytes(L, G, N, M);
+    return G;
+}
+
+template <int PRO, int EPI>
+static cudaError_t launch_dst(const LaunchSet& ls, cudaStream_t st) {
+    size_t bytes;
+    const int G = pick_group(ls.maxL, ls.maxN, ls.maxN / 2, &bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_dst_rows<PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    const int* prefix = (EPI == EPI_SPEC) ? ls.prefix_rows_interior : ls.prefix_rows_all;
+    const int nctas = (EPI == EPI_SPEC) ? ls.ctas_rows_interior : ls.ctas_rows_all;
+    k_dst_rows<PRO, EPI><<<nctas, DST_THREADS, bytes, st>>>(ls.members, prefix, ls.nmem, G, EPI == EPI_SPEC ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, cudaStream_t st) {
+    switch (prologue) {
+        case PRO_PLAIN: return launch_dst<PRO_PLAIN, EPI_SPEC>(ls, st);
+        case PRO_MODAL: return launch_dst<PRO_MODAL, EPI_SPEC>(ls, st);
+        default: return launch_dst<PRO_STEP, EPI_SPEC>(ls, st);
+    }
+}
+
+cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, cudaStream_t st) {
+    if (epilogue == EPI_HELM) return launch_dst<PRO_PLAIN, EPI_HELM>(ls, st);
+    return launch_dst<PRO_PLAIN, EPI_PV>(ls, st);
+}
+
+cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, cudaStream_t st) {
+    const size_t bytes = (size_t)(ls.maxJ - 2) * TRI_PAD * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    k_tridiag<<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
+    return cudaGetLastError();
+}
+
+}  // namespace pq

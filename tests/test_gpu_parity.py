@@ -1,0 +1,220 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Plain FP64 form tolerances: relative L2 <= 1e-12 for one solve or one step,
+<= 1e-9 after 100 steps, on fields and energy diagnostics.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import pequod_b200 as pq
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-12
+TOL_100 = 1e-9
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b.ravel())
+    return np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0)
+
+
+def helm_cfg(ii, jj, ss):
+    """A context whose layers are Helmholtz problems with the given ss."""
+    L = len(ss)
+    d = pq.ModelDesc()
+    d.ii, d.jj, d.layers = ii, jj, L
+    d.limiter, d.bc_type, d.dt = 1, pq.BC_FREE_SLIP, 1.0
+    for k in range(L):
+        d.ss[k] = ss[k]
+        d.h[k] = 1.0
+        for m in range(L):
+            d.m2z[k + L * m] = 1.0 if k == m else 0.0
+            d.z2m[k + L * m] = 1.0 if k == m else 0.0
+    return pq.Config(d, None, 1.0)
+
+
+@pytest.mark.parametrize("ii,jj,ss", [
+    (5, 5, [0.0]),
+    (9, 9, [0.0, 0.5]),
+    (17, 33, [0.0, 1.3, 7.0]),
+    (33, 20, [0.25]),
+    (65, 65, [0.0, 2.0, 9.0]),
+    (129, 257, [0.0, 0.7]),
+    (257, 129, [0.0, 3.0, 11.0]),
+    (1025, 1025, [0.0, 1.07613857, 3.31661571]),
+])
+def test_helm_matches_oracle(ii, jj, ss):
+    rng = np.random.default_rng(ii * 7 + jj)
+    L = len(ss)
+    rhs = np.asfortranarray(rng.standard_normal((ii, jj, L)))
+    g = pq.Model(helm_cfg(ii, jj, ss))
+    out = g.helm(rhs)
+    ref = O.Helm(ii, jj, L, ss)(rhs)
+    for l in range(L):
+        assert rel_l2(out[:, :, l], ref[:, :, l]) <= TOL_STEP, (l, rel_l2(out[:, :, l], ref[:, :, l]))
+    # Untouched entries keep the input (helm's in-place semantics).
+    assert np.array_equal(out[0, :, :], rhs[0, :, :])
+    assert np.array_equal(out[:, -1, :], rhs[:, -1, :])
+
+
+@pytest.mark.parametrize("ss,min_order", [(0.0, 2.0), (0.5, 3.9)])
+def test_helm_convergence_gpu(ss, min_order):
+    """test_helmholtz.F90:27-137 through the CUDA path."""
+    PI = math.pi
+    sizes = (33, 65, 129, 257, 513, 1025, 2049)
+    errs = []
+    for g in sizes:
+        i = np.arange(1, g + 1)[:, None]
+        j = np.arange(1, g + 1)[None, :]
+        x = (j - 1) / (g - 1)
+        y = (g - i) / (g - 1)
+        exact = np.sin(PI * x) * np.sin(PI * y)
+        if ss == 0.0:
+            rhs = -PI * PI * exact * (2.0 / (g - 1) ** 2)
+        else:
+            rhs = -exact * (2.0 * PI * PI / (g - 1) ** 2 + ss)
+        m = pq.Model(helm_cfg(g, g, [ss]))
+        out = m.helm(np.asfortranarray(rhs[:, :, None]))
+        out = O.apply_dirichlet_bc(out, 0.0)
+        errs.append(np.abs(out[:, :, 0] - exact).max())
+        m.close()
+    orders = [-math.log10(errs[n] / errs[n - 1]) / math.log10(sizes[n] / sizes[n - 1]) for n in range(1, len(errs))]
+    assert min(orders) >= min_order, orders
+
+
+def test_laplace_bc_gpu():
+    """test_laplace_bc.F90:21-31: Dirichlet BC = 1 with zero RHS gives psi == 1."""
+    ii = jj = 9
+    m = pq.Model(helm_cfg(ii, jj, [0.0]))
+    rhs = O.add_laplace_bc_rhs(np.zeros((ii, jj), order="F"), 1.0)
+    out = O.apply_dirichlet_bc(m.helm(rhs[:, :, None]), 1.0)
+    assert np.abs(out - 1.0).max() <= 1e-14
+
+
+def double_gyre(ii, layers=3, dt=1800.0, **kw):
+    H = {1: (1.0e5,), 2: (1.0e5, 3.0e5), 3: (3.0e4, 7.0e4, 3.0e5),
+         5: (2.5e4, 5.0e4, 7.5e4, 1.0e5, 1.5e5)}[layers]
+    gp = {1: (), 2: (1.5,), 3: (1.5, 0.75), 5: (1.5, 0.75, 0.375, 0.1875)}[layers]
+    p = pq.double_gyre_physical(ii, layers=layers, dt=dt, dx=3.84e8 / (ii - 1), H=H, gprime=gp, **kw)
+    return pq.Config.from_physical(p)
+
+
+@pytest.mark.parametrize("ii,layers", [(33, 1), (65, 2), (129, 3), (65, 5)])
+def test_pv_inversion_matches_oracle(ii, layers):
+    cfg = double_gyre(ii, layers)
+    rng = np.random.default_rng(ii + layers)
+    zeta = np.asfortranarray(rng.standard_normal((ii, ii, layers)))
+    g = pq.Model(cfg)
+    psi = g.pv_inversion(zeta)
+    om = O.Model(cfg.oracle_cfg())
+    zd = np.zeros((ii + 2, ii + 2, layers), order="F")
+    zd[1:-1, 1:-1, :] = zeta
+    ref = om.pv_inversion(zd)[1:-1, 1:-1, :]
+    assert rel_l2(psi, ref) <= TOL_STEP, rel_l2(psi, ref)
+
+
+def start(cfg, seed=1):
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    g = pq.Model(cfg)
+    g.init_perturb(ic)
+    o = O.Model(cfg.oracle_cfg())
+    o.init(ic)
+    return g, o
+
+
+FIELDS = ["psi", "zeta", "ui", "uj", "uimo", "ujmo", "zeta_fi", "zeta_fj", "res", "res_beta"]
+
+
+def compare(g, o, tol, fields=FIELDS):
+    worst = {}
+    for f in fields:
+        a, b = g.get(f), o.get(f)
+        worst[f] = rel_l2(a, b)
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, worst
+    return worst
+
+
+def test_init_matches_oracle():
+    cfg = double_gyre(65, 3)
+    g, o = start(cfg)
+    compare(g, o, TOL_STEP, ["psi", "zeta", "zeta_old"])
+    assert rel_l2(g.get("rel"), o.get("rel")) <= TOL_STEP
+
+
+@pytest.mark.parametrize("ii,layers", [(33, 1), (65, 3), (129, 3), (65, 5)])
+def test_one_step_matches_oracle(ii, layers):
+    cfg = double_gyre(ii, layers)
+    g, o = start(cfg)
+    g.step(1)
+    o.step(1)
+    compare(g, o, TOL_STEP)
+    assert rel_l2(g.get("rel"), o.get("rel")) <= TOL_STEP
+
+
+def test_ten_steps_each_matches_oracle():
+    cfg = double_gyre(129, 3)
+    g, o = start(cfg, seed=2)
+    for s in range(10):
+        g.step(1)
+        o.step(1)
+        compare(g, o, TOL_STEP * 10, ["psi", "zeta"])
+    compare(g, o, TOL_STEP * 10)
+
+
+def test_hundred_steps_and_energy():
+    cfg = double_gyre(129, 3)
+    g, o = start(cfg, seed=3)
+    g.step(100)
+    o.step(100)
+    compare(g, o, TOL_100)
+    ek_g, ep_g = g.energy()
+    ek_o, ep_o = o.energy()
+    assert rel_l2(ek_g, ek_o) <= TOL_100
+    assert abs(ep_g - ep_o) <= TOL_100 * abs(ep_o)
+    assert abs(g.cfl() - o.cfl()) <= TOL_100 * o.cfl()
+    sc = g.scalars()
+    assert abs(sc["model_time"] - o.scalars()["model_time"]) <= 1e-12 * sc["model_time"]
+
+
+def test_adaptive_dt_matches_oracle():
+    cfg = double_gyre(65, 3, adapt_dt=1, target_cfl=0.1, max_dt=86400.0)
+    g, o = start(cfg, seed=4)
+    g.step(20)
+    o.step(20)
+    compare(g, o, 1e-10)
+    sg, so = g.scalars(), o.scalars()
+    for k in ("dt", "tweight_a", "tweight_u"):
+        assert abs(sg[k] - so[k]) <= 1e-10 * abs(so[k]), (k, sg[k], so[k])
+
+
+def test_energy_kats_gpu():
+    """test_energy_2.F90:42-66 through the device energy reduction."""
+    cfg = double_gyre(9, 2)
+    g = pq.Model(cfg)
+    ii = jj = 9
+    psi = np.zeros((ii + 2, jj + 2, 2), order="F")
+    h = np.array(cfg.desc.h[:2])
+    s2 = np.array(cfg.desc.s2[:2])
+    for v1, v2 in ((1.0, 0.0), (2.0, 0.0), (0.0, 0.0)):
+        psi[1:-1, 1:-1, 0] = v1
+        psi[1:-1, 1:-1, 1] = v2
+        g.set("psi", psi)
+        ek, ep = g.energy()
+        ek_o, ep_o = O.energy(psi, h, s2)
+        assert abs(ep - ep_o) <= 1e-14 * max(abs(ep_o), 1e-300)
+        assert np.allclose(ek, ek_o, rtol=0, atol=1e-14)
+    for i in range(ii):
+        psi[i + 1, 1:-1, 0] = i + 1.0
+        psi[i + 1, 1:-1, 1] = i + 2.0
+    g.set("psi", psi)
+    ek, ep = g.energy()
+    ek_o, ep_o = O.energy(psi, h, s2)
+    assert np.allclose(ek, ek_o, rtol=1e-13, atol=0)
+    assert abs(ep - ep_o) <= 1e-13 * abs(ep_o)
