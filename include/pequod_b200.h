@@ -227,6 +227,29 @@ PQ_API void* pq_stream(pq_ctx* ctx);
 PQ_API int pq_kernel_timing(pq_ctx* ctx, int enable);
 PQ_API int pq_kernel_times(pq_ctx* ctx, double* ms4, long* launches4);
 
+/* ---- energy for callers that cannot allocate device memory --------------
+ * No counterpart in the reference: its energy() (qg3p_diagnostics.F90:778-
+ * 863) runs on host arrays.  pq_energy_noalloc computes the same ekin / epot
+ * as pq_energy on a psi array the caller already owns on the device, without
+ * a context and without allocating anything: for a host driver that is
+ * capturing a CUDA graph (where cudaMalloc is not allowed) or whose device
+ * memory is fully reserved by an HBM budget.
+ *   psi    device, (ld, jj, layers) column-major, node values (sdata)
+ *   h, s2  host, layers entries (strat%h, strat%s2)
+ *   out    device, layers + 1 doubles: ekin(1:layers), then epot
+ *   stream cudaStream_t to order the work on (NULL: legacy default stream)
+ * Limits: jj <= PQ_NOALLOC_MAX_JJ, layers <= PQ_MAX_LAYERS; larger sizes
+ * return PQ_ERR_ARG.  The reduction's scratch (row partials and a counter,
+ * about 300 KB) is a fixed array inside the library that every GPU which
+ * loads it keeps until exit; all calls share it, so calls whose device work
+ * overlaps race and must be serialised by the caller.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress); make
+ * that first call before starting any stream capture.  Asynchronous: `out`
+ * is valid once the stream has reached the call. */
+#define PQ_NOALLOC_MAX_JJ 4097
+PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int ld, const double* h,
+                             const double* s2, double* out, void* stream);
+
 /* Number of kernel launches the last pq_step enqueued. */
 PQ_API long pq_last_launch_count(const pq_ctx* ctx);
 

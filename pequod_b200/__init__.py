@@ -96,6 +96,8 @@ SIGNATURES = {
     "pq_last_launch_count": (C.c_long, [C.c_void_p]),
     "pq_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "pq_kernel_times": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_long)]),
+    "pq_energy_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_void_p,
+                                    C.c_void_p]),
 }
 
 KERNELS = ("dst_forward", "tridiag", "dst_inverse_backproject", "cabaret_fused")
