@@ -227,8 +227,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     const size_t lstride = (size_t)c->pitch * jj;
     c->field_bytes = lstride * L * sizeof(double);
     const int ntiles_tri = L * ((n + 7) / 8);
-    const int ntx = (ii + CAB_TX - 1) / CAB_TX, nty = (jj + CAB_TY - 1) / CAB_TY;
-    const int ntiles_cab = ntx * nty;
+    const int ntiles_cab = cabaret_ctas(ii, jj, L);
 
     // Tables.
     std::vector<double2> tw(M), wsplit(M);

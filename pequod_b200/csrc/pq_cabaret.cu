@@ -1,9 +1,7 @@
 // pq_cabaret.cu -- the CABARET advection step after the PV inversion, fused.
 //
-// One CTA owns a 32 x 8 tile of nodes (all layers).  It stages psi (all
-// layers, halo 2) and, layer by layer, the inputs with the halo each stage
-// needs, then computes in shared memory, in the reference's order
-// (qg3.F90:641-957):
+// Everything between the PV inversion and the next step's predictor, in the
+// reference's order (qg3.F90:641-957), in one pass over the fields:
 //   rel_from_zeta_and_psi + apply_rel_bc     qg3p_aux.F90:738-915
 //   update_zeta_bc                           :643-734
 //   cabaret_forcing                          :1065-1164
@@ -11,19 +9,13 @@
 //   cabaret_extrapolator (+ limiter)         :1317-1544
 //   cabaret_flux                             :1547-1594
 //   cabaret_corrector + set(zeta_old, zeta)  :1597-1642, qg3.F90:957
-// and writes back only the fields the next step needs.  Halo values are
-// recomputed, never exchanged.  The face fields that are read at neighbour
-// faces (ui, zeta_fi, zeta_fj) are ping-ponged; the others are updated in
-// place (each face is read and written by its owner CTA only).
+// writing back only the fields the next step needs.  Halo values are
+// recomputed, never exchanged.  Fields read at nodes or faces owned by another
+// warp (zeta_old, uimo, ujmo, zeta_fi, zeta_fj) are ping-ponged.
 #include "pq_common.cuh"
 #include "pq_kernels.h"
 
 namespace pq {
-
-constexpr int CAB_THREADS = CAB_TX * CAB_TY;
-constexpr int HW = CAB_TX + 4;  // staged width (halo 2)
-constexpr int HH = CAB_TY + 4;  // staged height (halo 2)
-constexpr int HA = HW * HH;
 
 __device__ __forceinline__ void load_member_c(Member& dst, const Member* src) {
     const int n = sizeof(Member) / 4;
@@ -72,193 +64,267 @@ __device__ __forceinline__ double zeta_bc_node(const Member& Mb, PS ps, double r
     return rel - Mb.s1[l] * (p - ps(i, j, l - 1)) - Mb.s2[l] * (p - ps(i, j, l + 1));
 }
 
-__global__ void __launch_bounds__(CAB_THREADS) k_cabaret_fused(const Member* __restrict__ mems,
-                                                                 const int* __restrict__ prefix, int nmem) {
+// Sweep decomposition: a warp owns one layer of a strip of 32 columns
+// (CAB_SW = 28 output columns plus 2 halo lanes on each side) and marches down
+// a band of CAB_SH output rows.  Every per-lane quantity lives in registers as
+// a rolling window over rows; the i-neighbours come from warp shuffles.  At
+// iteration r (s = r - 2) the warp loads psi row s+2 and the inputs of rows
+// s, s-1, and produces
+//   rel(s), zeta after BC/forcing at row s-1, uj on face row s, ui on row s-1,
+//   zeta_fj on face row s-1, zeta_fi on row s-1, and res / zeta_old at row s-2,
+// so output row o is final at iteration o + 4.
+constexpr int CAB_WARPS = 4;
+constexpr int CAB_SW = 28;  // output columns per warp
+constexpr int CAB_SH = 16;  // output rows per warp
+
+__device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+__global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* __restrict__ mems,
+                                                                    const int* __restrict__ prefix, int nmem) {
     __shared__ Member Mb;
-    __shared__ double sRel[HA], sZf[HA], sZo[HA], sZp[HA];
-    __shared__ double sUi[HA], sUj[HA], sFi[HA], sFj[HA];
-    __shared__ double sFlxI[HA], sFlxJ[HA];
-    __shared__ double red[CAB_THREADS / 32];
+    __shared__ double red[CAB_WARPS];
     __shared__ int is_last;
-    extern __shared__ __align__(16) double sPsi[];  // [L][HA]
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
     load_member_c(Mb, mems + mi);
     __syncthreads();
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
-    const int ntx = (ii + CAB_TX - 1) / CAB_TX;
-    const int ty = local / ntx, tx = local - ty * ntx;
-    const int i0 = tx * CAB_TX, j0 = ty * CAB_TY;
-    const int ib = i0 - 2, jb = j0 - 2;  // staged origin
-    const double dt = Mb.sc->dt, tu = Mb.sc->tweight_u;
-    const int cur = Mb.cur, nxt = cur ^ 1;
-
-    auto sidx = [&](int i, int j) { return (j - jb) * HW + (i - ib); };
-    auto inside = [&](int i, int j) { return i >= 0 && i < ii && j >= 0 && j < jj; };
-    auto ps = [&](int i, int j, int l) { return sPsi[l * HA + sidx(i, j)]; };
-
-    // P0: psi, all layers, halo 2.
-    for (int t = threadIdx.x; t < L * HA; t += blockDim.x) {
-        const int l = t / HA, r = t - l * HA;
-        const int j = jb + r / HW, i = ib + r % HW;
-        sPsi[t] = inside(i, j) ? Mb.psi[(long long)j * pitch + i + l * ls] : 0.0;
-    }
-
-    const double* zeta_pb = reinterpret_cast<const double*>(Mb.zeta);
-    const double* zeta_old = reinterpret_cast<const double*>(Mb.zeta_old[cur]);
-    double* zeta_new = reinterpret_cast<double*>(Mb.zeta_old[nxt]);
-    double* res = reinterpret_cast<double*>(Mb.res);
-    double* ui_new = reinterpret_cast<double*>(Mb.ui);
-    double* uj = reinterpret_cast<double*>(Mb.uj);
-    const double* uimo = reinterpret_cast<const double*>(Mb.uimo[cur]);
-    double* uimo_new = reinterpret_cast<double*>(Mb.uimo[nxt]);
-    const double* ujmo = reinterpret_cast<const double*>(Mb.ujmo[cur]);
-    double* ujmo_new = reinterpret_cast<double*>(Mb.ujmo[nxt]);
-    const double* zfi_old = reinterpret_cast<const double*>(Mb.zfi[cur]);
-    double* zfi_new = reinterpret_cast<double*>(Mb.zfi[nxt]);
-    const double* zfj_old = reinterpret_cast<const double*>(Mb.zfj[cur]);
-    double* zfj_new = reinterpret_cast<double*>(Mb.zfj[nxt]);
+    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + CAB_SH - 1) / CAB_SH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int task = local * CAB_WARPS + warp;
     double umax = 0.0;
-
-    for (int l = 0; l < L; ++l) {
+    if (task < nstrips * nbands * L) {
+        const int l = task % L;
+        const int sb = task / L;
+        const int strip = sb % nstrips, band = sb / nstrips;
+        const int i0 = strip * CAB_SW, j0 = band * CAB_SH;
+        const int i = i0 - 2 + lane;
+        const bool in_i = (i >= 0 && i < ii);
+        const bool out_i = (lane >= 2 && lane < 2 + CAB_SW && in_i);  // owner of node / i-face / j-face column i
+        const int cur = Mb.cur, nxt = cur ^ 1;
+        const double dt = Mb.sc->dt, tu = Mb.sc->tweight_u;
+        const double hdt = 0.5 * dt;
         const long long lo = l * ls;
-        // P1: staged zeta (after predictor + beta) and zeta_old, halo 2.
-        for (int r = threadIdx.x; r < HA; r += blockDim.x) {
-            const int j = jb + r / HW, i = ib + r % HW;
-            const bool in = inside(i, j);
-            const long long o = (long long)j * pitch + i + lo;
-            const bool interior = in && i > 0 && i < ii - 1 && j > 0 && j < jj - 1;
-            sZp[r] = interior ? zeta_pb[o] : 0.0;
-            sZo[r] = in ? zeta_old[o] : 0.0;
-            // Face fields read at neighbour faces: zeta_fi (i-faces) and
-            // zeta_fj (j-faces), plus the old velocities for extrapolation.
-            sFi[r] = in ? zfi_old[o] : 0.0;
-            sFj[r] = in ? zfj_old[o] : 0.0;
-        }
-        __syncthreads();
-        // P2: relative vorticity on the staged region.
-        for (int r = threadIdx.x; r < HA; r += blockDim.x) {
-            const int j = jb + r / HW, i = ib + r % HW;
-            sRel[r] = inside(i, j) ? rel_node(Mb, ps, sZp[r], i, j, l) : 0.0;
-        }
-        __syncthreads();
-        // P3: zeta after update_zeta_bc and cabaret_forcing, halo 1.
-        for (int r = threadIdx.x; r < HA; r += blockDim.x) {
-            const int j = jb + r / HW, i = ib + r % HW;
-            double v = 0.0;
-            if (inside(i, j) && i >= ib + 1 && i < ib + HW - 1 && j >= jb + 1 && j < jb + HH - 1) {
-                const bool boundary = (i == 0 || i == ii - 1 || j == 0 || j == jj - 1);
-                if (boundary) {
-                    v = zeta_bc_node(Mb, ps, sRel[r], i, j, l);
-                } else {
-                    const double rc = sRel[r];
-                    const double lap = -4.0 * rc + sRel[r - 1] + sRel[r + 1] + sRel[r - HW] + sRel[r + HW];
-                    double rv;
-                    const double nu = Mb.viscosity, vb = Mb.visc_bot;
-                    if (L == 1) {
-                        const double fw = Mb.wind ? Mb.wind[(long long)j * pitch + i] : 0.0;
-                        rv = dt * (fw - vb * rc + nu * lap);
-                    } else if (l == 0) {
-                        const double fw = Mb.wind ? Mb.wind[(long long)j * pitch + i] : 0.0;
-                        rv = dt * (fw + nu * lap);
-                    } else if (l == L - 1) {
-                        rv = dt * (-vb * rc + nu * lap);
-                    } else {
-                        rv = dt * nu * lap;
-                    }
-                    v = sZp[r] + rv;
-                }
-            }
-            sZf[r] = v;
-        }
-        // P4: face velocities (time-extrapolated), i-faces a in [i0-1, i0+33]
-        // on interior rows, j-faces b in [j0-1, j0+9] on interior columns.
-        // psi_edge(a, b) is the corner value between nodes a-1, a and b-1, b.
-        auto pe = [&](int a, int b) {
-            return 0.25 * (ps(a, b, l) + ps(a, b - 1, l) + ps(a - 1, b, l) + ps(a - 1, b - 1, l));
-        };
-        for (int r = threadIdx.x; r < HA; r += blockDim.x) {
-            const int j = jb + r / HW, i = ib + r % HW;
-            double u = 0.0;
-            // i-face a = i on row j
-            if (i >= 1 && i <= ii - 1 && j >= 1 && j <= jj - 2 && i >= i0 - 1 && i <= i0 + CAB_TX + 1 &&
-                j >= j0 && j < j0 + CAB_TY) {
-                const double uim = -pe(i, j + 1) + pe(i, j);
-                const long long o = (long long)j * pitch + i + lo;
-                u = (1.0 + tu) * uim - tu * uimo[o];
-                if (i >= i0 && i < i0 + CAB_TX) {
-                    // owner: record the new extrapolation base
-                    sFlxI[r] = uim;
-                }
-            }
-            sUi[r] = u;
-            double w = 0.0;
-            if (i >= 1 && i <= ii - 2 && j >= 1 && j <= jj - 1 && j >= j0 - 1 && j <= j0 + CAB_TY + 1 &&
-                i >= i0 && i < i0 + CAB_TX) {
-                const double ujm = pe(i + 1, j) - pe(i, j);
-                const long long o = (long long)j * pitch + i + lo;
-                w = (1.0 + tu) * ujm - tu * ujmo[o];
-                if (j >= j0 && j < j0 + CAB_TY) sFlxJ[r] = ujm;
-            }
-            sUj[r] = w;
-        }
-        __syncthreads();
-        // Write the owned face velocities and extrapolation bases; track max |u|.
-        for (int r = threadIdx.x; r < CAB_TX * CAB_TY; r += blockDim.x) {
-            const int i = i0 + (r % CAB_TX), j = j0 + (r / CAB_TX);
-            const int s = sidx(i, j);
-            const long long o = (long long)j * pitch + i + lo;
-            if (i >= 1 && i <= ii - 1 && j >= 1 && j <= jj - 2) {
-                ui_new[o] = sUi[s];
-                uimo_new[o] = sFlxI[s];
-                umax = fmax(umax, fabs(sUi[s]));
-            }
-            if (i >= 1 && i <= ii - 2 && j >= 1 && j <= jj - 1) {
-                uj[o] = sUj[s];
-                ujmo_new[o] = sFlxJ[s];
-                umax = fmax(umax, fabs(sUj[s]));
-            }
-        }
-        __syncthreads();
-        // P5: extrapolator + limiter, then fluxes, on faces a in [i0, i0+32]
-        // (rows of the tile) and b in [j0, j0+8] (columns of the tile).
+        const double* psi = Mb.psi;
+        const double* zeta_pb = reinterpret_cast<const double*>(Mb.zeta) + lo;
+        const double* zeta_old = reinterpret_cast<const double*>(Mb.zeta_old[cur]) + lo;
+        double* zeta_new = reinterpret_cast<double*>(Mb.zeta_old[nxt]) + lo;
+        double* res = reinterpret_cast<double*>(Mb.res) + lo;
+        double* ui_new = reinterpret_cast<double*>(Mb.ui) + lo;
+        double* uj_new = reinterpret_cast<double*>(Mb.uj) + lo;
+        const double* uimo = reinterpret_cast<const double*>(Mb.uimo[cur]) + lo;
+        double* uimo_new = reinterpret_cast<double*>(Mb.uimo[nxt]) + lo;
+        const double* ujmo = reinterpret_cast<const double*>(Mb.ujmo[cur]) + lo;
+        double* ujmo_new = reinterpret_cast<double*>(Mb.ujmo[nxt]) + lo;
+        const double* zfi_old = reinterpret_cast<const double*>(Mb.zfi[cur]) + lo;
+        double* zfi_new = reinterpret_cast<double*>(Mb.zfi[nxt]) + lo;
+        const double* zfj_old = reinterpret_cast<const double*>(Mb.zfj[cur]) + lo;
+        double* zfj_new = reinterpret_cast<double*>(Mb.zfj[nxt]) + lo;
+        const double* psil = psi + lo;
+        const double* psim = (l > 0) ? psi + lo - ls : psil;
+        const double* psip = (l < L - 1) ? psi + lo + ls : psil;
+        const double* wind = (l == 0) ? Mb.wind : nullptr;
+        const double nu = Mb.viscosity, vb = Mb.visc_bot;
+        const double s1 = Mb.s1[l], s2 = Mb.s2[l];
+        const int bc = Mb.bc_type;
+        const double cffbc = Mb.alpha / (Mb.alpha + 3.0);
         const bool lim = Mb.limiter != 0;
-        for (int r = threadIdx.x; r < HA; r += blockDim.x) {
-            const int j = jb + r / HW, i = ib + r % HW;
-            double fxi = 0.0;
-            if (i >= 1 && i <= ii - 1 && j >= 1 && j <= jj - 2 && i >= i0 && i <= i0 + CAB_TX && j >= j0 &&
-                j < j0 + CAB_TY) {
-                const double u1 = sUi[r], fi1 = sFi[r];
+
+        auto ld = [&](const double* base, int row) -> double {
+            return (in_i && row >= 0 && row < jj) ? base[(long long)row * pitch + i] : 0.0;
+        };
+        // Rolling windows.
+        double P0 = 0, P1 = ld(psil, j0 - 4), P2 = ld(psil, j0 - 3), P3 = ld(psil, j0 - 2), P4 = ld(psil, j0 - 1);
+        double Rm2 = 0, Rm1 = 0;           // rel rows s-2, s-1
+        double ZFm2 = 0;                   // zeta after forcing, row s-2
+        double ZOm2 = 0;                   // zeta_old row s-2
+        double UJm2 = 0, UJm1 = 0;         // uj faces s-2, s-1
+        double FJm2 = 0, FJm1 = 0;         // zeta_fj (old) faces s-2, s-1
+        double FLJm2 = 0;                  // flux_j face s-2
+        double FLI = 0;                    // flux_i row s-2 (face a = i)
+        double zpb_prev = 0, pm_prev = 0, pp_prev = 0, pe_prev = 0;
+
+        for (int r = j0; r < j0 + CAB_SH + 4; ++r) {
+            const int s = r - 2;
+            // ---- loads -------------------------------------------------------
+            P0 = P1;
+            P1 = P2;
+            P2 = P3;
+            P3 = P4;
+            P4 = ld(psil, s + 2);
+            const bool node_s = in_i && s >= 0 && s < jj;
+            const bool int_s = node_s && i > 0 && i < ii - 1 && s > 0 && s < jj - 1;
+            const double zpb_s = int_s ? zeta_pb[(long long)s * pitch + i] : 0.0;
+            const double pm_s = (L > 1) ? ld(psim, s) : 0.0;
+            const double pp_s = (L > 1) ? ld(psip, s) : 0.0;
+            const double zo_1 = ld(zeta_old, s - 1);
+            const double uimo_1 = ld(uimo, s - 1);
+            const double ujmo_s = ld(ujmo, s);
+            const double fio_1 = ld(zfi_old, s - 1);
+            const double fj_s = ld(zfj_old, s);
+            const double w_1 = wind ? ld(wind, s - 1) : 0.0;
+
+            // ---- rel(s): rel_from_zeta_and_psi + apply_rel_bc ---------------
+            const double up1 = shup(P2, 1), up2 = shup(P2, 2), dn1 = shdn(P2, 1), dn2 = shdn(P2, 2);
+            double rel_s = 0.0;
+            if (node_s) {
+                const bool bj = (s == 0 || s == jj - 1), bi = (i == 0 || i == ii - 1);
+                if (bj || bi) {
+                    if (bc != 3) {
+                        double q1, q2;
+                        if (bj) {
+                            q1 = (s == 0) ? P3 : P1;
+                            q2 = (s == 0) ? P4 : P0;
+                        } else {
+                            q1 = (i == 0) ? dn1 : up1;
+                            q2 = (i == 0) ? dn2 : up2;
+                        }
+                        rel_s = (bc == 1) ? cffbc * (-3.5 * P2 + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - P2);
+                    }
+                } else if (L == 1) {
+                    rel_s = zpb_s;
+                } else if (l == 0) {
+                    rel_s = zpb_s + s2 * (P2 - pp_s);
+                } else if (l == L - 1) {
+                    rel_s = zpb_s + s1 * (P2 - pm_s);
+                } else {
+                    rel_s = zpb_s + s1 * (P2 - pm_s) + s2 * (P2 - pp_s);
+                }
+            }
+
+            // ---- zeta at row s-1 after update_zeta_bc and cabaret_forcing ---
+            const int s1r = s - 1;
+            const double rl_up = shup(Rm1, 1), rl_dn = shdn(Rm1, 1);
+            double zf_1 = 0.0;
+            const bool node_1 = in_i && s1r >= 0 && s1r < jj;
+            if (node_1) {
+                const bool bnd = (s1r == 0 || s1r == jj - 1 || i == 0 || i == ii - 1);
+                if (bnd) {
+                    // update_zeta_bc: rel - coupling(psi)
+                    if (L == 1)
+                        zf_1 = Rm1;
+                    else if (l == 0)
+                        zf_1 = Rm1 - s2 * (P1 - pp_prev);
+                    else if (l == L - 1)
+                        zf_1 = Rm1 - s1 * (P1 - pm_prev);
+                    else
+                        zf_1 = Rm1 - s1 * (P1 - pm_prev) - s2 * (P1 - pp_prev);
+                } else {
+                    const double lap = -4.0 * Rm1 + rl_up + rl_dn + Rm2 + rel_s;
+                    double rv;
+                    if (L == 1)
+                        rv = dt * (w_1 - vb * Rm1 + nu * lap);
+                    else if (l == 0)
+                        rv = dt * (w_1 + nu * lap);
+                    else if (l == L - 1)
+                        rv = dt * (-vb * Rm1 + nu * lap);
+                    else
+                        rv = dt * nu * lap;
+                    zf_1 = zpb_prev + rv;
+                }
+            }
+
+            // ---- corner psi and face velocities ------------------------------
+            // pe_here: corner between nodes (i-1, i) x (s-1, s).
+            const double pe_here = 0.25 * (P2 + P1 + up1 + shup(P1, 1));
+            const double pe_dn = shdn(pe_here, 1);
+            // uj on face b = s (between rows s-1 and s), column i.
+            double uj_s = 0.0, ujm_s = 0.0;
+            const bool fj_ok = (s >= 1 && s <= jj - 1 && i >= 1 && i <= ii - 2);
+            if (fj_ok) {
+                ujm_s = pe_dn - pe_here;
+                uj_s = (1.0 + tu) * ujm_s - tu * ujmo_s;
+            }
+            // ui on row s-1, face a = i (between columns i-1 and i).
+            double ui_1 = 0.0, uim_1 = 0.0;
+            const bool fi_ok = (i >= 1 && i <= ii - 1 && s1r >= 1 && s1r <= jj - 2);
+            if (fi_ok) {
+                uim_1 = -pe_here + pe_prev;
+                ui_1 = (1.0 + tu) * uim_1 - tu * uimo_1;
+            }
+
+            // ---- extrapolator, j-faces: face b = s-1 ------------------------
+            double fjn = 0.0;
+            const int bf = s - 1;
+            const bool bfj_ok = (bf >= 1 && bf <= jj - 1 && i >= 1 && i <= ii - 2);
+            if (bfj_ok) {
+                const double u1 = UJm1, fi1 = FJm1;
                 double fi2, psi_n, psi_o, d_f;
                 if (u1 >= 0.0) {
-                    const int up = r - 1;  // node a-1
+                    if (bf > 1) {
+                        const double u2 = UJm2;
+                        fi2 = FJm2;
+                        const double v0 = (u1 + u2) / 2.0;
+                        psi_n = ZFm2;
+                        psi_o = ZOm2;
+                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2);
+                    } else {
+                        fi2 = ZFm2;
+                        psi_n = ZFm2;
+                        psi_o = ZOm2;
+                        d_f = -(psi_n - psi_o);
+                    }
+                } else {
+                    if (bf < jj - 1) {
+                        const double u2 = uj_s;
+                        fi2 = fj_s;
+                        const double v0 = (u1 + u2) / 2.0;
+                        psi_n = zf_1;
+                        psi_o = zo_1;
+                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
+                    } else {
+                        fi2 = zf_1;
+                        psi_n = zf_1;
+                        psi_o = zo_1;
+                        d_f = -(psi_n - psi_o);
+                    }
+                }
+                double v = 2.0 * psi_n - fi2;
+                if (lim) {
+                    const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+                    const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+                    if (v > fmx) v = fmx;
+                    if (v < fmn) v = fmn;
+                }
+                fjn = v;
+            }
+
+            // ---- extrapolator, i-faces on row s-1: face a = i ----------------
+            const double ui_up = shup(ui_1, 1), ui_dn = shdn(ui_1, 1);
+            const double fi_up = shup(fio_1, 1), fi_dn = shdn(fio_1, 1);
+            const double zf_up = shup(zf_1, 1), zo_up = shup(zo_1, 1);
+            double fin = 0.0;
+            if (fi_ok) {
+                const double u1 = ui_1, fi1 = fio_1;
+                double fi2, psi_n, psi_o, d_f;
+                if (u1 >= 0.0) {
                     if (i > 1) {
-                        const double u2 = sUi[r - 1];
-                        fi2 = sFi[r - 1];
+                        const double u2 = ui_up;
+                        fi2 = fi_up;
                         const double v0 = (u1 + u2) / 2.0;
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
+                        psi_n = zf_up;
+                        psi_o = zo_up;
                         d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2);
                     } else {
-                        fi2 = sZf[up];
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
+                        fi2 = zf_up;
+                        psi_n = zf_up;
+                        psi_o = zo_up;
                         d_f = -(psi_n - psi_o);
                     }
                 } else {
-                    const int up = r;  // node a
                     if (i < ii - 1) {
-                        const double u2 = sUi[r + 1];
-                        fi2 = sFi[r + 1];
+                        const double u2 = ui_dn;
+                        fi2 = fi_dn;
                         const double v0 = (u1 + u2) / 2.0;
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
+                        psi_n = zf_1;
+                        psi_o = zo_1;
                         d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
                     } else {
-                        fi2 = sZf[up];
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
+                        fi2 = zf_1;
+                        psi_n = zf_1;
+                        psi_o = zo_1;
                         d_f = -(psi_n - psi_o);
                     }
                 }
@@ -269,76 +335,59 @@ __global__ void __launch_bounds__(CAB_THREADS) k_cabaret_fused(const Member* __r
                     if (v > fmx) v = fmx;
                     if (v < fmn) v = fmn;
                 }
-                if (i < i0 + CAB_TX) zfi_new[(long long)j * pitch + i + lo] = v;
-                fxi = u1 * v;
+                fin = v;
             }
-            double fxj = 0.0;
-            if (i >= 1 && i <= ii - 2 && j >= 1 && j <= jj - 1 && j >= j0 && j <= j0 + CAB_TY && i >= i0 &&
-                i < i0 + CAB_TX) {
-                const double u1 = sUj[r], fi1 = sFj[r];
-                double fi2, psi_n, psi_o, d_f;
-                if (u1 >= 0.0) {
-                    const int up = r - HW;
-                    if (j > 1) {
-                        const double u2 = sUj[r - HW];
-                        fi2 = sFj[r - HW];
-                        const double v0 = (u1 + u2) / 2.0;
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
-                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2);
-                    } else {
-                        fi2 = sZf[up];
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
-                        d_f = -(psi_n - psi_o);
-                    }
-                } else {
-                    const int up = r;
-                    if (j < jj - 1) {
-                        const double u2 = sUj[r + HW];
-                        fi2 = sFj[r + HW];
-                        const double v0 = (u1 + u2) / 2.0;
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
-                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
-                    } else {
-                        fi2 = sZf[up];
-                        psi_n = sZf[up];
-                        psi_o = sZo[up];
-                        d_f = -(psi_n - psi_o);
-                    }
+            const double flj_1 = UJm1 * fjn;  // flux_j on face s-1
+            const double fli_1 = ui_1 * fin;  // flux_i on row s-1, face i
+
+            // ---- corrector at row o = s-2 -------------------------------------
+            const int o = s - 2;
+            const double fli_dn = shdn(FLI, 1);
+            const bool band_o = (o >= j0 && o < j0 + CAB_SH && o >= 0 && o < jj);
+            if (out_i && band_o) {
+                const bool bnd = (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
+                double z = ZFm2;
+                const long long off = (long long)o * pitch + i;
+                if (!bnd) {
+                    const double rr = -(fli_dn - FLI + flj_1 - FLJm2);
+                    res[off] = rr;
+                    z = z + hdt * rr;
                 }
-                double v = 2.0 * psi_n - fi2;
-                if (lim) {
-                    const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
-                    const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
-                    if (v > fmx) v = fmx;
-                    if (v < fmn) v = fmn;
-                }
-                if (j < j0 + CAB_TY) zfj_new[(long long)j * pitch + i + lo] = v;
-                fxj = u1 * v;
+                zeta_new[off] = z;
             }
-            sFlxI[r] = fxi;
-            sFlxJ[r] = fxj;
+            // ---- owned face writes ---------------------------------------------
+            if (out_i) {
+                if (fi_ok && s1r >= j0 && s1r < j0 + CAB_SH) {
+                    const long long off = (long long)s1r * pitch + i;
+                    ui_new[off] = ui_1;
+                    uimo_new[off] = uim_1;
+                    zfi_new[off] = fin;
+                    umax = fmax(umax, fabs(ui_1));
+                }
+                if (fj_ok && s >= j0 && s < j0 + CAB_SH) {
+                    const long long off = (long long)s * pitch + i;
+                    uj_new[off] = uj_s;
+                    ujmo_new[off] = ujm_s;
+                    umax = fmax(umax, fabs(uj_s));
+                }
+                if (bfj_ok && bf >= j0 && bf < j0 + CAB_SH) zfj_new[(long long)bf * pitch + i] = fjn;
+            }
+            // ---- shift the windows -------------------------------------------
+            Rm2 = Rm1;
+            Rm1 = rel_s;
+            ZFm2 = zf_1;
+            ZOm2 = zo_1;
+            UJm2 = UJm1;
+            UJm1 = uj_s;
+            FJm2 = FJm1;
+            FJm1 = fj_s;
+            FLJm2 = flj_1;
+            FLI = fli_1;
+            zpb_prev = zpb_s;
+            pm_prev = pm_s;
+            pp_prev = pp_s;
+            pe_prev = pe_here;
         }
-        __syncthreads();
-        // P6: corrector on the tile's nodes; zeta_old <- zeta.
-        {
-            const int i = i0 + (threadIdx.x % CAB_TX), j = j0 + (threadIdx.x / CAB_TX);
-            if (i < ii && j < jj) {
-                const int s = sidx(i, j);
-                const long long o = (long long)j * pitch + i + lo;
-                const bool boundary = (i == 0 || i == ii - 1 || j == 0 || j == jj - 1);
-                double z = sZf[s];
-                if (!boundary) {
-                    const double rr = -(sFlxI[s + 1] - sFlxI[s] + sFlxJ[s + HW] - sFlxJ[s]);
-                    res[o] = rr;
-                    z = z + 0.5 * dt * rr;
-                }
-                zeta_new[o] = z;
-            }
-        }
-        __syncthreads();
     }
 
     // Max |u| of the new face velocities (cabaret_cfl / cabaret_adapt_dt);
@@ -346,11 +395,11 @@ __global__ void __launch_bounds__(CAB_THREADS) k_cabaret_fused(const Member* __r
     // time stepping is on, sets dt and the time weights for the next step
     // (cabaret_adapt_dt, qg3p_aux.F90:946-990).
     umax = warp_max(umax);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = umax;
+    if (lane == 0) red[warp] = umax;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int w = 0; w < CAB_THREADS / 32; ++w) t = fmax(t, red[w]);
+        for (int w = 0; w < CAB_WARPS; ++w) t = fmax(t, red[w]);
         Mb.maxu_part[local] = t;
         __threadfence();
         const unsigned prev = atomicAdd(&Mb.counters[1], 1u);
@@ -383,11 +432,13 @@ __global__ void __launch_bounds__(CAB_THREADS) k_cabaret_fused(const Member* __r
     }
 }
 
+int cabaret_ctas(int ii, int jj, int L) {
+    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + CAB_SH - 1) / CAB_SH;
+    return (nstrips * nbands * L + CAB_WARPS - 1) / CAB_WARPS;
+}
+
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, cudaStream_t st) {
-    const size_t bytes = (size_t)ls.maxL * HA * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(k_cabaret_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
-    k_cabaret_fused<<<ls.ctas_cab, CAB_THREADS, bytes, st>>>(ls.members, ls.prefix_cab, ls.nmem);
+    k_cabaret_fused<<<ls.ctas_cab, CAB_WARPS * 32, 0, st>>>(ls.members, ls.prefix_cab, ls.nmem);
     return cudaGetLastError();
 }
 

@@ -38,7 +38,6 @@ enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
 constexpr int DST_THREADS = 256;
 constexpr int TRI_THREADS = 256;
 constexpr int TRI_KT = 8;   // wavenumbers per tridiagonal CTA (one per warp)
-constexpr int TRI_PAD = 9;  // padded row stride of the staged strip
 
 __device__ __forceinline__ void load_member(Member& dst, const Member* src) {
     const int n = sizeof(Member) / 4;
@@ -65,28 +64,28 @@ __device__ __forceinline__ double block_inclusive_scan(double v, double* wsum) {
     return s + off;
 }
 
-// Radix-4/2 Stockham FFT of G complex rows of length M (a power of two) in
-// shared memory, forward sign.  Rows g at a + g*M.  Returns the buffer that
-// holds the result (a or b).
-__device__ double2* fft_stockham(double2* a, double2* b, int G, int M, const double2* __restrict__ tw) {
-    int Ns = 1;
-    const int M4 = M >> 2;
+// Radix-4/2 Stockham FFT of G complex rows of length M = 2^logM in shared
+// memory, forward sign.  Rows g at a + g*M.  Returns the buffer that holds
+// the result (a or b).  All index arithmetic is shifts and masks.
+__device__ double2* fft_stockham(double2* a, double2* b, int G, int M, int logM, const double2* __restrict__ tw) {
+    int Ns = 1, logNs = 0;
+    const int M4 = M >> 2, logM4 = logM - 2;
     while (Ns * 4 <= M) {
-        const int st = M / (4 * Ns);
+        const int lst = logM4 - logNs;  // log2(M / (4 Ns))
         for (int w = threadIdx.x; w < G * M4; w += blockDim.x) {
-            const int g = w / M4, jj = w - g * M4;
-            const double2* ag = a + g * M;
-            double2* bg = b + g * M;
+            const int g = w >> logM4, jj = w & (M4 - 1);
+            const double2* ag = a + (g << logM);
+            double2* bg = b + (g << logM);
             double2 v0 = ag[jj], v1 = ag[jj + M4], v2 = ag[jj + 2 * M4], v3 = ag[jj + 3 * M4];
-            const int k = jj % Ns;
+            const int k = jj & (Ns - 1);
             if (k) {
-                v1 = cmul(v1, __ldg(&tw[k * st]));
-                v2 = cmul(v2, __ldg(&tw[2 * k * st]));
-                v3 = cmul(v3, __ldg(&tw[3 * k * st]));
+                v1 = cmul(v1, __ldg(&tw[k << lst]));
+                v2 = cmul(v2, __ldg(&tw[(2 * k) << lst]));
+                v3 = cmul(v3, __ldg(&tw[(3 * k) << lst]));
             }
             double2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), d3 = csub(v1, v3);
             double2 t3 = make_double2(d3.y, -d3.x);  // (v1 - v3) * (-i)
-            const int idx = (jj / Ns) * Ns * 4 + k;
+            const int idx = ((jj >> logNs) << (logNs + 2)) + k;
             bg[idx] = cadd(t0, t2);
             bg[idx + Ns] = cadd(t1, t3);
             bg[idx + 2 * Ns] = csub(t0, t2);
@@ -96,19 +95,20 @@ __device__ double2* fft_stockham(double2* a, double2* b, int G, int M, const dou
         double2* t = a;
         a = b;
         b = t;
-        Ns *= 4;
+        Ns <<= 2;
+        logNs += 2;
     }
     if (Ns < M) {
-        const int M2 = M >> 1;
-        const int st = M / (2 * Ns);
+        const int M2 = M >> 1, logM2 = logM - 1;
+        const int lst = logM2 - logNs;  // log2(M / (2 Ns))
         for (int w = threadIdx.x; w < G * M2; w += blockDim.x) {
-            const int g = w / M2, jj = w - g * M2;
-            const double2* ag = a + g * M;
-            double2* bg = b + g * M;
+            const int g = w >> logM2, jj = w & (M2 - 1);
+            const double2* ag = a + (g << logM);
+            double2* bg = b + (g << logM);
             double2 v0 = ag[jj], v1 = ag[jj + M2];
-            const int k = jj % Ns;
-            if (k) v1 = cmul(v1, __ldg(&tw[k * st]));
-            const int idx = (jj / Ns) * Ns * 2 + k;
+            const int k = jj & (Ns - 1);
+            if (k) v1 = cmul(v1, __ldg(&tw[k << lst]));
+            const int idx = ((jj >> logNs) << (logNs + 1)) + k;
             bg[idx] = cadd(v0, v1);
             bg[idx + Ns] = csub(v0, v1);
         }
@@ -124,11 +124,11 @@ __device__ double2* fft_stockham(double2* a, double2* b, int G, int M, const dou
 // memory at xr + g*xs, entries 1..n (entries 0 and N are scratch).
 // za, zb: shared complex scratch of G*M each.  wsum: 32 doubles.
 __device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, double* wsum, const Member& Mb) {
-    const int N = Mb.N, M = Mb.M, N2 = N >> 1;
+    const int N = Mb.N, M = Mb.M, N2 = N >> 1, logM = Mb.logM;
     const double* __restrict__ was = Mb.was;
     // Pre-twiddle (sint1, qg3p_helmholtz.F90:1404-1413) and pack.
     for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
-        const int g = w / M, t = w - g * M;
+        const int g = w >> logM, t = w & (M - 1);
         const double* x = xr + g * xs;
         double c[2];
 #pragma unroll
@@ -152,13 +152,13 @@ __device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, do
         za[w] = make_double2(c[0], c[1]);
     }
     __syncthreads();
-    double2* Z = fft_stockham(za, zb, G, M, Mb.tw);
+    double2* Z = fft_stockham(za, zb, G, M, logM, Mb.tw);
     double2* other = (Z == za) ? zb : za;
     double* R = reinterpret_cast<double*>(other);  // G*M reals of scratch
     // Real-FFT split; even outputs directly, R_q to scratch for the scan.
     for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
-        const int g = w / M, q = w - g * M;
-        const double2* Zg = Z + g * M;
+        const int g = w >> logM, q = w & (M - 1);
+        const double2* Zg = Z + (g << logM);
         const double2 zq = Zg[q];
         const double2 zr = Zg[(M - q) & (M - 1)];
         const double2 zc = make_double2(zr.x, -zr.y);
@@ -326,17 +326,27 @@ __global__ void __launch_bounds__(DST_THREADS) k_dst_rows(const Member* __restri
 
 // ---------------------------------------------------------------------------
 // Tridiagonal solves along j for 8 wavenumbers of one mode.
-__device__ __forceinline__ double pivot(const Member& Mb, int mk, int p) {
-    const int len = __ldg(&Mb.piv_len[mk]);
-    return p <= len ? __ldg(&Mb.piv[__ldg(&Mb.piv_off[mk]) + p - 1]) : __ldg(&Mb.piv_fix[mk]);
-}
+//
+// The strip (Mr = jj - 2 rows x 8 wavenumbers) is staged in shared memory by
+// wavenumber, and within a wavenumber by chunk: row p (0-based) of chunk
+// q = p / R, t = p % R lives at c*CS + q*RS + t with RS = R | 1 and
+// CS = 32*RS + 1 both odd, so the 32 lanes of a warp (one chunk each) hit 32
+// distinct banks and the staging writes of 8 wavenumbers do too.  Lane q of
+// warp c runs the forward and backward Thomas recurrences of its chunk of
+// wavenumber c.
+struct PivotRow {
+    const double* piv;  // explicit reciprocal pivots, piv[p - 1] for p <= len
+    int len;
+    double fix;         // the fixed point for p > len
+    __device__ __forceinline__ double operator()(int p) const { return p <= len ? __ldg(&piv[p - 1]) : fix; }
+};
 
 __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restrict__ mems,
                                                           const int* __restrict__ prefix, int nmem, int do_mean) {
     __shared__ Member Mb;
     __shared__ double wpart[TRI_KT];
     __shared__ int is_last;
-    extern __shared__ __align__(16) double strip[];  // [Mr][TRI_PAD]
+    extern __shared__ __align__(16) double strip[];
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
     load_member(Mb, mems + mi);
@@ -347,11 +357,19 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     const int tile = local - m * tiles_per_mode;
     const int k0 = tile * TRI_KT;  // 0-based column (wavenumber k0+1)
     const int Mr = jj - 2;
+    const int R = (Mr + 31) >> 5;
+    const int RS = R | 1;
+    const int CS = 32 * RS + 1;
     double* spec = reinterpret_cast<double*>(Mb.spec) + (long long)m * Mb.lstride;
 
-    for (int idx = threadIdx.x; idx < Mr * TRI_KT; idx += blockDim.x) {
-        const int p = idx / TRI_KT, c = idx - p * TRI_KT;
-        strip[p * TRI_PAD + c] = (k0 + c < n) ? spec[(long long)(p + 1) * pitch + k0 + c] : 0.0;
+    // Stage: thread -> (column c = tid & 7, chunk q = tid >> 3); loop over t.
+    {
+        const int c = threadIdx.x & 7, q = threadIdx.x >> 3;
+        const bool colok = (k0 + c < n);
+        const double* g = spec + (long long)(q * R + 1) * pitch + k0 + c;
+        double* sdst = strip + c * CS + q * RS;
+        const int Rq = min(R, Mr - q * R);
+        for (int t = 0; t < Rq; ++t) sdst[t] = colok ? g[(long long)t * pitch] : 0.0;
     }
     __syncthreads();
 
@@ -361,20 +379,22 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     double colsum = 0.0;
     if (kk < n) {
         const int mk = m * n + kk;
-        const int C = (Mr + 31) / 32;
-        const int a = lane * C + 1, b = min(Mr, (lane + 1) * C);
-        double* s = strip + c;  // s[(p-1)*TRI_PAD] is row position p
-        // Forward elimination, local pass: y~_a = f_a, y~_p = f_p - g_{p-1} y~_{p-1}.
+        PivotRow g{Mb.piv + __ldg(&Mb.piv_off[mk]), __ldg(&Mb.piv_len[mk]), __ldg(&Mb.piv_fix[mk])};
+        const int a = lane * R + 1;                 // first row position (1-based) of the chunk
+        const int cnt = max(0, min(R, Mr - lane * R));
+        const int b = a + cnt - 1;
+        double* s = strip + c * CS + lane * RS;     // s[t] is position a + t
+        // Forward elimination, local: y~_a = f_a, y~_p = f_p - g_{p-1} y~_{p-1};
+        // y_p = y~_p + A_p y_{a-1}, A_a = -g_{a-1}, A_p = -g_{p-1} A_{p-1}.
         double A = 1.0, cend = 0.0;
-        if (a <= b) {
-            double y = s[(a - 1) * TRI_PAD];
-            A = (a > 1) ? -pivot(Mb, mk, a - 1) : 0.0;
-            double gprev = pivot(Mb, mk, a);
-            for (int p = a + 1; p <= b; ++p) {
-                y = s[(p - 1) * TRI_PAD] - gprev * y;
-                s[(p - 1) * TRI_PAD] = y;
-                A = -gprev * A;
-                gprev = pivot(Mb, mk, p);
+        if (cnt > 0) {
+            double y = s[0];
+            A = (a > 1) ? -g(a - 1) : 0.0;
+            for (int t = 1; t < cnt; ++t) {
+                const double gp = g(a + t - 1);
+                y = s[t] - gp * y;
+                s[t] = y;
+                A = -gp * A;
             }
             cend = y;
         }
@@ -391,25 +411,25 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         }
         double yin = __shfl_up_sync(0xffffffffu, sc, 1);
         if (lane == 0) yin = 0.0;
-        if (a <= b) {
-            double Ap = (a > 1) ? -pivot(Mb, mk, a - 1) : 0.0;
-            s[(a - 1) * TRI_PAD] = s[(a - 1) * TRI_PAD] + Ap * yin;
-            for (int p = a + 1; p <= b; ++p) {
-                Ap = -pivot(Mb, mk, p - 1) * Ap;
-                s[(p - 1) * TRI_PAD] = s[(p - 1) * TRI_PAD] + Ap * yin;
-            }
-        }
-        // Back substitution, local pass: x~_b = y_b g_b, x~_p = (y_p - x~_{p+1}) g_p.
+        // Fix-up of y, then the local back substitution from the chunk end:
+        // x~_b = y_b g_b, x~_p = (y_p - x~_{p+1}) g_p; x_p = x~_p + B_p x_{b+1},
+        // B_b = -g_b, B_p = -g_p B_{p+1}.
         double B = 1.0, cstart = 0.0;
-        if (a <= b) {
-            double gb = pivot(Mb, mk, b);
-            double x = s[(b - 1) * TRI_PAD] * gb;
-            s[(b - 1) * TRI_PAD] = x;
+        if (cnt > 0) {
+            double Ap = (a > 1) ? -g(a - 1) : 0.0;
+            s[0] = s[0] + Ap * yin;
+            for (int t = 1; t < cnt; ++t) {
+                Ap = -g(a + t - 1) * Ap;
+                s[t] = s[t] + Ap * yin;
+            }
+            const double gb = g(b);
+            double x = s[cnt - 1] * gb;
+            s[cnt - 1] = x;
             B = -gb;
-            for (int p = b - 1; p >= a; --p) {
-                const double gp = pivot(Mb, mk, p);
-                x = (s[(p - 1) * TRI_PAD] - x) * gp;
-                s[(p - 1) * TRI_PAD] = x;
+            for (int t = cnt - 2; t >= 0; --t) {
+                const double gp = g(a + t);
+                x = (s[t] - x) * gp;
+                s[t] = x;
                 B = -gp * B;
             }
             cstart = x;
@@ -428,15 +448,15 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         double xin = __shfl_down_sync(0xffffffffu, rc, 1);
         if (lane == 31) xin = 0.0;
         double lsum = 0.0;
-        if (a <= b) {
-            double Bp = -pivot(Mb, mk, b);
-            double v = s[(b - 1) * TRI_PAD] + Bp * xin;
-            s[(b - 1) * TRI_PAD] = v;
+        if (cnt > 0) {
+            double Bp = -g(b);
+            double v = s[cnt - 1] + Bp * xin;
+            s[cnt - 1] = v;
             lsum += v;
-            for (int p = b - 1; p >= a; --p) {
-                Bp = -pivot(Mb, mk, p) * Bp;
-                v = s[(p - 1) * TRI_PAD] + Bp * xin;
-                s[(p - 1) * TRI_PAD] = v;
+            for (int t = cnt - 2; t >= 0; --t) {
+                Bp = -g(a + t) * Bp;
+                v = s[t] + Bp * xin;
+                s[t] = v;
                 lsum += v;
             }
         }
@@ -444,9 +464,14 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     }
     if (lane == 0) wpart[warp] = colsum;
     __syncthreads();
-    for (int idx = threadIdx.x; idx < Mr * TRI_KT; idx += blockDim.x) {
-        const int p = idx / TRI_KT, cc = idx - p * TRI_KT;
-        if (k0 + cc < n) spec[(long long)(p + 1) * pitch + k0 + cc] = strip[p * TRI_PAD + cc];
+    {
+        const int cc = threadIdx.x & 7, q = threadIdx.x >> 3;
+        if (k0 + cc < n) {
+            double* gdst = spec + (long long)(q * R + 1) * pitch + k0 + cc;
+            const double* ssrc = strip + cc * CS + q * RS;
+            const int Rq = min(R, Mr - q * R);
+            for (int t = 0; t < Rq; ++t) gdst[(long long)t * pitch] = ssrc[t];
+        }
     }
     if (!do_mean) return;
     if (threadIdx.x == 0) {
@@ -473,6 +498,11 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         else if (fabs(pc) > 1.0e100) atomicOr(Mb.status, (int)ST_LARGE_PSIC);
     }
     if (threadIdx.x == 0) Mb.counters[0] = 0u;
+}
+
+__host__ __device__ inline size_t tri_smem_bytes(int jj) {
+    const int Mr = jj - 2, R = (Mr + 31) >> 5, RS = R | 1;
+    return (size_t)TRI_KT * (32 * RS + 1) * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -510,7 +540,7 @@ cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, cudaStream_t s
 }
 
 cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, cudaStream_t st) {
-    const size_t bytes = (size_t)(ls.maxJ - 2) * TRI_PAD * sizeof(double);
+    const size_t bytes = tri_smem_bytes(ls.maxJ);
     cudaError_t e = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     k_tridiag<<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);

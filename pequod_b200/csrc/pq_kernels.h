@@ -19,12 +19,10 @@ struct LaunchSet {
     int ctas_rows_all;
     const int* prefix_tri;            // L * ceil(n / 8) CTAs per member
     int ctas_tri;
-    const int* prefix_cab;            // ceil(ii/32) * ceil(jj/8) CTAs per member
+    const int* prefix_cab;            // cabaret_ctas(ii, jj, L) CTAs per member
     int ctas_cab;
 };
 
-constexpr int CAB_TX = 32;
-constexpr int CAB_TY = 8;
 
 // pq_helm.cu
 cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, cudaStream_t st);
@@ -33,6 +31,7 @@ cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, cudaStream_t st);
 
 // pq_cabaret.cu
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, cudaStream_t st);
+int cabaret_ctas(int ii, int jj, int L);  // CTAs of k_cabaret_fused per member
 cudaError_t launch_rel(const LaunchSet& ls, cudaStream_t st);
 cudaError_t launch_energy(const LaunchSet& ls, cudaStream_t st);
 
