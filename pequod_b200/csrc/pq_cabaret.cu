@@ -76,21 +76,333 @@ __device__ __forceinline__ double zeta_bc_node(const Member& Mb, PS ps, double r
 constexpr int CAB_WARPS = 4;
 constexpr int CAB_SW = 28;  // output columns per warp
 constexpr int CAB_SH = 16;  // output rows per warp
+constexpr int CAB_D = 4;    // depth of the per-warp cp.async row pipeline
+// Streamed inputs of one iteration (rows relative to s = r - 2).
+enum { F_PSI2 = 0, F_ZPB, F_PSIM, F_PSIP, F_ZO, F_UIMO, F_UJMO, F_FIO, F_FJ, F_WIND, CAB_NF };
+constexpr int CAB_RING = CAB_D * CAB_NF * 32;  // doubles per warp
 
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+// One warp's sweep over layer l of the strip starting at column i0 and the
+// band starting at row j0.  EDGE = false is the specialisation for warps
+// whose whole footprint (columns i0-2 .. i0+29, rows j0-4 .. j0+CAB_SH+3) lies
+// at least two nodes inside the domain: no bounds checks, no boundary
+// branches.  Returns the largest |u| of the faces it wrote.
+template <bool EDGE>
+__device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int j0, int lane, double* ring) {
+    const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
+    const long long ls = Mb.lstride;
+    const int i = i0 - 2 + lane;
+    const bool in_i = !EDGE || (i >= 0 && i < ii);
+    const bool out_i = (lane >= 2 && lane < 2 + CAB_SW && in_i);  // owner of node / i-face / j-face column i
+    const int cur = Mb.cur, nxt = cur ^ 1;
+    const double dt = Mb.sc->dt, tu = Mb.sc->tweight_u;
+    const double hdt = 0.5 * dt;
+    const long long lo = l * ls + i;  // every field pointer below is offset to column i
+    const double* psil = Mb.psi + lo;
+    const double* psim = (l > 0) ? psil - ls : psil;
+    const double* psip = (l < L - 1) ? psil + ls : psil;
+    const double* zeta_pb = reinterpret_cast<const double*>(Mb.zeta) + lo;
+    const double* zeta_old = reinterpret_cast<const double*>(Mb.zeta_old[cur]) + lo;
+    double* zeta_new = reinterpret_cast<double*>(Mb.zeta_old[nxt]) + lo;
+    double* res = reinterpret_cast<double*>(Mb.res) + lo;
+    double* ui_new = reinterpret_cast<double*>(Mb.ui) + lo;
+    double* uj_new = reinterpret_cast<double*>(Mb.uj) + lo;
+    const double* uimo = reinterpret_cast<const double*>(Mb.uimo[cur]) + lo;
+    double* uimo_new = reinterpret_cast<double*>(Mb.uimo[nxt]) + lo;
+    const double* ujmo = reinterpret_cast<const double*>(Mb.ujmo[cur]) + lo;
+    double* ujmo_new = reinterpret_cast<double*>(Mb.ujmo[nxt]) + lo;
+    const double* zfi_old = reinterpret_cast<const double*>(Mb.zfi[cur]) + lo;
+    double* zfi_new = reinterpret_cast<double*>(Mb.zfi[nxt]) + lo;
+    const double* zfj_old = reinterpret_cast<const double*>(Mb.zfj[cur]) + lo;
+    double* zfj_new = reinterpret_cast<double*>(Mb.zfj[nxt]) + lo;
+    const double* wind = (l == 0 && Mb.wind) ? Mb.wind + i : nullptr;
+    const double nu = Mb.viscosity, vb = Mb.visc_bot;
+    const double s1 = Mb.s1[l], s2 = Mb.s2[l];
+    const int bc = Mb.bc_type;
+    const double cffbc = Mb.alpha / (Mb.alpha + 3.0);
+    const bool lim = Mb.limiter != 0;
+    const bool top = (l == 0), bottom = (l == L - 1);
+    double umax = 0.0;
+
+    auto ld = [&](const double* base, int row) -> double {
+        if (EDGE) return (in_i && row >= 0 && row < jj) ? base[row * pitch] : 0.0;
+        return base[row * pitch];
+    };
+    // rel_from_zeta_and_psi coupling for an interior node.
+    auto rel_int = [&](double z, double p, double pm, double pp) -> double {
+        if (L == 1) return z;
+        if (top) return z + s2 * (p - pp);
+        if (bottom) return z + s1 * (p - pm);
+        return z + s1 * (p - pm) + s2 * (p - pp);
+    };
+    // Limited upwind extrapolation (cabaret_extrapolator, interior branch).
+    auto extrap = [&](double u1, double u2, double fi1, double fi2, double psi_n, double psi_o, bool pos) -> double {
+        const double v0 = (u1 + u2) / 2.0;
+        const double d_f = pos ? -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2)
+                               : -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
+        double v = 2.0 * psi_n - fi2;
+        if (lim) {
+            const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+            const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+            if (v > fmx) v = fmx;
+            if (v < fmn) v = fmn;
+        }
+        return v;
+    };
+    // The wall branch of the extrapolator: upwind node on the boundary.
+    auto extrap_wall = [&](double fi1, double psi_n, double psi_o) -> double {
+        const double fi2 = psi_n;
+        const double d_f = -(psi_n - psi_o);
+        double v = 2.0 * psi_n - fi2;
+        if (lim) {
+            const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+            const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+            if (v > fmx) v = fmx;
+            if (v < fmn) v = fmn;
+        }
+        return v;
+    };
+
+    // Rolling windows.
+    // Row copies of iteration r into ring stage r % CAB_D (cp.async, 8 bytes
+    // per lane; rows outside the domain, and zeta at non-interior nodes, are
+    // zero-filled by a source size of 0 with the source clamped in range).
+    const int rend = j0 + CAB_SH + 4;
+    auto cp = [&](double* dst, const double* base, int row, bool ok) {
+        const int rr = ok ? row : 0;
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(base + (long long)rr * pitch),
+                     "r"(ok ? 8 : 0)
+                     : "memory");
+    };
+    auto rowok = [&](int row) { return !EDGE || (in_i && row >= 0 && row < jj); };
+    auto issue = [&](int rr) {
+        const int ss = rr - 2;
+        double* d = ring + ((rr % CAB_D) * CAB_NF << 5) + lane;
+        cp(d + (F_PSI2 << 5), psil, ss + 2, rowok(ss + 2));
+        const bool intn = !EDGE || (in_i && i > 0 && i < ii - 1 && ss > 0 && ss < jj - 1);
+        cp(d + (F_ZPB << 5), zeta_pb, ss, intn);
+        if (L > 1) {
+            cp(d + (F_PSIM << 5), psim, ss, rowok(ss));
+            cp(d + (F_PSIP << 5), psip, ss, rowok(ss));
+        }
+        cp(d + (F_ZO << 5), zeta_old, ss - 1, rowok(ss - 1));
+        cp(d + (F_UIMO << 5), uimo, ss - 1, rowok(ss - 1));
+        cp(d + (F_UJMO << 5), ujmo, ss, rowok(ss));
+        cp(d + (F_FIO << 5), zfi_old, ss - 1, rowok(ss - 1));
+        cp(d + (F_FJ << 5), zfj_old, ss, rowok(ss));
+        if (wind) cp(d + (F_WIND << 5), wind, ss - 1, rowok(ss - 1));
+    };
+    for (int rr = j0; rr < j0 + CAB_D - 1; ++rr) {
+        issue(rr);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    double P0 = 0, P1 = ld(psil, j0 - 4), P2 = ld(psil, j0 - 3), P3 = ld(psil, j0 - 2), P4 = ld(psil, j0 - 1);
+    double Rm2 = 0, Rm1 = 0;    // rel rows s-2, s-1
+    double ZFm2 = 0;            // zeta after forcing, row s-2
+    double ZOm2 = 0;            // zeta_old row s-2
+    double UJm2 = 0, UJm1 = 0;  // uj faces s-2, s-1
+    double FJm2 = 0, FJm1 = 0;  // zeta_fj (old) faces s-2, s-1
+    double FLJm2 = 0;           // flux_j face s-2
+    double FLI = 0;             // flux_i row s-2 (face a = i)
+    double zpb_prev = 0, pm_prev = 0, pp_prev = 0, pe_prev = 0;
+
+#pragma unroll 1
+    for (int r = j0; r < j0 + CAB_SH + 4; ++r) {
+        const int s = r - 2;
+        // ---- loads -----------------------------------------------------------
+        // Keep CAB_D - 1 iterations of row copies in flight.
+        if (r + CAB_D - 1 < rend) issue(r + CAB_D - 1);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(CAB_D - 1) : "memory");
+        const double* st = ring + ((r % CAB_D) * CAB_NF << 5) + lane;
+        P0 = P1;
+        P1 = P2;
+        P2 = P3;
+        P3 = P4;
+        P4 = st[F_PSI2 << 5];
+        const bool node_s = !EDGE || (in_i && s >= 0 && s < jj);
+        const double zpb_s = st[F_ZPB << 5];
+        const double pm_s = (L > 1) ? st[F_PSIM << 5] : 0.0;
+        const double pp_s = (L > 1) ? st[F_PSIP << 5] : 0.0;
+        const double zo_1 = st[F_ZO << 5];
+        const double uimo_1 = st[F_UIMO << 5];
+        const double ujmo_s = st[F_UJMO << 5];
+        const double fio_1 = st[F_FIO << 5];
+        const double fj_s = st[F_FJ << 5];
+        const double w_1 = wind ? st[F_WIND << 5] : 0.0;
+
+        // ---- rel(s): rel_from_zeta_and_psi + apply_rel_bc -------------------
+        double up1 = 0.0, up2 = 0.0, dn1 = 0.0, dn2 = 0.0;
+        if (EDGE) {
+            up1 = shup(P2, 1);
+            up2 = shup(P2, 2);
+            dn1 = shdn(P2, 1);
+            dn2 = shdn(P2, 2);
+        } else {
+            up1 = shup(P2, 1);
+        }
+        double rel_s = 0.0;
+        if (!EDGE) {
+            rel_s = rel_int(zpb_s, P2, pm_s, pp_s);
+        } else if (node_s) {
+            const bool bj = (s == 0 || s == jj - 1), bi = (i == 0 || i == ii - 1);
+            if (bj || bi) {
+                if (bc != 3) {
+                    double q1, q2;
+                    if (bj) {
+                        q1 = (s == 0) ? P3 : P1;
+                        q2 = (s == 0) ? P4 : P0;
+                    } else {
+                        q1 = (i == 0) ? dn1 : up1;
+                        q2 = (i == 0) ? dn2 : up2;
+                    }
+                    rel_s = (bc == 1) ? cffbc * (-3.5 * P2 + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - P2);
+                }
+            } else {
+                rel_s = rel_int(zpb_s, P2, pm_s, pp_s);
+            }
+        }
+
+        // ---- zeta at row s-1 after update_zeta_bc and cabaret_forcing -------
+        const int s1r = s - 1;
+        const double rl_up = shup(Rm1, 1), rl_dn = shdn(Rm1, 1);
+        double zf_1 = 0.0;
+        const bool node_1 = !EDGE || (in_i && s1r >= 0 && s1r < jj);
+        if (node_1) {
+            const bool bnd = EDGE && (s1r == 0 || s1r == jj - 1 || i == 0 || i == ii - 1);
+            if (bnd) {
+                if (L == 1)
+                    zf_1 = Rm1;
+                else if (top)
+                    zf_1 = Rm1 - s2 * (P1 - pp_prev);
+                else if (bottom)
+                    zf_1 = Rm1 - s1 * (P1 - pm_prev);
+                else
+                    zf_1 = Rm1 - s1 * (P1 - pm_prev) - s2 * (P1 - pp_prev);
+            } else {
+                const double lap = -4.0 * Rm1 + rl_up + rl_dn + Rm2 + rel_s;
+                double rv;
+                if (L == 1)
+                    rv = dt * (w_1 - vb * Rm1 + nu * lap);
+                else if (top)
+                    rv = dt * (w_1 + nu * lap);
+                else if (bottom)
+                    rv = dt * (-vb * Rm1 + nu * lap);
+                else
+                    rv = dt * nu * lap;
+                zf_1 = zpb_prev + rv;
+            }
+        }
+
+        // ---- corner psi and face velocities ------------------------------------
+        // pe_here: corner between nodes (i-1, i) x (s-1, s).
+        const double pe_here = 0.25 * (P2 + P1 + up1 + shup(P1, 1));
+        const double pe_dn = shdn(pe_here, 1);
+        double uj_s = 0.0, ujm_s = 0.0;  // face b = s, column i
+        const bool fj_ok = !EDGE || (s >= 1 && s <= jj - 1 && i >= 1 && i <= ii - 2);
+        if (fj_ok) {
+            ujm_s = pe_dn - pe_here;
+            uj_s = (1.0 + tu) * ujm_s - tu * ujmo_s;
+        }
+        double ui_1 = 0.0, uim_1 = 0.0;  // row s-1, face a = i
+        const bool fi_ok = !EDGE || (i >= 1 && i <= ii - 1 && s1r >= 1 && s1r <= jj - 2);
+        if (fi_ok) {
+            uim_1 = -pe_here + pe_prev;
+            ui_1 = (1.0 + tu) * uim_1 - tu * uimo_1;
+        }
+
+        // ---- extrapolator, j-faces: face b = s-1 -------------------------------
+        double fjn = 0.0;
+        const int bf = s - 1;
+        const bool bfj_ok = !EDGE || (bf >= 1 && bf <= jj - 1 && i >= 1 && i <= ii - 2);
+        if (bfj_ok) {
+            const double u1 = UJm1;
+            if (u1 >= 0.0)
+                fjn = (!EDGE || bf > 1) ? extrap(u1, UJm2, FJm1, FJm2, ZFm2, ZOm2, true) : extrap_wall(FJm1, ZFm2, ZOm2);
+            else
+                fjn = (!EDGE || bf < jj - 1) ? extrap(u1, uj_s, FJm1, fj_s, zf_1, zo_1, false)
+                                              : extrap_wall(FJm1, zf_1, zo_1);
+        }
+
+        // ---- extrapolator, i-faces on row s-1: face a = i ------------------------
+        const double ui_up = shup(ui_1, 1), ui_dn = shdn(ui_1, 1);
+        const double fi_up = shup(fio_1, 1), fi_dn = shdn(fio_1, 1);
+        const double zf_up = shup(zf_1, 1), zo_up = shup(zo_1, 1);
+        double fin = 0.0;
+        if (fi_ok) {
+            const double u1 = ui_1;
+            if (u1 >= 0.0)
+                fin = (!EDGE || i > 1) ? extrap(u1, ui_up, fio_1, fi_up, zf_up, zo_up, true)
+                                       : extrap_wall(fio_1, zf_up, zo_up);
+            else
+                fin = (!EDGE || i < ii - 1) ? extrap(u1, ui_dn, fio_1, fi_dn, zf_1, zo_1, false)
+                                            : extrap_wall(fio_1, zf_1, zo_1);
+        }
+        const double flj_1 = UJm1 * fjn;  // flux_j on face s-1
+        const double fli_1 = ui_1 * fin;  // flux_i on row s-1, face i
+
+        // ---- corrector at row o = s-2 -----------------------------------------
+        const int o = s - 2;
+        const double fli_dn = shdn(FLI, 1);
+        const bool band_o = (o >= j0 && o < j0 + CAB_SH) && (!EDGE || (o >= 0 && o < jj));
+        if (out_i && band_o) {
+            const bool bnd = EDGE && (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
+            double z = ZFm2;
+            if (!bnd) {
+                const double rr = -(fli_dn - FLI + flj_1 - FLJm2);
+                res[o * pitch] = rr;
+                z = z + hdt * rr;
+            }
+            zeta_new[o * pitch] = z;
+        }
+        // ---- owned face writes ---------------------------------------------------
+        if (out_i) {
+            if (fi_ok && s1r >= j0 && s1r < j0 + CAB_SH) {
+                ui_new[s1r * pitch] = ui_1;
+                uimo_new[s1r * pitch] = uim_1;
+                zfi_new[s1r * pitch] = fin;
+                umax = fmax(umax, fabs(ui_1));
+            }
+            if (fj_ok && s >= j0 && s < j0 + CAB_SH) {
+                uj_new[s * pitch] = uj_s;
+                ujmo_new[s * pitch] = ujm_s;
+                umax = fmax(umax, fabs(uj_s));
+            }
+            if (bfj_ok && bf >= j0 && bf < j0 + CAB_SH) zfj_new[bf * pitch] = fjn;
+        }
+        // ---- shift the windows ---------------------------------------------------
+        Rm2 = Rm1;
+        Rm1 = rel_s;
+        ZFm2 = zf_1;
+        ZOm2 = zo_1;
+        UJm2 = UJm1;
+        UJm1 = uj_s;
+        FJm2 = FJm1;
+        FJm1 = fj_s;
+        FLJm2 = flj_1;
+        FLI = fli_1;
+        zpb_prev = zpb_s;
+        pm_prev = pm_s;
+        pp_prev = pp_s;
+        pe_prev = pe_here;
+    }
+    return umax;
+}
 
 __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* __restrict__ mems,
                                                                     const int* __restrict__ prefix, int nmem) {
     __shared__ Member Mb;
     __shared__ double red[CAB_WARPS];
     __shared__ int is_last;
+    extern __shared__ __align__(16) double cab_ring[];  // [CAB_WARPS][CAB_RING]
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
     load_member_c(Mb, mems + mi);
     __syncthreads();
-    const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
-    const long long ls = Mb.lstride;
+    const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
     const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + CAB_SH - 1) / CAB_SH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int task = local * CAB_WARPS + warp;
@@ -100,294 +412,9 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
         const int sb = task / L;
         const int strip = sb % nstrips, band = sb / nstrips;
         const int i0 = strip * CAB_SW, j0 = band * CAB_SH;
-        const int i = i0 - 2 + lane;
-        const bool in_i = (i >= 0 && i < ii);
-        const bool out_i = (lane >= 2 && lane < 2 + CAB_SW && in_i);  // owner of node / i-face / j-face column i
-        const int cur = Mb.cur, nxt = cur ^ 1;
-        const double dt = Mb.sc->dt, tu = Mb.sc->tweight_u;
-        const double hdt = 0.5 * dt;
-        const long long lo = l * ls;
-        const double* psi = Mb.psi;
-        const double* zeta_pb = reinterpret_cast<const double*>(Mb.zeta) + lo;
-        const double* zeta_old = reinterpret_cast<const double*>(Mb.zeta_old[cur]) + lo;
-        double* zeta_new = reinterpret_cast<double*>(Mb.zeta_old[nxt]) + lo;
-        double* res = reinterpret_cast<double*>(Mb.res) + lo;
-        double* ui_new = reinterpret_cast<double*>(Mb.ui) + lo;
-        double* uj_new = reinterpret_cast<double*>(Mb.uj) + lo;
-        const double* uimo = reinterpret_cast<const double*>(Mb.uimo[cur]) + lo;
-        double* uimo_new = reinterpret_cast<double*>(Mb.uimo[nxt]) + lo;
-        const double* ujmo = reinterpret_cast<const double*>(Mb.ujmo[cur]) + lo;
-        double* ujmo_new = reinterpret_cast<double*>(Mb.ujmo[nxt]) + lo;
-        const double* zfi_old = reinterpret_cast<const double*>(Mb.zfi[cur]) + lo;
-        double* zfi_new = reinterpret_cast<double*>(Mb.zfi[nxt]) + lo;
-        const double* zfj_old = reinterpret_cast<const double*>(Mb.zfj[cur]) + lo;
-        double* zfj_new = reinterpret_cast<double*>(Mb.zfj[nxt]) + lo;
-        const double* psil = psi + lo;
-        const double* psim = (l > 0) ? psi + lo - ls : psil;
-        const double* psip = (l < L - 1) ? psi + lo + ls : psil;
-        const double* wind = (l == 0) ? Mb.wind : nullptr;
-        const double nu = Mb.viscosity, vb = Mb.visc_bot;
-        const double s1 = Mb.s1[l], s2 = Mb.s2[l];
-        const int bc = Mb.bc_type;
-        const double cffbc = Mb.alpha / (Mb.alpha + 3.0);
-        const bool lim = Mb.limiter != 0;
-
-        auto ld = [&](const double* base, int row) -> double {
-            return (in_i && row >= 0 && row < jj) ? base[(long long)row * pitch + i] : 0.0;
-        };
-        // Rolling windows.
-        double P0 = 0, P1 = ld(psil, j0 - 4), P2 = ld(psil, j0 - 3), P3 = ld(psil, j0 - 2), P4 = ld(psil, j0 - 1);
-        double Rm2 = 0, Rm1 = 0;           // rel rows s-2, s-1
-        double ZFm2 = 0;                   // zeta after forcing, row s-2
-        double ZOm2 = 0;                   // zeta_old row s-2
-        double UJm2 = 0, UJm1 = 0;         // uj faces s-2, s-1
-        double FJm2 = 0, FJm1 = 0;         // zeta_fj (old) faces s-2, s-1
-        double FLJm2 = 0;                  // flux_j face s-2
-        double FLI = 0;                    // flux_i row s-2 (face a = i)
-        double zpb_prev = 0, pm_prev = 0, pp_prev = 0, pe_prev = 0;
-
-        for (int r = j0; r < j0 + CAB_SH + 4; ++r) {
-            const int s = r - 2;
-            // ---- loads -------------------------------------------------------
-            P0 = P1;
-            P1 = P2;
-            P2 = P3;
-            P3 = P4;
-            P4 = ld(psil, s + 2);
-            const bool node_s = in_i && s >= 0 && s < jj;
-            const bool int_s = node_s && i > 0 && i < ii - 1 && s > 0 && s < jj - 1;
-            const double zpb_s = int_s ? zeta_pb[(long long)s * pitch + i] : 0.0;
-            const double pm_s = (L > 1) ? ld(psim, s) : 0.0;
-            const double pp_s = (L > 1) ? ld(psip, s) : 0.0;
-            const double zo_1 = ld(zeta_old, s - 1);
-            const double uimo_1 = ld(uimo, s - 1);
-            const double ujmo_s = ld(ujmo, s);
-            const double fio_1 = ld(zfi_old, s - 1);
-            const double fj_s = ld(zfj_old, s);
-            const double w_1 = wind ? ld(wind, s - 1) : 0.0;
-
-            // ---- rel(s): rel_from_zeta_and_psi + apply_rel_bc ---------------
-            const double up1 = shup(P2, 1), up2 = shup(P2, 2), dn1 = shdn(P2, 1), dn2 = shdn(P2, 2);
-            double rel_s = 0.0;
-            if (node_s) {
-                const bool bj = (s == 0 || s == jj - 1), bi = (i == 0 || i == ii - 1);
-                if (bj || bi) {
-                    if (bc != 3) {
-                        double q1, q2;
-                        if (bj) {
-                            q1 = (s == 0) ? P3 : P1;
-                            q2 = (s == 0) ? P4 : P0;
-                        } else {
-                            q1 = (i == 0) ? dn1 : up1;
-                            q2 = (i == 0) ? dn2 : up2;
-                        }
-                        rel_s = (bc == 1) ? cffbc * (-3.5 * P2 + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - P2);
-                    }
-                } else if (L == 1) {
-                    rel_s = zpb_s;
-                } else if (l == 0) {
-                    rel_s = zpb_s + s2 * (P2 - pp_s);
-                } else if (l == L - 1) {
-                    rel_s = zpb_s + s1 * (P2 - pm_s);
-                } else {
-                    rel_s = zpb_s + s1 * (P2 - pm_s) + s2 * (P2 - pp_s);
-                }
-            }
-
-            // ---- zeta at row s-1 after update_zeta_bc and cabaret_forcing ---
-            const int s1r = s - 1;
-            const double rl_up = shup(Rm1, 1), rl_dn = shdn(Rm1, 1);
-            double zf_1 = 0.0;
-            const bool node_1 = in_i && s1r >= 0 && s1r < jj;
-            if (node_1) {
-                const bool bnd = (s1r == 0 || s1r == jj - 1 || i == 0 || i == ii - 1);
-                if (bnd) {
-                    // update_zeta_bc: rel - coupling(psi)
-                    if (L == 1)
-                        zf_1 = Rm1;
-                    else if (l == 0)
-                        zf_1 = Rm1 - s2 * (P1 - pp_prev);
-                    else if (l == L - 1)
-                        zf_1 = Rm1 - s1 * (P1 - pm_prev);
-                    else
-                        zf_1 = Rm1 - s1 * (P1 - pm_prev) - s2 * (P1 - pp_prev);
-                } else {
-                    const double lap = -4.0 * Rm1 + rl_up + rl_dn + Rm2 + rel_s;
-                    double rv;
-                    if (L == 1)
-                        rv = dt * (w_1 - vb * Rm1 + nu * lap);
-                    else if (l == 0)
-                        rv = dt * (w_1 + nu * lap);
-                    else if (l == L - 1)
-                        rv = dt * (-vb * Rm1 + nu * lap);
-                    else
-                        rv = dt * nu * lap;
-                    zf_1 = zpb_prev + rv;
-                }
-            }
-
-            // ---- corner psi and face velocities ------------------------------
-            // pe_here: corner between nodes (i-1, i) x (s-1, s).
-            const double pe_here = 0.25 * (P2 + P1 + up1 + shup(P1, 1));
-            const double pe_dn = shdn(pe_here, 1);
-            // uj on face b = s (between rows s-1 and s), column i.
-            double uj_s = 0.0, ujm_s = 0.0;
-            const bool fj_ok = (s >= 1 && s <= jj - 1 && i >= 1 && i <= ii - 2);
-            if (fj_ok) {
-                ujm_s = pe_dn - pe_here;
-                uj_s = (1.0 + tu) * ujm_s - tu * ujmo_s;
-            }
-            // ui on row s-1, face a = i (between columns i-1 and i).
-            double ui_1 = 0.0, uim_1 = 0.0;
-            const bool fi_ok = (i >= 1 && i <= ii - 1 && s1r >= 1 && s1r <= jj - 2);
-            if (fi_ok) {
-                uim_1 = -pe_here + pe_prev;
-                ui_1 = (1.0 + tu) * uim_1 - tu * uimo_1;
-            }
-
-            // ---- extrapolator, j-faces: face b = s-1 ------------------------
-            double fjn = 0.0;
-            const int bf = s - 1;
-            const bool bfj_ok = (bf >= 1 && bf <= jj - 1 && i >= 1 && i <= ii - 2);
-            if (bfj_ok) {
-                const double u1 = UJm1, fi1 = FJm1;
-                double fi2, psi_n, psi_o, d_f;
-                if (u1 >= 0.0) {
-                    if (bf > 1) {
-                        const double u2 = UJm2;
-                        fi2 = FJm2;
-                        const double v0 = (u1 + u2) / 2.0;
-                        psi_n = ZFm2;
-                        psi_o = ZOm2;
-                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2);
-                    } else {
-                        fi2 = ZFm2;
-                        psi_n = ZFm2;
-                        psi_o = ZOm2;
-                        d_f = -(psi_n - psi_o);
-                    }
-                } else {
-                    if (bf < jj - 1) {
-                        const double u2 = uj_s;
-                        fi2 = fj_s;
-                        const double v0 = (u1 + u2) / 2.0;
-                        psi_n = zf_1;
-                        psi_o = zo_1;
-                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
-                    } else {
-                        fi2 = zf_1;
-                        psi_n = zf_1;
-                        psi_o = zo_1;
-                        d_f = -(psi_n - psi_o);
-                    }
-                }
-                double v = 2.0 * psi_n - fi2;
-                if (lim) {
-                    const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
-                    const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
-                    if (v > fmx) v = fmx;
-                    if (v < fmn) v = fmn;
-                }
-                fjn = v;
-            }
-
-            // ---- extrapolator, i-faces on row s-1: face a = i ----------------
-            const double ui_up = shup(ui_1, 1), ui_dn = shdn(ui_1, 1);
-            const double fi_up = shup(fio_1, 1), fi_dn = shdn(fio_1, 1);
-            const double zf_up = shup(zf_1, 1), zo_up = shup(zo_1, 1);
-            double fin = 0.0;
-            if (fi_ok) {
-                const double u1 = ui_1, fi1 = fio_1;
-                double fi2, psi_n, psi_o, d_f;
-                if (u1 >= 0.0) {
-                    if (i > 1) {
-                        const double u2 = ui_up;
-                        fi2 = fi_up;
-                        const double v0 = (u1 + u2) / 2.0;
-                        psi_n = zf_up;
-                        psi_o = zo_up;
-                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2);
-                    } else {
-                        fi2 = zf_up;
-                        psi_n = zf_up;
-                        psi_o = zo_up;
-                        d_f = -(psi_n - psi_o);
-                    }
-                } else {
-                    if (i < ii - 1) {
-                        const double u2 = ui_dn;
-                        fi2 = fi_dn;
-                        const double v0 = (u1 + u2) / 2.0;
-                        psi_n = zf_1;
-                        psi_o = zo_1;
-                        d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
-                    } else {
-                        fi2 = zf_1;
-                        psi_n = zf_1;
-                        psi_o = zo_1;
-                        d_f = -(psi_n - psi_o);
-                    }
-                }
-                double v = 2.0 * psi_n - fi2;
-                if (lim) {
-                    const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
-                    const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
-                    if (v > fmx) v = fmx;
-                    if (v < fmn) v = fmn;
-                }
-                fin = v;
-            }
-            const double flj_1 = UJm1 * fjn;  // flux_j on face s-1
-            const double fli_1 = ui_1 * fin;  // flux_i on row s-1, face i
-
-            // ---- corrector at row o = s-2 -------------------------------------
-            const int o = s - 2;
-            const double fli_dn = shdn(FLI, 1);
-            const bool band_o = (o >= j0 && o < j0 + CAB_SH && o >= 0 && o < jj);
-            if (out_i && band_o) {
-                const bool bnd = (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
-                double z = ZFm2;
-                const long long off = (long long)o * pitch + i;
-                if (!bnd) {
-                    const double rr = -(fli_dn - FLI + flj_1 - FLJm2);
-                    res[off] = rr;
-                    z = z + hdt * rr;
-                }
-                zeta_new[off] = z;
-            }
-            // ---- owned face writes ---------------------------------------------
-            if (out_i) {
-                if (fi_ok && s1r >= j0 && s1r < j0 + CAB_SH) {
-                    const long long off = (long long)s1r * pitch + i;
-                    ui_new[off] = ui_1;
-                    uimo_new[off] = uim_1;
-                    zfi_new[off] = fin;
-                    umax = fmax(umax, fabs(ui_1));
-                }
-                if (fj_ok && s >= j0 && s < j0 + CAB_SH) {
-                    const long long off = (long long)s * pitch + i;
-                    uj_new[off] = uj_s;
-                    ujmo_new[off] = ujm_s;
-                    umax = fmax(umax, fabs(uj_s));
-                }
-                if (bfj_ok && bf >= j0 && bf < j0 + CAB_SH) zfj_new[(long long)bf * pitch + i] = fjn;
-            }
-            // ---- shift the windows -------------------------------------------
-            Rm2 = Rm1;
-            Rm1 = rel_s;
-            ZFm2 = zf_1;
-            ZOm2 = zo_1;
-            UJm2 = UJm1;
-            UJm1 = uj_s;
-            FJm2 = FJm1;
-            FJm1 = fj_s;
-            FLJm2 = flj_1;
-            FLI = fli_1;
-            zpb_prev = zpb_s;
-            pm_prev = pm_s;
-            pp_prev = pp_s;
-            pe_prev = pe_here;
-        }
+        const bool interior = (i0 - 2 >= 2) && (i0 + 29 <= ii - 3) && (j0 - 4 >= 2) && (j0 + CAB_SH + 3 <= jj - 3);
+        double* ring = cab_ring + warp * CAB_RING;
+        umax = interior ? cab_sweep<false>(Mb, l, i0, j0, lane, ring) : cab_sweep<true>(Mb, l, i0, j0, lane, ring);
     }
 
     // Max |u| of the new face velocities (cabaret_cfl / cabaret_adapt_dt);
@@ -438,7 +465,10 @@ int cabaret_ctas(int ii, int jj, int L) {
 }
 
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, cudaStream_t st) {
-    k_cabaret_fused<<<ls.ctas_cab, CAB_WARPS * 32, 0, st>>>(ls.members, ls.prefix_cab, ls.nmem);
+    const size_t bytes = (size_t)CAB_WARPS * CAB_RING * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k_cabaret_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    k_cabaret_fused<<<ls.ctas_cab, CAB_WARPS * 32, bytes, st>>>(ls.members, ls.prefix_cab, ls.nmem);
     return cudaGetLastError();
 }
 

@@ -363,13 +363,22 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     double* spec = reinterpret_cast<double*>(Mb.spec) + (long long)m * Mb.lstride;
 
     // Stage: thread -> (column c = tid & 7, chunk q = tid >> 3); loop over t.
+    // Asynchronous 8-byte copies (cp.async), so the loads of a thread do not
+    // wait for one another; columns past n are zero-filled (source size 0).
     {
         const int c = threadIdx.x & 7, q = threadIdx.x >> 3;
         const bool colok = (k0 + c < n);
-        const double* g = spec + (long long)(q * R + 1) * pitch + k0 + c;
+        const double* g = spec + (long long)(q * R + 1) * pitch + (colok ? k0 + c : 0);
         double* sdst = strip + c * CS + q * RS;
         const int Rq = min(R, Mr - q * R);
-        for (int t = 0; t < Rq; ++t) sdst[t] = colok ? g[(long long)t * pitch] : 0.0;
+        const unsigned sbase = (unsigned)__cvta_generic_to_shared(sdst);
+        const int nbytes = colok ? 8 : 0;
+        for (int t = 0; t < Rq; ++t)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sbase + 8u * t),
+                         "l"(g + (long long)t * pitch), "r"(nbytes)
+                         : "memory");
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
 
