@@ -250,6 +250,19 @@ PQ_API int pq_kernel_times(pq_ctx* ctx, double* ms4, long* launches4);
 PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int ld, const double* h,
                              const double* s2, double* out, void* stream);
 
+/* Tile parameters of the step kernels (chosen per grid size by the
+ * autotuner, pequod_b200/autotune.py; defaults are set by pq_create).
+ *   cab_band   output rows per warp of the fused CABARET sweep, 4..128
+ *   dst_group  vertical modes transformed together by one DST CTA
+ *              (0: automatic, by shared-memory footprint) */
+typedef struct pq_tuning {
+    int cab_band;
+    int dst_group;
+    int reserved[6];
+} pq_tuning;
+PQ_API int pq_set_tuning(pq_ctx* ctx, const pq_tuning* t);
+PQ_API int pq_get_tuning(pq_ctx* ctx, pq_tuning* t);
+
 /* Number of kernel launches the last pq_step enqueued. */
 PQ_API long pq_last_launch_count(const pq_ctx* ctx);
 

@@ -57,6 +57,10 @@ class ModelDesc(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("cab_band", C.c_int), ("dst_group", C.c_int), ("reserved", C.c_int * 6)]
+
+
 class Physical(C.Structure):
     _fields_ = [
         ("ii", C.c_int), ("jj", C.c_int), ("layers", C.c_int),
@@ -95,6 +99,8 @@ SIGNATURES = {
     "pq_stream": (C.c_void_p, [C.c_void_p]),
     "pq_last_launch_count": (C.c_long, [C.c_void_p]),
     "pq_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "pq_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    "pq_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "pq_kernel_times": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_long)]),
     "pq_energy_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_void_p,
                                     C.c_void_p]),
@@ -332,6 +338,18 @@ class Model:
 
     def last_launch_count(self) -> int:
         return int(lib().pq_last_launch_count(self.ctx))
+
+    def set_tuning(self, **kw) -> None:
+        t = Tuning()
+        _check(lib().pq_get_tuning(self.ctx, C.byref(t)), self.ctx)
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        _check(lib().pq_set_tuning(self.ctx, C.byref(t)), self.ctx)
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        _check(lib().pq_get_tuning(self.ctx, C.byref(t)), self.ctx)
+        return {"cab_band": t.cab_band, "dst_group": t.dst_group}
 
     def kernel_timing(self, enable: bool) -> None:
         _check(lib().pq_kernel_timing(self.ctx, int(enable)), self.ctx)

@@ -22,6 +22,9 @@ enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+constexpr int kMinBand = 4;   // smallest CABARET band height a tuning may select
+constexpr int kMaxBand = 128;
+
 bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
 
 }  // namespace
@@ -217,6 +220,8 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     }
     *out = c;
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int sm_count = 0;
+    CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
     if (d->force_wind) c->wind.assign(d->force_wind, d->force_wind + (size_t)ii * jj);
     c->desc.force_wind = nullptr;
 
@@ -227,7 +232,9 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     const size_t lstride = (size_t)c->pitch * jj;
     c->field_bytes = lstride * L * sizeof(double);
     const int ntiles_tri = L * ((n + 7) / 8);
-    const int ntiles_cab = cabaret_ctas(ii, jj, L);
+    const int cab_sh = 16;
+    const int ntiles_cab = cabaret_ctas(ii, jj, L, cab_sh);
+    const int ntiles_cab_max = cabaret_ctas(ii, jj, L, kMinBand);
 
     // Tables.
     std::vector<double2> tw(M), wsplit(M);
@@ -269,7 +276,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     const size_t o_pfix = take(pv.fix.size() * sizeof(double));
     const size_t npart = std::max((size_t)ntiles_tri, (size_t)jj * (PQ_MAXL + 1));
     const size_t o_part = take(npart * sizeof(double));
-    const size_t o_maxu = take(ntiles_cab * sizeof(double));
+    const size_t o_maxu = take(ntiles_cab_max * sizeof(double));
     const size_t o_cnt = take(4 * sizeof(unsigned));
     const size_t o_sc = take(sizeof(Scalars));
     const size_t o_st = take(sizeof(int));
@@ -358,6 +365,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     m.status = reinterpret_cast<int*>(A + o_st);
     m.ntiles_tri = ntiles_tri;
     m.ntiles_cab = ntiles_cab;
+    m.cab_sh = cab_sh;
     m.adapt_dt = d->adapt_dt;
     m.target_cfl = d->target_cfl;
     m.max_dt = d->max_dt;
@@ -388,6 +396,8 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
         s.ctas_rows_all = jj;
         s.ctas_tri = ntiles_tri;
         s.ctas_cab = ntiles_cab;
+        s.dst_group = 0;
+        s.sm_count = sm_count;
     }
     // Scalars: dt and the initial time weights.
     Scalars sc;
@@ -570,6 +580,35 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         launches += 4;
     }
     c->last_launches = launches;
+    return PQ_OK;
+}
+
+int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
+    if (!c || !t) return PQ_ERR_ARG;
+    if (t->cab_band < kMinBand || t->cab_band > kMaxBand) return fail(c, PQ_ERR_ARG, "cab_band out of range");
+    CK(cudaStreamSynchronize(c->stream));
+    if (t->dst_group < 0 || t->dst_group > c->L) return fail(c, PQ_ERR_ARG, "dst_group out of range");
+    for (int p = 0; p < 2; ++p) {
+        c->hm[p].cab_sh = t->cab_band;
+        c->hm[p].ntiles_cab = cabaret_ctas(c->ii, c->jj, c->L, t->cab_band);
+        c->ls[p].ctas_cab = c->hm[p].ntiles_cab;
+        c->ls[p].dst_group = t->dst_group;
+    }
+    int rc = upload_members(c);
+    if (rc) return rc;
+    if (c->graph2) {
+        cudaGraphExecDestroy(c->graph2);
+        c->graph2 = nullptr;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return PQ_OK;
+}
+
+int pq_get_tuning(pq_ctx* c, pq_tuning* t) {
+    if (!c || !t) return PQ_ERR_ARG;
+    std::memset(t, 0, sizeof(*t));
+    t->cab_band = c->hm[0].cab_sh;
+    t->dst_group = c->ls[0].dst_group;
     return PQ_OK;
 }
 

@@ -66,7 +66,7 @@ __device__ __forceinline__ double zeta_bc_node(const Member& Mb, PS ps, double r
 
 // Sweep decomposition: a warp owns one layer of a strip of 32 columns
 // (CAB_SW = 28 output columns plus 2 halo lanes on each side) and marches down
-// a band of CAB_SH output rows.  Every per-lane quantity lives in registers as
+// a band of Mb.cab_sh output rows (a tuning parameter).  Every per-lane quantity lives in registers as
 // a rolling window over rows; the i-neighbours come from warp shuffles.  At
 // iteration r (s = r - 2) the warp loads psi row s+2 and the inputs of rows
 // s, s-1, and produces
@@ -75,7 +75,6 @@ __device__ __forceinline__ double zeta_bc_node(const Member& Mb, PS ps, double r
 // so output row o is final at iteration o + 4.
 constexpr int CAB_WARPS = 4;
 constexpr int CAB_SW = 28;  // output columns per warp
-constexpr int CAB_SH = 16;  // output rows per warp
 constexpr int CAB_D = 4;    // depth of the per-warp cp.async row pipeline
 // Streamed inputs of one iteration (rows relative to s = r - 2).
 enum { F_PSI2 = 0, F_ZPB, F_PSIM, F_PSIP, F_ZO, F_UIMO, F_UJMO, F_FIO, F_FJ, F_WIND, CAB_NF };
@@ -86,7 +85,7 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 
 // One warp's sweep over layer l of the strip starting at column i0 and the
 // band starting at row j0.  EDGE = false is the specialisation for warps
-// whose whole footprint (columns i0-2 .. i0+29, rows j0-4 .. j0+CAB_SH+3) lies
+// whose whole footprint (columns i0-2 .. i0+29, rows j0-4 .. j0+sh+3) lies
 // at least two nodes inside the domain: no bounds checks, no boundary
 // branches.  Returns the largest |u| of the faces it wrote.
 template <bool EDGE>
@@ -99,25 +98,32 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const int cur = Mb.cur, nxt = cur ^ 1;
     const double dt = Mb.sc->dt, tu = Mb.sc->tweight_u;
     const double hdt = 0.5 * dt;
-    const long long lo = l * ls + i;  // every field pointer below is offset to column i
-    const double* psil = Mb.psi + lo;
-    const double* psim = (l > 0) ? psil - ls : psil;
-    const double* psip = (l < L - 1) ? psil + ls : psil;
-    const double* zeta_pb = reinterpret_cast<const double*>(Mb.zeta) + lo;
-    const double* zeta_old = reinterpret_cast<const double*>(Mb.zeta_old[cur]) + lo;
-    double* zeta_new = reinterpret_cast<double*>(Mb.zeta_old[nxt]) + lo;
-    double* res = reinterpret_cast<double*>(Mb.res) + lo;
-    double* ui_new = reinterpret_cast<double*>(Mb.ui) + lo;
-    double* uj_new = reinterpret_cast<double*>(Mb.uj) + lo;
-    const double* uimo = reinterpret_cast<const double*>(Mb.uimo[cur]) + lo;
-    double* uimo_new = reinterpret_cast<double*>(Mb.uimo[nxt]) + lo;
-    const double* ujmo = reinterpret_cast<const double*>(Mb.ujmo[cur]) + lo;
-    double* ujmo_new = reinterpret_cast<double*>(Mb.ujmo[nxt]) + lo;
-    const double* zfi_old = reinterpret_cast<const double*>(Mb.zfi[cur]) + lo;
-    double* zfi_new = reinterpret_cast<double*>(Mb.zfi[nxt]) + lo;
-    const double* zfj_old = reinterpret_cast<const double*>(Mb.zfj[cur]) + lo;
-    double* zfj_new = reinterpret_cast<double*>(Mb.zfj[nxt]) + lo;
-    const double* wind = (l == 0 && Mb.wind) ? Mb.wind + i : nullptr;
+    const int SH = Mb.cab_sh;
+    // All fields of a member live in one allocation: address them by 32-bit
+    // element offsets from one base (fewer live registers than 16 pointers).
+    const double* B = Mb.psi;
+    auto ofs = [&](const void* f) { return (int)(reinterpret_cast<const double*>(f) - B); };
+    const int lo = (int)(l * ls) + i;  // layer and column part of every offset
+    const int o_psil = lo;
+    const int o_psim = (l > 0) ? lo - (int)ls : lo;
+    const int o_psip = (l < L - 1) ? lo + (int)ls : lo;
+    const int o_zpb = ofs(Mb.zeta) + lo;
+    const int o_zo = ofs(Mb.zeta_old[cur]) + lo;
+    const int o_zn = ofs(Mb.zeta_old[nxt]) + lo;
+    const int o_res = ofs(Mb.res) + lo;
+    const int o_ui = ofs(Mb.ui) + lo;
+    const int o_uj = ofs(Mb.uj) + lo;
+    const int o_uimo = ofs(Mb.uimo[cur]) + lo;
+    const int o_uimon = ofs(Mb.uimo[nxt]) + lo;
+    const int o_ujmo = ofs(Mb.ujmo[cur]) + lo;
+    const int o_ujmon = ofs(Mb.ujmo[nxt]) + lo;
+    const int o_fio = ofs(Mb.zfi[cur]) + lo;
+    const int o_fin = ofs(Mb.zfi[nxt]) + lo;
+    const int o_fjo = ofs(Mb.zfj[cur]) + lo;
+    const int o_fjn = ofs(Mb.zfj[nxt]) + lo;
+    const bool has_wind = (l == 0 && Mb.wind);
+    const int o_wind = has_wind ? ofs(Mb.wind) + i : 0;
+    double* W = const_cast<double*>(B);
     const double nu = Mb.viscosity, vb = Mb.visc_bot;
     const double s1 = Mb.s1[l], s2 = Mb.s2[l];
     const int bc = Mb.bc_type;
@@ -126,9 +132,9 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const bool top = (l == 0), bottom = (l == L - 1);
     double umax = 0.0;
 
-    auto ld = [&](const double* base, int row) -> double {
-        if (EDGE) return (in_i && row >= 0 && row < jj) ? base[row * pitch] : 0.0;
-        return base[row * pitch];
+    auto ld = [&](int off, int row) -> double {
+        if (EDGE) return (in_i && row >= 0 && row < jj) ? B[off + row * pitch] : 0.0;
+        return B[off + row * pitch];
     };
     // rel_from_zeta_and_psi coupling for an interior node.
     auto rel_int = [&](double z, double p, double pm, double pp) -> double {
@@ -169,11 +175,11 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     // Row copies of iteration r into ring stage r % CAB_D (cp.async, 8 bytes
     // per lane; rows outside the domain, and zeta at non-interior nodes, are
     // zero-filled by a source size of 0 with the source clamped in range).
-    const int rend = j0 + CAB_SH + 4;
-    auto cp = [&](double* dst, const double* base, int row, bool ok) {
+    const int rend = j0 + SH + 4;
+    auto cp = [&](double* dst, int off, int row, bool ok) {
         const int rr = ok ? row : 0;
         const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(base + (long long)rr * pitch),
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(B + (off + rr * pitch)),
                      "r"(ok ? 8 : 0)
                      : "memory");
     };
@@ -181,25 +187,25 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     auto issue = [&](int rr) {
         const int ss = rr - 2;
         double* d = ring + ((rr % CAB_D) * CAB_NF << 5) + lane;
-        cp(d + (F_PSI2 << 5), psil, ss + 2, rowok(ss + 2));
+        cp(d + (F_PSI2 << 5), o_psil, ss + 2, rowok(ss + 2));
         const bool intn = !EDGE || (in_i && i > 0 && i < ii - 1 && ss > 0 && ss < jj - 1);
-        cp(d + (F_ZPB << 5), zeta_pb, ss, intn);
+        cp(d + (F_ZPB << 5), o_zpb, ss, intn);
         if (L > 1) {
-            cp(d + (F_PSIM << 5), psim, ss, rowok(ss));
-            cp(d + (F_PSIP << 5), psip, ss, rowok(ss));
+            cp(d + (F_PSIM << 5), o_psim, ss, rowok(ss));
+            cp(d + (F_PSIP << 5), o_psip, ss, rowok(ss));
         }
-        cp(d + (F_ZO << 5), zeta_old, ss - 1, rowok(ss - 1));
-        cp(d + (F_UIMO << 5), uimo, ss - 1, rowok(ss - 1));
-        cp(d + (F_UJMO << 5), ujmo, ss, rowok(ss));
-        cp(d + (F_FIO << 5), zfi_old, ss - 1, rowok(ss - 1));
-        cp(d + (F_FJ << 5), zfj_old, ss, rowok(ss));
-        if (wind) cp(d + (F_WIND << 5), wind, ss - 1, rowok(ss - 1));
+        cp(d + (F_ZO << 5), o_zo, ss - 1, rowok(ss - 1));
+        cp(d + (F_UIMO << 5), o_uimo, ss - 1, rowok(ss - 1));
+        cp(d + (F_UJMO << 5), o_ujmo, ss, rowok(ss));
+        cp(d + (F_FIO << 5), o_fio, ss - 1, rowok(ss - 1));
+        cp(d + (F_FJ << 5), o_fjo, ss, rowok(ss));
+        if (has_wind) cp(d + (F_WIND << 5), o_wind, ss - 1, rowok(ss - 1));
     };
     for (int rr = j0; rr < j0 + CAB_D - 1; ++rr) {
         issue(rr);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    double P0 = 0, P1 = ld(psil, j0 - 4), P2 = ld(psil, j0 - 3), P3 = ld(psil, j0 - 2), P4 = ld(psil, j0 - 1);
+    double P0 = 0, P1 = ld(o_psil, j0 - 4), P2 = ld(o_psil, j0 - 3), P3 = ld(o_psil, j0 - 2), P4 = ld(o_psil, j0 - 1);
     double Rm2 = 0, Rm1 = 0;    // rel rows s-2, s-1
     double ZFm2 = 0;            // zeta after forcing, row s-2
     double ZOm2 = 0;            // zeta_old row s-2
@@ -210,7 +216,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     double zpb_prev = 0, pm_prev = 0, pp_prev = 0, pe_prev = 0;
 
 #pragma unroll 1
-    for (int r = j0; r < j0 + CAB_SH + 4; ++r) {
+    for (int r = j0; r < rend; ++r) {
         const int s = r - 2;
         // ---- loads -----------------------------------------------------------
         // Keep CAB_D - 1 iterations of row copies in flight.
@@ -232,7 +238,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         const double ujmo_s = st[F_UJMO << 5];
         const double fio_1 = st[F_FIO << 5];
         const double fj_s = st[F_FJ << 5];
-        const double w_1 = wind ? st[F_WIND << 5] : 0.0;
+        const double w_1 = has_wind ? st[F_WIND << 5] : 0.0;
 
         // ---- rel(s): rel_from_zeta_and_psi + apply_rel_bc -------------------
         double up1 = 0.0, up2 = 0.0, dn1 = 0.0, dn2 = 0.0;
@@ -347,31 +353,31 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         // ---- corrector at row o = s-2 -----------------------------------------
         const int o = s - 2;
         const double fli_dn = shdn(FLI, 1);
-        const bool band_o = (o >= j0 && o < j0 + CAB_SH) && (!EDGE || (o >= 0 && o < jj));
+        const bool band_o = (o >= j0 && o < j0 + SH) && (!EDGE || (o >= 0 && o < jj));
         if (out_i && band_o) {
             const bool bnd = EDGE && (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
             double z = ZFm2;
             if (!bnd) {
                 const double rr = -(fli_dn - FLI + flj_1 - FLJm2);
-                res[o * pitch] = rr;
+                W[o_res + o * pitch] = rr;
                 z = z + hdt * rr;
             }
-            zeta_new[o * pitch] = z;
+            W[o_zn + o * pitch] = z;
         }
         // ---- owned face writes ---------------------------------------------------
         if (out_i) {
-            if (fi_ok && s1r >= j0 && s1r < j0 + CAB_SH) {
-                ui_new[s1r * pitch] = ui_1;
-                uimo_new[s1r * pitch] = uim_1;
-                zfi_new[s1r * pitch] = fin;
+            if (fi_ok && s1r >= j0 && s1r < j0 + SH) {
+                W[o_ui + s1r * pitch] = ui_1;
+                W[o_uimon + s1r * pitch] = uim_1;
+                W[o_fin + s1r * pitch] = fin;
                 umax = fmax(umax, fabs(ui_1));
             }
-            if (fj_ok && s >= j0 && s < j0 + CAB_SH) {
-                uj_new[s * pitch] = uj_s;
-                ujmo_new[s * pitch] = ujm_s;
+            if (fj_ok && s >= j0 && s < j0 + SH) {
+                W[o_uj + s * pitch] = uj_s;
+                W[o_ujmon + s * pitch] = ujm_s;
                 umax = fmax(umax, fabs(uj_s));
             }
-            if (bfj_ok && bf >= j0 && bf < j0 + CAB_SH) zfj_new[bf * pitch] = fjn;
+            if (bfj_ok && bf >= j0 && bf < j0 + SH) W[o_fjn + bf * pitch] = fjn;
         }
         // ---- shift the windows ---------------------------------------------------
         Rm2 = Rm1;
@@ -403,7 +409,8 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
     load_member_c(Mb, mems + mi);
     __syncthreads();
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
-    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + CAB_SH - 1) / CAB_SH;
+    const int SH = Mb.cab_sh;
+    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + SH - 1) / SH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int task = local * CAB_WARPS + warp;
     double umax = 0.0;
@@ -411,8 +418,8 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
         const int l = task % L;
         const int sb = task / L;
         const int strip = sb % nstrips, band = sb / nstrips;
-        const int i0 = strip * CAB_SW, j0 = band * CAB_SH;
-        const bool interior = (i0 - 2 >= 2) && (i0 + 29 <= ii - 3) && (j0 - 4 >= 2) && (j0 + CAB_SH + 3 <= jj - 3);
+        const int i0 = strip * CAB_SW, j0 = band * SH;
+        const bool interior = (i0 - 2 >= 2) && (i0 + 29 <= ii - 3) && (j0 - 4 >= 2) && (j0 + SH + 3 <= jj - 3);
         double* ring = cab_ring + warp * CAB_RING;
         umax = interior ? cab_sweep<false>(Mb, l, i0, j0, lane, ring) : cab_sweep<true>(Mb, l, i0, j0, lane, ring);
     }
@@ -459,8 +466,8 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
     }
 }
 
-int cabaret_ctas(int ii, int jj, int L) {
-    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + CAB_SH - 1) / CAB_SH;
+int cabaret_ctas(int ii, int jj, int L, int sh) {
+    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + sh - 1) / sh;
     return (nstrips * nbands * L + CAB_WARPS - 1) / CAB_WARPS;
 }
 

@@ -107,6 +107,7 @@ struct Member {
     int* status;
     int ntiles_tri;       // L * ceil(n / 8)
     int ntiles_cab;
+    int cab_sh;           // output rows per warp of the fused CABARET sweep
     int cur;              // ping-pong parity for ui / zfi / zfj (host-managed)
     int adapt_dt;
     double target_cfl, max_dt, max_dt_increase;

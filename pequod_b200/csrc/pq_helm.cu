@@ -46,50 +46,83 @@ __device__ __forceinline__ void load_member(Member& dst, const Member* src) {
     for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
 }
 
-// Block-wide inclusive scan of v over the CTA (blockDim.x a multiple of 32,
-// at most 1024).  wsum: shared scratch of 32 doubles.
-__device__ __forceinline__ double block_inclusive_scan(double v, double* wsum) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double s = warp_inclusive_scan(v);
-    if (lane == 31) wsum[warp] = s;
-    __syncthreads();
-    if (warp == 0) {
-        double t = lane < nw ? wsum[lane] : 0.0;
-        t = warp_inclusive_scan(t);
-        if (lane < nw) wsum[lane] = t;
-    }
-    __syncthreads();
-    double off = warp > 0 ? wsum[warp - 1] : 0.0;
-    __syncthreads();
-    return s + off;
-}
+// Complex scratch rows are padded by one entry per 8 (index t -> t + t/8) so
+// that the strided writes of the early Stockham stages hit distinct banks.
+__device__ __forceinline__ int cpad(int t) { return t + (t >> 3); }
+__host__ __device__ inline int crow(int M) { return M + (M >> 3); }  // padded row length
 
-// Radix-4/2 Stockham FFT of G complex rows of length M = 2^logM in shared
-// memory, forward sign.  Rows g at a + g*M.  Returns the buffer that holds
-// the result (a or b).  All index arithmetic is shifts and masks.
-__device__ double2* fft_stockham(double2* a, double2* b, int G, int M, int logM, const double2* __restrict__ tw) {
+__device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }  // a * (-i)
+
+// Stockham FFT (radix 8, then 4, then 2) of G complex rows of length
+// M = 2^logM in shared memory, forward sign; row g at a + g*crow(M), padded
+// indexing.  Returns the buffer that holds the result (a or b).
+__device__ double2* fft_stockham(double2* a, double2* b, int G, int M, int logM, const double2* tw) {
+    const int MP = crow(M);
     int Ns = 1, logNs = 0;
-    const int M4 = M >> 2, logM4 = logM - 2;
-    while (Ns * 4 <= M) {
-        const int lst = logM4 - logNs;  // log2(M / (4 Ns))
-        for (int w = threadIdx.x; w < G * M4; w += blockDim.x) {
-            const int g = w >> logM4, jj = w & (M4 - 1);
-            const double2* ag = a + (g << logM);
-            double2* bg = b + (g << logM);
-            double2 v0 = ag[jj], v1 = ag[jj + M4], v2 = ag[jj + 2 * M4], v3 = ag[jj + 3 * M4];
+    const double c8 = 0.70710678118654752440;  // sqrt(2)/2
+    while (Ns * 8 <= M) {
+        const int M8 = M >> 3, logM8 = logM - 3;
+        const int lst = logM8 - logNs;  // log2(M / (8 Ns))
+        for (int w = threadIdx.x; w < G * M8; w += blockDim.x) {
+            const int g = w >> logM8, jj = w & (M8 - 1);
+            const double2* ag = a + g * MP;
+            double2* bg = b + g * MP;
+            double2 v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = ag[cpad(jj + r * M8)];
             const int k = jj & (Ns - 1);
             if (k) {
-                v1 = cmul(v1, __ldg(&tw[k << lst]));
-                v2 = cmul(v2, __ldg(&tw[(2 * k) << lst]));
-                v3 = cmul(v3, __ldg(&tw[(3 * k) << lst]));
+#pragma unroll
+                for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], tw[(r * k) << lst]);
             }
-            double2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), d3 = csub(v1, v3);
-            double2 t3 = make_double2(d3.y, -d3.x);  // (v1 - v3) * (-i)
+            // 8-point DFT: two 4-point DFTs of the even and odd inputs.
+            const double2 e0 = cadd(v[0], v[4]), e1 = csub(v[0], v[4]), e2 = cadd(v[2], v[6]),
+                          e3 = mul_mi(csub(v[2], v[6]));
+            const double2 E0 = cadd(e0, e2), E1 = cadd(e1, e3), E2 = csub(e0, e2), E3 = csub(e1, e3);
+            const double2 o0 = cadd(v[1], v[5]), o1 = csub(v[1], v[5]), o2 = cadd(v[3], v[7]),
+                          o3 = mul_mi(csub(v[3], v[7]));
+            double2 O0 = cadd(o0, o2), O1 = cadd(o1, o3), O2 = csub(o0, o2), O3 = csub(o1, o3);
+            // W8^1 = (1 - i)/sqrt2, W8^2 = -i, W8^3 = (-1 - i)/sqrt2
+            O1 = make_double2(c8 * (O1.x + O1.y), c8 * (O1.y - O1.x));
+            O2 = mul_mi(O2);
+            O3 = make_double2(c8 * (O3.y - O3.x), -c8 * (O3.x + O3.y));
+            const int idx = ((jj >> logNs) << (logNs + 3)) + k;
+            bg[cpad(idx)] = cadd(E0, O0);
+            bg[cpad(idx + Ns)] = cadd(E1, O1);
+            bg[cpad(idx + 2 * Ns)] = cadd(E2, O2);
+            bg[cpad(idx + 3 * Ns)] = cadd(E3, O3);
+            bg[cpad(idx + 4 * Ns)] = csub(E0, O0);
+            bg[cpad(idx + 5 * Ns)] = csub(E1, O1);
+            bg[cpad(idx + 6 * Ns)] = csub(E2, O2);
+            bg[cpad(idx + 7 * Ns)] = csub(E3, O3);
+        }
+        __syncthreads();
+        double2* t = a;
+        a = b;
+        b = t;
+        Ns <<= 3;
+        logNs += 3;
+    }
+    if (Ns * 4 <= M) {
+        const int M4 = M >> 2, logM4 = logM - 2;
+        const int lst = logM4 - logNs;
+        for (int w = threadIdx.x; w < G * M4; w += blockDim.x) {
+            const int g = w >> logM4, jj = w & (M4 - 1);
+            const double2* ag = a + g * MP;
+            double2* bg = b + g * MP;
+            double2 v0 = ag[cpad(jj)], v1 = ag[cpad(jj + M4)], v2 = ag[cpad(jj + 2 * M4)], v3 = ag[cpad(jj + 3 * M4)];
+            const int k = jj & (Ns - 1);
+            if (k) {
+                v1 = cmul(v1, tw[k << lst]);
+                v2 = cmul(v2, tw[(2 * k) << lst]);
+                v3 = cmul(v3, tw[(3 * k) << lst]);
+            }
+            const double2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = mul_mi(csub(v1, v3));
             const int idx = ((jj >> logNs) << (logNs + 2)) + k;
-            bg[idx] = cadd(t0, t2);
-            bg[idx + Ns] = cadd(t1, t3);
-            bg[idx + 2 * Ns] = csub(t0, t2);
-            bg[idx + 3 * Ns] = csub(t1, t3);
+            bg[cpad(idx)] = cadd(t0, t2);
+            bg[cpad(idx + Ns)] = cadd(t1, t3);
+            bg[cpad(idx + 2 * Ns)] = csub(t0, t2);
+            bg[cpad(idx + 3 * Ns)] = csub(t1, t3);
         }
         __syncthreads();
         double2* t = a;
@@ -100,17 +133,17 @@ __device__ double2* fft_stockham(double2* a, double2* b, int G, int M, int logM,
     }
     if (Ns < M) {
         const int M2 = M >> 1, logM2 = logM - 1;
-        const int lst = logM2 - logNs;  // log2(M / (2 Ns))
+        const int lst = logM2 - logNs;
         for (int w = threadIdx.x; w < G * M2; w += blockDim.x) {
             const int g = w >> logM2, jj = w & (M2 - 1);
-            const double2* ag = a + (g << logM);
-            double2* bg = b + (g << logM);
-            double2 v0 = ag[jj], v1 = ag[jj + M2];
+            const double2* ag = a + g * MP;
+            double2* bg = b + g * MP;
+            double2 v0 = ag[cpad(jj)], v1 = ag[cpad(jj + M2)];
             const int k = jj & (Ns - 1);
-            if (k) v1 = cmul(v1, __ldg(&tw[k << lst]));
+            if (k) v1 = cmul(v1, tw[k << lst]);
             const int idx = ((jj >> logNs) << (logNs + 1)) + k;
-            bg[idx] = cadd(v0, v1);
-            bg[idx + Ns] = csub(v0, v1);
+            bg[cpad(idx)] = cadd(v0, v1);
+            bg[cpad(idx + Ns)] = csub(v0, v1);
         }
         __syncthreads();
         double2* t = a;
@@ -122,10 +155,11 @@ __device__ double2* fft_stockham(double2* a, double2* b, int G, int M, int logM,
 
 // In-place DST-I (FFTPACK sint convention) of G real rows held in shared
 // memory at xr + g*xs, entries 1..n (entries 0 and N are scratch).
-// za, zb: shared complex scratch of G*M each.  wsum: 32 doubles.
-__device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, double* wsum, const Member& Mb) {
-    const int N = Mb.N, M = Mb.M, N2 = N >> 1, logM = Mb.logM;
-    const double* __restrict__ was = Mb.was;
+// za, zb: shared complex scratch of G*crow(M) each.  tw, wsp, was: the
+// twiddle tables staged in shared memory.
+__device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, const Member& Mb, const double2* tw,
+                         const double2* wsp, const double* was) {
+    const int N = Mb.N, M = Mb.M, N2 = N >> 1, logM = Mb.logM, MP = crow(M);
     // Pre-twiddle (sint1, qg3p_helmholtz.F90:1404-1413) and pack.
     for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
         const int g = w >> logM, t = w & (M - 1);
@@ -141,46 +175,45 @@ __device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, do
                 v = 4.0 * x[N2];
             } else if (k < N2) {
                 const double xa = x[k], xb = x[N - k];
-                v = (xa - xb) + __ldg(&was[k]) * (xa + xb);
+                v = (xa - xb) + was[k] * (xa + xb);
             } else {
                 const int kk = N - k;
                 const double xa = x[kk], xb = x[k];
-                v = __ldg(&was[kk]) * (xa + xb) - (xa - xb);
+                v = was[kk] * (xa + xb) - (xa - xb);
             }
             c[e] = v;
         }
-        za[w] = make_double2(c[0], c[1]);
+        za[g * MP + cpad(t)] = make_double2(c[0], c[1]);
     }
     __syncthreads();
-    double2* Z = fft_stockham(za, zb, G, M, logM, Mb.tw);
+    double2* Z = fft_stockham(za, zb, G, M, logM, tw);
     double2* other = (Z == za) ? zb : za;
-    double* R = reinterpret_cast<double*>(other);  // G*M reals of scratch
     // Real-FFT split; even outputs directly, R_q to scratch for the scan.
     for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
         const int g = w >> logM, q = w & (M - 1);
-        const double2* Zg = Z + (g << logM);
-        const double2 zq = Zg[q];
-        const double2 zr = Zg[(M - q) & (M - 1)];
+        const double2* Zg = Z + g * MP;
+        const double2 zq = Zg[cpad(q)];
+        const double2 zr = Zg[cpad((M - q) & (M - 1))];
         const double2 zc = make_double2(zr.x, -zr.y);
         const double2 E = make_double2(0.5 * (zq.x + zc.x), 0.5 * (zq.y + zc.y));
         const double2 d = csub(zq, zc);
         const double2 O = make_double2(0.5 * d.y, -0.5 * d.x);
-        const double2 C = cadd(E, cmul(__ldg(&Mb.wsplit[q]), O));
-        R[w] = (q == 0) ? 0.5 * C.x : C.x;
+        const double2 C = cadd(E, cmul(wsp[q], O));
+        reinterpret_cast<double*>(other + g * MP)[q] = (q == 0) ? 0.5 * C.x : C.x;
         if (q >= 1) xr[g * xs + 2 * q] = -C.y;
     }
     __syncthreads();
-    // X_{2q+1} = inclusive prefix sum of R over q, one row at a time.
-    const int per = (M + blockDim.x - 1) / blockDim.x;
-    for (int g = 0; g < G; ++g) {
-        const double* Rg = R + g * M;
-        const int q0 = threadIdx.x * per;
+    // X_{2q+1} = inclusive prefix sum of R over q: one warp per row, each lane
+    // a contiguous run of M/32 values (or one value when M < 32).
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int per = M >= 32 ? (M >> 5) : 1;
+    for (int g = warp; g < G; g += nw) {
+        const double* Rg = reinterpret_cast<const double*>(other + g * MP);
+        const int q0 = lane * per;
         double loc = 0.0;
-        for (int e = 0; e < per; ++e) {
-            const int q = q0 + e;
-            if (q < M) loc += Rg[q];
-        }
-        const double incl = block_inclusive_scan(loc, wsum);
+        for (int e = 0; e < per; ++e)
+            if (q0 + e < M) loc += Rg[q0 + e];
+        const double incl = warp_inclusive_scan(loc);
         double run = incl - loc;
         double* x = xr + g * xs;
         for (int e = 0; e < per; ++e) {
@@ -194,47 +227,141 @@ __device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, do
     __syncthreads();
 }
 
-// Shared memory plan of k_dst_rows for G modes at a time.
-__host__ __device__ inline size_t dst_smem_bytes(int L, int G, int N, int M) {
-    size_t xr = (size_t)L * (N + 2) * sizeof(double);
-    size_t z = 2 * (size_t)G * M * sizeof(double2);
-    return xr + z + 32 * sizeof(double);
+// Persistent, software-pipelined row transforms.
+//
+// Each CTA walks the rows (tasks) blockIdx.x, blockIdx.x + gridDim.x, ...
+// With two staging buffers it issues the asynchronous copies (cp.async) of the
+// next row's inputs before transforming the current row, so the global-load
+// latency of a row overlaps the previous row's FFT.  A staging buffer holds
+// the L real rows (stride N + 2, entries 1..n) and, for the psi epilogue, the
+// L - 1 correction rows of the baroclinic modes (stride cs).
+
+__device__ __forceinline__ void cp8(double* dst, const double* src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+struct DstPlan {
+    int G, nbuf;
+    size_t buf_doubles;  // per staging buffer
+    size_t bytes;        // dynamic shared memory
+};
+
+// Shared-memory tables of the DST for transform length N: tw[M], wsplit[M]
+// (complex), was[N/2 + 1]; rounded up to an even count so that the complex
+// scratch behind it stays 16-byte aligned.
+__host__ __device__ inline size_t dst_tab_doubles(int N) { return ((size_t)2 * N + (N / 2 + 3)) & ~(size_t)1; }
+
+__host__ inline DstPlan dst_plan(int L, int N, int ii, int want_G, bool with_corr) {
+    DstPlan p;
+    const int M = N / 2;
+    (void)ii;
+    (void)with_corr;
+    p.buf_doubles = (size_t)L * (N + 2);
+    int G = want_G > 0 ? (want_G < L ? want_G : L) : L;
+    auto total = [&](int g, int nb) {
+        return nb * p.buf_doubles * sizeof(double) + dst_tab_doubles(N) * sizeof(double) +
+               2 * (size_t)g * crow(M) * sizeof(double2);
+    };
+    if (want_G <= 0)
+        while (G > 1 && total(G, 2) > 110 * 1024) --G;
+    p.G = G;
+    p.nbuf = total(G, 2) <= 200 * 1024 ? 2 : 1;
+    p.bytes = total(G, p.nbuf);
+    return p;
 }
 
 template <int PRO, int EPI>
 __global__ void __launch_bounds__(DST_THREADS) k_dst_rows(const Member* __restrict__ mems,
                                                             const int* __restrict__ prefix, int nmem, int G,
-                                                            int row_offset) {
+                                                            int nbuf, int row_offset, int total, size_t bufd) {
     __shared__ Member Mb;
     extern __shared__ __align__(16) double sm[];
-    int local;
-    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
-    load_member(Mb, mems + mi);
-    __syncthreads();
-    const int j = local + row_offset;  // FWD: interior rows (offset 1); INV: all rows (offset 0)
-    const int L = Mb.L, N = Mb.N, n = Mb.n, ii = Mb.ii, jj = Mb.jj, pitch = Mb.pitch;
-    const long long ls = Mb.lstride;
-    const int xs = N + 2;
-    double* xr = sm;                                    // [L][N+2]
-    double2* za = reinterpret_cast<double2*>(xr + (size_t)L * xs);
-    double2* zb = za + (size_t)G * Mb.M;
-    double* wsum = reinterpret_cast<double*>(zb + (size_t)G * Mb.M);
+    double* bufs[2] = {sm, sm + bufd};
+    double* tab = sm + nbuf * bufd;  // twiddle tables of the current member
+    double2* s_tw = reinterpret_cast<double2*>(tab);
+    double2* za = nullptr;  // set once the member's N is known
 
-    const bool interior_row = (j >= 1 && j <= jj - 2);
+    // Asynchronous copies of a task's inputs into a staging buffer.
+    auto issue = [&](int task, double* buf) {
+        int loc;
+        const int mi = find_member(prefix, nmem, task, &loc);
+        const Member* M = mems + mi;
+        const int j = loc + row_offset;
+        const int L = M->L, n = M->n, N = M->N, jj = M->jj, pitch = M->pitch;
+        const long long ls = M->lstride;
+        const int xs = N + 2;
+        if (EPI == EPI_SPEC) {
+            if (PRO == PRO_STEP) return;  // loaded synchronously (needs four fields)
+            const double* src = reinterpret_cast<const double*>(PRO == PRO_PLAIN ? M->helm_io : M->zeta);
+            for (int l = 0; l < L; ++l) {
+                const double* g = src + l * ls + (long long)j * pitch;
+                for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) cp8(buf + l * xs + k, g + k);
+            }
+        } else {
+            if (j >= 1 && j <= jj - 2) {
+                const double* spec = reinterpret_cast<const double*>(M->spec);
+                for (int m = 0; m < L; ++m) {
+                    const double* g = spec + m * ls + (long long)j * pitch - 1;
+                    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) cp8(buf + m * xs + k, g + k);
+                }
+            }
+        }
+    };
 
-    if (EPI == EPI_SPEC) {
-        // ---------------- forward: load + prologue -------------------------
-        const double cff = 0.5 / (double)(ii - 1);
-        const double dt = Mb.sc->dt, ta = Mb.sc->tweight_a;
-        for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
-            const long long o = (long long)j * pitch + k;
-            double v[PQ_MAXL];
-            if (PRO == PRO_PLAIN) {
-                const double* src = reinterpret_cast<const double*>(Mb.helm_io);
-                for (int l = 0; l < L; ++l) v[l] = src[o + l * ls];
-            } else {
+    int cur_mi = -1, it = 0;
+    int task = blockIdx.x;
+    if (task < total) issue(task, bufs[0]);
+    cp_commit();
+    for (; task < total; task += gridDim.x, ++it) {
+        double* xr = bufs[nbuf == 2 ? (it & 1) : 0];
+        const int nt = task + gridDim.x;
+        if (nbuf == 2) {
+            if (nt < total) issue(nt, bufs[(it + 1) & 1]);
+            cp_commit();
+            cp_wait1();
+        } else {
+            cp_wait0();
+        }
+        __syncthreads();
+        int local;
+        const int mi = find_member(prefix, nmem, task, &local);
+        if (mi != cur_mi) {
+            load_member(Mb, mems + mi);
+            __syncthreads();
+            // Stage this member's twiddle tables in shared memory.
+            const int Mm = Mb.M, Nn = Mb.N;
+            for (int t = threadIdx.x; t < Mm; t += blockDim.x) {
+                s_tw[t] = Mb.tw[t];
+                s_tw[Mm + t] = Mb.wsplit[t];
+            }
+            for (int t = threadIdx.x; t <= Nn / 2; t += blockDim.x) tab[4 * Mm + t] = Mb.was[t];
+            za = reinterpret_cast<double2*>(tab + dst_tab_doubles(Nn));
+            __syncthreads();
+            cur_mi = mi;
+        }
+        const double2* t_tw = s_tw;
+        const double2* t_ws = s_tw + Mb.M;
+        const double* t_was = tab + 4 * Mb.M;
+        const int j = local + row_offset;
+        const int L = Mb.L, N = Mb.N, n = Mb.n, ii = Mb.ii, jj = Mb.jj, pitch = Mb.pitch;
+        const long long ls = Mb.lstride;
+        const int xs = N + 2;
+        double2* zb = za + (size_t)G * crow(Mb.M);
+        const bool interior_row = (j >= 1 && j <= jj - 2);
+
+        if (EPI == EPI_SPEC) {
+            // ---------------- forward: prologue ----------------------------------
+            const double cff = 0.5 / (double)(ii - 1);
+            for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
+                const long long o = (long long)j * pitch + k;
+                double v[PQ_MAXL];
                 double z[PQ_MAXL];
                 if (PRO == PRO_STEP) {
+                    const double dt = Mb.sc->dt, ta = Mb.sc->tweight_a;
                     const double* zo = reinterpret_cast<const double*>(Mb.zeta_old[Mb.cur]);
                     const double* rs = reinterpret_cast<const double*>(Mb.res);
                     double* rb = reinterpret_cast<double*>(Mb.res_beta);
@@ -252,76 +379,74 @@ __global__ void __launch_bounds__(DST_THREADS) k_dst_rows(const Member* __restri
                         z[l] = zz;
                     }
                 } else {
-                    const double* zsrc = reinterpret_cast<const double*>(Mb.zeta);
-                    for (int l = 0; l < L; ++l) z[l] = zsrc[o + l * ls];
+                    for (int l = 0; l < L; ++l) z[l] = xr[l * xs + k];
                 }
-                // z_to_modes, qg3p_diagnostics.F90:545-549
-                for (int m = 0; m < L; ++m) {
-                    double s = 0.0;
-                    for (int l = 0; l < L; ++l) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
-                    v[m] = s;
+                if (PRO == PRO_PLAIN) {
+                    for (int m = 0; m < L; ++m) v[m] = z[m];
+                } else {
+                    // z_to_modes, qg3p_diagnostics.F90:545-549
+                    for (int m = 0; m < L; ++m) {
+                        double s = 0.0;
+                        for (int l = 0; l < L; ++l) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
+                        v[m] = s;
+                    }
+                }
+                for (int m = 0; m < L; ++m) xr[m * xs + k] = cff * v[m];
+            }
+            __syncthreads();
+            for (int m0 = 0; m0 < L; m0 += G)
+                dst_rows(xr + m0 * xs, xs, min(G, L - m0), za, zb, Mb, t_tw, t_ws, t_was);
+            double* spec = reinterpret_cast<double*>(Mb.spec);
+            for (int m = 0; m < L; ++m) {
+                double* g = spec + m * ls + (long long)j * pitch - 1;
+                for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) g[k] = xr[m * xs + k];
+            }
+        } else {
+            // ---------------- inverse: DST of the solved spectral rows ----------
+            if (interior_row)
+                for (int m0 = 0; m0 < L; m0 += G)
+                    dst_rows(xr + m0 * xs, xs, min(G, L - m0), za, zb, Mb, t_tw, t_ws, t_was);
+            if (EPI == EPI_HELM) {
+                // helm's in-place output: interior entries of interior rows, row
+                // i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1) (:1055-1057).
+                double* io = reinterpret_cast<double*>(Mb.helm_io);
+                if (interior_row) {
+                    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
+                        for (int m = 0; m < L; ++m) io[(long long)j * pitch + k + m * ls] = xr[m * xs + k];
+                    if (threadIdx.x == 0)
+                        for (int m = 0; m < L; ++m) io[(long long)j * pitch + (ii - 1) + m * ls] = 0.0;
+                } else if (j == 0) {
+                    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
+                        for (int m = 0; m < L; ++m) io[k + m * ls] = 0.0;
+                }
+            } else {
+                // psi_l = phi_1 - psiC_1 + sum_{m>=2} m2z(l,m) (phi_m - psiC_m corr_m)
+                // (modes_to_z_btcu) on every node of row j; phi is zero on the
+                // boundary (apply_dirichlet_bc(0), qg3p_aux.F90:470).
+                const double* psiC = Mb.sc->psiC;
+                const double* corr = Mb.corr;
+                double* psi = Mb.psi;
+                for (int i = threadIdx.x; i < ii; i += blockDim.x) {
+                    const bool inner = interior_row && i >= 1 && i <= n;
+                    const long long o = (long long)j * pitch + i;
+                    double ph[PQ_MAXL];
+                    for (int m = 0; m < L; ++m) ph[m] = inner ? xr[m * xs + i] : 0.0;
+                    for (int l = 0; l < L; ++l) {
+                        double dot = 0.0;
+                        for (int m = 1; m < L; ++m)
+                            dot += Mb.m2z[l * PQ_MAXL + m] * (ph[m] - psiC[m] * corr[o + m * ls]);
+                        psi[o + l * ls] = (ph[0] - psiC[0]) + dot;
+                    }
                 }
             }
-            for (int m = 0; m < L; ++m) xr[m * xs + k] = cff * v[m];
         }
         __syncthreads();
-        for (int m0 = 0; m0 < L; m0 += G) {
-            const int g = min(G, L - m0);
-            dst_rows(xr + m0 * xs, xs, g, za, zb, wsum, Mb);
-        }
-        double* spec = reinterpret_cast<double*>(Mb.spec);
-        for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
-            const long long o = (long long)j * pitch + (k - 1);
-            for (int m = 0; m < L; ++m) spec[o + m * ls] = xr[m * xs + k];
-        }
-        return;
-    }
-
-    // ---------------- inverse: DST of the solved spectral rows --------------
-    if (interior_row) {
-        const double* spec = reinterpret_cast<const double*>(Mb.spec);
-        for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
-            const long long o = (long long)j * pitch + (k - 1);
-            for (int m = 0; m < L; ++m) xr[m * xs + k] = spec[o + m * ls];
-        }
-        __syncthreads();
-        for (int m0 = 0; m0 < L; m0 += G) {
-            const int g = min(G, L - m0);
-            dst_rows(xr + m0 * xs, xs, g, za, zb, wsum, Mb);
+        if (nbuf == 1) {
+            if (nt < total) issue(nt, bufs[0]);
+            cp_commit();
         }
     }
-    if (EPI == EPI_HELM) {
-        // helm's in-place output: interior entries of interior rows, row
-        // i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1) (:1055-1057).
-        double* io = reinterpret_cast<double*>(Mb.helm_io);
-        if (interior_row) {
-            for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
-                for (int m = 0; m < L; ++m) io[(long long)j * pitch + k + m * ls] = xr[m * xs + k];
-            if (threadIdx.x == 0)
-                for (int m = 0; m < L; ++m) io[(long long)j * pitch + (ii - 1) + m * ls] = 0.0;
-        } else if (j == 0) {
-            for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
-                for (int m = 0; m < L; ++m) io[k + m * ls] = 0.0;
-        }
-        return;
-    }
-    // EPI_PV: psi_l = phi_1 - psiC_1 + sum_{m>=2} m2z(l,m) (phi_m - psiC_m corr_m)
-    // (modes_to_z_btcu) on every node of row j; phi is zero on the boundary
-    // (apply_dirichlet_bc(0), qg3p_aux.F90:470).
-    const double* psiC = Mb.sc->psiC;
-    const double* corr = Mb.corr;
-    double* psi = Mb.psi;
-    for (int i = threadIdx.x; i < ii; i += blockDim.x) {
-        const bool inner = interior_row && i >= 1 && i <= n;
-        const long long o = (long long)j * pitch + i;
-        double ph[PQ_MAXL];
-        for (int m = 0; m < L; ++m) ph[m] = inner ? xr[m * xs + i] : 0.0;
-        for (int l = 0; l < L; ++l) {
-            double dot = 0.0;
-            for (int m = 1; m < L; ++m) dot += Mb.m2z[l * PQ_MAXL + m] * (ph[m] - psiC[m] * corr[o + m * ls]);
-            psi[o + l * ls] = (ph[0] - psiC[0]) + dot;
-        }
-    }
+    cp_wait0();
 }
 
 // ---------------------------------------------------------------------------
@@ -516,22 +641,21 @@ __host__ __device__ inline size_t tri_smem_bytes(int jj) {
 
 // ---------------------------------------------------------------------------
 // Host launchers.
-static int pick_group(int L, int N, int M, size_t* bytes) {
-    int G = L;
-    while (G > 1 && dst_smem_bytes(L, G, N, M) > 112 * 1024) --G;
-    *bytes = dst_smem_bytes(L, G, N, M);
-    return G;
-}
-
 template <int PRO, int EPI>
 static cudaError_t launch_dst(const LaunchSet& ls, cudaStream_t st) {
-    size_t bytes;
-    const int G = pick_group(ls.maxL, ls.maxN, ls.maxN / 2, &bytes);
-    cudaError_t e = cudaFuncSetAttribute(k_dst_rows<PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    const DstPlan p = dst_plan(ls.maxL, ls.maxN, ls.maxI, ls.dst_group, EPI == EPI_PV);
+    cudaError_t e = cudaFuncSetAttribute(k_dst_rows<PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.bytes);
     if (e != cudaSuccess) return e;
     const int* prefix = (EPI == EPI_SPEC) ? ls.prefix_rows_interior : ls.prefix_rows_all;
-    const int nctas = (EPI == EPI_SPEC) ? ls.ctas_rows_interior : ls.ctas_rows_all;
-    k_dst_rows<PRO, EPI><<<nctas, DST_THREADS, bytes, st>>>(ls.members, prefix, ls.nmem, G, EPI == EPI_SPEC ? 1 : 0);
+    const int total = (EPI == EPI_SPEC) ? ls.ctas_rows_interior : ls.ctas_rows_all;
+    // Persistent grid: as many CTAs as fit on the device at once.
+    int per_sm = (int)((227 * 1024) / (p.bytes + 2048));
+    if (per_sm < 1) per_sm = 1;
+    if (per_sm > 4) per_sm = 4;
+    int grid = ls.sm_count * per_sm;
+    if (grid > total) grid = total;
+    k_dst_rows<PRO, EPI><<<grid, DST_THREADS, p.bytes, st>>>(ls.members, prefix, ls.nmem, p.G, p.nbuf,
+                                                            EPI == EPI_SPEC ? 1 : 0, total, p.buf_doubles);
     return cudaGetLastError();
 }
 

@@ -21,6 +21,8 @@ struct LaunchSet {
     int ctas_tri;
     const int* prefix_cab;            // cabaret_ctas(ii, jj, L) CTAs per member
     int ctas_cab;
+    int dst_group;                    // modes per DST CTA pass (0: automatic)
+    int sm_count;                     // SMs of the device (persistent grids)
 };
 
 
@@ -31,7 +33,7 @@ cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, cudaStream_t st);
 
 // pq_cabaret.cu
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, cudaStream_t st);
-int cabaret_ctas(int ii, int jj, int L);  // CTAs of k_cabaret_fused per member
+int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of k_cabaret_fused per member (band height sh)
 cudaError_t launch_rel(const LaunchSet& ls, cudaStream_t st);
 cudaError_t launch_energy(const LaunchSet& ls, cudaStream_t st);
 

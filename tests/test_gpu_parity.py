@@ -218,3 +218,15 @@ def test_energy_kats_gpu():
     ek_o, ep_o = O.energy(psi, h, s2)
     assert np.allclose(ek, ek_o, rtol=1e-13, atol=0)
     assert abs(ep - ep_o) <= 1e-13 * abs(ep_o)
+
+
+@pytest.mark.parametrize("band", [4, 8, 32, 128])
+def test_tile_parameters_do_not_change_results(band):
+    """The CABARET band height is a tuning knob: results must match the oracle for any choice."""
+    cfg = double_gyre(129, 3)
+    g, o = start(cfg, seed=5)
+    g.set_tuning(cab_band=band)
+    assert g.get_tuning()["cab_band"] == band
+    g.step(3)
+    o.step(3)
+    compare(g, o, TOL_STEP * 10)
