@@ -253,8 +253,8 @@ PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int 
 /* Tile parameters of the step kernels (chosen per grid size by the
  * autotuner, pequod_b200/autotune.py; defaults are set by pq_create).
  *   cab_band   output rows per warp of the fused CABARET sweep, 4..128
- *   dst_group  vertical modes transformed together by one DST CTA
- *              (0: automatic, by shared-memory footprint) */
+ *   dst_group  row groups per DST CTA: a CTA holds dst_group * layers
+ *              warps (0: automatic, 1); layers * dst_group <= 8 */
 typedef struct pq_tuning {
     int cab_band;
     int dst_group;

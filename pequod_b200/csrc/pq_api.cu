@@ -42,8 +42,11 @@ struct pq_ctx {
     size_t arena_bytes = 0;
     Scalars* d_sc = nullptr;
     int* d_status = nullptr;
-    int cur = 0;
+    int cur = 0;          // parity of the next step
     bool initialized = false;
+    bool fuse = false;        // fixed dt: the CABARET kernel applies the next predictor
+    bool pred_ready = false;  // zeta[cur] / res_beta[cur] already hold the next step's predictor
+    int zpar = 0;             // parity whose zeta entered the last inversion
     cudaGraphExec_t graph2 = nullptr;
     std::string err;
     long last_launches = 0;
@@ -166,14 +169,18 @@ int run_step(pq_ctx* c, int par) {
         for (int k = 0; k < 5; ++k) CK(cudaEventCreate(&ev[k]));
         CK(cudaEventRecord(ev[0], c->stream));
     }
-    CK(launch_dst_forward(c->ls[par], PRO_STEP, c->stream));
+    // The predictor + beta update runs in the forward DST unless the previous
+    // fused step already produced this step's inversion input.
+    CK(launch_dst_forward(c->ls[par], (c->fuse && c->pred_ready) ? PRO_MODAL : PRO_STEP, c->stream));
     if (ev) CK(cudaEventRecord(ev[1], c->stream));
     CK(launch_tridiag(c->ls[par], 1, c->stream));
     if (ev) CK(cudaEventRecord(ev[2], c->stream));
     CK(launch_dst_inverse(c->ls[par], EPI_PV, c->stream));
     if (ev) CK(cudaEventRecord(ev[3], c->stream));
-    CK(launch_cabaret_fused(c->ls[par], c->stream));
+    CK(launch_cabaret_fused(c->ls[par], c->fuse ? 1 : 0, c->stream));
     if (ev) CK(cudaEventRecord(ev[4], c->stream));
+    c->pred_ready = c->fuse;
+    c->zpar = par;
     return PQ_OK;
 }
 
@@ -232,7 +239,9 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     const size_t lstride = (size_t)c->pitch * jj;
     c->field_bytes = lstride * L * sizeof(double);
     const int ntiles_tri = L * ((n + 7) / 8);
-    const int cab_sh = 16;
+    // Default CABARET band height by grid size (measured on B200: shorter
+    // bands give small grids enough warps, taller ones cut halo rows on big ones).
+    const int cab_sh = jj <= 300 ? 8 : jj <= 700 ? 32 : 64;
     const int ntiles_cab = cabaret_ctas(ii, jj, L, cab_sh);
     const int ntiles_cab_max = cabaret_ctas(ii, jj, L, kMinBand);
 
@@ -254,7 +263,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     PivotTables pv = build_pivots(ii, jj, L, d->ss);
 
     // Arena layout.
-    const int nfields = 2 /*zeta_old*/ + 1 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 1 /*res_beta*/ + 1 /*ui*/ + 1 /*uj*/ +
+    const int nfields = 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 2 /*res_beta*/ + 1 /*ui*/ + 1 /*uj*/ +
                         2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ + 1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ +
                         1 /*corr*/;
     const size_t fb = align256(c->field_bytes);
@@ -339,10 +348,10 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     auto fld = [&]() { return (void*)(F + fb * (fi++)); };
     m.zeta_old[0] = fld();
     m.zeta_old[1] = fld();
-    m.zeta = fld();
+    void* zpb0 = fld();
     m.psi = (double*)fld();
     m.res = fld();
-    m.res_beta = fld();
+    void* rb0 = fld();
     m.ui = fld();
     m.uj = fld();
     m.uimo[0] = fld();
@@ -353,6 +362,8 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     m.zfi[1] = fld();
     m.zfj[0] = fld();
     m.zfj[1] = fld();
+    void* zpb1 = fld();
+    void* rb1 = fld();
     m.rel = fld();
     m.helm_io = fld();
     m.spec = fld();
@@ -376,6 +387,13 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     c->hm[1] = m;
     c->hm[0].cur = 0;
     c->hm[1].cur = 1;
+    // zeta (after predictor and beta) and res_beta are ping-ponged so that
+    // the fused step can write the next step's values.
+    c->hm[0].zeta = c->hm[1].zeta_next = zpb0;
+    c->hm[1].zeta = c->hm[0].zeta_next = zpb1;
+    c->hm[0].res_beta = c->hm[1].res_beta_other = rb0;
+    c->hm[1].res_beta = c->hm[0].res_beta_other = rb1;
+    c->fuse = !d->adapt_dt;
 
     e = cudaMalloc(&c->d_members, 2 * sizeof(Member) + 256);
     if (e != cudaSuccess) return fail(c, PQ_ERR_NOMEM, "device allocation failed");
@@ -389,6 +407,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
         s.nmem = 1;
         s.maxL = L;
         s.maxN = N;
+        s.maxPitch = c->pitch;
         s.maxJ = jj;
         s.maxI = ii;
         s.prefix_rows_interior = s.prefix_rows_all = s.prefix_tri = s.prefix_cab = c->d_prefix;
@@ -456,8 +475,10 @@ int pq_helm(pq_ctx* c, double* zeta, int ptr_kind) {
 int pq_pv_inversion(pq_ctx* c, const double* zeta, double* psi, int ptr_kind) {
     if (!c || !zeta || !psi) return PQ_ERR_ARG;
     CK(cudaSetDevice(c->device));
-    int rc = copy_in(c, c->hm[0].zeta, zeta, ptr_kind);
+    int rc = copy_in(c, c->hm[c->cur].zeta, zeta, ptr_kind);
     if (rc) return rc;
+    c->pred_ready = false;
+    c->zpar = c->cur;
     rc = run_helm(c, c->cur, PRO_MODAL, EPI_PV, 1);
     if (rc) return rc;
     rc = copy_out(c, psi, c->hm[0].psi, ptr_kind);
@@ -484,9 +505,10 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     const Member& m = c->hm[0];
     // Zero all CABARET fields and both parities (qg3.F90:393-404).
     const size_t fb = align256(c->field_bytes);
-    // Fields 0..15 of the arena: zeta_old[2], zeta, psi, res, res_beta, ui,
-    // uj, uimo[2], ujmo[2], zeta_fi[2], zeta_fj[2] (corr is kept).
-    CK(cudaMemsetAsync(m.zeta_old[0], 0, fb * 16, c->stream));
+    // Fields 0..17 of the arena: zeta_old[2], zeta[0], psi, res, res_beta[0],
+    // ui, uj, uimo[2], ujmo[2], zeta_fi[2], zeta_fj[2], zeta[1], res_beta[1]
+    // (corr is kept).
+    CK(cudaMemsetAsync(m.zeta_old[0], 0, fb * 18, c->stream));
     int rc = copy_in(c, m.zeta, z.data(), PQ_PTR_HOST);
     if (rc) return rc;
     Scalars sc;
@@ -501,6 +523,8 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     rc = copy_in(c, m.zeta, z.data(), PQ_PTR_HOST);
     if (rc) return rc;
     c->cur = 0;
+    c->zpar = 0;
+    c->pred_ready = false;
     rc = run_helm(c, 0, PRO_MODAL, EPI_PV, 1);
     if (rc) return rc;
     CK(launch_init_finish(c->ls[0], c->stream));
@@ -526,6 +550,7 @@ int pq_step_exchange(pq_ctx* c, const double* zeta_in, double* psi_out, int ptr_
     if (zeta_in) {
         int rc = copy_in(c, c->hm[c->cur].zeta_old[c->cur], zeta_in, ptr_kind);
         if (rc) return rc;
+        c->pred_ready = false;
     }
     int rc = pq_step_async(c, 1);
     if (rc) return rc;
@@ -542,11 +567,12 @@ int pq_step_async(pq_ctx* c, int nsteps) {
     CK(cudaSetDevice(c->device));
     int done = 0;
     long launches = 0;
-    // An odd step first so that the graph always starts at parity 0.
-    if (c->cur == 1 && nsteps > 0) {
-        int rc = run_step(c, 1);
+    // Eager steps until the graph's entry state: parity 0 and, with the fused
+    // predictor, the next step's inversion input already computed.
+    while (done < nsteps && (c->cur == 1 || (c->fuse && !c->pred_ready))) {
+        int rc = run_step(c, c->cur);
         if (rc) return rc;
-        c->cur = 0;
+        c->cur ^= 1;
         ++done;
         launches += 4;
     }
@@ -587,7 +613,7 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     if (!c || !t) return PQ_ERR_ARG;
     if (t->cab_band < kMinBand || t->cab_band > kMaxBand) return fail(c, PQ_ERR_ARG, "cab_band out of range");
     CK(cudaStreamSynchronize(c->stream));
-    if (t->dst_group < 0 || t->dst_group > c->L) return fail(c, PQ_ERR_ARG, "dst_group out of range");
+    if (t->dst_group < 0 || c->L * t->dst_group > 8) return fail(c, PQ_ERR_ARG, "dst_group out of range");
     for (int p = 0; p < 2; ++p) {
         c->hm[p].cab_sh = t->cab_band;
         c->hm[p].ntiles_cab = cabaret_ctas(c->ii, c->jj, c->L, t->cab_band);
@@ -722,7 +748,7 @@ void* field_ptr(pq_ctx* c, int field) {
         case PQ_F_ZETA_FI: return m.zfi[cur];
         case PQ_F_ZETA_FJ: return m.zfj[cur];
         case PQ_F_RES: return m.res;
-        case PQ_F_RES_BETA: return m.res_beta;
+        case PQ_F_RES_BETA: return m.res_beta_other;  // res_beta of the last step
         case PQ_F_CORR: return (void*)m.corr;
     }
     return nullptr;
@@ -737,7 +763,7 @@ int pq_get_field(pq_ctx* c, int field, double* out) {
     RefShape s;
     if (!ref_shape(field, c->ii, c->jj, &s)) return fail(c, PQ_ERR_ARG, "unknown field");
     CK(cudaSetDevice(c->device));
-    if (field == PQ_F_REL) CK(launch_rel(c->ls[c->cur], c->stream));
+    if (field == PQ_F_REL) CK(launch_rel(c->ls[c->zpar], c->stream));
     std::vector<double> dense((size_t)c->ii * c->jj * c->L);
     int rc = copy_out(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST);
     if (rc) return rc;
@@ -765,8 +791,12 @@ int pq_set_field(pq_ctx* c, int field, const double* in) {
                     in[(size_t)(i + s.oi) + (size_t)s.n1 * ((j + s.oj) + (size_t)s.n2 * l)];
     int rc = copy_in(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST);
     if (rc) return rc;
-    if (field == PQ_F_ZETA) rc = copy_in(c, c->hm[0].zeta, dense.data(), PQ_PTR_HOST);
+    if (field == PQ_F_ZETA) {
+        rc = copy_in(c, c->hm[c->cur].zeta, dense.data(), PQ_PTR_HOST);
+        c->zpar = c->cur;
+    }
     if (rc) return rc;
+    c->pred_ready = false;
     CK(cudaStreamSynchronize(c->stream));
     c->initialized = true;
     return PQ_OK;

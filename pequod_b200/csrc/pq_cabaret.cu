@@ -77,7 +77,7 @@ constexpr int CAB_WARPS = 4;
 constexpr int CAB_SW = 28;  // output columns per warp
 constexpr int CAB_D = 4;    // depth of the per-warp cp.async row pipeline
 // Streamed inputs of one iteration (rows relative to s = r - 2).
-enum { F_PSI2 = 0, F_ZPB, F_PSIM, F_PSIP, F_ZO, F_UIMO, F_UJMO, F_FIO, F_FJ, F_WIND, CAB_NF };
+enum { F_PSI2 = 0, F_ZPB, F_PSIM, F_PSIP, F_ZO, F_UIMO, F_UJMO, F_FIO, F_FJ, F_WIND, F_RB, CAB_NF };
 constexpr int CAB_RING = CAB_D * CAB_NF * 32;  // doubles per warp
 
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
@@ -87,8 +87,11 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 // band starting at row j0.  EDGE = false is the specialisation for warps
 // whose whole footprint (columns i0-2 .. i0+29, rows j0-4 .. j0+sh+3) lies
 // at least two nodes inside the domain: no bounds checks, no boundary
-// branches.  Returns the largest |u| of the faces it wrote.
-template <bool EDGE>
+// branches.  PRED = true also applies the next step's cabaret_predictor and
+// cabaret_beta (fixed dt) to every interior node it finishes, writing the
+// next step's inversion input zeta_next and res_beta_other.  Returns the
+// largest |u| of the faces it wrote.
+template <bool EDGE, bool PRED>
 __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int j0, int lane, double* ring) {
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
@@ -121,6 +124,10 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const int o_fin = ofs(Mb.zfi[nxt]) + lo;
     const int o_fjo = ofs(Mb.zfj[cur]) + lo;
     const int o_fjn = ofs(Mb.zfj[nxt]) + lo;
+    const int o_rb = PRED ? ofs(Mb.res_beta) + lo : 0;
+    const int o_rbn = PRED ? ofs(Mb.res_beta_other) + lo : 0;
+    const int o_zpn = PRED ? ofs(Mb.zeta_next) + lo : 0;
+    const double ta = Mb.sc->tweight_a, beta_l = Mb.beta[l];
     const bool has_wind = (l == 0 && Mb.wind);
     const int o_wind = has_wind ? ofs(Mb.wind) + i : 0;
     double* W = const_cast<double*>(B);
@@ -200,6 +207,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         cp(d + (F_FIO << 5), o_fio, ss - 1, rowok(ss - 1));
         cp(d + (F_FJ << 5), o_fjo, ss, rowok(ss));
         if (has_wind) cp(d + (F_WIND << 5), o_wind, ss - 1, rowok(ss - 1));
+        if (PRED) cp(d + (F_RB << 5), o_rb, ss - 2, rowok(ss - 2));
     };
     for (int rr = j0; rr < j0 + CAB_D - 1; ++rr) {
         issue(rr);
@@ -213,6 +221,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     double FJm2 = 0, FJm1 = 0;  // zeta_fj (old) faces s-2, s-1
     double FLJm2 = 0;           // flux_j face s-2
     double FLI = 0;             // flux_i row s-2 (face a = i)
+    double UIm2 = 0;            // ui row s-2 (face a = i)
     double zpb_prev = 0, pm_prev = 0, pp_prev = 0, pe_prev = 0;
 
 #pragma unroll 1
@@ -239,6 +248,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         const double fio_1 = st[F_FIO << 5];
         const double fj_s = st[F_FJ << 5];
         const double w_1 = has_wind ? st[F_WIND << 5] : 0.0;
+        const double rb_2 = PRED ? st[F_RB << 5] : 0.0;
 
         // ---- rel(s): rel_from_zeta_and_psi + apply_rel_bc -------------------
         double up1 = 0.0, up2 = 0.0, dn1 = 0.0, dn2 = 0.0;
@@ -353,6 +363,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         // ---- corrector at row o = s-2 -----------------------------------------
         const int o = s - 2;
         const double fli_dn = shdn(FLI, 1);
+        const double ui_e = PRED ? shdn(UIm2, 1) : 0.0;  // ui on face a = i + 1, row o
         const bool band_o = (o >= j0 && o < j0 + SH) && (!EDGE || (o >= 0 && o < jj));
         if (out_i && band_o) {
             const bool bnd = EDGE && (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
@@ -361,6 +372,15 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
                 const double rr = -(fli_dn - FLI + flj_1 - FLJm2);
                 W[o_res + o * pitch] = rr;
                 z = z + hdt * rr;
+                if (PRED) {
+                    // Next step: cabaret_predictor (qg3p_aux.F90:1012-1018) and
+                    // cabaret_beta (:1051-1059) with this step's ui.
+                    double zz = z + hdt * rr;
+                    const double rbn = dt * (0.5 * (ui_e + UIm2) * beta_l);
+                    zz = zz + (1.0 + ta) * rbn - ta * rb_2;
+                    W[o_rbn + o * pitch] = rbn;
+                    W[o_zpn + o * pitch] = zz;
+                }
             }
             W[o_zn + o * pitch] = z;
         }
@@ -390,6 +410,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         FJm1 = fj_s;
         FLJm2 = flj_1;
         FLI = fli_1;
+        UIm2 = ui_1;
         zpb_prev = zpb_s;
         pm_prev = pm_s;
         pp_prev = pp_s;
@@ -398,6 +419,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     return umax;
 }
 
+template <bool PRED>
 __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* __restrict__ mems,
                                                                     const int* __restrict__ prefix, int nmem) {
     __shared__ Member Mb;
@@ -421,7 +443,8 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
         const int i0 = strip * CAB_SW, j0 = band * SH;
         const bool interior = (i0 - 2 >= 2) && (i0 + 29 <= ii - 3) && (j0 - 4 >= 2) && (j0 + SH + 3 <= jj - 3);
         double* ring = cab_ring + warp * CAB_RING;
-        umax = interior ? cab_sweep<false>(Mb, l, i0, j0, lane, ring) : cab_sweep<true>(Mb, l, i0, j0, lane, ring);
+        umax = interior ? cab_sweep<false, PRED>(Mb, l, i0, j0, lane, ring)
+                        : cab_sweep<true, PRED>(Mb, l, i0, j0, lane, ring);
     }
 
     // Max |u| of the new face velocities (cabaret_cfl / cabaret_adapt_dt);
@@ -471,12 +494,18 @@ int cabaret_ctas(int ii, int jj, int L, int sh) {
     return (nstrips * nbands * L + CAB_WARPS - 1) / CAB_WARPS;
 }
 
-cudaError_t launch_cabaret_fused(const LaunchSet& ls, cudaStream_t st) {
+template <bool PRED>
+static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
     const size_t bytes = (size_t)CAB_WARPS * CAB_RING * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(k_cabaret_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_cabaret_fused<PRED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    k_cabaret_fused<<<ls.ctas_cab, CAB_WARPS * 32, bytes, st>>>(ls.members, ls.prefix_cab, ls.nmem);
+    k_cabaret_fused<PRED><<<ls.ctas_cab, CAB_WARPS * 32, bytes, st>>>(ls.members, ls.prefix_cab, ls.nmem);
     return cudaGetLastError();
+}
+
+cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, cudaStream_t st) {
+    return predict_next ? launch_cab<true>(ls, st) : launch_cab<false>(ls, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -83,9 +83,12 @@ struct Member {
     // another CTA are ping-ponged: [cur] is read, [cur ^ 1] written.
     void* zeta_old[2];
     void* zeta;       // zeta after predictor and beta (input of the inversion)
+    void* zeta_next;  // the same for the next step (written by the fused step)
     double* psi;
     void* res;
-    void* res_beta;
+    void* res_beta;        // res_beta of this step
+    void* res_beta_other;  // of the previous step (read by the predictor) or
+                           // of the next step (written by the fused step)
     void* ui;         // written by the fused step, read by the next step's beta term
     void* uj;
     void* uimo[2];

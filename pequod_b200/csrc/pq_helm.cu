@@ -35,7 +35,6 @@ namespace pq {
 enum { PRO_PLAIN = 0, PRO_MODAL = 1, PRO_STEP = 2 };
 enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
 
-constexpr int DST_THREADS = 256;
 constexpr int TRI_THREADS = 256;
 constexpr int TRI_KT = 8;   // wavenumbers per tridiagonal CTA (one per warp)
 
@@ -46,407 +45,465 @@ __device__ __forceinline__ void load_member(Member& dst, const Member* src) {
     for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
 }
 
-// Complex scratch rows are padded by one entry per 8 (index t -> t + t/8) so
-// that the strided writes of the early Stockham stages hit distinct banks.
-__device__ __forceinline__ int cpad(int t) { return t + (t >> 3); }
-__host__ __device__ inline int crow(int M) { return M + (M >> 3); }  // padded row length
-
-__device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }  // a * (-i)
-
-// Stockham FFT (radix 8, then 4, then 2) of G complex rows of length
-// M = 2^logM in shared memory, forward sign; row g at a + g*crow(M), padded
-// indexing.  Returns the buffer that holds the result (a or b).
-__device__ double2* fft_stockham(double2* a, double2* b, int G, int M, int logM, const double2* tw) {
-    const int MP = crow(M);
-    int Ns = 1, logNs = 0;
-    const double c8 = 0.70710678118654752440;  // sqrt(2)/2
-    while (Ns * 8 <= M) {
-        const int M8 = M >> 3, logM8 = logM - 3;
-        const int lst = logM8 - logNs;  // log2(M / (8 Ns))
-        for (int w = threadIdx.x; w < G * M8; w += blockDim.x) {
-            const int g = w >> logM8, jj = w & (M8 - 1);
-            const double2* ag = a + g * MP;
-            double2* bg = b + g * MP;
-            double2 v[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) v[r] = ag[cpad(jj + r * M8)];
-            const int k = jj & (Ns - 1);
-            if (k) {
-#pragma unroll
-                for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], tw[(r * k) << lst]);
-            }
-            // 8-point DFT: two 4-point DFTs of the even and odd inputs.
-            const double2 e0 = cadd(v[0], v[4]), e1 = csub(v[0], v[4]), e2 = cadd(v[2], v[6]),
-                          e3 = mul_mi(csub(v[2], v[6]));
-            const double2 E0 = cadd(e0, e2), E1 = cadd(e1, e3), E2 = csub(e0, e2), E3 = csub(e1, e3);
-            const double2 o0 = cadd(v[1], v[5]), o1 = csub(v[1], v[5]), o2 = cadd(v[3], v[7]),
-                          o3 = mul_mi(csub(v[3], v[7]));
-            double2 O0 = cadd(o0, o2), O1 = cadd(o1, o3), O2 = csub(o0, o2), O3 = csub(o1, o3);
-            // W8^1 = (1 - i)/sqrt2, W8^2 = -i, W8^3 = (-1 - i)/sqrt2
-            O1 = make_double2(c8 * (O1.x + O1.y), c8 * (O1.y - O1.x));
-            O2 = mul_mi(O2);
-            O3 = make_double2(c8 * (O3.y - O3.x), -c8 * (O3.x + O3.y));
-            const int idx = ((jj >> logNs) << (logNs + 3)) + k;
-            bg[cpad(idx)] = cadd(E0, O0);
-            bg[cpad(idx + Ns)] = cadd(E1, O1);
-            bg[cpad(idx + 2 * Ns)] = cadd(E2, O2);
-            bg[cpad(idx + 3 * Ns)] = cadd(E3, O3);
-            bg[cpad(idx + 4 * Ns)] = csub(E0, O0);
-            bg[cpad(idx + 5 * Ns)] = csub(E1, O1);
-            bg[cpad(idx + 6 * Ns)] = csub(E2, O2);
-            bg[cpad(idx + 7 * Ns)] = csub(E3, O3);
-        }
-        __syncthreads();
-        double2* t = a;
-        a = b;
-        b = t;
-        Ns <<= 3;
-        logNs += 3;
-    }
-    if (Ns * 4 <= M) {
-        const int M4 = M >> 2, logM4 = logM - 2;
-        const int lst = logM4 - logNs;
-        for (int w = threadIdx.x; w < G * M4; w += blockDim.x) {
-            const int g = w >> logM4, jj = w & (M4 - 1);
-            const double2* ag = a + g * MP;
-            double2* bg = b + g * MP;
-            double2 v0 = ag[cpad(jj)], v1 = ag[cpad(jj + M4)], v2 = ag[cpad(jj + 2 * M4)], v3 = ag[cpad(jj + 3 * M4)];
-            const int k = jj & (Ns - 1);
-            if (k) {
-                v1 = cmul(v1, tw[k << lst]);
-                v2 = cmul(v2, tw[(2 * k) << lst]);
-                v3 = cmul(v3, tw[(3 * k) << lst]);
-            }
-            const double2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = mul_mi(csub(v1, v3));
-            const int idx = ((jj >> logNs) << (logNs + 2)) + k;
-            bg[cpad(idx)] = cadd(t0, t2);
-            bg[cpad(idx + Ns)] = cadd(t1, t3);
-            bg[cpad(idx + 2 * Ns)] = csub(t0, t2);
-            bg[cpad(idx + 3 * Ns)] = csub(t1, t3);
-        }
-        __syncthreads();
-        double2* t = a;
-        a = b;
-        b = t;
-        Ns <<= 2;
-        logNs += 2;
-    }
-    if (Ns < M) {
-        const int M2 = M >> 1, logM2 = logM - 1;
-        const int lst = logM2 - logNs;
-        for (int w = threadIdx.x; w < G * M2; w += blockDim.x) {
-            const int g = w >> logM2, jj = w & (M2 - 1);
-            const double2* ag = a + g * MP;
-            double2* bg = b + g * MP;
-            double2 v0 = ag[cpad(jj)], v1 = ag[cpad(jj + M2)];
-            const int k = jj & (Ns - 1);
-            if (k) v1 = cmul(v1, tw[k << lst]);
-            const int idx = ((jj >> logNs) << (logNs + 1)) + k;
-            bg[cpad(idx)] = cadd(v0, v1);
-            bg[cpad(idx + Ns)] = csub(v0, v1);
-        }
-        __syncthreads();
-        double2* t = a;
-        a = b;
-        b = t;
-    }
-    return a;
-}
-
-// In-place DST-I (FFTPACK sint convention) of G real rows held in shared
-// memory at xr + g*xs, entries 1..n (entries 0 and N are scratch).
-// za, zb: shared complex scratch of G*crow(M) each.  tw, wsp, was: the
-// twiddle tables staged in shared memory.
-__device__ void dst_rows(double* xr, int xs, int G, double2* za, double2* zb, const Member& Mb, const double2* tw,
-                         const double2* wsp, const double* was) {
-    const int N = Mb.N, M = Mb.M, N2 = N >> 1, logM = Mb.logM, MP = crow(M);
-    // Pre-twiddle (sint1, qg3p_helmholtz.F90:1404-1413) and pack.
-    for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
-        const int g = w >> logM, t = w & (M - 1);
-        const double* x = xr + g * xs;
-        double c[2];
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const int k = 2 * t + e;
-            double v;
-            if (k == 0) {
-                v = 0.0;
-            } else if (k == N2) {
-                v = 4.0 * x[N2];
-            } else if (k < N2) {
-                const double xa = x[k], xb = x[N - k];
-                v = (xa - xb) + was[k] * (xa + xb);
-            } else {
-                const int kk = N - k;
-                const double xa = x[kk], xb = x[k];
-                v = was[kk] * (xa + xb) - (xa - xb);
-            }
-            c[e] = v;
-        }
-        za[g * MP + cpad(t)] = make_double2(c[0], c[1]);
-    }
-    __syncthreads();
-    double2* Z = fft_stockham(za, zb, G, M, logM, tw);
-    double2* other = (Z == za) ? zb : za;
-    // Real-FFT split; even outputs directly, R_q to scratch for the scan.
-    for (int w = threadIdx.x; w < G * M; w += blockDim.x) {
-        const int g = w >> logM, q = w & (M - 1);
-        const double2* Zg = Z + g * MP;
-        const double2 zq = Zg[cpad(q)];
-        const double2 zr = Zg[cpad((M - q) & (M - 1))];
-        const double2 zc = make_double2(zr.x, -zr.y);
-        const double2 E = make_double2(0.5 * (zq.x + zc.x), 0.5 * (zq.y + zc.y));
-        const double2 d = csub(zq, zc);
-        const double2 O = make_double2(0.5 * d.y, -0.5 * d.x);
-        const double2 C = cadd(E, cmul(wsp[q], O));
-        reinterpret_cast<double*>(other + g * MP)[q] = (q == 0) ? 0.5 * C.x : C.x;
-        if (q >= 1) xr[g * xs + 2 * q] = -C.y;
-    }
-    __syncthreads();
-    // X_{2q+1} = inclusive prefix sum of R over q: one warp per row, each lane
-    // a contiguous run of M/32 values (or one value when M < 32).
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int per = M >= 32 ? (M >> 5) : 1;
-    for (int g = warp; g < G; g += nw) {
-        const double* Rg = reinterpret_cast<const double*>(other + g * MP);
-        const int q0 = lane * per;
-        double loc = 0.0;
-        for (int e = 0; e < per; ++e)
-            if (q0 + e < M) loc += Rg[q0 + e];
-        const double incl = warp_inclusive_scan(loc);
-        double run = incl - loc;
-        double* x = xr + g * xs;
-        for (int e = 0; e < per; ++e) {
-            const int q = q0 + e;
-            if (q < M) {
-                run += Rg[q];
-                x[2 * q + 1] = run;
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// Persistent, software-pipelined row transforms.
+// ---------------------------------------------------------------------------
+// Row DSTs: one group of P lanes per (row, mode) unit.
 //
-// Each CTA walks the rows (tasks) blockIdx.x, blockIdx.x + gridDim.x, ...
-// With two staging buffers it issues the asynchronous copies (cp.async) of the
-// next row's inputs before transforming the current row, so the global-load
-// latency of a row overlaps the previous row's FFT.  A staging buffer holds
-// the L real rows (stride N + 2, entries 1..n) and, for the psi epilogue, the
-// L - 1 correction rows of the baroclinic modes (stride cs).
+// The complex FFT of length M = N/2 is a Stockham FFT in which every lane of
+// a group owns V = M / P values for the whole transform: the pre-twiddle
+// computes a lane's first-pass inputs straight into registers, each radix-8
+// (then 4 or 2) pass is a set of V/R in-register butterflies, and values cross
+// lanes only through the unit's shared-memory row between passes (under
+// __syncwarp, never a block barrier).  The real-FFT split and the prefix sum
+// of the odd outputs run on V contiguous wavenumbers per lane with one
+// segmented warp scan.  V = 8 up to M = 256 (P = M/8 lanes), then 16, 32.
+//
+// Unit buffer (U scalars per unit): plain real row x[k] (input), padded
+// complex rows (Stockham passes, index t -> t + t/8), padded real output row
+// (index k -> k + 2*(k/16), so that the pair stores of the split are
+// bank-conflict free).
 
-__device__ __forceinline__ void cp8(double* dst, const double* src) {
+__device__ __forceinline__ int cpad(int t) { return t + (t >> 3); }
+__device__ __forceinline__ int xpad(int k) { return k + ((k >> 4) << 1); }
+
+template <typename T2> __device__ __forceinline__ T2 c_mi(T2 a) {  // a * (-i)
+    T2 r;
+    r.x = a.y;
+    r.y = -a.x;
+    return r;
+}
+
+// In-register forward DFT of R points (R = 2, 4, 8), natural order.
+template <int R, typename T2> __device__ __forceinline__ void dft_reg(T2* v) {
+    if constexpr (R == 2) {
+        const T2 a = cadd(v[0], v[1]), b = csub(v[0], v[1]);
+        v[0] = a;
+        v[1] = b;
+    } else if constexpr (R == 4) {
+        const T2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]), t3 = c_mi(csub(v[1], v[3]));
+        v[0] = cadd(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[2] = csub(t0, t2);
+        v[3] = csub(t1, t3);
+    } else {
+        using T = decltype(v[0].x);
+        const T c8 = (T)0.70710678118654752440;  // sqrt(2)/2
+        const T2 e0 = cadd(v[0], v[4]), e1 = csub(v[0], v[4]), e2 = cadd(v[2], v[6]), e3 = c_mi(csub(v[2], v[6]));
+        const T2 E0 = cadd(e0, e2), E1 = cadd(e1, e3), E2 = csub(e0, e2), E3 = csub(e1, e3);
+        const T2 o0 = cadd(v[1], v[5]), o1 = csub(v[1], v[5]), o2 = cadd(v[3], v[7]), o3 = c_mi(csub(v[3], v[7]));
+        T2 O0 = cadd(o0, o2), O1 = cadd(o1, o3), O2 = csub(o0, o2), O3 = csub(o1, o3);
+        // W8^1 = (1 - i)/sqrt2, W8^2 = -i, W8^3 = (-1 - i)/sqrt2
+        T2 t;
+        t.x = c8 * (O1.x + O1.y);
+        t.y = c8 * (O1.y - O1.x);
+        O1 = t;
+        O2 = c_mi(O2);
+        t.x = c8 * (O3.y - O3.x);
+        t.y = -c8 * (O3.x + O3.y);
+        O3 = t;
+        v[0] = cadd(E0, O0);
+        v[1] = cadd(E1, O1);
+        v[2] = cadd(E2, O2);
+        v[3] = cadd(E3, O3);
+        v[4] = csub(E0, O0);
+        v[5] = csub(E1, O1);
+        v[6] = csub(E2, O2);
+        v[7] = csub(E3, O3);
+    }
+}
+
+// One radix-R Stockham pass over the unit's M values (Ns = length of the
+// sub-transforms already done).  Lane p owns butterflies j = p + P*b; its
+// values v[b*R + r] are the butterfly inputs j + r*(M/R).  With `load` false
+// the inputs are already in registers (first pass).  Output is stored to the
+// unit's padded complex row.
+template <int V, int R, typename T2>
+__device__ __forceinline__ void fft_pass(T2 (&v)[V], T2* z, int p, int P, int M, int logM, int Ns, int logNs,
+                                         const T2* __restrict__ tw, bool load) {
+    constexpr int logR = (R == 8) ? 3 : (R == 4) ? 2 : 1;
+    const int MR = M >> logR;
+    if (load) {
+#pragma unroll
+        for (int b = 0; b < V / R; ++b)
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[b * R + r] = z[cpad(p + P * b + r * MR)];
+    }
+    const int lst = logM - logR - logNs;  // log2(M / (Ns R))
+#pragma unroll
+    for (int b = 0; b < V / R; ++b) {
+        const int j = p + P * b, k = j & (Ns - 1);
+        if (k) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], __ldg(&tw[(r * k) << lst]));
+        }
+        dft_reg<R>(&v[b * R]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < V / R; ++b) {
+        const int j = p + P * b, k = j & (Ns - 1);
+        const int o = ((j >> logNs) << (logNs + logR)) + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) z[cpad(o + r * Ns)] = v[b * R + r];
+    }
+    __syncwarp();
+}
+
+// DST-I (FFTPACK sint convention, qg3p_helmholtz.F90:1370-1426) of the real
+// row held in the unit buffer (x_k at buf[k], k = 1..N-1), output X_k at
+// buf[xpad(k)], k = 1..N-1.  Every lane of the warp must call this.
+template <int V, typename T>
+__device__ __forceinline__ void dst_unit(T* buf, int p, int P, int N, int M, int logM,
+                                         const typename Cplx<T>::type* __restrict__ tw,
+                                         const typename Cplx<T>::type* __restrict__ wsp,
+                                         const T* __restrict__ was) {
+    using T2 = typename Cplx<T>::type;
+    constexpr int R0 = V >= 8 ? 8 : V;
+    T2 v[V];
+    // Pre-twiddle (sint1, :1404-1413) into the first pass's inputs:
+    // c_k = (x_k - x_{N-k}) + 2 sin(k pi / N) (x_k + x_{N-k}), c_0 = 0,
+    // packed c_{2t} + i c_{2t+1}.
+    {
+        const int MR0 = M / R0;
+#pragma unroll
+        for (int b = 0; b < V / R0; ++b)
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int t = p + P * b + r * MR0;
+                const int k = 2 * t;
+                const T2 xa = *reinterpret_cast<const T2*>(buf + k);  // x_k, x_{k+1}
+                const T xb0 = buf[N - k], xb1 = buf[N - k - 1];
+                const bool lo = 2 * k < N;  // then k + 1 <= N/2 too
+                const T w0 = __ldg(&was[lo ? k : N - k]), w1 = __ldg(&was[lo ? k + 1 : N - k - 1]);
+                const T c0 = (t == 0) ? (T)0 : (xa.x - xb0) + w0 * (xa.x + xb0);
+                const T c1 = (xa.y - xb1) + w1 * (xa.y + xb1);
+                v[b * R0 + r].x = c0;
+                v[b * R0 + r].y = c1;
+            }
+    }
+    T2* z = reinterpret_cast<T2*>(buf);
+    {
+        int Ns = 1, logNs = 0;
+        bool first = true;
+        while (Ns < M) {
+            const int rem = M >> logNs;
+            if constexpr (V >= 8) {
+                if (rem >= 8) {
+                    fft_pass<V, 8>(v, z, p, P, M, logM, Ns, logNs, tw, !first);
+                    Ns <<= 3;
+                    logNs += 3;
+                    first = false;
+                    continue;
+                }
+            }
+            if constexpr (V >= 4) {
+                if (rem == 4) {
+                    fft_pass<V, 4>(v, z, p, P, M, logM, Ns, logNs, tw, !first);
+                    Ns <<= 2;
+                    logNs += 2;
+                    first = false;
+                    continue;
+                }
+            }
+            fft_pass<V, 2>(v, z, p, P, M, logM, Ns, logNs, tw, !first);
+            Ns <<= 1;
+            logNs += 1;
+            first = false;
+        }
+    }
+    // Real-FFT split on V contiguous wavenumbers q = p*V + e:
+    // C_q = E_q + W_q O_q, R_q = Re C_q (halved at q = 0), X_2q = -Im C_q,
+    // X_{2q+1} = sum_{s <= q} R_s.
+    T Xe[V], Xo[V];
+    T run = (T)0;
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+        const int q = p * V + e;
+        const T2 zq = z[cpad(q)];
+        const T2 zr = z[cpad((M - q) & (M - 1))];
+        const T ex = (T)0.5 * (zq.x + zr.x), ey = (T)0.5 * (zq.y - zr.y);
+        const T dx = zq.x - zr.x, dy = zq.y + zr.y;
+        T2 O;
+        O.x = (T)0.5 * dy;
+        O.y = (T)-0.5 * dx;
+        const T2 w = __ldg(&wsp[q]);
+        const T cx = ex + (w.x * O.x - w.y * O.y);
+        const T cy = ey + (w.x * O.y + w.y * O.x);
+        Xe[e] = (q == 0) ? (T)0 : -cy;
+        run += (q == 0) ? (T)0.5 * cx : cx;
+        Xo[e] = run;
+    }
+    // Segmented (width P) exclusive scan of the lanes' totals.
+    T incl = run;
+    for (int d = 1; d < P; d <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, incl, d, P);
+        if (p >= d) incl += y;
+    }
+    const T excl = incl - run;
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+        const int q = p * V + e;
+        T2 pr;
+        pr.x = Xe[e];
+        pr.y = Xo[e] + excl;
+        *reinterpret_cast<T2*>(buf + xpad(2 * q)) = pr;
+    }
+    __syncwarp();
+}
+
+// Launch geometry shared by host and device: V per M, rows per CTA, scalars
+// per unit buffer.
+__host__ __device__ inline int dst_v(int M) { return M <= 2 ? 2 : M == 4 ? 4 : M <= 256 ? 8 : M / 32; }
+__host__ __device__ inline int dst_rows_per_cta(int M, int L, int c) {
+    const int P = M / dst_v(M);
+    if (c <= 0) c = 1;  // one row group per CTA: the most CTAs, measured fastest
+    return c * (32 / P);
+}
+__host__ __device__ inline int dst_unit_len(int N) { return (N + N / 8 + 2 + 1) & ~1; }
+
+__device__ __forceinline__ void cp16(double* dst, const double* src, bool ok) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(ok ? 16 : 0) : "memory");
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-struct DstPlan {
-    int G, nbuf;
-    size_t buf_doubles;  // per staging buffer
-    size_t bytes;        // dynamic shared memory
-};
-
-// Shared-memory tables of the DST for transform length N: tw[M], wsplit[M]
-// (complex), was[N/2 + 1]; rounded up to an even count so that the complex
-// scratch behind it stays 16-byte aligned.
-__host__ __device__ inline size_t dst_tab_doubles(int N) { return ((size_t)2 * N + (N / 2 + 3)) & ~(size_t)1; }
-
-__host__ inline DstPlan dst_plan(int L, int N, int ii, int want_G, bool with_corr) {
-    DstPlan p;
-    const int M = N / 2;
-    (void)ii;
-    (void)with_corr;
-    p.buf_doubles = (size_t)L * (N + 2);
-    int G = want_G > 0 ? (want_G < L ? want_G : L) : L;
-    auto total = [&](int g, int nb) {
-        return nb * p.buf_doubles * sizeof(double) + dst_tab_doubles(N) * sizeof(double) +
-               2 * (size_t)g * crow(M) * sizeof(double2);
-    };
-    if (want_G <= 0)
-        while (G > 1 && total(G, 2) > 110 * 1024) --G;
-    p.G = G;
-    p.nbuf = total(G, 2) <= 200 * 1024 ? 2 : 1;
-    p.bytes = total(G, p.nbuf);
-    return p;
+__device__ __forceinline__ void cp8z(double* dst, const double* src, bool ok) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_commit_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-template <int PRO, int EPI>
-__global__ void __launch_bounds__(DST_THREADS) k_dst_rows(const Member* __restrict__ mems,
-                                                            const int* __restrict__ prefix, int nmem, int G,
-                                                            int nbuf, int row_offset, int total, size_t bufd) {
+// Row DST kernel.  A CTA holds R rows x L modes = L*R units of P lanes.
+//
+// Forward (EPI_SPEC, interior rows 1..jj-2): the raw layer rows are copied
+// asynchronously into the unit buffers (16-byte copies: node k of a row and
+// entry k of the buffer have the same alignment), projected onto the modes
+// in place (z_to_modes) and scaled by 0.5/(ii-1); PRO_STEP instead computes
+// the CABARET predictor + beta update per node in registers.  Each unit then
+// transforms its row and writes spec(m, j, k-1) = X_k.
+//
+// Inverse (EPI_HELM / EPI_PV, rows 0..jj-1): the solved spectral rows are
+// copied in (8-byte copies: spec offset k-1 -> buffer entry k), transformed, and written
+// out; for EPI_PV the correction rows corr_m (m >= 1) are prefetched into
+// shared memory before the transform and the mass-corrected back-projection
+// writes psi.
+template <int V, int PRO, int EPI>
+__global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
+                                             int nmem, int row_offset, int c, int corr_smem) {
     __shared__ Member Mb;
     extern __shared__ __align__(16) double sm[];
-    double* bufs[2] = {sm, sm + bufd};
-    double* tab = sm + nbuf * bufd;  // twiddle tables of the current member
-    double2* s_tw = reinterpret_cast<double2*>(tab);
-    double2* za = nullptr;  // set once the member's N is known
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
+    load_member(Mb, mems + mi);
+    __syncthreads();
+    const int L = Mb.L, N = Mb.N, M = Mb.M, logM = Mb.logM, n = Mb.n, ii = Mb.ii, jj = Mb.jj, pitch = Mb.pitch;
+    const long long ls = Mb.lstride;
+    const int P = M / V;
+    const int R = dst_rows_per_cta(M, L, c);
+    const int U = dst_unit_len(N);
+    const int j0 = row_offset + local * R;                 // first row of this CTA
+    const int jend = (EPI == EPI_SPEC) ? jj - 1 : jj;       // one past the last row
+    const int nthr = blockDim.x;
+    const int half = N >> 1;                                // 16-byte copies per row
+    double* corr_s = sm + (size_t)L * R * U;                // EPI_PV: [R][L-1][pitch]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = nthr >> 5;
 
-    // Asynchronous copies of a task's inputs into a staging buffer.
-    auto issue = [&](int task, double* buf) {
-        int loc;
-        const int mi = find_member(prefix, nmem, task, &loc);
-        const Member* M = mems + mi;
-        const int j = loc + row_offset;
-        const int L = M->L, n = M->n, N = M->N, jj = M->jj, pitch = M->pitch;
-        const long long ls = M->lstride;
-        const int xs = N + 2;
-        if (EPI == EPI_SPEC) {
-            if (PRO == PRO_STEP) return;  // loaded synchronously (needs four fields)
-            const double* src = reinterpret_cast<const double*>(PRO == PRO_PLAIN ? M->helm_io : M->zeta);
-            for (int l = 0; l < L; ++l) {
-                const double* g = src + l * ls + (long long)j * pitch;
-                for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) cp8(buf + l * xs + k, g + k);
+    // ---------------- stage the rows --------------------------------------
+    if (EPI == EPI_SPEC) {
+        const double cff = 0.5 / (double)(ii - 1);
+        if (PRO != PRO_STEP) {
+            const double* src = reinterpret_cast<const double*>(PRO == PRO_PLAIN ? Mb.helm_io : Mb.zeta);
+            // unit (r, l) <- layer l of row j0 + r, entries 0..N-1; one warp
+            // per unit row.
+            for (int rl = warp; rl < R * L; rl += nwarp) {
+                const int r = rl / L, l = rl - r * L;
+                const int j = j0 + r;
+                const bool ok = j < jend;
+                const double* g = src + l * ls + (long long)(ok ? j : 1) * pitch;
+                double* d = sm + (size_t)rl * U;
+                for (int q = lane; q < half; q += 32) cp16(d + 2 * q, g + 2 * q, ok);
             }
-        } else {
-            if (j >= 1 && j <= jj - 2) {
-                const double* spec = reinterpret_cast<const double*>(M->spec);
-                for (int m = 0; m < L; ++m) {
-                    const double* g = spec + m * ls + (long long)j * pitch - 1;
-                    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) cp8(buf + m * xs + k, g + k);
-                }
-            }
-        }
-    };
-
-    int cur_mi = -1, it = 0;
-    int task = blockIdx.x;
-    if (task < total) issue(task, bufs[0]);
-    cp_commit();
-    for (; task < total; task += gridDim.x, ++it) {
-        double* xr = bufs[nbuf == 2 ? (it & 1) : 0];
-        const int nt = task + gridDim.x;
-        if (nbuf == 2) {
-            if (nt < total) issue(nt, bufs[(it + 1) & 1]);
-            cp_commit();
-            cp_wait1();
-        } else {
-            cp_wait0();
-        }
-        __syncthreads();
-        int local;
-        const int mi = find_member(prefix, nmem, task, &local);
-        if (mi != cur_mi) {
-            load_member(Mb, mems + mi);
+            cp_commit_wait_all();
             __syncthreads();
-            // Stage this member's twiddle tables in shared memory.
-            const int Mm = Mb.M, Nn = Mb.N;
-            for (int t = threadIdx.x; t < Mm; t += blockDim.x) {
-                s_tw[t] = Mb.tw[t];
-                s_tw[Mm + t] = Mb.wsplit[t];
-            }
-            for (int t = threadIdx.x; t <= Nn / 2; t += blockDim.x) tab[4 * Mm + t] = Mb.was[t];
-            za = reinterpret_cast<double2*>(tab + dst_tab_doubles(Nn));
-            __syncthreads();
-            cur_mi = mi;
-        }
-        const double2* t_tw = s_tw;
-        const double2* t_ws = s_tw + Mb.M;
-        const double* t_was = tab + 4 * Mb.M;
-        const int j = local + row_offset;
-        const int L = Mb.L, N = Mb.N, n = Mb.n, ii = Mb.ii, jj = Mb.jj, pitch = Mb.pitch;
-        const long long ls = Mb.lstride;
-        const int xs = N + 2;
-        double2* zb = za + (size_t)G * crow(Mb.M);
-        const bool interior_row = (j >= 1 && j <= jj - 2);
-
-        if (EPI == EPI_SPEC) {
-            // ---------------- forward: prologue ----------------------------------
-            const double cff = 0.5 / (double)(ii - 1);
-            for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
-                const long long o = (long long)j * pitch + k;
-                double v[PQ_MAXL];
+            // In place: node k of the L layer rows -> node k of the L mode rows.
+            for (int r = 0; r < R; ++r)
+            for (int k = threadIdx.x; k < N; k += nthr) {
+                double* b = sm + (size_t)r * L * U + k;
                 double z[PQ_MAXL];
-                if (PRO == PRO_STEP) {
-                    const double dt = Mb.sc->dt, ta = Mb.sc->tweight_a;
-                    const double* zo = reinterpret_cast<const double*>(Mb.zeta_old[Mb.cur]);
-                    const double* rs = reinterpret_cast<const double*>(Mb.res);
-                    double* rb = reinterpret_cast<double*>(Mb.res_beta);
-                    const double* ui = reinterpret_cast<const double*>(Mb.ui);
-                    double* zp = reinterpret_cast<double*>(Mb.zeta);
-                    for (int l = 0; l < L; ++l) {
-                        const long long ol = o + l * ls;
-                        // cabaret_predictor, qg3p_aux.F90:1012-1018
-                        double zz = zo[ol] + 0.5 * dt * rs[ol];
-                        // cabaret_beta, qg3p_aux.F90:1051-1059
-                        const double rbn = dt * (0.5 * (ui[ol + 1] + ui[ol]) * Mb.beta[l]);
-                        zz = zz + (1.0 + ta) * rbn - ta * rb[ol];
-                        rb[ol] = rbn;
-                        zp[ol] = zz;
-                        z[l] = zz;
-                    }
-                } else {
-                    for (int l = 0; l < L; ++l) z[l] = xr[l * xs + k];
-                }
+#pragma unroll
+                for (int l = 0; l < PQ_MAXL; ++l)
+                    if (l < L) z[l] = b[(size_t)l * U];
                 if (PRO == PRO_PLAIN) {
-                    for (int m = 0; m < L; ++m) v[m] = z[m];
-                } else {
-                    // z_to_modes, qg3p_diagnostics.F90:545-549
-                    for (int m = 0; m < L; ++m) {
-                        double s = 0.0;
-                        for (int l = 0; l < L; ++l) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
-                        v[m] = s;
+#pragma unroll
+                    for (int m = 0; m < PQ_MAXL; ++m)
+                        if (m < L) b[(size_t)m * U] = cff * z[m];
+                    continue;
+                }
+#pragma unroll 1
+                for (int m = 0; m < L; ++m) {
+                    {
+                        double s;
+                        {
+                            // z_to_modes, qg3p_diagnostics.F90:545-549
+                            s = 0.0;
+#pragma unroll
+                            for (int l = 0; l < PQ_MAXL; ++l)
+                                if (l < L) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
+                        }
+                        b[(size_t)m * U] = cff * s;
                     }
                 }
-                for (int m = 0; m < L; ++m) xr[m * xs + k] = cff * v[m];
-            }
-            __syncthreads();
-            for (int m0 = 0; m0 < L; m0 += G)
-                dst_rows(xr + m0 * xs, xs, min(G, L - m0), za, zb, Mb, t_tw, t_ws, t_was);
-            double* spec = reinterpret_cast<double*>(Mb.spec);
-            for (int m = 0; m < L; ++m) {
-                double* g = spec + m * ls + (long long)j * pitch - 1;
-                for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) g[k] = xr[m * xs + k];
             }
         } else {
-            // ---------------- inverse: DST of the solved spectral rows ----------
-            if (interior_row)
-                for (int m0 = 0; m0 < L; m0 += G)
-                    dst_rows(xr + m0 * xs, xs, min(G, L - m0), za, zb, Mb, t_tw, t_ws, t_was);
-            if (EPI == EPI_HELM) {
-                // helm's in-place output: interior entries of interior rows, row
-                // i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1) (:1055-1057).
-                double* io = reinterpret_cast<double*>(Mb.helm_io);
-                if (interior_row) {
-                    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
-                        for (int m = 0; m < L; ++m) io[(long long)j * pitch + k + m * ls] = xr[m * xs + k];
-                    if (threadIdx.x == 0)
-                        for (int m = 0; m < L; ++m) io[(long long)j * pitch + (ii - 1) + m * ls] = 0.0;
-                } else if (j == 0) {
-                    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
-                        for (int m = 0; m < L; ++m) io[k + m * ls] = 0.0;
-                }
-            } else {
-                // psi_l = phi_1 - psiC_1 + sum_{m>=2} m2z(l,m) (phi_m - psiC_m corr_m)
-                // (modes_to_z_btcu) on every node of row j; phi is zero on the
-                // boundary (apply_dirichlet_bc(0), qg3p_aux.F90:470).
-                const double* psiC = Mb.sc->psiC;
-                const double* corr = Mb.corr;
-                double* psi = Mb.psi;
-                for (int i = threadIdx.x; i < ii; i += blockDim.x) {
-                    const bool inner = interior_row && i >= 1 && i <= n;
-                    const long long o = (long long)j * pitch + i;
-                    double ph[PQ_MAXL];
-                    for (int m = 0; m < L; ++m) ph[m] = inner ? xr[m * xs + i] : 0.0;
-                    for (int l = 0; l < L; ++l) {
-                        double dot = 0.0;
-                        for (int m = 1; m < L; ++m)
-                            dot += Mb.m2z[l * PQ_MAXL + m] * (ph[m] - psiC[m] * corr[o + m * ls]);
-                        psi[o + l * ls] = (ph[0] - psiC[0]) + dot;
+            const double dt = Mb.sc->dt, ta = Mb.sc->tweight_a;
+            const double* __restrict__ zo = reinterpret_cast<const double*>(Mb.zeta_old[Mb.cur]);
+            const double* __restrict__ rs = reinterpret_cast<const double*>(Mb.res);
+            const double* __restrict__ rbo = reinterpret_cast<const double*>(Mb.res_beta_other);
+            double* __restrict__ rb = reinterpret_cast<double*>(Mb.res_beta);
+            const double* __restrict__ ui = reinterpret_cast<const double*>(Mb.ui);
+            double* __restrict__ zp = reinterpret_cast<double*>(Mb.zeta);
+            for (int r = 0; r < R; ++r) {
+                const int j = j0 + r;
+                const bool ok = j < jend;
+                for (int k = 1 + threadIdx.x; k <= n; k += nthr) {
+                    const long long o = (long long)j * pitch + k;
+                    double a0[PQ_MAXL], a1[PQ_MAXL], a2[PQ_MAXL], a3[PQ_MAXL], a4[PQ_MAXL];
+                    // All loads of the node first, then the arithmetic and stores.
+#pragma unroll
+                    for (int l = 0; l < PQ_MAXL; ++l) {
+                        if (l < L && ok) {
+                            const long long ol = o + l * ls;
+                            a0[l] = zo[ol];
+                            a1[l] = rs[ol];
+                            a2[l] = ui[ol];
+                            a3[l] = ui[ol + 1];
+                            a4[l] = rbo[ol];
+                        }
+                    }
+                    double z[PQ_MAXL];
+#pragma unroll
+                    for (int l = 0; l < PQ_MAXL; ++l) {
+                        if (l < L) {
+                            double zz = 0.0;
+                            if (ok) {
+                                const long long ol = o + l * ls;
+                                // cabaret_predictor, qg3p_aux.F90:1012-1018
+                                zz = a0[l] + 0.5 * dt * a1[l];
+                                // cabaret_beta, qg3p_aux.F90:1051-1059
+                                const double rbn = dt * (0.5 * (a3[l] + a2[l]) * Mb.beta[l]);
+                                zz = zz + (1.0 + ta) * rbn - ta * a4[l];
+                                rb[ol] = rbn;
+                                zp[ol] = zz;
+                            }
+                            z[l] = zz;
+                        }
+                    }
+#pragma unroll 1
+                    for (int m = 0; m < L; ++m) {
+                        {
+                            double s = 0.0;
+#pragma unroll
+                            for (int l = 0; l < PQ_MAXL; ++l)
+                                if (l < L) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
+                            sm[(size_t)(r * L + m) * U + k] = cff * s;
+                        }
                     }
                 }
             }
         }
+    } else {
+        const double* spec = reinterpret_cast<const double*>(Mb.spec);
+        // unit (r, m) entries 1..n <- spec(m, j, 0..n-1); one warp per unit row
+        for (int rm = warp; rm < R * L; rm += nwarp) {
+            const int r = rm / L, m = rm - r * L;
+            const int j = j0 + r;
+            const bool ok = j >= 1 && j <= jj - 2 && j < jend;
+            const double* g = spec + m * ls + (long long)(ok ? j : 1) * pitch - 1;
+            double* d = sm + (size_t)rm * U;
+            for (int k = 1 + lane; k <= n; k += 32) cp8z(d + k, g + k, ok);
+        }
+        if (EPI == EPI_PV && corr_smem) {
+            const double* corr = Mb.corr;
+            const int cw = pitch >> 1;
+            for (int rm = warp; rm < R * (L - 1); rm += nwarp) {
+                const int r = rm / (L - 1), m = 1 + rm - r * (L - 1);
+                const int j = j0 + r;
+                const bool ok = j < jend;
+                const double* g = corr + m * ls + (long long)(ok ? j : 0) * pitch;
+                double* d = corr_s + (size_t)rm * pitch;
+                for (int q = lane; q < cw; q += 32) cp16(d + 2 * q, g + 2 * q, ok);
+            }
+        }
+        cp_commit_wait_all();
+    }
+    __syncthreads();
+
+    // ---------------- per-unit transform ----------------------------------
+    const int u = threadIdx.x / P, p = threadIdx.x & (P - 1);
+    const int ur = u / L, um = u - ur * L;
+    const int ju = j0 + ur;
+    double* buf = sm + (size_t)u * U;
+    const bool interior = ju >= 1 && ju <= jj - 2 && ju < jend;
+    dst_unit<V, double>(buf, p, P, N, M, logM, Mb.tw, Mb.wsplit, Mb.was);
+
+    if (EPI == EPI_SPEC) {
+        if (ju < jend) {
+            double* spec = reinterpret_cast<double*>(Mb.spec) + um * ls + (long long)ju * pitch - 1;
+            for (int k = 1 + p; k <= n; k += P) spec[k] = buf[xpad(k)];
+        }
+    } else if (EPI == EPI_HELM) {
+        // helm's in-place output: interior entries of interior rows, row
+        // i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1) (:1055-1057).
+        double* io = reinterpret_cast<double*>(Mb.helm_io) + um * ls + (long long)ju * pitch;
+        if (interior) {
+            for (int k = 1 + p; k <= n; k += P) io[k] = buf[xpad(k)];
+            if (p == 0) io[ii - 1] = 0.0;
+        } else if (ju == 0) {
+            for (int k = 1 + p; k <= n; k += P) io[k] = 0.0;
+        }
+    } else {
+        // psi_l = phi_1 - psiC_1 + sum_{m>=2} m2z(l,m) (phi_m - psiC_m corr_m)
+        // (modes_to_z_btcu, qg3p_diagnostics.F90:615-635) on every node of the
+        // row; phi is zero on the boundary (apply_dirichlet_bc(0),
+        // qg3p_aux.F90:470).
         __syncthreads();
-        if (nbuf == 1) {
-            if (nt < total) issue(nt, bufs[0]);
-            cp_commit();
+        const double* psiC = Mb.sc->psiC;
+        double pc[PQ_MAXL];
+#pragma unroll
+        for (int m = 0; m < PQ_MAXL; ++m) pc[m] = (m < L) ? psiC[m] : 0.0;
+        double* psi = Mb.psi;
+        for (int r = 0; r < R; ++r)
+        for (int i = threadIdx.x; i < ii; i += nthr) {
+            const int j = j0 + r;
+            if (j >= jend) break;
+            const bool inner = j >= 1 && j <= jj - 2 && i >= 1 && i <= n;
+            const double* row = sm + (size_t)(r * L) * U;
+            // corr_m at cr[m * cst] (staged rows, or the field itself)
+            const double* cr = corr_smem ? corr_s + ((long long)r * (L - 1) - 1) * pitch + i
+                                         : Mb.corr + (long long)j * pitch + i;
+            const long long cst = corr_smem ? (long long)pitch : ls;
+            double ph[PQ_MAXL];
+#pragma unroll
+            for (int m = 0; m < PQ_MAXL; ++m)
+                if (m < L) ph[m] = inner ? row[(size_t)m * U + xpad(i)] : 0.0;
+#pragma unroll
+            for (int m = 1; m < PQ_MAXL; ++m)
+                if (m < L) ph[m] -= pc[m] * cr[m * cst];
+            const double b0 = ph[0] - pc[0];
+            const long long o = (long long)j * pitch + i;
+#pragma unroll
+            for (int l = 0; l < PQ_MAXL; ++l) {
+                if (l < L) {
+                    double dot = 0.0;
+#pragma unroll
+                    for (int m = 1; m < PQ_MAXL; ++m)
+                        if (m < L) dot += Mb.m2z[l * PQ_MAXL + m] * ph[m];
+                    psi[o + l * ls] = b0 + dot;
+                }
+            }
         }
     }
-    cp_wait0();
 }
 
 // ---------------------------------------------------------------------------
@@ -641,22 +698,34 @@ __host__ __device__ inline size_t tri_smem_bytes(int jj) {
 
 // ---------------------------------------------------------------------------
 // Host launchers.
+template <int V, int PRO, int EPI>
+static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
+    const int M = ls.maxN / 2, L = ls.maxL;
+    const int R = dst_rows_per_cta(M, L, ls.dst_group);
+    const int threads = L * R * (M / V);
+    size_t bytes = (size_t)L * R * dst_unit_len(ls.maxN) * sizeof(double);
+    const size_t cbytes = (size_t)R * (L - 1) * ls.maxPitch * sizeof(double);
+    const int corr_smem = (EPI == EPI_PV && bytes + cbytes <= 200 * 1024) ? 1 : 0;
+    if (corr_smem) bytes += cbytes;
+    cudaError_t e = cudaFuncSetAttribute(k_dst<V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    const int rows = (EPI == EPI_SPEC) ? ls.maxJ - 2 : ls.maxJ;
+    const int grid = (rows + R - 1) / R;
+    k_dst<V, PRO, EPI><<<grid * ls.nmem, threads, bytes, st>>>(ls.members, ls.prefix_rows_interior, ls.nmem,
+                                                             EPI == EPI_SPEC ? 1 : 0, ls.dst_group, corr_smem);
+    return cudaGetLastError();
+}
+
 template <int PRO, int EPI>
 static cudaError_t launch_dst(const LaunchSet& ls, cudaStream_t st) {
-    const DstPlan p = dst_plan(ls.maxL, ls.maxN, ls.maxI, ls.dst_group, EPI == EPI_PV);
-    cudaError_t e = cudaFuncSetAttribute(k_dst_rows<PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.bytes);
-    if (e != cudaSuccess) return e;
-    const int* prefix = (EPI == EPI_SPEC) ? ls.prefix_rows_interior : ls.prefix_rows_all;
-    const int total = (EPI == EPI_SPEC) ? ls.ctas_rows_interior : ls.ctas_rows_all;
-    // Persistent grid: as many CTAs as fit on the device at once.
-    int per_sm = (int)((227 * 1024) / (p.bytes + 2048));
-    if (per_sm < 1) per_sm = 1;
-    if (per_sm > 4) per_sm = 4;
-    int grid = ls.sm_count * per_sm;
-    if (grid > total) grid = total;
-    k_dst_rows<PRO, EPI><<<grid, DST_THREADS, p.bytes, st>>>(ls.members, prefix, ls.nmem, p.G, p.nbuf,
-                                                            EPI == EPI_SPEC ? 1 : 0, total, p.buf_doubles);
-    return cudaGetLastError();
+    switch (dst_v(ls.maxN / 2)) {
+        case 2: return launch_dst_v<2, PRO, EPI>(ls, st);
+        case 4: return launch_dst_v<4, PRO, EPI>(ls, st);
+        case 8: return launch_dst_v<8, PRO, EPI>(ls, st);
+        case 16: return launch_dst_v<16, PRO, EPI>(ls, st);
+        case 32: return launch_dst_v<32, PRO, EPI>(ls, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, cudaStream_t st) {

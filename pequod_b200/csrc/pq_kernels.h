@@ -12,7 +12,7 @@ namespace pq {
 struct LaunchSet {
     const Member* members;  // device
     int nmem;
-    int maxL, maxN, maxJ, maxI;
+    int maxL, maxN, maxJ, maxI, maxPitch;
     const int* prefix_rows_interior;  // jj - 2 CTAs per member
     int ctas_rows_interior;
     const int* prefix_rows_all;       // jj CTAs per member
@@ -32,7 +32,8 @@ cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, cudaStream_t s
 cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, cudaStream_t st);
 
 // pq_cabaret.cu
-cudaError_t launch_cabaret_fused(const LaunchSet& ls, cudaStream_t st);
+// predict_next: also apply the next step's predictor + beta (fixed dt only)
+cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, cudaStream_t st);
 int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of k_cabaret_fused per member (band height sh)
 cudaError_t launch_rel(const LaunchSet& ls, cudaStream_t st);
 cudaError_t launch_energy(const LaunchSet& ls, cudaStream_t st);

@@ -220,13 +220,40 @@ def test_energy_kats_gpu():
     assert abs(ep - ep_o) <= 1e-13 * abs(ep_o)
 
 
-@pytest.mark.parametrize("band", [4, 8, 32, 128])
-def test_tile_parameters_do_not_change_results(band):
-    """The CABARET band height is a tuning knob: results must match the oracle for any choice."""
+@pytest.mark.parametrize("band,group", [(4, 0), (8, 1), (32, 2), (128, 1)])
+def test_tile_parameters_do_not_change_results(band, group):
+    """The CABARET band height and the DST CTA width are tuning knobs: results
+    must match the oracle for any choice."""
     cfg = double_gyre(129, 3)
     g, o = start(cfg, seed=5)
-    g.set_tuning(cab_band=band)
-    assert g.get_tuning()["cab_band"] == band
+    g.set_tuning(cab_band=band, dst_group=group)
+    assert g.get_tuning() == {"cab_band": band, "dst_group": group}
     g.step(3)
     o.step(3)
+    compare(g, o, TOL_STEP * 10)
+
+
+def test_state_writes_between_steps():
+    """Fixed-dt steps carry the next step's predictor in the fused CABARET
+    kernel; writing the state between steps must drop it and give the same
+    trajectory as the oracle."""
+    cfg = double_gyre(65, 3)
+    g, o = start(cfg, seed=6)
+    g.step(3)
+    o.step(3)
+    for f in ("zeta", "res", "res_beta", "ui"):
+        g.set(f, g.get(f))
+    g.step(2)
+    o.step(2)
+    compare(g, o, TOL_STEP * 10)
+    assert rel_l2(g.get("rel"), o.get("rel")) <= TOL_STEP * 10
+
+
+def test_odd_step_counts_match_oracle():
+    """Eager steps, two-step graphs and trailing steps interleave by parity."""
+    cfg = double_gyre(65, 3)
+    g, o = start(cfg, seed=7)
+    for n in (1, 3, 2, 5):
+        g.step(n)
+        o.step(n)
     compare(g, o, TOL_STEP * 10)
