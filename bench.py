@@ -50,13 +50,9 @@ def workload_args(a):
 
 
 def make_config(ii, layers, dt, precision=0):
-    import pequod_b200 as pq
+    from pequod_b200.workloads import double_gyre
 
-    H = {3: (3.0e4, 7.0e4, 3.0e5), 5: (2.5e4, 5.0e4, 7.5e4, 1.0e5, 1.5e5)}[layers]
-    gp = {3: (1.5, 0.75), 5: (1.5, 0.75, 0.375, 0.1875)}[layers]
-    dx = 3.84e8 / (ii - 1)
-    p = pq.double_gyre_physical(ii, layers=layers, dt=dt, dx=dx, H=H, gprime=gp, precision=precision)
-    return pq.Config.from_physical(p)
+    return double_gyre(ii, layers, dt, precision)
 
 
 class ClockSampler:
@@ -119,17 +115,19 @@ def peaks():
 
 
 def kernel_bytes_per_cell_layer(L, elem=8):
-    """Algorithmic bytes per cell-layer of each kernel of the FP64 step."""
+    """Algorithmic bytes per cell-layer of each kernel of the fixed-dt FP64 step
+    (each array the kernel must touch, read or written once)."""
     return {
-        # zeta_old, res, ui, res_beta in; zeta, res_beta, spectral rows out
-        "dst_forward": 7 * elem,
+        # zeta after predictor + beta in, spectral rows out
+        "dst_forward": 2 * elem,
         # spectral rows in and out
         "tridiag": 2 * elem,
-        # spectral rows in, corr for the baroclinic modes, psi out
+        # spectral rows in, corr of the baroclinic modes in, psi out
         "dst_inverse_backproject": (2 + (L - 1) / L) * elem,
-        # psi, zeta, zeta_old, uimo, ujmo, zeta_fi, zeta_fj, wind/L in;
-        # zeta_old, res, ui, uj, uimo, ujmo, zeta_fi, zeta_fj out
-        "cabaret_fused": (15 + 1.0 / L) * elem,
+        # in: psi, zeta, zeta_old, uimo, ujmo, zeta_fi, zeta_fj, res_beta, wind/L;
+        # out: zeta_old, res, ui, uj, uimo, ujmo, zeta_fi, zeta_fj, and the next
+        # step's zeta and res_beta
+        "cabaret_fused": (18 + 1.0 / L) * elem,
     }
 
 
