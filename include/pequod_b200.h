@@ -210,7 +210,9 @@ PQ_API int pq_cfl(pq_ctx* ctx, double* cfl);
 PQ_API int pq_get_field(pq_ctx* ctx, int field, double* out);
 PQ_API int pq_set_field(pq_ctx* ctx, int field, const double* in);
 
-/* dt, tweight_a, tweight_u, model_time (non-dimensional). */
+/* dt, tweight_a, tweight_u the last step ran with, and model_time
+ * (non-dimensional): the reference's state after a step (it adapts dt at the
+ * start of the next one, qg3.F90 timestep loop). */
 PQ_API int pq_get_scalars(pq_ctx* ctx, double* out4);
 
 /* Block until the context's queued device work is complete. */

@@ -10,7 +10,6 @@
 #include "pq_kernels.h"
 
 namespace pq {
-cudaError_t launch_init_finish(const LaunchSet& ls, cudaStream_t st);
 }
 
 using namespace pq;
@@ -45,6 +44,7 @@ struct pq_ctx {
     int cur = 0;          // parity of the next step
     bool initialized = false;
     bool fuse = false;        // fixed dt: the CABARET kernel applies the next predictor
+    bool mixed = false;       // PQ_PREC_MIXED
     bool pred_ready = false;  // zeta[cur] / res_beta[cur] already hold the next step's predictor
     int zpar = 0;             // parity whose zeta entered the last inversion
     cudaGraphExec_t graph2 = nullptr;
@@ -139,6 +139,22 @@ int copy_out(pq_ctx* c, double* dst, const void* src, int kind) {
     return PQ_OK;
 }
 
+// State fields (the CABARET fields, zeta and rel) are FP32 in the mixed
+// form: copies go through the FP64 helm_io field and a conversion kernel.
+int copy_in_state(pq_ctx* c, void* dst, const double* src, int kind) {
+    if (!c->mixed) return copy_in(c, dst, src, kind);
+    int rc = copy_in(c, c->hm[0].helm_io, src, kind);
+    if (rc) return rc;
+    CK(launch_convert(dst, c->hm[0].helm_io, (size_t)c->pitch * c->jj * c->L, 1, c->stream));
+    return PQ_OK;
+}
+
+int copy_out_state(pq_ctx* c, double* dst, const void* src, int kind) {
+    if (!c->mixed) return copy_out(c, dst, src, kind);
+    CK(launch_convert(c->hm[0].helm_io, src, (size_t)c->pitch * c->jj * c->L, 0, c->stream));
+    return copy_out(c, dst, c->hm[0].helm_io, kind);
+}
+
 int check_status(pq_ctx* c) {
     int st = 0;
     CK(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -155,9 +171,11 @@ int upload_members(pq_ctx* c) {
 
 // The three Helmholtz kernels.
 int run_helm(pq_ctx* c, int par, int prologue, int epilogue, int mean) {
-    CK(launch_dst_forward(c->ls[par], prologue, c->stream));
-    CK(launch_tridiag(c->ls[par], mean, c->stream));
-    CK(launch_dst_inverse(c->ls[par], epilogue, c->stream));
+    // The stand-alone helm entry (PRO_PLAIN / EPI_HELM) is always FP64.
+    const int f32 = (c->mixed && epilogue == EPI_PV) ? 1 : 0;
+    CK(launch_dst_forward(c->ls[par], prologue, f32, c->stream));
+    CK(launch_tridiag(c->ls[par], mean, f32, c->stream));
+    CK(launch_dst_inverse(c->ls[par], epilogue, f32, c->stream));
     return PQ_OK;
 }
 
@@ -171,13 +189,14 @@ int run_step(pq_ctx* c, int par) {
     }
     // The predictor + beta update runs in the forward DST unless the previous
     // fused step already produced this step's inversion input.
-    CK(launch_dst_forward(c->ls[par], (c->fuse && c->pred_ready) ? PRO_MODAL : PRO_STEP, c->stream));
+    const int f32 = c->mixed ? 1 : 0;
+    CK(launch_dst_forward(c->ls[par], (c->fuse && c->pred_ready) ? PRO_MODAL : PRO_STEP, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[1], c->stream));
-    CK(launch_tridiag(c->ls[par], 1, c->stream));
+    CK(launch_tridiag(c->ls[par], 1, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[2], c->stream));
-    CK(launch_dst_inverse(c->ls[par], EPI_PV, c->stream));
+    CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[3], c->stream));
-    CK(launch_cabaret_fused(c->ls[par], c->fuse ? 1 : 0, c->stream));
+    CK(launch_cabaret_fused(c->ls[par], c->fuse ? 1 : 0, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[4], c->stream));
     c->pred_ready = c->fuse;
     c->zpar = par;
@@ -212,7 +231,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     const int ii = d->ii, jj = d->jj, L = d->layers;
     if (ii < 5 || jj < 5 || !is_pow2(ii - 1) || L < 1 || L > PQ_MAX_LAYERS || d->periodic_j) return PQ_ERR_ARG;
     if (d->scheme != PQ_SCHEME_CABARET) return PQ_ERR_UNSUPPORTED;
-    if (d->precision != PQ_PREC_FP64) return PQ_ERR_UNSUPPORTED;
+    if (d->precision != PQ_PREC_FP64 && d->precision != PQ_PREC_MIXED) return PQ_ERR_UNSUPPORTED;
     pq_ctx* c = new pq_ctx;
     c->device = device;
     c->desc = *d;
@@ -265,7 +284,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     // Arena layout.
     const int nfields = 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 2 /*res_beta*/ + 1 /*ui*/ + 1 /*uj*/ +
                         2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ + 1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ +
-                        1 /*corr*/;
+                        1 /*corr*/ + 1 /*spec64*/;
     const size_t fb = align256(c->field_bytes);
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -278,6 +297,16 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     const size_t o_tw = take(M * sizeof(double2));
     const size_t o_ws = take(M * sizeof(double2));
     const size_t o_was = take(was.size() * sizeof(double));
+    std::vector<float2> tw_f(M), wsplit_f(M);
+    std::vector<float> was_f(was.size());
+    for (int t = 0; t < M; ++t) {
+        tw_f[t] = make_float2((float)tw[t].x, (float)tw[t].y);
+        wsplit_f[t] = make_float2((float)wsplit[t].x, (float)wsplit[t].y);
+    }
+    for (size_t k = 0; k < was.size(); ++k) was_f[k] = (float)was[k];
+    const size_t o_twf = take(M * sizeof(float2));
+    const size_t o_wsf = take(M * sizeof(float2));
+    const size_t o_wasf = take(was_f.size() * sizeof(float));
     const size_t o_wm = take(wmean.size() * sizeof(double));
     const size_t o_poff = take(pv.off.size() * sizeof(int));
     const size_t o_plen = take(pv.len.size() * sizeof(int));
@@ -297,6 +326,9 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     CK(cudaMemcpyAsync(A + o_tw, tw.data(), M * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_ws, wsplit.data(), M * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_was, was.data(), was.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_twf, tw_f.data(), M * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_wsf, wsplit_f.data(), M * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_wasf, was_f.data(), was_f.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_wm, wmean.data(), wmean.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_poff, pv.off.data(), pv.off.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_plen, pv.len.data(), pv.len.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -338,6 +370,11 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     m.tw = reinterpret_cast<const double2*>(A + o_tw);
     m.wsplit = reinterpret_cast<const double2*>(A + o_ws);
     m.was = reinterpret_cast<const double*>(A + o_was);
+    m.tw_f = reinterpret_cast<const float2*>(A + o_twf);
+    m.wsplit_f = reinterpret_cast<const float2*>(A + o_wsf);
+    m.was_f = reinterpret_cast<const float*>(A + o_wasf);
+    m.mixed = d->precision == PQ_PREC_MIXED ? 1 : 0;
+    c->mixed = m.mixed != 0;
     m.wmean = reinterpret_cast<const double*>(A + o_wm);
     m.piv_off = reinterpret_cast<const int*>(A + o_poff);
     m.piv_len = reinterpret_cast<const int*>(A + o_plen);
@@ -368,6 +405,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     m.helm_io = fld();
     m.spec = fld();
     m.corr = (const double*)fld();
+    m.spec64 = (double*)fld();
     m.wind = c->wind.empty() ? nullptr : reinterpret_cast<const double*>(A + o_wind);
     m.partials = reinterpret_cast<double*>(A + o_part);
     m.maxu_part = reinterpret_cast<double*>(A + o_maxu);
@@ -421,9 +459,9 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     // Scalars: dt and the initial time weights.
     Scalars sc;
     std::memset(&sc, 0, sizeof(sc));
-    sc.dt = d->dt;
-    sc.tweight_a = 0.5;
-    sc.tweight_u = 0.5;
+    sc.dt = sc.dt_last = d->dt;
+    sc.tweight_a = sc.tweight_a_last = 0.5;
+    sc.tweight_u = sc.tweight_u_last = 0.5;
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
 
     // Correction function for mass conservation, correction_function_mass
@@ -475,7 +513,7 @@ int pq_helm(pq_ctx* c, double* zeta, int ptr_kind) {
 int pq_pv_inversion(pq_ctx* c, const double* zeta, double* psi, int ptr_kind) {
     if (!c || !zeta || !psi) return PQ_ERR_ARG;
     CK(cudaSetDevice(c->device));
-    int rc = copy_in(c, c->hm[c->cur].zeta, zeta, ptr_kind);
+    int rc = copy_in_state(c, c->hm[c->cur].zeta, zeta, ptr_kind);
     if (rc) return rc;
     c->pred_ready = false;
     c->zpar = c->cur;
@@ -509,7 +547,7 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     // ui, uj, uimo[2], ujmo[2], zeta_fi[2], zeta_fj[2], zeta[1], res_beta[1]
     // (corr is kept).
     CK(cudaMemsetAsync(m.zeta_old[0], 0, fb * 18, c->stream));
-    int rc = copy_in(c, m.zeta, z.data(), PQ_PTR_HOST);
+    int rc = copy_in_state(c, m.zeta, z.data(), PQ_PTR_HOST);
     if (rc) return rc;
     Scalars sc;
     std::memset(&sc, 0, sizeof(sc));
@@ -517,17 +555,20 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     sc.tweight_a = 0.5;
     sc.tweight_u = 0.5;
     sc.model_time = c->desc.dt / 2.0;
+    sc.dt_last = sc.dt;
+    sc.tweight_a_last = sc.tweight_a;
+    sc.tweight_u_last = sc.tweight_u;
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
     // zeta was cleared together with the other fields; upload it again.
-    rc = copy_in(c, m.zeta, z.data(), PQ_PTR_HOST);
+    rc = copy_in_state(c, m.zeta, z.data(), PQ_PTR_HOST);
     if (rc) return rc;
     c->cur = 0;
     c->zpar = 0;
     c->pred_ready = false;
     rc = run_helm(c, 0, PRO_MODAL, EPI_PV, 1);
     if (rc) return rc;
-    CK(launch_init_finish(c->ls[0], c->stream));
+    CK(launch_init_finish(c->ls[0], c->mixed ? 1 : 0, c->stream));
     c->initialized = true;
     return check_status(c);
 }
@@ -548,7 +589,7 @@ int pq_step_exchange(pq_ctx* c, const double* zeta_in, double* psi_out, int ptr_
     if (!c->initialized) return fail(c, PQ_ERR_STATE, "pq_step_exchange before pq_init_perturb");
     CK(cudaSetDevice(c->device));
     if (zeta_in) {
-        int rc = copy_in(c, c->hm[c->cur].zeta_old[c->cur], zeta_in, ptr_kind);
+        int rc = copy_in_state(c, c->hm[c->cur].zeta_old[c->cur], zeta_in, ptr_kind);
         if (rc) return rc;
         c->pred_ready = false;
     }
@@ -687,7 +728,7 @@ int pq_cfl(pq_ctx* c, double* cfl) {
     Scalars sc;
     CK(cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    *cfl = sc.max_u * sc.dt;
+    *cfl = sc.cfl;  // max |u| times the dt of the step that produced u
     return PQ_OK;
 }
 
@@ -696,9 +737,9 @@ int pq_get_scalars(pq_ctx* c, double* out4) {
     Scalars sc;
     CK(cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    out4[0] = sc.dt;
-    out4[1] = sc.tweight_a;
-    out4[2] = sc.tweight_u;
+    out4[0] = sc.dt_last;
+    out4[1] = sc.tweight_a_last;
+    out4[2] = sc.tweight_u_last;
     out4[3] = sc.model_time;
     return PQ_OK;
 }
@@ -763,9 +804,10 @@ int pq_get_field(pq_ctx* c, int field, double* out) {
     RefShape s;
     if (!ref_shape(field, c->ii, c->jj, &s)) return fail(c, PQ_ERR_ARG, "unknown field");
     CK(cudaSetDevice(c->device));
-    if (field == PQ_F_REL) CK(launch_rel(c->ls[c->zpar], c->stream));
+    if (field == PQ_F_REL) CK(launch_rel(c->ls[c->zpar], c->mixed ? 1 : 0, c->stream));
     std::vector<double> dense((size_t)c->ii * c->jj * c->L);
-    int rc = copy_out(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST);
+    int rc = (field == PQ_F_PSI || field == PQ_F_CORR) ? copy_out(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST)
+                                                      : copy_out_state(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST);
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
     const size_t n = (size_t)s.n1 * s.n2 * c->L;
@@ -789,10 +831,11 @@ int pq_set_field(pq_ctx* c, int field, const double* in) {
             for (int i = 0; i < c->ii; ++i)
                 dense[(size_t)i + (size_t)c->ii * (j + (size_t)c->jj * l)] =
                     in[(size_t)(i + s.oi) + (size_t)s.n1 * ((j + s.oj) + (size_t)s.n2 * l)];
-    int rc = copy_in(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST);
+    int rc = (field == PQ_F_PSI) ? copy_in(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST)
+                                 : copy_in_state(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST);
     if (rc) return rc;
     if (field == PQ_F_ZETA) {
-        rc = copy_in(c, c->hm[c->cur].zeta, dense.data(), PQ_PTR_HOST);
+        rc = copy_in_state(c, c->hm[c->cur].zeta, dense.data(), PQ_PTR_HOST);
         c->zpar = c->cur;
     }
     if (rc) return rc;

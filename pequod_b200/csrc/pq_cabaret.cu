@@ -82,6 +82,8 @@ constexpr int CAB_RING = CAB_D * CAB_NF * 32;  // doubles per warp
 
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ float shup(float v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ float shdn(float v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 
 // One warp's sweep over layer l of the strip starting at column i0 and the
 // band starting at row j0.  EDGE = false is the specialisation for warps
@@ -89,9 +91,13 @@ __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_syn
 // at least two nodes inside the domain: no bounds checks, no boundary
 // branches.  PRED = true also applies the next step's cabaret_predictor and
 // cabaret_beta (fixed dt) to every interior node it finishes, writing the
-// next step's inversion input zeta_next and res_beta_other.  Returns the
-// largest |u| of the faces it wrote.
-template <bool EDGE, bool PRED>
+// next step's inversion input zeta_next and res_beta_other.  T is the type
+// of the CABARET fields (double, or float in the mixed form); psi is FP64
+// and everything computed from psi differences (the rel coupling, the
+// boundary rel, the corner streamfunction and the face velocities before
+// the time weighting) is evaluated in FP64.  Returns the largest |u| of the
+// faces it wrote.
+template <bool EDGE, bool PRED, typename T>
 __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int j0, int lane, double* ring) {
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
@@ -99,39 +105,43 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const bool in_i = !EDGE || (i >= 0 && i < ii);
     const bool out_i = (lane >= 2 && lane < 2 + CAB_SW && in_i);  // owner of node / i-face / j-face column i
     const int cur = Mb.cur, nxt = cur ^ 1;
-    const double dt = Mb.sc->dt, tu = Mb.sc->tweight_u;
-    const double hdt = 0.5 * dt;
+    const double dt64 = Mb.sc->dt;
+    const T dt = (T)dt64, tu = (T)Mb.sc->tweight_u;
+    const T hdt = (T)0.5 * dt;
     const int SH = Mb.cab_sh;
     // All fields of a member live in one allocation: address them by 32-bit
-    // element offsets from one base (fewer live registers than 16 pointers).
+    // element offsets from one base (fewer live registers than 16 pointers);
+    // FP64 fields (psi, wind) from B, T fields from BT.
     const double* B = Mb.psi;
+    const T* BT = reinterpret_cast<const T*>(B);
     auto ofs = [&](const void* f) { return (int)(reinterpret_cast<const double*>(f) - B); };
+    auto ofst = [&](const void* f) { return (int)(reinterpret_cast<const T*>(f) - BT); };
     const int lo = (int)(l * ls) + i;  // layer and column part of every offset
     const int o_psil = lo;
     const int o_psim = (l > 0) ? lo - (int)ls : lo;
     const int o_psip = (l < L - 1) ? lo + (int)ls : lo;
-    const int o_zpb = ofs(Mb.zeta) + lo;
-    const int o_zo = ofs(Mb.zeta_old[cur]) + lo;
-    const int o_zn = ofs(Mb.zeta_old[nxt]) + lo;
-    const int o_res = ofs(Mb.res) + lo;
-    const int o_ui = ofs(Mb.ui) + lo;
-    const int o_uj = ofs(Mb.uj) + lo;
-    const int o_uimo = ofs(Mb.uimo[cur]) + lo;
-    const int o_uimon = ofs(Mb.uimo[nxt]) + lo;
-    const int o_ujmo = ofs(Mb.ujmo[cur]) + lo;
-    const int o_ujmon = ofs(Mb.ujmo[nxt]) + lo;
-    const int o_fio = ofs(Mb.zfi[cur]) + lo;
-    const int o_fin = ofs(Mb.zfi[nxt]) + lo;
-    const int o_fjo = ofs(Mb.zfj[cur]) + lo;
-    const int o_fjn = ofs(Mb.zfj[nxt]) + lo;
-    const int o_rb = PRED ? ofs(Mb.res_beta) + lo : 0;
-    const int o_rbn = PRED ? ofs(Mb.res_beta_other) + lo : 0;
-    const int o_zpn = PRED ? ofs(Mb.zeta_next) + lo : 0;
-    const double ta = Mb.sc->tweight_a, beta_l = Mb.beta[l];
+    const int o_zpb = ofst(Mb.zeta) + lo;
+    const int o_zo = ofst(Mb.zeta_old[cur]) + lo;
+    const int o_zn = ofst(Mb.zeta_old[nxt]) + lo;
+    const int o_res = ofst(Mb.res) + lo;
+    const int o_ui = ofst(Mb.ui) + lo;
+    const int o_uj = ofst(Mb.uj) + lo;
+    const int o_uimo = ofst(Mb.uimo[cur]) + lo;
+    const int o_uimon = ofst(Mb.uimo[nxt]) + lo;
+    const int o_ujmo = ofst(Mb.ujmo[cur]) + lo;
+    const int o_ujmon = ofst(Mb.ujmo[nxt]) + lo;
+    const int o_fio = ofst(Mb.zfi[cur]) + lo;
+    const int o_fin = ofst(Mb.zfi[nxt]) + lo;
+    const int o_fjo = ofst(Mb.zfj[cur]) + lo;
+    const int o_fjn = ofst(Mb.zfj[nxt]) + lo;
+    const int o_rb = PRED ? ofst(Mb.res_beta) + lo : 0;
+    const int o_rbn = PRED ? ofst(Mb.res_beta_other) + lo : 0;
+    const int o_zpn = PRED ? ofst(Mb.zeta_next) + lo : 0;
+    const T ta = (T)Mb.sc->tweight_a, beta_l = (T)Mb.beta[l];
     const bool has_wind = (l == 0 && Mb.wind);
     const int o_wind = has_wind ? ofs(Mb.wind) + i : 0;
-    double* W = const_cast<double*>(B);
-    const double nu = Mb.viscosity, vb = Mb.visc_bot;
+    T* W = const_cast<T*>(BT);
+    const T nu = (T)Mb.viscosity, vb = (T)Mb.visc_bot;
     const double s1 = Mb.s1[l], s2 = Mb.s2[l];
     const int bc = Mb.bc_type;
     const double cffbc = Mb.alpha / (Mb.alpha + 3.0);
@@ -144,34 +154,34 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         return B[off + row * pitch];
     };
     // rel_from_zeta_and_psi coupling for an interior node.
-    auto rel_int = [&](double z, double p, double pm, double pp) -> double {
+    auto rel_int = [&](T z, double p, double pm, double pp) -> T {
         if (L == 1) return z;
-        if (top) return z + s2 * (p - pp);
-        if (bottom) return z + s1 * (p - pm);
-        return z + s1 * (p - pm) + s2 * (p - pp);
+        if (top) return (T)((double)z + s2 * (p - pp));
+        if (bottom) return (T)((double)z + s1 * (p - pm));
+        return (T)((double)z + s1 * (p - pm) + s2 * (p - pp));
     };
     // Limited upwind extrapolation (cabaret_extrapolator, interior branch).
-    auto extrap = [&](double u1, double u2, double fi1, double fi2, double psi_n, double psi_o, bool pos) -> double {
-        const double v0 = (u1 + u2) / 2.0;
-        const double d_f = pos ? -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2)
-                               : -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
-        double v = 2.0 * psi_n - fi2;
+    auto extrap = [&](T u1, T u2, T fi1, T fi2, T psi_n, T psi_o, bool pos) -> T {
+        const T v0 = (u1 + u2) / (T)2;
+        const T d_f = pos ? -(psi_n - psi_o) * (T)2 - dt * v0 * (fi1 - fi2)
+                          : -(psi_n - psi_o) * (T)2 - dt * v0 * (fi2 - fi1);
+        T v = (T)2 * psi_n - fi2;
         if (lim) {
-            const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
-            const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+            const T fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+            const T fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
             if (v > fmx) v = fmx;
             if (v < fmn) v = fmn;
         }
         return v;
     };
     // The wall branch of the extrapolator: upwind node on the boundary.
-    auto extrap_wall = [&](double fi1, double psi_n, double psi_o) -> double {
-        const double fi2 = psi_n;
-        const double d_f = -(psi_n - psi_o);
-        double v = 2.0 * psi_n - fi2;
+    auto extrap_wall = [&](T fi1, T psi_n, T psi_o) -> T {
+        const T fi2 = psi_n;
+        const T d_f = -(psi_n - psi_o);
+        T v = (T)2 * psi_n - fi2;
         if (lim) {
-            const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
-            const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+            const T fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+            const T fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
             if (v > fmx) v = fmx;
             if (v < fmn) v = fmn;
         }
@@ -179,50 +189,64 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     };
 
     // Rolling windows.
-    // Row copies of iteration r into ring stage r % CAB_D (cp.async, 8 bytes
-    // per lane; rows outside the domain, and zeta at non-interior nodes, are
+    // Row copies of iteration r into ring stage r % CAB_D (cp.async per lane;
+    // rows outside the domain, and zeta at non-interior nodes, are
     // zero-filled by a source size of 0 with the source clamped in range).
+    // Every field has a slot of 32 doubles per stage; T fields use its start.
     const int rend = j0 + SH + 4;
-    auto cp = [&](double* dst, int off, int row, bool ok) {
+    auto cp64 = [&](double* slot, int off, int row, bool ok) {
         const int rr = ok ? row : 0;
-        const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(slot + lane);
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(B + (off + rr * pitch)),
                      "r"(ok ? 8 : 0)
                      : "memory");
     };
+    auto cpt = [&](double* slot, int off, int row, bool ok) {
+        const int rr = ok ? row : 0;
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(reinterpret_cast<T*>(slot) + lane);
+        if (sizeof(T) == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(BT + (off + rr * pitch)),
+                         "r"(ok ? 8 : 0)
+                         : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(BT + (off + rr * pitch)),
+                         "r"(ok ? 4 : 0)
+                         : "memory");
+    };
     auto rowok = [&](int row) { return !EDGE || (in_i && row >= 0 && row < jj); };
     auto issue = [&](int rr) {
         const int ss = rr - 2;
-        double* d = ring + ((rr % CAB_D) * CAB_NF << 5) + lane;
-        cp(d + (F_PSI2 << 5), o_psil, ss + 2, rowok(ss + 2));
+        double* d = ring + ((rr % CAB_D) * CAB_NF << 5);
+        cp64(d + (F_PSI2 << 5), o_psil, ss + 2, rowok(ss + 2));
         const bool intn = !EDGE || (in_i && i > 0 && i < ii - 1 && ss > 0 && ss < jj - 1);
-        cp(d + (F_ZPB << 5), o_zpb, ss, intn);
+        cpt(d + (F_ZPB << 5), o_zpb, ss, intn);
         if (L > 1) {
-            cp(d + (F_PSIM << 5), o_psim, ss, rowok(ss));
-            cp(d + (F_PSIP << 5), o_psip, ss, rowok(ss));
+            cp64(d + (F_PSIM << 5), o_psim, ss, rowok(ss));
+            cp64(d + (F_PSIP << 5), o_psip, ss, rowok(ss));
         }
-        cp(d + (F_ZO << 5), o_zo, ss - 1, rowok(ss - 1));
-        cp(d + (F_UIMO << 5), o_uimo, ss - 1, rowok(ss - 1));
-        cp(d + (F_UJMO << 5), o_ujmo, ss, rowok(ss));
-        cp(d + (F_FIO << 5), o_fio, ss - 1, rowok(ss - 1));
-        cp(d + (F_FJ << 5), o_fjo, ss, rowok(ss));
-        if (has_wind) cp(d + (F_WIND << 5), o_wind, ss - 1, rowok(ss - 1));
-        if (PRED) cp(d + (F_RB << 5), o_rb, ss - 2, rowok(ss - 2));
+        cpt(d + (F_ZO << 5), o_zo, ss - 1, rowok(ss - 1));
+        cpt(d + (F_UIMO << 5), o_uimo, ss - 1, rowok(ss - 1));
+        cpt(d + (F_UJMO << 5), o_ujmo, ss, rowok(ss));
+        cpt(d + (F_FIO << 5), o_fio, ss - 1, rowok(ss - 1));
+        cpt(d + (F_FJ << 5), o_fjo, ss, rowok(ss));
+        if (has_wind) cp64(d + (F_WIND << 5), o_wind, ss - 1, rowok(ss - 1));
+        if (PRED) cpt(d + (F_RB << 5), o_rb, ss - 2, rowok(ss - 2));
     };
     for (int rr = j0; rr < j0 + CAB_D - 1; ++rr) {
         issue(rr);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     double P0 = 0, P1 = ld(o_psil, j0 - 4), P2 = ld(o_psil, j0 - 3), P3 = ld(o_psil, j0 - 2), P4 = ld(o_psil, j0 - 1);
-    double Rm2 = 0, Rm1 = 0;    // rel rows s-2, s-1
-    double ZFm2 = 0;            // zeta after forcing, row s-2
-    double ZOm2 = 0;            // zeta_old row s-2
-    double UJm2 = 0, UJm1 = 0;  // uj faces s-2, s-1
-    double FJm2 = 0, FJm1 = 0;  // zeta_fj (old) faces s-2, s-1
-    double FLJm2 = 0;           // flux_j face s-2
-    double FLI = 0;             // flux_i row s-2 (face a = i)
-    double UIm2 = 0;            // ui row s-2 (face a = i)
-    double zpb_prev = 0, pm_prev = 0, pp_prev = 0, pe_prev = 0;
+    T Rm2 = 0, Rm1 = 0;    // rel rows s-2, s-1
+    T ZFm2 = 0;            // zeta after forcing, row s-2
+    T ZOm2 = 0;            // zeta_old row s-2
+    T UJm2 = 0, UJm1 = 0;  // uj faces s-2, s-1
+    T FJm2 = 0, FJm1 = 0;  // zeta_fj (old) faces s-2, s-1
+    T FLJm2 = 0;           // flux_j face s-2
+    T FLI = 0;             // flux_i row s-2 (face a = i)
+    T UIm2 = 0;            // ui row s-2 (face a = i)
+    T zpb_prev = 0;
+    double pm_prev = 0, pp_prev = 0, pe_prev = 0;
 
 #pragma unroll 1
     for (int r = j0; r < rend; ++r) {
@@ -232,23 +256,25 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         if (r + CAB_D - 1 < rend) issue(r + CAB_D - 1);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group %0;\n" ::"n"(CAB_D - 1) : "memory");
-        const double* st = ring + ((r % CAB_D) * CAB_NF << 5) + lane;
+        const double* st = ring + ((r % CAB_D) * CAB_NF << 5);
+        auto get64 = [&](int f) { return st[(f << 5) + lane]; };
+        auto gett = [&](int f) { return reinterpret_cast<const T*>(st + (f << 5))[lane]; };
         P0 = P1;
         P1 = P2;
         P2 = P3;
         P3 = P4;
-        P4 = st[F_PSI2 << 5];
+        P4 = get64(F_PSI2);
         const bool node_s = !EDGE || (in_i && s >= 0 && s < jj);
-        const double zpb_s = st[F_ZPB << 5];
-        const double pm_s = (L > 1) ? st[F_PSIM << 5] : 0.0;
-        const double pp_s = (L > 1) ? st[F_PSIP << 5] : 0.0;
-        const double zo_1 = st[F_ZO << 5];
-        const double uimo_1 = st[F_UIMO << 5];
-        const double ujmo_s = st[F_UJMO << 5];
-        const double fio_1 = st[F_FIO << 5];
-        const double fj_s = st[F_FJ << 5];
-        const double w_1 = has_wind ? st[F_WIND << 5] : 0.0;
-        const double rb_2 = PRED ? st[F_RB << 5] : 0.0;
+        const T zpb_s = gett(F_ZPB);
+        const double pm_s = (L > 1) ? get64(F_PSIM) : 0.0;
+        const double pp_s = (L > 1) ? get64(F_PSIP) : 0.0;
+        const T zo_1 = gett(F_ZO);
+        const T uimo_1 = gett(F_UIMO);
+        const T ujmo_s = gett(F_UJMO);
+        const T fio_1 = gett(F_FIO);
+        const T fj_s = gett(F_FJ);
+        const T w_1 = has_wind ? (T)get64(F_WIND) : (T)0;
+        const T rb_2 = PRED ? gett(F_RB) : (T)0;
 
         // ---- rel(s): rel_from_zeta_and_psi + apply_rel_bc -------------------
         double up1 = 0.0, up2 = 0.0, dn1 = 0.0, dn2 = 0.0;
@@ -260,7 +286,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         } else {
             up1 = shup(P2, 1);
         }
-        double rel_s = 0.0;
+        T rel_s = 0;
         if (!EDGE) {
             rel_s = rel_int(zpb_s, P2, pm_s, pp_s);
         } else if (node_s) {
@@ -275,7 +301,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
                         q1 = (i == 0) ? dn1 : up1;
                         q2 = (i == 0) ? dn2 : up2;
                     }
-                    rel_s = (bc == 1) ? cffbc * (-3.5 * P2 + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - P2);
+                    rel_s = (T)((bc == 1) ? cffbc * (-3.5 * P2 + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - P2));
                 }
             } else {
                 rel_s = rel_int(zpb_s, P2, pm_s, pp_s);
@@ -284,8 +310,8 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
 
         // ---- zeta at row s-1 after update_zeta_bc and cabaret_forcing -------
         const int s1r = s - 1;
-        const double rl_up = shup(Rm1, 1), rl_dn = shdn(Rm1, 1);
-        double zf_1 = 0.0;
+        const T rl_up = shup(Rm1, 1), rl_dn = shdn(Rm1, 1);
+        T zf_1 = 0;
         const bool node_1 = !EDGE || (in_i && s1r >= 0 && s1r < jj);
         if (node_1) {
             const bool bnd = EDGE && (s1r == 0 || s1r == jj - 1 || i == 0 || i == ii - 1);
@@ -293,14 +319,14 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
                 if (L == 1)
                     zf_1 = Rm1;
                 else if (top)
-                    zf_1 = Rm1 - s2 * (P1 - pp_prev);
+                    zf_1 = (T)((double)Rm1 - s2 * (P1 - pp_prev));
                 else if (bottom)
-                    zf_1 = Rm1 - s1 * (P1 - pm_prev);
+                    zf_1 = (T)((double)Rm1 - s1 * (P1 - pm_prev));
                 else
-                    zf_1 = Rm1 - s1 * (P1 - pm_prev) - s2 * (P1 - pp_prev);
+                    zf_1 = (T)((double)Rm1 - s1 * (P1 - pm_prev) - s2 * (P1 - pp_prev));
             } else {
-                const double lap = -4.0 * Rm1 + rl_up + rl_dn + Rm2 + rel_s;
-                double rv;
+                const T lap = (T)-4 * Rm1 + rl_up + rl_dn + Rm2 + rel_s;
+                T rv;
                 if (L == 1)
                     rv = dt * (w_1 - vb * Rm1 + nu * lap);
                 else if (top)
@@ -317,26 +343,26 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         // pe_here: corner between nodes (i-1, i) x (s-1, s).
         const double pe_here = 0.25 * (P2 + P1 + up1 + shup(P1, 1));
         const double pe_dn = shdn(pe_here, 1);
-        double uj_s = 0.0, ujm_s = 0.0;  // face b = s, column i
+        T uj_s = 0, ujm_s = 0;  // face b = s, column i
         const bool fj_ok = !EDGE || (s >= 1 && s <= jj - 1 && i >= 1 && i <= ii - 2);
         if (fj_ok) {
-            ujm_s = pe_dn - pe_here;
-            uj_s = (1.0 + tu) * ujm_s - tu * ujmo_s;
+            ujm_s = (T)(pe_dn - pe_here);
+            uj_s = ((T)1 + tu) * ujm_s - tu * ujmo_s;
         }
-        double ui_1 = 0.0, uim_1 = 0.0;  // row s-1, face a = i
+        T ui_1 = 0, uim_1 = 0;  // row s-1, face a = i
         const bool fi_ok = !EDGE || (i >= 1 && i <= ii - 1 && s1r >= 1 && s1r <= jj - 2);
         if (fi_ok) {
-            uim_1 = -pe_here + pe_prev;
-            ui_1 = (1.0 + tu) * uim_1 - tu * uimo_1;
+            uim_1 = (T)(-pe_here + pe_prev);
+            ui_1 = ((T)1 + tu) * uim_1 - tu * uimo_1;
         }
 
         // ---- extrapolator, j-faces: face b = s-1 -------------------------------
-        double fjn = 0.0;
+        T fjn = 0;
         const int bf = s - 1;
         const bool bfj_ok = !EDGE || (bf >= 1 && bf <= jj - 1 && i >= 1 && i <= ii - 2);
         if (bfj_ok) {
-            const double u1 = UJm1;
-            if (u1 >= 0.0)
+            const T u1 = UJm1;
+            if (u1 >= (T)0)
                 fjn = (!EDGE || bf > 1) ? extrap(u1, UJm2, FJm1, FJm2, ZFm2, ZOm2, true) : extrap_wall(FJm1, ZFm2, ZOm2);
             else
                 fjn = (!EDGE || bf < jj - 1) ? extrap(u1, uj_s, FJm1, fj_s, zf_1, zo_1, false)
@@ -344,40 +370,40 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         }
 
         // ---- extrapolator, i-faces on row s-1: face a = i ------------------------
-        const double ui_up = shup(ui_1, 1), ui_dn = shdn(ui_1, 1);
-        const double fi_up = shup(fio_1, 1), fi_dn = shdn(fio_1, 1);
-        const double zf_up = shup(zf_1, 1), zo_up = shup(zo_1, 1);
-        double fin = 0.0;
+        const T ui_up = shup(ui_1, 1), ui_dn = shdn(ui_1, 1);
+        const T fi_up = shup(fio_1, 1), fi_dn = shdn(fio_1, 1);
+        const T zf_up = shup(zf_1, 1), zo_up = shup(zo_1, 1);
+        T fin = 0;
         if (fi_ok) {
-            const double u1 = ui_1;
-            if (u1 >= 0.0)
+            const T u1 = ui_1;
+            if (u1 >= (T)0)
                 fin = (!EDGE || i > 1) ? extrap(u1, ui_up, fio_1, fi_up, zf_up, zo_up, true)
                                        : extrap_wall(fio_1, zf_up, zo_up);
             else
                 fin = (!EDGE || i < ii - 1) ? extrap(u1, ui_dn, fio_1, fi_dn, zf_1, zo_1, false)
                                             : extrap_wall(fio_1, zf_1, zo_1);
         }
-        const double flj_1 = UJm1 * fjn;  // flux_j on face s-1
-        const double fli_1 = ui_1 * fin;  // flux_i on row s-1, face i
+        const T flj_1 = UJm1 * fjn;  // flux_j on face s-1
+        const T fli_1 = ui_1 * fin;  // flux_i on row s-1, face i
 
         // ---- corrector at row o = s-2 -----------------------------------------
         const int o = s - 2;
-        const double fli_dn = shdn(FLI, 1);
-        const double ui_e = PRED ? shdn(UIm2, 1) : 0.0;  // ui on face a = i + 1, row o
+        const T fli_dn = shdn(FLI, 1);
+        const T ui_e = PRED ? shdn(UIm2, 1) : (T)0;  // ui on face a = i + 1, row o
         const bool band_o = (o >= j0 && o < j0 + SH) && (!EDGE || (o >= 0 && o < jj));
         if (out_i && band_o) {
             const bool bnd = EDGE && (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
-            double z = ZFm2;
+            T z = ZFm2;
             if (!bnd) {
-                const double rr = -(fli_dn - FLI + flj_1 - FLJm2);
+                const T rr = -(fli_dn - FLI + flj_1 - FLJm2);
                 W[o_res + o * pitch] = rr;
                 z = z + hdt * rr;
                 if (PRED) {
                     // Next step: cabaret_predictor (qg3p_aux.F90:1012-1018) and
                     // cabaret_beta (:1051-1059) with this step's ui.
-                    double zz = z + hdt * rr;
-                    const double rbn = dt * (0.5 * (ui_e + UIm2) * beta_l);
-                    zz = zz + (1.0 + ta) * rbn - ta * rb_2;
+                    T zz = z + hdt * rr;
+                    const T rbn = dt * ((T)0.5 * (ui_e + UIm2) * beta_l);
+                    zz = zz + ((T)1 + ta) * rbn - ta * rb_2;
                     W[o_rbn + o * pitch] = rbn;
                     W[o_zpn + o * pitch] = zz;
                 }
@@ -390,12 +416,12 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
                 W[o_ui + s1r * pitch] = ui_1;
                 W[o_uimon + s1r * pitch] = uim_1;
                 W[o_fin + s1r * pitch] = fin;
-                umax = fmax(umax, fabs(ui_1));
+                umax = fmax(umax, (double)fabs(ui_1));
             }
             if (fj_ok && s >= j0 && s < j0 + SH) {
                 W[o_uj + s * pitch] = uj_s;
                 W[o_ujmon + s * pitch] = ujm_s;
-                umax = fmax(umax, fabs(uj_s));
+                umax = fmax(umax, (double)fabs(uj_s));
             }
             if (bfj_ok && bf >= j0 && bf < j0 + SH) W[o_fjn + bf * pitch] = fjn;
         }
@@ -419,7 +445,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     return umax;
 }
 
-template <bool PRED>
+template <bool PRED, typename T>
 __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* __restrict__ mems,
                                                                     const int* __restrict__ prefix, int nmem) {
     __shared__ Member Mb;
@@ -443,8 +469,8 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
         const int i0 = strip * CAB_SW, j0 = band * SH;
         const bool interior = (i0 - 2 >= 2) && (i0 + 29 <= ii - 3) && (j0 - 4 >= 2) && (j0 + SH + 3 <= jj - 3);
         double* ring = cab_ring + warp * CAB_RING;
-        umax = interior ? cab_sweep<false, PRED>(Mb, l, i0, j0, lane, ring)
-                        : cab_sweep<true, PRED>(Mb, l, i0, j0, lane, ring);
+        umax = interior ? cab_sweep<false, PRED, T>(Mb, l, i0, j0, lane, ring)
+                        : cab_sweep<true, PRED, T>(Mb, l, i0, j0, lane, ring);
     }
 
     // Max |u| of the new face velocities (cabaret_cfl / cabaret_adapt_dt);
@@ -471,6 +497,9 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
         Scalars* sc = Mb.sc;
         sc->max_u = mu;
         sc->cfl = mu * sc->dt;
+        sc->dt_last = sc->dt;
+        sc->tweight_a_last = sc->tweight_a;
+        sc->tweight_u_last = sc->tweight_u;
         sc->model_time += sc->dt;
         if (Mb.adapt_dt) {
             const double old_dt = sc->dt;
@@ -494,23 +523,25 @@ int cabaret_ctas(int ii, int jj, int L, int sh) {
     return (nstrips * nbands * L + CAB_WARPS - 1) / CAB_WARPS;
 }
 
-template <bool PRED>
+template <bool PRED, typename T>
 static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
     const size_t bytes = (size_t)CAB_WARPS * CAB_RING * sizeof(double);
     cudaError_t e =
-        cudaFuncSetAttribute(k_cabaret_fused<PRED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        cudaFuncSetAttribute(k_cabaret_fused<PRED, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    k_cabaret_fused<PRED><<<ls.ctas_cab, CAB_WARPS * 32, bytes, st>>>(ls.members, ls.prefix_cab, ls.nmem);
+    k_cabaret_fused<PRED, T><<<ls.ctas_cab, CAB_WARPS * 32, bytes, st>>>(ls.members, ls.prefix_cab, ls.nmem);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, cudaStream_t st) {
-    return predict_next ? launch_cab<true>(ls, st) : launch_cab<false>(ls, st);
+cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, int f32, cudaStream_t st) {
+    if (f32) return predict_next ? launch_cab<true, float>(ls, st) : launch_cab<false, float>(ls, st);
+    return predict_next ? launch_cab<true, double>(ls, st) : launch_cab<false, double>(ls, st);
 }
 
 // ---------------------------------------------------------------------------
 // rel on demand (rel_from_zeta_and_psi + apply_rel_bc) from the zeta that
 // entered the inversion and the current psi.  One thread per node.
+template <typename T>
 __global__ void k_rel(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
@@ -518,25 +549,29 @@ __global__ void k_rel(const Member* __restrict__ mems, const int* __restrict__ p
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
     const int j = local;
-    const double* zp = reinterpret_cast<const double*>(Mb.zeta);
-    double* rel = reinterpret_cast<double*>(Mb.rel);
+    const T* zp = reinterpret_cast<const T*>(Mb.zeta);
+    T* rel = reinterpret_cast<T*>(Mb.rel);
     auto ps = [&](int i, int jn, int l) { return Mb.psi[(long long)jn * pitch + i + l * ls]; };
     for (int i = threadIdx.x; i < ii; i += blockDim.x)
         for (int l = 0; l < L; ++l) {
             const long long o = (long long)j * pitch + i + l * ls;
             const bool interior = i > 0 && i < ii - 1 && j > 0 && j < jj - 1;
-            rel[o] = rel_node(Mb, ps, interior ? zp[o] : 0.0, i, j, l);
+            rel[o] = (T)rel_node(Mb, ps, interior ? (double)zp[o] : 0.0, i, j, l);
         }
 }
 
-cudaError_t launch_rel(const LaunchSet& ls, cudaStream_t st) {
-    k_rel<<<ls.ctas_rows_all, 256, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+cudaError_t launch_rel(const LaunchSet& ls, int f32, cudaStream_t st) {
+    if (f32)
+        k_rel<float><<<ls.ctas_rows_all, 256, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    else
+        k_rel<double><<<ls.ctas_rows_all, 256, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
     return cudaGetLastError();
 }
 
 // End of the START_PERTURB initialisation (qg3.F90:389-391, 450-452): rel
 // from zeta and the new psi, boundary zeta from update_zeta_bc, and
 // zeta_old = zeta.  One thread per node, one CTA per row.
+template <typename T>
 __global__ void k_init_finish(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
@@ -544,22 +579,25 @@ __global__ void k_init_finish(const Member* __restrict__ mems, const int* __rest
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
     const int j = local;
-    const double* zp = reinterpret_cast<const double*>(Mb.zeta);
-    double* rel = reinterpret_cast<double*>(Mb.rel);
-    double* zo = reinterpret_cast<double*>(Mb.zeta_old[Mb.cur]);
+    const T* zp = reinterpret_cast<const T*>(Mb.zeta);
+    T* rel = reinterpret_cast<T*>(Mb.rel);
+    T* zo = reinterpret_cast<T*>(Mb.zeta_old[Mb.cur]);
     auto ps = [&](int i, int jn, int l) { return Mb.psi[(long long)jn * pitch + i + l * ls]; };
     for (int i = threadIdx.x; i < ii; i += blockDim.x)
         for (int l = 0; l < L; ++l) {
             const long long o = (long long)j * pitch + i + l * ls;
             const bool interior = i > 0 && i < ii - 1 && j > 0 && j < jj - 1;
-            const double r = rel_node(Mb, ps, zp[o], i, j, l);
-            rel[o] = r;
-            zo[o] = interior ? zp[o] : zeta_bc_node(Mb, ps, r, i, j, l);
+            const double r = rel_node(Mb, ps, (double)zp[o], i, j, l);
+            rel[o] = (T)r;
+            zo[o] = interior ? zp[o] : (T)zeta_bc_node(Mb, ps, r, i, j, l);
         }
 }
 
-cudaError_t launch_init_finish(const LaunchSet& ls, cudaStream_t st) {
-    k_init_finish<<<ls.ctas_rows_all, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+cudaError_t launch_init_finish(const LaunchSet& ls, int f32, cudaStream_t st) {
+    if (f32)
+        k_init_finish<float><<<ls.ctas_rows_all, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    else
+        k_init_finish<double><<<ls.ctas_rows_all, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
     return cudaGetLastError();
 }
 
@@ -639,6 +677,28 @@ __global__ void __launch_bounds__(256) k_energy(const Member* __restrict__ mems,
 
 cudaError_t launch_energy(const LaunchSet& ls, cudaStream_t st) {
     k_energy<<<ls.ctas_rows_all, 256, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    return cudaGetLastError();
+}
+
+}  // namespace pq
+
+namespace pq {
+
+// FP64 <-> FP32 copies of pitched fields (the mixed form's state I/O).
+__global__ void k_convert(void* __restrict__ dst, const void* __restrict__ src, size_t count, int to_f32) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride) {
+        if (to_f32)
+            static_cast<float*>(dst)[t] = (float)static_cast<const double*>(src)[t];
+        else
+            static_cast<double*>(dst)[t] = (double)static_cast<const float*>(src)[t];
+    }
+}
+
+cudaError_t launch_convert(void* dst, const void* src, size_t count, int to_f32, cudaStream_t st) {
+    size_t blocks = (count + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_convert<<<(unsigned)blocks, 256, 0, st>>>(dst, src, count, to_f32);
     return cudaGetLastError();
 }
 

@@ -37,7 +37,11 @@ struct Scalars {
     double ekin[PQ_MAXL];
     double epot;
     double model_time;  // advanced by dt at the end of every fused step
-    double pad[2];
+    // dt and time weights the last step ran with (dt above is already the
+    // next step's when adaptive stepping is on); what the reference's state
+    // holds after a step, since it adapts at the start of the next one.
+    double dt_last, tweight_a_last, tweight_u_last;
+    double pad;
 };
 
 // Device status bits (read by the host after a step).
@@ -72,6 +76,11 @@ struct Member {
     const double* was;      // [N/2] 2 sin(k pi / N), index k (0 unused)
     const double2* wsplit;  // [M]  exp(-2 pi i q / N)
     const double* wmean;    // [n]  2 * sum_i sin(i k pi / N), index k-1
+    const float2* tw_f;     // FP32 copies of tw, wsplit, was (mixed path)
+    const float2* wsplit_f;
+    const float* was_f;
+    int mixed;              // 1: FP32 storage of the CABARET fields and the
+                            // baroclinic spectral rows (see spec64)
     // Compressed tridiagonal pivots, per (mode, k): piv[off + p - 1] for
     // p < len, then the fixed point piv_fix.
     const int* piv_off;     // [L * n]
@@ -100,7 +109,7 @@ struct Member {
     void* flux_i;
     void* flux_j;
     void* spec;
-    double* spec64;   // barotropic-mode spectral scratch of the mixed path
+    double* spec64;   // barotropic-mode spectral rows of the mixed path (FP64)
     const double* corr;
     const double* wind;
     double* partials;     // [L * ntiles_tri]

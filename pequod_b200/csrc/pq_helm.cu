@@ -261,7 +261,7 @@ __host__ __device__ inline int dst_rows_per_cta(int M, int L, int c) {
 }
 __host__ __device__ inline int dst_unit_len(int N) { return (N + N / 8 + 2 + 1) & ~1; }
 
-__device__ __forceinline__ void cp16(double* dst, const double* src, bool ok) {
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool ok) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(ok ? 16 : 0) : "memory");
 }
@@ -274,23 +274,36 @@ __device__ __forceinline__ void cp_commit_wait_all() {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Row DST kernel.  A CTA holds R rows x L modes = L*R units of P lanes.
+__device__ __forceinline__ void cp4z(void* dst, const void* src, bool ok) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(src), "r"(ok ? 4 : 0) : "memory");
+}
+
+// Row DST kernel.  A CTA holds R rows x L modes = L*R units of P lanes,
+// ordered mode-major (unit (m, r) at index m*R + r), so that every warp's
+// units share one mode.
 //
 // Forward (EPI_SPEC, interior rows 1..jj-2): the raw layer rows are copied
-// asynchronously into the unit buffers (16-byte copies: node k of a row and
+// asynchronously into shared memory (16-byte copies: node k of a row and
 // entry k of the buffer have the same alignment), projected onto the modes
-// in place (z_to_modes) and scaled by 0.5/(ii-1); PRO_STEP instead computes
-// the CABARET predictor + beta update per node in registers.  Each unit then
+// (z_to_modes) and scaled by 0.5/(ii-1); PRO_STEP instead computes the
+// CABARET predictor + beta update per node in registers.  Each unit then
 // transforms its row and writes spec(m, j, k-1) = X_k.
 //
 // Inverse (EPI_HELM / EPI_PV, rows 0..jj-1): the solved spectral rows are
-// copied in (8-byte copies: spec offset k-1 -> buffer entry k), transformed, and written
+// copied in (spec offset k-1 -> buffer entry k), transformed, and written
 // out; for EPI_PV the correction rows corr_m (m >= 1) are prefetched into
 // shared memory before the transform and the mass-corrected back-projection
 // writes psi.
-template <int V, int PRO, int EPI>
+//
+// S is the storage type of the state and spectral fields.  S = float is the
+// mixed form: the layer fields and the baroclinic spectral rows are FP32 and
+// transformed in FP32, while the barotropic mode (m = 0) is kept in FP64
+// end to end (spec64), as are the projection, the back-projection and psi.
+template <typename S, int V, int PRO, int EPI>
 __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
                                              int nmem, int row_offset, int c, int corr_smem) {
+    constexpr bool MX = sizeof(S) == 4;
     __shared__ Member Mb;
     extern __shared__ __align__(16) double sm[];
     int local;
@@ -305,64 +318,74 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
     const int j0 = row_offset + local * R;                 // first row of this CTA
     const int jend = (EPI == EPI_SPEC) ? jj - 1 : jj;       // one past the last row
     const int nthr = blockDim.x;
-    const int half = N >> 1;                                // 16-byte copies per row
-    double* corr_s = sm + (size_t)L * R * U;                // EPI_PV: [R][L-1][pitch]
+    double* extra = sm + (size_t)L * R * U;                 // EPI_PV: corr rows [R][L-1][pitch];
+                                                            // mixed forward: staged rows [R][L][N] (FP32)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = nthr >> 5;
+    auto ubuf = [&](int m, int r) { return sm + (size_t)(m * R + r) * U; };
+    // Unit (m, r) buffers hold FP64 values, except the baroclinic ones of the mixed form.
+    auto fp64_mode = [&](int m) { return !MX || m == 0; };
+    auto put = [&](int m, int r, int k, double v) {
+        if (fp64_mode(m))
+            ubuf(m, r)[k] = v;
+        else
+            reinterpret_cast<float*>(ubuf(m, r))[k] = (float)v;
+    };
+    auto get = [&](int m, int r, int k) -> double {
+        return fp64_mode(m) ? ubuf(m, r)[k] : (double)reinterpret_cast<const float*>(ubuf(m, r))[k];
+    };
 
     // ---------------- stage the rows --------------------------------------
     if (EPI == EPI_SPEC) {
         const double cff = 0.5 / (double)(ii - 1);
         if (PRO != PRO_STEP) {
-            const double* src = reinterpret_cast<const double*>(PRO == PRO_PLAIN ? Mb.helm_io : Mb.zeta);
-            // unit (r, l) <- layer l of row j0 + r, entries 0..N-1; one warp
-            // per unit row.
+            const S* src = reinterpret_cast<const S*>(PRO == PRO_PLAIN ? Mb.helm_io : Mb.zeta);
+            // Layer l of row j0 + r: FP64 into unit (l, r) (projected in place
+            // below), FP32 into the staging rows; one warp per row.
+            constexpr int PER16 = 16 / sizeof(S);
             for (int rl = warp; rl < R * L; rl += nwarp) {
                 const int r = rl / L, l = rl - r * L;
                 const int j = j0 + r;
                 const bool ok = j < jend;
-                const double* g = src + l * ls + (long long)(ok ? j : 1) * pitch;
-                double* d = sm + (size_t)rl * U;
-                for (int q = lane; q < half; q += 32) cp16(d + 2 * q, g + 2 * q, ok);
+                const S* g = src + l * ls + (long long)(ok ? j : 1) * pitch;
+                S* d = MX ? reinterpret_cast<S*>(extra) + (size_t)rl * N : reinterpret_cast<S*>(ubuf(l, r));
+                for (int q = lane; q < N / PER16; q += 32) cp16(d + PER16 * q, g + PER16 * q, ok);
             }
             cp_commit_wait_all();
             __syncthreads();
-            // In place: node k of the L layer rows -> node k of the L mode rows.
+            // Node k of the L layer rows -> node k of the L mode rows (in
+            // place for FP64: a node's values are read before they are written).
             for (int r = 0; r < R; ++r)
-            for (int k = threadIdx.x; k < N; k += nthr) {
-                double* b = sm + (size_t)r * L * U + k;
-                double z[PQ_MAXL];
+                for (int k = threadIdx.x; k < N; k += nthr) {
+                    double z[PQ_MAXL];
 #pragma unroll
-                for (int l = 0; l < PQ_MAXL; ++l)
-                    if (l < L) z[l] = b[(size_t)l * U];
-                if (PRO == PRO_PLAIN) {
+                    for (int l = 0; l < PQ_MAXL; ++l)
+                        if (l < L)
+                            z[l] = MX ? (double)reinterpret_cast<const float*>(extra)[(size_t)(r * L + l) * N + k]
+                                      : ubuf(l, r)[k];
+                    if constexpr (PRO == PRO_PLAIN) {
 #pragma unroll
-                    for (int m = 0; m < PQ_MAXL; ++m)
-                        if (m < L) b[(size_t)m * U] = cff * z[m];
-                    continue;
-                }
+                        for (int m = 0; m < PQ_MAXL; ++m)
+                            if (m < L) put(m, r, k, cff * z[m]);
+                    } else {
 #pragma unroll 1
-                for (int m = 0; m < L; ++m) {
-                    {
-                        double s;
-                        {
+                        for (int m = 0; m < L; ++m) {
                             // z_to_modes, qg3p_diagnostics.F90:545-549
-                            s = 0.0;
+                            double sacc = 0.0;
 #pragma unroll
                             for (int l = 0; l < PQ_MAXL; ++l)
-                                if (l < L) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
+                                if (l < L) sacc += Mb.z2m[m * PQ_MAXL + l] * z[l];
+                            put(m, r, k, cff * sacc);
                         }
-                        b[(size_t)m * U] = cff * s;
                     }
                 }
-            }
         } else {
             const double dt = Mb.sc->dt, ta = Mb.sc->tweight_a;
-            const double* __restrict__ zo = reinterpret_cast<const double*>(Mb.zeta_old[Mb.cur]);
-            const double* __restrict__ rs = reinterpret_cast<const double*>(Mb.res);
-            const double* __restrict__ rbo = reinterpret_cast<const double*>(Mb.res_beta_other);
-            double* __restrict__ rb = reinterpret_cast<double*>(Mb.res_beta);
-            const double* __restrict__ ui = reinterpret_cast<const double*>(Mb.ui);
-            double* __restrict__ zp = reinterpret_cast<double*>(Mb.zeta);
+            const S* __restrict__ zo = reinterpret_cast<const S*>(Mb.zeta_old[Mb.cur]);
+            const S* __restrict__ rs = reinterpret_cast<const S*>(Mb.res);
+            const S* __restrict__ rbo = reinterpret_cast<const S*>(Mb.res_beta_other);
+            S* __restrict__ rb = reinterpret_cast<S*>(Mb.res_beta);
+            const S* __restrict__ ui = reinterpret_cast<const S*>(Mb.ui);
+            S* __restrict__ zp = reinterpret_cast<S*>(Mb.zeta);
             for (int r = 0; r < R; ++r) {
                 const int j = j0 + r;
                 const bool ok = j < jend;
@@ -393,35 +416,40 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
                                 // cabaret_beta, qg3p_aux.F90:1051-1059
                                 const double rbn = dt * (0.5 * (a3[l] + a2[l]) * Mb.beta[l]);
                                 zz = zz + (1.0 + ta) * rbn - ta * a4[l];
-                                rb[ol] = rbn;
-                                zp[ol] = zz;
+                                rb[ol] = (S)rbn;
+                                zp[ol] = (S)zz;
+                                if (MX) zz = (double)(S)zz;  // the stored (FP32) value
                             }
                             z[l] = zz;
                         }
                     }
 #pragma unroll 1
                     for (int m = 0; m < L; ++m) {
-                        {
-                            double s = 0.0;
+                        double sacc = 0.0;
 #pragma unroll
-                            for (int l = 0; l < PQ_MAXL; ++l)
-                                if (l < L) s += Mb.z2m[m * PQ_MAXL + l] * z[l];
-                            sm[(size_t)(r * L + m) * U + k] = cff * s;
-                        }
+                        for (int l = 0; l < PQ_MAXL; ++l)
+                            if (l < L) sacc += Mb.z2m[m * PQ_MAXL + l] * z[l];
+                        put(m, r, k, cff * sacc);
                     }
                 }
             }
         }
     } else {
-        const double* spec = reinterpret_cast<const double*>(Mb.spec);
-        // unit (r, m) entries 1..n <- spec(m, j, 0..n-1); one warp per unit row
+        // unit (m, r) entries 1..n <- spec(m, j, 0..n-1); one warp per unit row
         for (int rm = warp; rm < R * L; rm += nwarp) {
-            const int r = rm / L, m = rm - r * L;
+            const int m = rm / R, r = rm - m * R;
             const int j = j0 + r;
             const bool ok = j >= 1 && j <= jj - 2 && j < jend;
-            const double* g = spec + m * ls + (long long)(ok ? j : 1) * pitch - 1;
-            double* d = sm + (size_t)rm * U;
-            for (int k = 1 + lane; k <= n; k += 32) cp8z(d + k, g + k, ok);
+            if (fp64_mode(m)) {
+                const double* g = (MX ? Mb.spec64 : reinterpret_cast<const double*>(Mb.spec)) + m * ls +
+                                  (long long)(ok ? j : 1) * pitch - 1;
+                double* d = ubuf(m, r);
+                for (int k = 1 + lane; k <= n; k += 32) cp8z(d + k, g + k, ok);
+            } else {
+                const float* g = reinterpret_cast<const float*>(Mb.spec) + m * ls + (long long)(ok ? j : 1) * pitch - 1;
+                float* d = reinterpret_cast<float*>(ubuf(m, r));
+                for (int k = 1 + lane; k <= n; k += 32) cp4z(d + k, g + k, ok);
+            }
         }
         if (EPI == EPI_PV && corr_smem) {
             const double* corr = Mb.corr;
@@ -431,7 +459,7 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
                 const int j = j0 + r;
                 const bool ok = j < jend;
                 const double* g = corr + m * ls + (long long)(ok ? j : 0) * pitch;
-                double* d = corr_s + (size_t)rm * pitch;
+                double* d = extra + (size_t)rm * pitch;
                 for (int q = lane; q < cw; q += 32) cp16(d + 2 * q, g + 2 * q, ok);
             }
         }
@@ -441,26 +469,39 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
 
     // ---------------- per-unit transform ----------------------------------
     const int u = threadIdx.x / P, p = threadIdx.x & (P - 1);
-    const int ur = u / L, um = u - ur * L;
+    const int um = u / R, ur = u - um * R;
     const int ju = j0 + ur;
-    double* buf = sm + (size_t)u * U;
+    double* buf = ubuf(um, ur);
     const bool interior = ju >= 1 && ju <= jj - 2 && ju < jend;
-    dst_unit<V, double>(buf, p, P, N, M, logM, Mb.tw, Mb.wsplit, Mb.was);
+    if (fp64_mode(um))
+        dst_unit<V, double>(buf, p, P, N, M, logM, Mb.tw, Mb.wsplit, Mb.was);
+    else
+        dst_unit<V, float>(reinterpret_cast<float*>(buf), p, P, N, M, logM, Mb.tw_f, Mb.wsplit_f, Mb.was_f);
 
     if (EPI == EPI_SPEC) {
         if (ju < jend) {
-            double* spec = reinterpret_cast<double*>(Mb.spec) + um * ls + (long long)ju * pitch - 1;
-            for (int k = 1 + p; k <= n; k += P) spec[k] = buf[xpad(k)];
+            if (fp64_mode(um)) {
+                double* spec = (MX ? Mb.spec64 : reinterpret_cast<double*>(Mb.spec)) + um * ls +
+                               (long long)ju * pitch - 1;
+                for (int k = 1 + p; k <= n; k += P) spec[k] = buf[xpad(k)];
+            } else {
+                float* spec = reinterpret_cast<float*>(Mb.spec) + um * ls + (long long)ju * pitch - 1;
+                const float* fb = reinterpret_cast<const float*>(buf);
+                for (int k = 1 + p; k <= n; k += P) spec[k] = fb[xpad(k)];
+            }
         }
     } else if (EPI == EPI_HELM) {
-        // helm's in-place output: interior entries of interior rows, row
-        // i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1) (:1055-1057).
-        double* io = reinterpret_cast<double*>(Mb.helm_io) + um * ls + (long long)ju * pitch;
-        if (interior) {
-            for (int k = 1 + p; k <= n; k += P) io[k] = buf[xpad(k)];
-            if (p == 0) io[ii - 1] = 0.0;
-        } else if (ju == 0) {
-            for (int k = 1 + p; k <= n; k += P) io[k] = 0.0;
+        // helm's in-place output (FP64 only): interior entries of interior
+        // rows, row i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1)
+        // (:1055-1057).
+        if (!MX) {
+            double* io = reinterpret_cast<double*>(Mb.helm_io) + um * ls + (long long)ju * pitch;
+            if (interior) {
+                for (int k = 1 + p; k <= n; k += P) io[k] = buf[xpad(k)];
+                if (p == 0) io[ii - 1] = 0.0;
+            } else if (ju == 0) {
+                for (int k = 1 + p; k <= n; k += P) io[k] = 0.0;
+            }
         }
     } else {
         // psi_l = phi_1 - psiC_1 + sum_{m>=2} m2z(l,m) (phi_m - psiC_m corr_m)
@@ -474,35 +515,34 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
         for (int m = 0; m < PQ_MAXL; ++m) pc[m] = (m < L) ? psiC[m] : 0.0;
         double* psi = Mb.psi;
         for (int r = 0; r < R; ++r)
-        for (int i = threadIdx.x; i < ii; i += nthr) {
-            const int j = j0 + r;
-            if (j >= jend) break;
-            const bool inner = j >= 1 && j <= jj - 2 && i >= 1 && i <= n;
-            const double* row = sm + (size_t)(r * L) * U;
-            // corr_m at cr[m * cst] (staged rows, or the field itself)
-            const double* cr = corr_smem ? corr_s + ((long long)r * (L - 1) - 1) * pitch + i
-                                         : Mb.corr + (long long)j * pitch + i;
-            const long long cst = corr_smem ? (long long)pitch : ls;
-            double ph[PQ_MAXL];
+            for (int i = threadIdx.x; i < ii; i += nthr) {
+                const int j = j0 + r;
+                if (j >= jend) break;
+                const bool inner = j >= 1 && j <= jj - 2 && i >= 1 && i <= n;
+                // corr_m at cr[m * cst] (staged rows, or the field itself)
+                const double* cr = corr_smem ? extra + ((long long)r * (L - 1) - 1) * pitch + i
+                                             : Mb.corr + (long long)j * pitch + i;
+                const long long cst = corr_smem ? (long long)pitch : ls;
+                double ph[PQ_MAXL];
 #pragma unroll
-            for (int m = 0; m < PQ_MAXL; ++m)
-                if (m < L) ph[m] = inner ? row[(size_t)m * U + xpad(i)] : 0.0;
+                for (int m = 0; m < PQ_MAXL; ++m)
+                    if (m < L) ph[m] = inner ? get(m, r, xpad(i)) : 0.0;
 #pragma unroll
-            for (int m = 1; m < PQ_MAXL; ++m)
-                if (m < L) ph[m] -= pc[m] * cr[m * cst];
-            const double b0 = ph[0] - pc[0];
-            const long long o = (long long)j * pitch + i;
+                for (int m = 1; m < PQ_MAXL; ++m)
+                    if (m < L) ph[m] -= pc[m] * cr[m * cst];
+                const double b0 = ph[0] - pc[0];
+                const long long o = (long long)j * pitch + i;
 #pragma unroll
-            for (int l = 0; l < PQ_MAXL; ++l) {
-                if (l < L) {
-                    double dot = 0.0;
+                for (int l = 0; l < PQ_MAXL; ++l) {
+                    if (l < L) {
+                        double dot = 0.0;
 #pragma unroll
-                    for (int m = 1; m < PQ_MAXL; ++m)
-                        if (m < L) dot += Mb.m2z[l * PQ_MAXL + m] * ph[m];
-                    psi[o + l * ls] = b0 + dot;
+                        for (int m = 1; m < PQ_MAXL; ++m)
+                            if (m < L) dot += Mb.m2z[l * PQ_MAXL + m] * ph[m];
+                        psi[o + l * ls] = b0 + dot;
+                    }
                 }
             }
-        }
     }
 }
 
@@ -523,6 +563,9 @@ struct PivotRow {
     __device__ __forceinline__ double operator()(int p) const { return p <= len ? __ldg(&piv[p - 1]) : fix; }
 };
 
+// S = float: the mixed form, whose baroclinic spectral rows are FP32 (staged
+// and solved in FP64); the barotropic mode (m = 0) comes from spec64.
+template <typename S>
 __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restrict__ mems,
                                                           const int* __restrict__ prefix, int nmem, int do_mean) {
     __shared__ Member Mb;
@@ -542,25 +585,35 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     const int R = (Mr + 31) >> 5;
     const int RS = R | 1;
     const int CS = 32 * RS + 1;
-    double* spec = reinterpret_cast<double*>(Mb.spec) + (long long)m * Mb.lstride;
+    const bool f32 = sizeof(S) == 4 && m > 0;  // this mode's rows are FP32
+    double* spec = ((sizeof(S) == 4) ? Mb.spec64 : reinterpret_cast<double*>(Mb.spec)) + (long long)m * Mb.lstride;
+    float* specf = reinterpret_cast<float*>(Mb.spec) + (long long)m * Mb.lstride;
 
     // Stage: thread -> (column c = tid & 7, chunk q = tid >> 3); loop over t.
     // Asynchronous 8-byte copies (cp.async), so the loads of a thread do not
     // wait for one another; columns past n are zero-filled (source size 0).
+    // FP32 rows are loaded and widened in registers.
     {
         const int c = threadIdx.x & 7, q = threadIdx.x >> 3;
         const bool colok = (k0 + c < n);
-        const double* g = spec + (long long)(q * R + 1) * pitch + (colok ? k0 + c : 0);
+        const long long go = (long long)(q * R + 1) * pitch + (colok ? k0 + c : 0);
         double* sdst = strip + c * CS + q * RS;
         const int Rq = min(R, Mr - q * R);
-        const unsigned sbase = (unsigned)__cvta_generic_to_shared(sdst);
-        const int nbytes = colok ? 8 : 0;
-        for (int t = 0; t < Rq; ++t)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sbase + 8u * t),
-                         "l"(g + (long long)t * pitch), "r"(nbytes)
-                         : "memory");
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        if (!f32) {
+            const double* g = spec + go;
+            const unsigned sbase = (unsigned)__cvta_generic_to_shared(sdst);
+            const int nbytes = colok ? 8 : 0;
+            for (int t = 0; t < Rq; ++t)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sbase + 8u * t),
+                             "l"(g + (long long)t * pitch), "r"(nbytes)
+                             : "memory");
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        } else {
+            const float* g = specf + go;
+#pragma unroll 4
+            for (int t = 0; t < Rq; ++t) sdst[t] = colok ? (double)g[(long long)t * pitch] : 0.0;
+        }
     }
     __syncthreads();
 
@@ -658,10 +711,16 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     {
         const int cc = threadIdx.x & 7, q = threadIdx.x >> 3;
         if (k0 + cc < n) {
-            double* gdst = spec + (long long)(q * R + 1) * pitch + k0 + cc;
+            const long long go = (long long)(q * R + 1) * pitch + k0 + cc;
             const double* ssrc = strip + cc * CS + q * RS;
             const int Rq = min(R, Mr - q * R);
-            for (int t = 0; t < Rq; ++t) gdst[(long long)t * pitch] = ssrc[t];
+            if (!f32) {
+                double* gdst = spec + go;
+                for (int t = 0; t < Rq; ++t) gdst[(long long)t * pitch] = ssrc[t];
+            } else {
+                float* gdst = specf + go;
+                for (int t = 0; t < Rq; ++t) gdst[(long long)t * pitch] = (float)ssrc[t];
+            }
         }
     }
     if (!do_mean) return;
@@ -698,7 +757,7 @@ __host__ __device__ inline size_t tri_smem_bytes(int jj) {
 
 // ---------------------------------------------------------------------------
 // Host launchers.
-template <int V, int PRO, int EPI>
+template <typename S, int V, int PRO, int EPI>
 static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const int M = ls.maxN / 2, L = ls.maxL;
     const int R = dst_rows_per_cta(M, L, ls.dst_group);
@@ -707,45 +766,55 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const size_t cbytes = (size_t)R * (L - 1) * ls.maxPitch * sizeof(double);
     const int corr_smem = (EPI == EPI_PV && bytes + cbytes <= 200 * 1024) ? 1 : 0;
     if (corr_smem) bytes += cbytes;
-    cudaError_t e = cudaFuncSetAttribute(k_dst<V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (sizeof(S) == 4 && EPI == EPI_SPEC && PRO != PRO_STEP) bytes += (size_t)R * L * ls.maxN * sizeof(float);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_dst<S, V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     const int rows = (EPI == EPI_SPEC) ? ls.maxJ - 2 : ls.maxJ;
     const int grid = (rows + R - 1) / R;
-    k_dst<V, PRO, EPI><<<grid * ls.nmem, threads, bytes, st>>>(ls.members, ls.prefix_rows_interior, ls.nmem,
-                                                             EPI == EPI_SPEC ? 1 : 0, ls.dst_group, corr_smem);
+    k_dst<S, V, PRO, EPI><<<grid * ls.nmem, threads, bytes, st>>>(ls.members, ls.prefix_rows_interior, ls.nmem,
+                                                                EPI == EPI_SPEC ? 1 : 0, ls.dst_group, corr_smem);
     return cudaGetLastError();
 }
 
-template <int PRO, int EPI>
+template <typename S, int PRO, int EPI>
 static cudaError_t launch_dst(const LaunchSet& ls, cudaStream_t st) {
     switch (dst_v(ls.maxN / 2)) {
-        case 2: return launch_dst_v<2, PRO, EPI>(ls, st);
-        case 4: return launch_dst_v<4, PRO, EPI>(ls, st);
-        case 8: return launch_dst_v<8, PRO, EPI>(ls, st);
-        case 16: return launch_dst_v<16, PRO, EPI>(ls, st);
-        case 32: return launch_dst_v<32, PRO, EPI>(ls, st);
+        case 2: return launch_dst_v<S, 2, PRO, EPI>(ls, st);
+        case 4: return launch_dst_v<S, 4, PRO, EPI>(ls, st);
+        case 8: return launch_dst_v<S, 8, PRO, EPI>(ls, st);
+        case 16: return launch_dst_v<S, 16, PRO, EPI>(ls, st);
+        case 32: return launch_dst_v<S, 32, PRO, EPI>(ls, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, cudaStream_t st) {
+cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, int f32, cudaStream_t st) {
     switch (prologue) {
-        case PRO_PLAIN: return launch_dst<PRO_PLAIN, EPI_SPEC>(ls, st);
-        case PRO_MODAL: return launch_dst<PRO_MODAL, EPI_SPEC>(ls, st);
-        default: return launch_dst<PRO_STEP, EPI_SPEC>(ls, st);
+        case PRO_PLAIN: return launch_dst<double, PRO_PLAIN, EPI_SPEC>(ls, st);
+        case PRO_MODAL:
+            return f32 ? launch_dst<float, PRO_MODAL, EPI_SPEC>(ls, st) : launch_dst<double, PRO_MODAL, EPI_SPEC>(ls, st);
+        default:
+            return f32 ? launch_dst<float, PRO_STEP, EPI_SPEC>(ls, st) : launch_dst<double, PRO_STEP, EPI_SPEC>(ls, st);
     }
 }
 
-cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, cudaStream_t st) {
-    if (epilogue == EPI_HELM) return launch_dst<PRO_PLAIN, EPI_HELM>(ls, st);
-    return launch_dst<PRO_PLAIN, EPI_PV>(ls, st);
+cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, int f32, cudaStream_t st) {
+    if (epilogue == EPI_HELM) return launch_dst<double, PRO_PLAIN, EPI_HELM>(ls, st);
+    return f32 ? launch_dst<float, PRO_PLAIN, EPI_PV>(ls, st) : launch_dst<double, PRO_PLAIN, EPI_PV>(ls, st);
 }
 
-cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, cudaStream_t st) {
+cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, int f32, cudaStream_t st) {
     const size_t bytes = tri_smem_bytes(ls.maxJ);
-    cudaError_t e = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
-    k_tridiag<<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
+    if (f32) {
+        cudaError_t e = cudaFuncSetAttribute(k_tridiag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        k_tridiag<float><<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
+    } else {
+        cudaError_t e = cudaFuncSetAttribute(k_tridiag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        k_tridiag<double><<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
+    }
     return cudaGetLastError();
 }
 

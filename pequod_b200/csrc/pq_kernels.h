@@ -27,15 +27,19 @@ struct LaunchSet {
 
 
 // pq_helm.cu
-cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, cudaStream_t st);
-cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, cudaStream_t st);
-cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, cudaStream_t st);
+// f32: the mixed form (FP32 layer fields and baroclinic spectral rows)
+cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, int f32, cudaStream_t st);
+cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, int f32, cudaStream_t st);
+cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, int f32, cudaStream_t st);
 
 // pq_cabaret.cu
 // predict_next: also apply the next step's predictor + beta (fixed dt only)
-cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, cudaStream_t st);
+cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, int f32, cudaStream_t st);
 int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of k_cabaret_fused per member (band height sh)
-cudaError_t launch_rel(const LaunchSet& ls, cudaStream_t st);
+cudaError_t launch_rel(const LaunchSet& ls, int f32, cudaStream_t st);
+cudaError_t launch_init_finish(const LaunchSet& ls, int f32, cudaStream_t st);
+// Elementwise FP64 <-> FP32 copy of `count` values (to_f32: double -> float).
+cudaError_t launch_convert(void* dst, const void* src, size_t count, int to_f32, cudaStream_t st);
 cudaError_t launch_energy(const LaunchSet& ls, cudaStream_t st);
 
 }  // namespace pq
