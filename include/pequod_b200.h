@@ -82,6 +82,11 @@ extern "C" {
 #define PQ_F_RES 10      /* res            (ii, jj, L) */
 #define PQ_F_RES_BETA 11 /* res_beta       (ii, jj, L) */
 #define PQ_F_CORR 12     /* hcache%corr    (ii, jj, L), read only */
+/* Leapfrog second time level (qg3.F90 psi(2), zeta(2), rel(2), zeta_old(2)). */
+#define PQ_F_PSI2 13
+#define PQ_F_ZETA2 14
+#define PQ_F_REL2 15
+#define PQ_F_ZETA_OLD2 16
 
 /* Model description in non-dimensional units.  Matrices are column-major
  * with leading dimension `layers` (the Fortran strat%modes_to_z layout). */
@@ -176,7 +181,9 @@ PQ_API int pq_pv_inversion(pq_ctx* ctx, const double* zeta_sdata, double* psi_sd
 
 /* START_PERTURB initialisation, qg3.F90:365-404 and :450-459: zeta sdata
  * (ii, jj, L) initial PV; Dirichlet 0, inversion, rel and boundary PV, zeroed
- * CABARET fields, zeta_old = zeta, tweights 0.5. */
+ * CABARET fields, zeta_old = zeta, tweights 0.5.  For the leapfrog scheme
+ * zeta_ic holds both time levels, (ii, jj, L, 2), and the forward-Euler start
+ * (:463-497) follows. */
 PQ_API int pq_init_perturb(pq_ctx* ctx, const double* zeta_ic, int ptr_kind);
 
 /* nsteps iterations of the CABARET timestep_loop body (qg3.F90:590-957):

@@ -31,6 +31,8 @@ MAX_LAYERS = 8
 FIELDS = {
     "psi": 0, "zeta": 1, "rel": 2, "zeta_old": 3, "ui": 4, "uj": 5, "uimo": 6, "ujmo": 7,
     "zeta_fi": 8, "zeta_fj": 9, "res": 10, "res_beta": 11, "corr": 12,
+    # leapfrog second time level
+    "psi2": 13, "zeta2": 14, "rel2": 15, "zeta_old2": 16,
 }
 
 _dp = C.POINTER(C.c_double)
@@ -271,7 +273,9 @@ class Model:
         return psi
 
     def init_perturb(self, zeta_ic: np.ndarray) -> None:
-        z = np.asfortranarray(zeta_ic, dtype=np.float64).reshape(self.shape, order="F")
+        """zeta_ic: (ii, jj, L), or (ii, jj, L, 2) -- both time levels -- for the leapfrog scheme."""
+        shape = self.shape + ((2,) if self.cfg.desc.scheme == SCHEME_LEAPFROG else ())
+        z = np.asfortranarray(zeta_ic, dtype=np.float64).reshape(shape, order="F")
         _check(lib().pq_init_perturb(self.ctx, _p(z), PTR_HOST), self.ctx)
 
     def step(self, n: int = 1) -> None:

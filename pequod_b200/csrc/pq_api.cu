@@ -45,6 +45,7 @@ struct pq_ctx {
     bool initialized = false;
     bool fuse = false;        // fixed dt: the CABARET kernel applies the next predictor
     bool mixed = false;       // PQ_PREC_MIXED
+    bool leapfrog = false;    // PQ_SCHEME_LEAPFROG: cur is the level advanced next (lf - 1)
     bool pred_ready = false;  // zeta[cur] / res_beta[cur] already hold the next step's predictor
     int zpar = 0;             // parity whose zeta entered the last inversion
     cudaGraphExec_t graph2 = nullptr;
@@ -187,6 +188,21 @@ int run_step(pq_ctx* c, int par) {
         for (int k = 0; k < 5; ++k) CK(cudaEventCreate(&ev[k]));
         CK(cudaEventRecord(ev[0], c->stream));
     }
+    if (c->leapfrog) {
+        // One DOLEAPFROG sub-step on level par (qg3.F90:615-651): centred
+        // step + RAW filter, inversion, rel and boundary zeta, model_time.
+        CK(launch_lf_step(c->ls[par], c->desc.ra_nu, c->desc.ra_alpha, c->stream));
+        CK(launch_dst_forward(c->ls[par], PRO_MODAL, 0, c->stream));
+        if (ev) CK(cudaEventRecord(ev[1], c->stream));
+        CK(launch_tridiag(c->ls[par], 1, 0, c->stream));
+        if (ev) CK(cudaEventRecord(ev[2], c->stream));
+        CK(launch_dst_inverse(c->ls[par], EPI_PV, 0, c->stream));
+        if (ev) CK(cudaEventRecord(ev[3], c->stream));
+        CK(launch_lf_rel_bc(c->ls[par], 0, 1, c->stream));
+        if (ev) CK(cudaEventRecord(ev[4], c->stream));
+        c->zpar = par;
+        return PQ_OK;
+    }
     // The predictor + beta update runs in the forward DST unless the previous
     // fused step already produced this step's inversion input.
     const int f32 = c->mixed ? 1 : 0;
@@ -230,8 +246,11 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     *out = nullptr;
     const int ii = d->ii, jj = d->jj, L = d->layers;
     if (ii < 5 || jj < 5 || !is_pow2(ii - 1) || L < 1 || L > PQ_MAX_LAYERS || d->periodic_j) return PQ_ERR_ARG;
-    if (d->scheme != PQ_SCHEME_CABARET) return PQ_ERR_UNSUPPORTED;
     if (d->precision != PQ_PREC_FP64 && d->precision != PQ_PREC_MIXED) return PQ_ERR_UNSUPPORTED;
+    if (d->scheme != PQ_SCHEME_CABARET && d->scheme != PQ_SCHEME_LEAPFROG) return PQ_ERR_UNSUPPORTED;
+    // The leapfrog scheme runs in FP64 with a fixed dt (the reference's
+    // adaptive step is a CABARET routine).
+    if (d->scheme == PQ_SCHEME_LEAPFROG && (d->precision != PQ_PREC_FP64 || d->adapt_dt)) return PQ_ERR_UNSUPPORTED;
     pq_ctx* c = new pq_ctx;
     c->device = device;
     c->desc = *d;
@@ -284,7 +303,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     // Arena layout.
     const int nfields = 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 2 /*res_beta*/ + 1 /*ui*/ + 1 /*uj*/ +
                         2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ + 1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ +
-                        1 /*corr*/ + 1 /*spec64*/;
+                        1 /*corr*/ + 1 /*spec64*/ + 2 /*leapfrog psi(2), rel(2)*/;
     const size_t fb = align256(c->field_bytes);
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -406,6 +425,8 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     m.spec = fld();
     m.corr = (const double*)fld();
     m.spec64 = (double*)fld();
+    double* psi2 = (double*)fld();
+    void* rel2 = fld();
     m.wind = c->wind.empty() ? nullptr : reinterpret_cast<const double*>(A + o_wind);
     m.partials = reinterpret_cast<double*>(A + o_part);
     m.maxu_part = reinterpret_cast<double*>(A + o_maxu);
@@ -432,6 +453,26 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     c->hm[0].res_beta = c->hm[1].res_beta_other = rb0;
     c->hm[1].res_beta = c->hm[0].res_beta_other = rb1;
     c->fuse = !d->adapt_dt;
+    c->leapfrog = d->scheme == PQ_SCHEME_LEAPFROG;
+    if (c->leapfrog) {
+        // Level descriptors: hm[p] advances level p with the other level q.
+        c->fuse = false;
+        void* zl[2] = {zpb0, zpb1};
+        double* pl[2] = {m.psi, psi2};
+        void* rl[2] = {m.rel, rel2};
+        for (int p = 0; p < 2; ++p) {
+            const int q = p ^ 1;
+            Member& h = c->hm[p];
+            h.zeta = zl[p];
+            h.zeta_next = zl[q];
+            h.zeta_old[0] = m.zeta_old[p];
+            h.zeta_old[1] = m.zeta_old[q];
+            h.psi = pl[p];
+            h.psi_other = pl[q];
+            h.rel = rl[p];
+            h.rel_other = rl[q];
+        }
+    }
 
     e = cudaMalloc(&c->d_members, 2 * sizeof(Member) + 256);
     if (e != cudaSuccess) return fail(c, PQ_ERR_NOMEM, "device allocation failed");
@@ -529,13 +570,14 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     if (!c || !zeta_ic) return PQ_ERR_ARG;
     CK(cudaSetDevice(c->device));
     const int ii = c->ii, jj = c->jj, L = c->L;
-    std::vector<double> z((size_t)ii * jj * L);
+    const int nlev = c->leapfrog ? 2 : 1;  // init_rand fills both leapfrog levels
+    std::vector<double> z((size_t)ii * jj * L * nlev);
     if (ptr_kind == PQ_PTR_DEVICE)
         CK(cudaMemcpy(z.data(), zeta_ic, z.size() * sizeof(double), cudaMemcpyDeviceToHost));
     else
         std::memcpy(z.data(), zeta_ic, z.size() * sizeof(double));
     // apply_dirichlet_bc(0, zeta), qg3.F90:383.
-    for (int l = 0; l < L; ++l) {
+    for (int l = 0; l < L * nlev; ++l) {
         double* p = z.data() + (size_t)ii * jj * l;
         for (int i = 0; i < ii; ++i) p[i] = p[i + (size_t)ii * (jj - 1)] = 0.0;
         for (int j = 0; j < jj; ++j) p[(size_t)ii * j] = p[(size_t)ii * j + ii - 1] = 0.0;
@@ -566,6 +608,25 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     c->cur = 0;
     c->zpar = 0;
     c->pred_ready = false;
+    if (c->leapfrog) {
+        // Both levels start from the initial condition (qg3.F90:382-404),
+        // then FORWARD_EULER_START (:463-497) makes level 2 one dt ahead.
+        sc.model_time = 0.0;
+        CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
+        rc = copy_in_state(c, c->hm[1].zeta, z.data() + (size_t)ii * jj * L, PQ_PTR_HOST);
+        if (rc) return rc;
+        for (int p = 0; p < 2; ++p) {
+            rc = run_helm(c, p, PRO_MODAL, EPI_PV, 1);
+            if (rc) return rc;
+            CK(launch_lf_rel_bc(c->ls[p], 1, 0, c->stream));
+        }
+        CK(launch_lf_forward_euler(c->ls[0], c->stream));
+        rc = run_helm(c, 1, PRO_MODAL, EPI_PV, 1);
+        if (rc) return rc;
+        CK(launch_lf_rel_bc(c->ls[1], 1, 1, c->stream));
+        c->initialized = true;
+        return check_status(c);
+    }
     rc = run_helm(c, 0, PRO_MODAL, EPI_PV, 1);
     if (rc) return rc;
     CK(launch_init_finish(c->ls[0], c->mixed ? 1 : 0, c->stream));
@@ -615,7 +676,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         if (rc) return rc;
         c->cur ^= 1;
         ++done;
-        launches += 4;
+        launches += c->leapfrog ? 5 : 4;
     }
     if (nsteps - done >= 2) {
         if (!c->graph2) {
@@ -636,7 +697,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         while (nsteps - done >= 2) {
             CK(cudaGraphLaunch(c->graph2, c->stream));
             done += 2;
-            launches += 8;
+            launches += c->leapfrog ? 10 : 8;
         }
     }
     if (done < nsteps) {
@@ -644,7 +705,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         if (rc) return rc;
         c->cur = 1;
         ++done;
-        launches += 4;
+        launches += c->leapfrog ? 5 : 4;
     }
     c->last_launches = launches;
     return PQ_OK;
@@ -714,7 +775,9 @@ int pq_kernel_times(pq_ctx* c, double* ms, long* launches) {
 int pq_energy(pq_ctx* c, double* ekin, double* epot) {
     if (!c || !ekin || !epot) return PQ_ERR_ARG;
     CK(cudaSetDevice(c->device));
-    CK(launch_energy(c->ls[c->cur], c->stream));
+    // energy(strat, psi BNLEAPFROG, ...) (qg3.F90:744): the second time level
+    // for the leapfrog scheme.
+    CK(launch_energy(c->ls[c->leapfrog ? 1 : 0], c->stream));
     Scalars sc;
     CK(cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
     int rc = check_status(c);
@@ -770,6 +833,10 @@ bool ref_shape(int field, int ii, int jj, RefShape* s) {
         case PQ_F_RES:
         case PQ_F_RES_BETA:
         case PQ_F_CORR: *s = {ii, jj, 0, 0}; return true;
+        case PQ_F_PSI2:
+        case PQ_F_ZETA2:
+        case PQ_F_REL2:
+        case PQ_F_ZETA_OLD2: *s = {ii + 2, jj + 2, 1, 1}; return true;
     }
     return false;
 }
@@ -777,6 +844,21 @@ bool ref_shape(int field, int ii, int jj, RefShape* s) {
 void* field_ptr(pq_ctx* c, int field) {
     const Member& m = c->hm[c->cur];
     const int cur = c->cur;
+    if (c->leapfrog) {
+        // Time levels 1 and 2 live in the level descriptors hm[0], hm[1].
+        const Member& a = c->hm[0];
+        const Member& b = c->hm[1];
+        switch (field) {
+            case PQ_F_PSI: return a.psi;
+            case PQ_F_ZETA: return a.zeta;
+            case PQ_F_REL: return a.rel;
+            case PQ_F_ZETA_OLD: return a.zeta_old[0];
+            case PQ_F_PSI2: return b.psi;
+            case PQ_F_ZETA2: return b.zeta;
+            case PQ_F_REL2: return b.rel;
+            case PQ_F_ZETA_OLD2: return b.zeta_old[0];
+        }
+    }
     switch (field) {
         case PQ_F_PSI: return m.psi;
         case PQ_F_ZETA:
@@ -804,9 +886,11 @@ int pq_get_field(pq_ctx* c, int field, double* out) {
     RefShape s;
     if (!ref_shape(field, c->ii, c->jj, &s)) return fail(c, PQ_ERR_ARG, "unknown field");
     CK(cudaSetDevice(c->device));
-    if (field == PQ_F_REL) CK(launch_rel(c->ls[c->zpar], c->mixed ? 1 : 0, c->stream));
+    if (field == PQ_F_REL && !c->leapfrog) CK(launch_rel(c->ls[c->zpar], c->mixed ? 1 : 0, c->stream));
+    if (!field_ptr(c, field)) return fail(c, PQ_ERR_ARG, "field not held by this scheme");
     std::vector<double> dense((size_t)c->ii * c->jj * c->L);
-    int rc = (field == PQ_F_PSI || field == PQ_F_CORR) ? copy_out(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST)
+    int rc = (field == PQ_F_PSI || field == PQ_F_PSI2 || field == PQ_F_CORR)
+                 ? copy_out(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST)
                                                       : copy_out_state(c, dense.data(), field_ptr(c, field), PQ_PTR_HOST);
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
@@ -824,6 +908,7 @@ int pq_set_field(pq_ctx* c, int field, const double* in) {
     if (!c || !in) return PQ_ERR_ARG;
     RefShape s;
     if (!ref_shape(field, c->ii, c->jj, &s) || field == PQ_F_CORR) return fail(c, PQ_ERR_ARG, "unknown field");
+    if (!field_ptr(c, field)) return fail(c, PQ_ERR_ARG, "field not held by this scheme");
     CK(cudaSetDevice(c->device));
     std::vector<double> dense((size_t)c->ii * c->jj * c->L);
     for (int l = 0; l < c->L; ++l)
@@ -831,10 +916,10 @@ int pq_set_field(pq_ctx* c, int field, const double* in) {
             for (int i = 0; i < c->ii; ++i)
                 dense[(size_t)i + (size_t)c->ii * (j + (size_t)c->jj * l)] =
                     in[(size_t)(i + s.oi) + (size_t)s.n1 * ((j + s.oj) + (size_t)s.n2 * l)];
-    int rc = (field == PQ_F_PSI) ? copy_in(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST)
+    int rc = (field == PQ_F_PSI || field == PQ_F_PSI2) ? copy_in(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST)
                                  : copy_in_state(c, field_ptr(c, field), dense.data(), PQ_PTR_HOST);
     if (rc) return rc;
-    if (field == PQ_F_ZETA) {
+    if (field == PQ_F_ZETA && !c->leapfrog) {
         rc = copy_in_state(c, c->hm[c->cur].zeta, dense.data(), PQ_PTR_HOST);
         c->zpar = c->cur;
     }

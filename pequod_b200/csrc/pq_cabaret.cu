@@ -24,46 +24,6 @@ __device__ __forceinline__ void load_member_c(Member& dst, const Member* src) {
     for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
 }
 
-// Relative vorticity at node (i, j) of layer l from zeta and psi
-// (rel_from_zeta_and_psi) with the boundary condition of apply_rel_bc.
-// ps(i, j, l) reads staged psi.  Corners take the j-boundary formula, which
-// the reference applies last.
-template <class PS>
-__device__ __forceinline__ double rel_node(const Member& Mb, PS ps, double zeta, int i, int j, int l) {
-    const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
-    const bool bj = (j == 0 || j == jj - 1), bi = (i == 0 || i == ii - 1);
-    if (bj || bi) {
-        if (Mb.bc_type == 3) return 0.0;
-        int di = 0, dj = 0;
-        if (bj)
-            dj = (j == 0) ? 1 : -1;
-        else
-            di = (i == 0) ? 1 : -1;
-        const double p0 = ps(i, j, l), p1 = ps(i + di, j + dj, l), p2 = ps(i + 2 * di, j + 2 * dj, l);
-        if (Mb.bc_type == 1) {
-            const double cff = Mb.alpha / (Mb.alpha + 3.0);
-            return cff * (-3.5 * p0 + 4.0 * p1 - 0.5 * p2);
-        }
-        return 2.0 * (p1 - p0);
-    }
-    if (L == 1) return zeta;
-    const double p = ps(i, j, l);
-    if (l == 0) return zeta + Mb.s2[0] * (p - ps(i, j, 1));
-    if (l == L - 1) return zeta + Mb.s1[l] * (p - ps(i, j, l - 1));
-    return zeta + Mb.s1[l] * (p - ps(i, j, l - 1)) + Mb.s2[l] * (p - ps(i, j, l + 1));
-}
-
-// Boundary relative PV from rel and psi (update_zeta_bc).
-template <class PS>
-__device__ __forceinline__ double zeta_bc_node(const Member& Mb, PS ps, double rel, int i, int j, int l) {
-    const int L = Mb.L;
-    if (L == 1) return rel;
-    const double p = ps(i, j, l);
-    if (l == 0) return rel - Mb.s2[0] * (p - ps(i, j, 1));
-    if (l == L - 1) return rel - Mb.s1[l] * (p - ps(i, j, l - 1));
-    return rel - Mb.s1[l] * (p - ps(i, j, l - 1)) - Mb.s2[l] * (p - ps(i, j, l + 1));
-}
-
 // Sweep decomposition: a warp owns one layer of a strip of 32 columns
 // (CAB_SW = 28 output columns plus 2 halo lanes on each side) and marches down
 // a band of Mb.cab_sh output rows (a tuning parameter).  Every per-lane quantity lives in registers as
