@@ -272,6 +272,31 @@ typedef struct pq_tuning {
 PQ_API int pq_set_tuning(pq_ctx* ctx, const pq_tuning* t);
 PQ_API int pq_get_tuning(pq_ctx* ctx, pq_tuning* t);
 
+/* ---- batched Helmholtz solves ---------------------------------------- */
+
+/* Many independent helm problems (qg3p_helmholtz.F90:614-769, each with its
+ * own helm_cache) of mixed sizes and mode counts, solved by grouped launches
+ * captured in one CUDA graph.  Member k is an (ii[k], jj[k], layers[k])
+ * problem whose layer l has the Helmholtz constant ss[sum_{q<k} layers[q] + l];
+ * its right-hand side goes in with pq_batch_set_rhs and the solution, with
+ * helm's in-place semantics (row ii zeroed, boundary entries untouched), comes
+ * out with pq_batch_get.  The data stay on the device between solves. */
+typedef struct pq_batch pq_batch;
+PQ_API int pq_batch_create(pq_batch** out, int n, const int* ii, const int* jj, const int* layers,
+                           const double* ss, int device);
+PQ_API void pq_batch_destroy(pq_batch* b);
+PQ_API const char* pq_batch_last_error(const pq_batch* b);
+PQ_API size_t pq_batch_device_bytes(const pq_batch* b);
+PQ_API void* pq_batch_stream(pq_batch* b);
+PQ_API int pq_batch_set_rhs(pq_batch* b, int k, const double* rhs, int ptr_kind);
+PQ_API int pq_batch_get(pq_batch* b, int k, double* out, int ptr_kind);
+PQ_API int pq_batch_solve_async(pq_batch* b); /* all members, on pq_batch_stream */
+PQ_API int pq_batch_sync(pq_batch* b);
+/* set_rhs + solve + get for every member (zeta[k] in/out), then sync. */
+PQ_API int pq_batch_helm(pq_batch* b, double* const* zeta, int ptr_kind);
+/* Kernel launches one solve makes (3 phases x classes). */
+PQ_API int pq_batch_launch_count(const pq_batch* b);
+
 /* Number of kernel launches the last pq_step enqueued. */
 PQ_API long pq_last_launch_count(const pq_ctx* ctx);
 

@@ -106,6 +106,18 @@ SIGNATURES = {
     "pq_kernel_times": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_long)]),
     "pq_energy_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_void_p,
                                     C.c_void_p]),
+    "pq_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), _dp, C.c_int]),
+    "pq_batch_destroy": (None, [C.c_void_p]),
+    "pq_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "pq_batch_device_bytes": (C.c_size_t, [C.c_void_p]),
+    "pq_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "pq_batch_set_rhs": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
+    "pq_batch_get": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
+    "pq_batch_solve_async": (C.c_int, [C.c_void_p]),
+    "pq_batch_sync": (C.c_int, [C.c_void_p]),
+    "pq_batch_helm": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.c_int]),
+    "pq_batch_launch_count": (C.c_int, [C.c_void_p]),
 }
 
 KERNELS = ("dst_forward", "tridiag", "dst_inverse_backproject", "cabaret_fused")
@@ -363,3 +375,78 @@ class Model:
         n = (C.c_long * 4)()
         _check(lib().pq_kernel_times(self.ctx, _p(ms), n), self.ctx)
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNELS)}
+
+
+class Batch:
+    """Batched Helmholtz solves (pq_batch_*): member k is an (ii, jj, L) helm
+    problem with per-layer constants ss[k] (a sequence of length L)."""
+
+    def __init__(self, shapes, ss, device: int = 0):
+        n = len(shapes)
+        self.shapes = [tuple(int(v) for v in s) for s in shapes]
+        ii = (C.c_int * n)(*[s[0] for s in self.shapes])
+        jj = (C.c_int * n)(*[s[1] for s in self.shapes])
+        ll = (C.c_int * n)(*[s[2] for s in self.shapes])
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(v, dtype=np.float64) for v in ss]))
+        if flat.size != sum(s[2] for s in self.shapes):
+            raise ValueError("ss lengths must match the layer counts")
+        self.ctx = C.c_void_p()
+        rc = lib().pq_batch_create(C.byref(self.ctx), n, ii, jj, ll, _p(flat), device)
+        if rc != PQ_OK:
+            msg = lib().pq_batch_last_error(self.ctx).decode() if self.ctx else ""
+            if self.ctx:
+                lib().pq_batch_destroy(self.ctx)
+                self.ctx = None
+            raise PQError(rc, msg)
+
+    def _chk(self, rc):
+        if rc != PQ_OK:
+            raise PQError(rc, lib().pq_batch_last_error(self.ctx).decode())
+
+    def __len__(self):
+        return len(self.shapes)
+
+    def set_rhs(self, k, rhs):
+        z = np.asfortranarray(rhs, dtype=np.float64).reshape(self.shapes[k], order="F")
+        self._chk(lib().pq_batch_set_rhs(self.ctx, k, _p(z), PTR_HOST))
+
+    def get(self, k):
+        out = np.zeros(self.shapes[k], order="F")
+        self._chk(lib().pq_batch_get(self.ctx, k, _p(out), PTR_HOST))
+        self._chk(lib().pq_batch_sync(self.ctx))
+        return out
+
+    def solve_async(self):
+        self._chk(lib().pq_batch_solve_async(self.ctx))
+
+    def sync(self):
+        self._chk(lib().pq_batch_sync(self.ctx))
+
+    def helm(self, rhs_list):
+        """Solve every member; returns the solutions (helm in-place semantics)."""
+        arrs = [np.array(np.asfortranarray(r, dtype=np.float64).reshape(self.shapes[k], order="F"), order="F")
+                for k, r in enumerate(rhs_list)]
+        ptrs = (_dp * len(arrs))(*[_p(a) for a in arrs])
+        self._chk(lib().pq_batch_helm(self.ctx, ptrs, PTR_HOST))
+        return arrs
+
+    @property
+    def stream(self):
+        return lib().pq_batch_stream(self.ctx)
+
+    def device_bytes(self):
+        return int(lib().pq_batch_device_bytes(self.ctx))
+
+    def launch_count(self):
+        return int(lib().pq_batch_launch_count(self.ctx))
+
+    def close(self):
+        if self.ctx:
+            lib().pq_batch_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

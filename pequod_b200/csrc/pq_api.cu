@@ -8,61 +8,19 @@
 #include "pequod_b200.h"
 #include "pq_common.cuh"
 #include "pq_kernels.h"
-
-namespace pq {
-}
+#include "pq_ctx.h"
 
 using namespace pq;
 
-namespace {
-
-enum { PRO_PLAIN = 0, PRO_MODAL = 1, PRO_STEP = 2 };
-enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
+namespace pq {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-constexpr int kMinBand = 4;   // smallest CABARET band height a tuning may select
-constexpr int kMaxBand = 128;
-
 bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
 
-}  // namespace
+}  // namespace pq
 
-struct pq_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    pq_model_desc desc{};
-    std::vector<double> wind;
-    Member hm[2];               // host copies of the two parity descriptors
-    Member* d_members = nullptr;  // device: [2]
-    int* d_prefix = nullptr;      // device: {0}
-    LaunchSet ls[2];
-    char* arena = nullptr;
-    size_t arena_bytes = 0;
-    Scalars* d_sc = nullptr;
-    int* d_status = nullptr;
-    int cur = 0;          // parity of the next step
-    bool initialized = false;
-    bool fuse = false;        // fixed dt: the CABARET kernel applies the next predictor
-    bool mixed = false;       // PQ_PREC_MIXED
-    bool leapfrog = false;    // PQ_SCHEME_LEAPFROG: cur is the level advanced next (lf - 1)
-    bool pred_ready = false;  // zeta[cur] / res_beta[cur] already hold the next step's predictor
-    int zpar = 0;             // parity whose zeta entered the last inversion
-    cudaGraphExec_t graph2 = nullptr;
-    std::string err;
-    long last_launches = 0;
-    // Per-kernel CUDA-event timing of eagerly launched steps.
-    struct StepEvents {
-        cudaEvent_t e[5];
-    };
-    bool timing = false;
-    std::vector<StepEvents> events;
-    // host copies of layout facts
-    int ii = 0, jj = 0, L = 0, pitch = 0;
-    size_t field_bytes = 0;  // bytes of one L-layer field
-};
-
-namespace {
+namespace pq {
 
 int fail(pq_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -72,12 +30,6 @@ int fail(pq_ctx* c, int code, const std::string& msg) {
 int cuda_fail(pq_ctx* c, cudaError_t e, const char* where) {
     return fail(c, PQ_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
-
-#define CK(call)                                           \
-    do {                                                   \
-        cudaError_t e_ = (call);                           \
-        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
-    } while (0)
 
 // Pivots of the tridiagonal j-solves, exactly as allocate_h1d_c computes
 // ge_fact (qg3p_helmholtz.F90:794-809), compressed: for each (mode, k) the
@@ -219,7 +171,7 @@ int run_step(pq_ctx* c, int par) {
     return PQ_OK;
 }
 
-}  // namespace
+}  // namespace pq
 
 extern "C" {
 
@@ -237,11 +189,17 @@ void pq_destroy(pq_ctx* c) {
     if (c->graph2) cudaGraphExecDestroy(c->graph2);
     if (c->arena) cudaFree(c->arena);
     if (c->d_members) cudaFree(c->d_members);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
 }
 
 int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
+    return create_ctx(out, d, device, false, nullptr);
+}
+
+}  // extern "C"
+
+int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_only, cudaStream_t stream) {
     if (!out || !d) return PQ_ERR_ARG;
     *out = nullptr;
     const int ii = d->ii, jj = d->jj, L = d->layers;
@@ -264,7 +222,13 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
         return rc;
     }
     *out = c;
-    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->helm_only = helm_only;
+    if (stream) {
+        c->stream = stream;
+        c->own_stream = false;
+    } else {
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    }
     int sm_count = 0;
     CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
     if (d->force_wind) c->wind.assign(d->force_wind, d->force_wind + (size_t)ii * jj);
@@ -301,9 +265,11 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     PivotTables pv = build_pivots(ii, jj, L, d->ss);
 
     // Arena layout.
-    const int nfields = 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 2 /*res_beta*/ + 1 /*ui*/ + 1 /*uj*/ +
-                        2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ + 1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ +
-                        1 /*corr*/ + 1 /*spec64*/ + 2 /*leapfrog psi(2), rel(2)*/;
+    const int nfields = helm_only ? 2 /*helm_io, spec*/
+                                  : 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 2 /*res_beta*/ +
+                                        1 /*ui*/ + 1 /*uj*/ + 2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ +
+                                        1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ + 1 /*corr*/ + 1 /*spec64*/ +
+                                        2 /*leapfrog psi(2), rel(2)*/;
     const size_t fb = align256(c->field_bytes);
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -402,31 +368,38 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     char* F = A + o_fields;
     int fi = 0;
     auto fld = [&]() { return (void*)(F + fb * (fi++)); };
-    m.zeta_old[0] = fld();
-    m.zeta_old[1] = fld();
-    void* zpb0 = fld();
-    m.psi = (double*)fld();
-    m.res = fld();
-    void* rb0 = fld();
-    m.ui = fld();
-    m.uj = fld();
-    m.uimo[0] = fld();
-    m.uimo[1] = fld();
-    m.ujmo[0] = fld();
-    m.ujmo[1] = fld();
-    m.zfi[0] = fld();
-    m.zfi[1] = fld();
-    m.zfj[0] = fld();
-    m.zfj[1] = fld();
-    void* zpb1 = fld();
-    void* rb1 = fld();
-    m.rel = fld();
-    m.helm_io = fld();
-    m.spec = fld();
-    m.corr = (const double*)fld();
-    m.spec64 = (double*)fld();
-    double* psi2 = (double*)fld();
-    void* rel2 = fld();
+    void *zpb0 = nullptr, *zpb1 = nullptr, *rb0 = nullptr, *rb1 = nullptr, *rel2 = nullptr;
+    double* psi2 = nullptr;
+    if (helm_only) {
+        m.helm_io = fld();
+        m.spec = fld();
+    } else {
+        m.zeta_old[0] = fld();
+        m.zeta_old[1] = fld();
+        zpb0 = fld();
+        m.psi = (double*)fld();
+        m.res = fld();
+        rb0 = fld();
+        m.ui = fld();
+        m.uj = fld();
+        m.uimo[0] = fld();
+        m.uimo[1] = fld();
+        m.ujmo[0] = fld();
+        m.ujmo[1] = fld();
+        m.zfi[0] = fld();
+        m.zfi[1] = fld();
+        m.zfj[0] = fld();
+        m.zfj[1] = fld();
+        zpb1 = fld();
+        rb1 = fld();
+        m.rel = fld();
+        m.helm_io = fld();
+        m.spec = fld();
+        m.corr = (const double*)fld();
+        m.spec64 = (double*)fld();
+        psi2 = (double*)fld();
+        rel2 = fld();
+    }
     m.wind = c->wind.empty() ? nullptr : reinterpret_cast<const double*>(A + o_wind);
     m.partials = reinterpret_cast<double*>(A + o_part);
     m.maxu_part = reinterpret_cast<double*>(A + o_maxu);
@@ -496,6 +469,10 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
         s.ctas_cab = ntiles_cab;
         s.dst_group = 0;
         s.sm_count = sm_count;
+        s.prefix_dst[0] = s.prefix_dst[1] = c->d_prefix;
+        const int R = dst_rows_per_cta_host(N / 2, L, 0);
+        s.ctas_dst[0] = (jj - 2 + R - 1) / R;
+        s.ctas_dst[1] = (jj + R - 1) / R;
     }
     // Scalars: dt and the initial time weights.
     Scalars sc;
@@ -509,7 +486,7 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     // (qg3p_aux.F90:196-230): solve with a unit right-hand side, Dirichlet 0,
     // then corr = (1 + ss psi) / (1 + ss mean(psi)) with the plain interior
     // mean the reference uses there.
-    {
+    if (!helm_only) {
         std::vector<double> ones((size_t)ii * jj * L, 1.0);
         rc = copy_in(c, m.helm_io, ones.data(), PQ_PTR_HOST);
         if (rc) return rc;
@@ -536,6 +513,8 @@ int pq_create(pq_ctx** out, const pq_model_desc* d, int device) {
     CK(cudaStreamSynchronize(c->stream));
     return PQ_OK;
 }
+
+extern "C" {
 
 int pq_helm(pq_ctx* c, double* zeta, int ptr_kind) {
     if (!c || !zeta) return PQ_ERR_ARG;
@@ -721,6 +700,9 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
         c->hm[p].ntiles_cab = cabaret_ctas(c->ii, c->jj, c->L, t->cab_band);
         c->ls[p].ctas_cab = c->hm[p].ntiles_cab;
         c->ls[p].dst_group = t->dst_group;
+        const int R = dst_rows_per_cta_host(c->hm[p].M, c->L, t->dst_group);
+        c->ls[p].ctas_dst[0] = (c->jj - 2 + R - 1) / R;
+        c->ls[p].ctas_dst[1] = (c->jj + R - 1) / R;
     }
     int rc = upload_members(c);
     if (rc) return rc;

@@ -757,6 +757,8 @@ __host__ __device__ inline size_t tri_smem_bytes(int jj) {
 
 // ---------------------------------------------------------------------------
 // Host launchers.
+int dst_rows_per_cta_host(int M, int L, int c) { return dst_rows_per_cta(M, L, c); }
+
 template <typename S, int V, int PRO, int EPI>
 static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const int M = ls.maxN / 2, L = ls.maxL;
@@ -770,10 +772,9 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     cudaError_t e =
         cudaFuncSetAttribute(k_dst<S, V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    const int rows = (EPI == EPI_SPEC) ? ls.maxJ - 2 : ls.maxJ;
-    const int grid = (rows + R - 1) / R;
-    k_dst<S, V, PRO, EPI><<<grid * ls.nmem, threads, bytes, st>>>(ls.members, ls.prefix_rows_interior, ls.nmem,
-                                                                EPI == EPI_SPEC ? 1 : 0, ls.dst_group, corr_smem);
+    const int dir = (EPI == EPI_SPEC) ? 0 : 1;
+    k_dst<S, V, PRO, EPI><<<ls.ctas_dst[dir], threads, bytes, st>>>(ls.members, ls.prefix_dst[dir], ls.nmem,
+                                                                  EPI == EPI_SPEC ? 1 : 0, ls.dst_group, corr_smem);
     return cudaGetLastError();
 }
 

@@ -21,12 +21,16 @@ struct LaunchSet {
     int ctas_tri;
     const int* prefix_cab;            // cabaret_ctas(ii, jj, L) CTAs per member
     int ctas_cab;
-    int dst_group;                    // modes per DST CTA pass (0: automatic)
+    const int* prefix_dst[2];         // DST CTAs per member, forward [0] and inverse [1]
+    int ctas_dst[2];                  //   (ceil(rows / dst_rows_per_cta) per member)
+    int dst_group;                    // row groups per DST CTA (0: automatic)
     int sm_count;                     // SMs of the device (persistent grids)
 };
 
 
 // pq_helm.cu
+// Rows per DST CTA for complex length M = N/2, L modes, row-group setting c.
+int dst_rows_per_cta_host(int M, int L, int c);
 // f32: the mixed form (FP32 layer fields and baroclinic spectral rows)
 cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, int f32, cudaStream_t st);
 cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, int f32, cudaStream_t st);
