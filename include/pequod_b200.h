@@ -297,6 +297,33 @@ PQ_API int pq_batch_helm(pq_batch* b, double* const* zeta, int ptr_kind);
 /* Kernel launches one solve makes (3 phases x classes). */
 PQ_API int pq_batch_launch_count(const pq_batch* b);
 
+/* ---- serving: many model runs, continuously batched --------------------- */
+
+/* Runs (CABARET, fixed dt) are queued by pq_server_submit and admitted while
+ * the device bytes of the admitted and pooled contexts stay within
+ * hbm_budget_bytes.  Each pq_server_poll retires finished runs, admits
+ * queued ones (initialisation + first step) and advances every active run
+ * by up to max_steps steps with one launch per kernel per shape group.  A
+ * run's result is bit-identical to running it alone (pq_init_perturb +
+ * pq_step).  Contexts of finished runs are pooled by configuration and
+ * reused. */
+typedef struct pq_server pq_server;
+PQ_API int pq_server_create(pq_server** out, size_t hbm_budget_bytes, int device);
+PQ_API void pq_server_destroy(pq_server* s);
+PQ_API const char* pq_server_last_error(const pq_server* s);
+/* zeta_ic: (ii, jj, L) host array, copied.  PQ_ERR_BUDGET: the run alone
+ * exceeds the budget. */
+PQ_API int pq_server_submit(pq_server* s, const pq_model_desc* desc, const double* zeta_ic, int nsteps, long* id);
+PQ_API int pq_server_poll(pq_server* s, int max_steps, int* active, int* queued);
+/* 0 queued, 1 running, 2 finished, -1 unknown id. */
+PQ_API int pq_server_status(pq_server* s, long id);
+/* psi (ii, jj, L) of a finished run and t3 = {submitted, started, finished}
+ * in seconds of pq_server_clock; releases the run (PQ_ERR_NOTFOUND after). */
+PQ_API int pq_server_collect(pq_server* s, long id, double* psi, double* t3);
+PQ_API size_t pq_server_device_bytes(const pq_server* s);
+PQ_API double pq_server_clock(const pq_server* s);
+PQ_API long pq_server_launches(const pq_server* s);
+
 /* Number of kernel launches the last pq_step enqueued. */
 PQ_API long pq_last_launch_count(const pq_ctx* ctx);
 

@@ -118,6 +118,16 @@ SIGNATURES = {
     "pq_batch_sync": (C.c_int, [C.c_void_p]),
     "pq_batch_helm": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.c_int]),
     "pq_batch_launch_count": (C.c_int, [C.c_void_p]),
+    "pq_server_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t, C.c_int]),
+    "pq_server_destroy": (None, [C.c_void_p]),
+    "pq_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "pq_server_submit": (C.c_int, [C.c_void_p, C.POINTER(ModelDesc), _dp, C.c_int, C.POINTER(C.c_long)]),
+    "pq_server_poll": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pq_server_status": (C.c_int, [C.c_void_p, C.c_long]),
+    "pq_server_collect": (C.c_int, [C.c_void_p, C.c_long, _dp, _dp]),
+    "pq_server_device_bytes": (C.c_size_t, [C.c_void_p]),
+    "pq_server_clock": (C.c_double, [C.c_void_p]),
+    "pq_server_launches": (C.c_long, [C.c_void_p]),
 }
 
 KERNELS = ("dst_forward", "tridiag", "dst_inverse_backproject", "cabaret_fused")
@@ -443,6 +453,74 @@ class Batch:
     def close(self):
         if self.ctx:
             lib().pq_batch_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuously batched serving of many runs (pq_server_*)."""
+
+    def __init__(self, hbm_budget_bytes: int, device: int = 0):
+        self.ctx = C.c_void_p()
+        self.shapes = {}
+        rc = lib().pq_server_create(C.byref(self.ctx), int(hbm_budget_bytes), device)
+        if rc != PQ_OK:
+            msg = lib().pq_server_last_error(self.ctx).decode() if self.ctx else ""
+            if self.ctx:
+                lib().pq_server_destroy(self.ctx)
+                self.ctx = None
+            raise PQError(rc, msg)
+
+    def _chk(self, rc):
+        if rc != PQ_OK:
+            raise PQError(rc, lib().pq_server_last_error(self.ctx).decode())
+
+    def submit(self, cfg: Config, zeta_ic, nsteps: int) -> int:
+        z = np.asfortranarray(zeta_ic, dtype=np.float64).reshape((cfg.ii, cfg.jj, cfg.layers), order="F")
+        rid = C.c_long()
+        self._chk(lib().pq_server_submit(self.ctx, C.byref(cfg.desc), _p(z), int(nsteps), C.byref(rid)))
+        self.shapes[rid.value] = (cfg.ii, cfg.jj, cfg.layers)
+        return rid.value
+
+    def poll(self, max_steps: int = 32):
+        a, q = C.c_int(), C.c_int()
+        self._chk(lib().pq_server_poll(self.ctx, int(max_steps), C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def status(self, rid: int) -> int:
+        return int(lib().pq_server_status(self.ctx, rid))
+
+    def collect(self, rid: int):
+        """(psi, (t_submit, t_start, t_done)) of a finished run."""
+        psi = np.zeros(self.shapes[rid], order="F")
+        t3 = np.zeros(3)
+        self._chk(lib().pq_server_collect(self.ctx, rid, _p(psi), _p(t3)))
+        del self.shapes[rid]
+        return psi, tuple(t3)
+
+    def run_until_done(self, max_steps: int = 32):
+        while True:
+            a, q = self.poll(max_steps)
+            if a == 0 and q == 0:
+                return
+
+    def clock(self) -> float:
+        return float(lib().pq_server_clock(self.ctx))
+
+    def device_bytes(self) -> int:
+        return int(lib().pq_server_device_bytes(self.ctx))
+
+    def launches(self) -> int:
+        return int(lib().pq_server_launches(self.ctx))
+
+    def close(self):
+        if self.ctx:
+            lib().pq_server_destroy(self.ctx)
             self.ctx = None
 
     def __del__(self):

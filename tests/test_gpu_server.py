@@ -1,0 +1,75 @@
+"""The continuously batched server (pq_server_*): every run's result is
+bit-identical to the same run alone (pq_init_perturb + pq_step), whatever it
+was batched with and however the budget staged it."""
+import numpy as np
+import pytest
+
+import pequod_b200 as pq
+
+pytestmark = pytest.mark.gpu
+
+
+def cfg_of(ii, layers, precision=pq.PREC_FP64, dt=1800.0):
+    H = {1: (1.0e5,), 2: (1.0e5, 3.0e5), 3: (3.0e4, 7.0e4, 3.0e5),
+         5: (2.5e4, 5.0e4, 7.5e4, 1.0e5, 1.5e5)}[layers]
+    gp = {1: (), 2: (1.5,), 3: (1.5, 0.75), 5: (1.5, 0.75, 0.375, 0.1875)}[layers]
+    p = pq.double_gyre_physical(ii, layers=layers, dt=dt, dx=3.84e8 / (ii - 1), H=H, gprime=gp,
+                                precision=precision)
+    return pq.Config.from_physical(p)
+
+
+def ic_of(cfg, seed):
+    return pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+
+
+def alone(cfg, ic, n):
+    m = pq.Model(cfg)
+    m.init_perturb(ic)
+    m.step(n)
+    out = m.get("psi")[1:-1, 1:-1, :]
+    m.close()
+    return out
+
+
+RUNS = [(65, 3, pq.PREC_FP64, 1, 7), (65, 3, pq.PREC_FP64, 2, 12), (129, 3, pq.PREC_FP64, 3, 5),
+        (65, 5, pq.PREC_FP64, 4, 9), (129, 3, pq.PREC_MIXED, 5, 6), (33, 1, pq.PREC_FP64, 6, 3),
+        (65, 3, pq.PREC_FP64, 7, 1)]
+
+
+def test_server_mix_equals_alone():
+    srv = pq.Server(8 << 30)
+    ids = []
+    for ii, L, prec, seed, n in RUNS:
+        cfg = cfg_of(ii, L, prec)
+        ids.append((srv.submit(cfg, ic_of(cfg, seed), n), cfg, seed, n))
+    srv.run_until_done(max_steps=4)
+    assert srv.launches() > 0
+    for rid, cfg, seed, n in ids:
+        assert srv.status(rid) == 2
+        psi, (t0, t1, t2) = srv.collect(rid)
+        assert t0 <= t1 <= t2
+        assert np.array_equal(psi, alone(cfg, ic_of(cfg, seed), n)), (cfg.ii, cfg.layers, n)
+        assert srv.status(rid) == -1
+    srv.close()
+
+
+def test_server_budget_staging_and_pool():
+    cfg = cfg_of(65, 3)
+    probe = pq.Model(cfg)
+    one = probe.device_bytes()
+    probe.close()
+    # Room for a single context: the runs go through one at a time, reusing it.
+    srv = pq.Server(int(one * 1.5))
+    rids = [srv.submit(cfg, ic_of(cfg, 10 + k), 4 + k) for k in range(3)]
+    a, q = srv.poll(2)
+    assert a == 1 and q == 2
+    srv.run_until_done(max_steps=2)
+    held = srv.device_bytes()
+    assert 0 < held <= int(one * 1.5)
+    for k, rid in enumerate(rids):
+        psi, _ = srv.collect(rid)
+        assert np.array_equal(psi, alone(cfg, ic_of(cfg, 10 + k), 4 + k))
+    with pytest.raises(pq.PQError) as e:
+        srv.submit(cfg_of(513, 5), np.zeros((513, 513, 5)), 1)
+    assert e.value.code == pq.PQ_ERR_BUDGET
+    srv.close()
