@@ -341,6 +341,181 @@ def run_ours(a, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_batched(a, rank, world, local_rank):
+    """Batched Helmholtz: 512 solves of mixed sizes (65..1025)^2 x 1..5 modes,
+    k^-3 Gaussian-random-field right-hand sides; one step = one solve of the
+    whole batch (device-resident data, graph replay).  Replicas for N > 1."""
+    import numpy as np
+    import torch
+
+    import pequod_b200 as pq
+    from pequod_b200.workloads import batched_helmholtz, gaussian_random_field
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    shapes, ss = batched_helmholtz(a.batch, seed=2 + rank)
+    b = pq.Batch(shapes, ss, device=local_rank)
+    # One right-hand side per distinct shape (the timing does not depend on the values).
+    rhs_of = {}
+    for k, sh in enumerate(shapes):
+        if sh not in rhs_of:
+            rhs_of[sh] = torch.from_numpy(np.asfortranarray(gaussian_random_field(*sh, seed=k)).ravel(order="F"))
+            rhs_of[sh] = rhs_of[sh].pin_memory()
+    for k, sh in enumerate(shapes):
+        lib = pq.lib()
+        lib.pq_batch_set_rhs(b.ctx, k, dptr(rhs_of[sh]), pq.PTR_HOST)
+    b.sync()
+    units = sum(i * j * l for i, j, l in shapes)
+    stream = torch.cuda.ExternalStream(b.stream, device=local_rank)
+    for _ in range(a.warmup):
+        b.solve_async()
+    b.sync()
+    K = a.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for k in range(K):
+            ev[k][0].record(stream)
+            b.solve_async()
+            ev[k][1].record(stream)
+        b.sync()
+    ms = float(sum(s_.elapsed_time(e_) for s_, e_ in ev))
+    # e2e: host right-hand sides in, solutions out, through pq_batch_helm.
+    arrs = [rhs_of[sh].clone().pin_memory() for sh in shapes]
+    ptrs = (pq._dp * len(arrs))(*[dptr(t) for t in arrs])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    KE = max(1, min(K, 5))
+    for _ in range(KE):
+        for k, sh in enumerate(shapes):
+            arrs[k].copy_(rhs_of[sh])
+        rc = pq.lib().pq_batch_helm(b.ctx, ptrs, pq.PTR_HOST)
+        assert rc == 0, pq.lib().pq_batch_last_error(b.ctx)
+    e2e_s = (time.perf_counter() - t0) / KE
+    if dist:
+        t = torch.tensor([ms, e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(t[0]), float(t[1])
+    if rank == 0:
+        peak, peak_kind = peaks()
+        per_solve_s = ms / K * 1e-3
+        alg = 48.0 * units  # forward DST 16 B, tridiagonal 16 B, inverse DST 16 B per cell-layer
+        cpu = None
+        if world == 1 and not a.no_cpu_baseline:
+            from oracle import oracle as O
+
+            t0 = time.perf_counter()
+            done_units, nsolve = 0, 0
+            order = sorted(range(len(shapes)), key=lambda k: shapes[k][0] * shapes[k][1] * shapes[k][2])
+            for k in order:
+                if time.perf_counter() - t0 > a.cpu_seconds:
+                    break
+                i, j, l = shapes[k]
+                O.Helm(i, j, l, list(ss[k]))(rhs_of[shapes[k]].numpy().reshape((i, j, l), order="F"))
+                done_units += i * j * l
+                nsolve += 1
+            secs = time.perf_counter() - t0
+            cpu = {"value": done_units / secs, "unit": "cell-layer-solves/s", "cores": 1, "kind": "port",
+                   "sample": f"{nsolve} smallest members solved by the oracle's helm in {secs:.1f} s"}
+        line = {
+            "metric": "cell-layer-solves/s", "value": world * units * K / (ms * 1e-3), "unit": "cell-layer-solves/s",
+            "n_gpus": world, "steps": K, "warmup": a.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"batched_helmholtz_{len(shapes)}", "solves_per_step": len(shapes),
+                       "cell_layers_per_step": units, "sizes": "ii, jj in {65..1025}, L in 1..5",
+                       "l2": f"inputs {8 * units / 1e9:.1f} GB >> L2", "parallelism": f"replicas{world}",
+                       "launches_per_solve": b.launch_count()},
+            "solves_per_s": world * len(shapes) * K / (ms * 1e-3),
+            "roofline": {"bound": "hbm", "kernel": "whole batch solve", "achieved": alg / per_solve_s / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": alg / per_solve_s / 1e9 / peak,
+                         "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * units / e2e_s, "unit": "cell-layer-solves/s",
+                    "h2d_bytes_per_step": 8 * units, "d2h_bytes_per_step": 8 * units},
+            "gpu_launches": b.launch_count() * K,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def dptr(t):
+    """double* of a torch tensor's storage."""
+    import ctypes
+
+    import pequod_b200 as pq
+
+    return ctypes.cast(ctypes.c_void_p(t.data_ptr()), pq._dp)
+
+
+def run_serving(a, rank, world, local_rank):
+    """Serving: Poisson arrivals at 200 runs/s over a window; double gyres of
+    129..1025 squared, 2-5 layers, 100-5000 steps; 150 GB HBM budget.  Reports
+    latency percentiles (arrival to result) and the aggregate throughput."""
+    import numpy as np
+    import torch
+
+    import pequod_b200 as pq
+    from pequod_b200.workloads import double_gyre, initial_condition, serving_requests
+
+    torch.cuda.set_device(local_rank)
+    reqs = serving_requests(rate=a.rate, window=a.window, seed=3 + rank)
+    cfgs = {}
+    srv = pq.Server(int(a.budget_gb * (1 << 30)), device=local_rank)
+    pending = list(reqs)
+    ids = {}
+    t_start = srv.clock()
+    with ClockSampler(local_rank) as clk:
+        while pending or ids:
+            now = srv.clock() - t_start
+            while pending and pending[0][0] <= now:
+                t_arr, ii, L, n, seed = pending.pop(0)
+                key = (ii, L)
+                if key not in cfgs:
+                    cfgs[key] = double_gyre(ii, L, 1800.0)
+                cfg = cfgs[key]
+                rid = srv.submit(cfg, initial_condition(cfg, seed), n)
+                ids[rid] = (t_arr, ii * ii * L * n)
+            if ids:
+                srv.poll(a.round_steps)
+            done = [rid for rid in ids if srv.status(rid) == 2]
+            for rid in done:
+                t_arr, work = ids.pop(rid)
+                _, t3 = srv.collect(rid)
+                lat = t3[2] - t_start - t_arr
+                ids_done.append((lat, work, t3[2] - t_start))
+            if not ids and pending:
+                time.sleep(max(0.0, min(0.01, pending[0][0] - (srv.clock() - t_start))))
+    lat = np.array([d[0] for d in ids_done])
+    work = float(sum(d[1] for d in ids_done))
+    span = max(d[2] for d in ids_done)
+    line = {
+        "metric": "serving latency p50/p99 (s)", "value": float(np.percentile(lat, 50)), "unit": "s",
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+        "n_gpus": 1, "steps": len(ids_done), "warmup": 0, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "serving_double_gyre", "rate_per_s": a.rate, "window_s": a.window,
+                   "runs": len(ids_done), "budget_gb": a.budget_gb, "round_steps": a.round_steps},
+        "throughput": {"value": work / span, "unit": "cell-layer-steps/s"},
+        "gpu_launches": srv.launches(), "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    srv.close()
+
+
+ids_done = []
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -353,13 +528,25 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="double-gyre", choices=["double-gyre", "batched-helm", "serving"])
+    ap.add_argument("--batch", type=int, default=512, help="batched-helm: solves per batch")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
+    ap.add_argument("--window", type=float, default=0.25, help="serving: seconds of arrivals")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
+    ap.add_argument("--round-steps", type=int, default=16, help="serving: steps per scheduling round")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if a.impl == "reference":
+    if a.workload == "batched-helm" and a.impl == "ours":
+        if a.steps == 2000:
+            a.steps = 20
+        run_batched(a, rank, world, local_rank)
+    elif a.workload == "serving" and a.impl == "ours":
+        run_serving(a, rank, world, local_rank)
+    elif a.impl == "reference":
         run_reference(a, rank, world)
     else:
         run_ours(a, rank, world, local_rank)

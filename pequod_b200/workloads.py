@@ -17,11 +17,16 @@ from __future__ import annotations
 
 import argparse
 
+import numpy as np
+
 import pequod_b200 as pq
 
 BASIN_CM = 3.84e8
 LAYERS = {
+    1: ((1.0e5,), ()),
+    2: ((1.0e5, 3.0e5), (1.5,)),
     3: ((3.0e4, 7.0e4, 3.0e5), (1.5, 0.75)),
+    4: ((3.0e4, 7.0e4, 1.5e5, 3.0e5), (1.5, 0.75, 0.375)),
     5: ((2.5e4, 5.0e4, 7.5e4, 1.0e5, 1.5e5), (1.5, 0.75, 0.375, 0.1875)),
 }
 
@@ -37,6 +42,63 @@ def double_gyre(ii: int, layers: int = 3, dt: float = 900.0, precision: int = pq
 
 def initial_condition(cfg: "pq.Config", seed: int = 1):
     return pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+
+
+GRID_SIZES = (65, 129, 257, 513, 1025)
+
+
+def gaussian_random_field(ii: int, jj: int, layers: int, seed: int, slope: float = -3.0):
+    """Seeded Gaussian random field with power spectrum |k|^slope (per layer),
+    unit RMS, Fortran order (ii, jj, layers)."""
+    rng = np.random.default_rng(seed)
+    ki = np.fft.fftfreq(ii)[:, None]
+    kj = np.fft.rfftfreq(jj)[None, :]
+    k = np.sqrt(ki * ki + kj * kj)
+    k[0, 0] = np.inf
+    amp = k ** (slope / 2.0)
+    out = np.empty((ii, jj, layers), order="F")
+    for l in range(layers):
+        w = np.fft.rfft2(rng.standard_normal((ii, jj)))
+        f = np.fft.irfft2(w * amp, s=(ii, jj))
+        out[:, :, l] = f / (np.sqrt(np.mean(f * f)) + 1e-300)
+    return out
+
+
+def batched_helmholtz(n: int = 512, seed: int = 2, sizes=GRID_SIZES, max_layers: int = 5):
+    """The batched-Helmholtz workload: n solves with ii and jj drawn
+    independently from `sizes`, L in 1..max_layers, layer depths
+    H ~ U[200, 4000] m and g'_k = 1.5 * 2^-k cm s^-2, ss from the
+    stratification eigenproblem of the double-gyre physics.  Returns
+    (shapes, ss) for pq.Batch."""
+    rng = np.random.default_rng(seed)
+    shapes, ss = [], []
+    for _ in range(n):
+        ii = int(rng.choice(sizes))
+        jj = int(rng.choice(sizes))
+        L = int(rng.integers(1, max_layers + 1))
+        H = tuple(float(h) for h in rng.uniform(2.0e4, 4.0e5, L))
+        gp = tuple(1.5 * 2.0 ** (-k) for k in range(L - 1))
+        p = pq.double_gyre_physical(ii, jj, layers=L, dt=900.0, dx=BASIN_CM / (ii - 1), H=H, gprime=gp)
+        cfg = pq.Config.from_physical(p)
+        shapes.append((ii, jj, L))
+        ss.append(np.array(cfg.desc.ss[:L]))
+    return shapes, ss
+
+
+def serving_requests(rate: float = 200.0, window: float = 1.0, seed: int = 3, sizes=(129, 257, 513, 1025),
+                     layers=(2, 3, 4, 5), steps=(100, 5000), dt: float = 1800.0):
+    """The serving workload: Poisson arrivals at `rate` per second over
+    `window` seconds; each request a double gyre on a size from `sizes`
+    (square), L from `layers`, a step count uniform in `steps`, and a seeded
+    1e-7 perturbation.  Returns [(arrival_s, ii, L, nsteps, seed)]."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > window:
+            return out
+        out.append((t, int(rng.choice(sizes)), int(rng.choice(layers)), int(rng.integers(steps[0], steps[1] + 1)),
+                    int(rng.integers(1 << 30))))
 
 
 def main(argv=None) -> None:
