@@ -114,20 +114,24 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def kernel_bytes_per_cell_layer(L, elem=8):
-    """Algorithmic bytes per cell-layer of each kernel of the fixed-dt FP64 step
-    (each array the kernel must touch, read or written once)."""
+def kernel_bytes_per_cell_layer(L, mixed=False):
+    """Algorithmic bytes per cell-layer of each kernel of the fixed-dt step
+    (each array the kernel must touch, read or written once, at its stored
+    width: FP64 everywhere, or for the mixed form FP32 layer fields and
+    baroclinic spectral rows with psi, corr, wind and the barotropic mode FP64)."""
+    w = 4 if mixed else 8                      # layer fields
+    spec = (8 + w * (L - 1)) / L               # spectral rows, averaged over the modes
     return {
         # zeta after predictor + beta in, spectral rows out
-        "dst_forward": 2 * elem,
+        "dst_forward": w + spec,
         # spectral rows in and out
-        "tridiag": 2 * elem,
+        "tridiag": 2 * spec,
         # spectral rows in, corr of the baroclinic modes in, psi out
-        "dst_inverse_backproject": (2 + (L - 1) / L) * elem,
-        # in: psi, zeta, zeta_old, uimo, ujmo, zeta_fi, zeta_fj, res_beta, wind/L;
-        # out: zeta_old, res, ui, uj, uimo, ujmo, zeta_fi, zeta_fj, and the next
-        # step's zeta and res_beta
-        "cabaret_fused": (18 + 1.0 / L) * elem,
+        "dst_inverse_backproject": spec + 8 * (L - 1) / L + 8,
+        # in: psi (FP64), wind/L (FP64), zeta, zeta_old, uimo, ujmo, zeta_fi,
+        # zeta_fj, res_beta; out: zeta_old, res, ui, uj, uimo, ujmo, zeta_fi,
+        # zeta_fj and the next step's zeta and res_beta
+        "cabaret_fused": 8 + 8.0 / L + 17 * w,
     }
 
 
@@ -297,14 +301,18 @@ def run_ours(a, rank, world, local_rank):
 
     # ---- roofline of the dominant kernel --------------------------------------
     peak, peak_kind = peaks()
-    bpc = kernel_bytes_per_cell_layer(cfg.layers)
+    bpc = kernel_bytes_per_cell_layer(cfg.layers, mixed=a.precision == "mixed")
     dom = max(kt, key=lambda k: kt[k][0])
     dom_ms = kt[dom][0] / max(1, kt[dom][1])
     alg = bpc[dom] * units
     achieved = alg / (dom_ms * 1e-3) / 1e9
     workload = f"double_gyre_{cfg.ii}x{cfg.jj}x{cfg.layers}_dt{int(a.dt)}s_cabaret"
     traffic = load_traffic(workload).get(dom)
-    step_alg = 8 * (22 + 1.0 / cfg.layers) * units  # SURVEY 8(d) B_alg(FP64) per step
+    # Compulsory bytes of one fused step (every array read or written once):
+    # 8 (22 + 1/L) B per cell-layer in FP64; 4 (20 + 1/L) + 8 * 2 B when all
+    # but psi is stored in FP32.
+    L_ = cfg.layers
+    step_alg = (8 * (22 + 1.0 / L_) if a.precision == "fp64" else 4 * (20 + 1.0 / L_) + 16) * units
     shares = {k: round(v[0] / max(1e-30, sum(x[0] for x in kt.values())), 4) for k, v in kt.items()}
     clocks = clk.summary()
 
