@@ -261,13 +261,17 @@ PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int 
 
 /* Tile parameters of the step kernels (chosen per grid size by the
  * autotuner, pequod_b200/autotune.py; defaults are set by pq_create).
- *   cab_band   output rows per warp of the fused CABARET sweep, 4..128
+ *   cab_kernel CABARET step formulation: 0 one CTA per 28 x 16 tile and
+ *              layer, 1 warp sweeps down bands of cab_band rows (default:
+ *              tiles up to jj = 700, sweeps above)
+ *   cab_band   output rows per warp of the sweep formulation, 4..128
  *   dst_group  row groups per DST CTA: a CTA holds dst_group * layers
  *              warps (0: automatic, 1); layers * dst_group <= 8 */
 typedef struct pq_tuning {
     int cab_band;
     int dst_group;
-    int reserved[6];
+    int cab_kernel;
+    int reserved[5];
 } pq_tuning;
 PQ_API int pq_set_tuning(pq_ctx* ctx, const pq_tuning* t);
 PQ_API int pq_get_tuning(pq_ctx* ctx, pq_tuning* t);

@@ -60,7 +60,7 @@ class ModelDesc(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("cab_band", C.c_int), ("dst_group", C.c_int), ("reserved", C.c_int * 6)]
+    _fields_ = [("cab_band", C.c_int), ("dst_group", C.c_int), ("cab_kernel", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class Physical(C.Structure):
@@ -375,7 +375,7 @@ class Model:
     def get_tuning(self) -> dict:
         t = Tuning()
         _check(lib().pq_get_tuning(self.ctx, C.byref(t)), self.ctx)
-        return {"cab_band": t.cab_band, "dst_group": t.dst_group}
+        return {"cab_band": t.cab_band, "dst_group": t.dst_group, "cab_kernel": t.cab_kernel}
 
     def kernel_timing(self, enable: bool) -> None:
         _check(lib().pq_kernel_timing(self.ctx, int(enable)), self.ctx)

@@ -1,4 +1,5 @@
 // pq_api.cu -- the C ABI: contexts, device state, tables and the time loop.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -244,8 +245,11 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     // Default CABARET band height by grid size (measured on B200: shorter
     // bands give small grids enough warps, taller ones cut halo rows on big ones).
     const int cab_sh = jj <= 300 ? 8 : jj <= 700 ? 32 : 64;
-    const int ntiles_cab = cabaret_ctas(ii, jj, L, cab_sh);
-    const int ntiles_cab_max = cabaret_ctas(ii, jj, L, kMinBand);
+    // CABARET formulation by grid size (measured on B200): tiles up to
+    // 700 rows, warp sweeps above (pq_tuning.cab_kernel overrides).
+    const int cab_kernel = jj <= 700 ? 0 : 1;
+    const int ntiles_cab = cab_kernel == 0 ? cabaret_tile_ctas(ii, jj, L) : cabaret_ctas(ii, jj, L, cab_sh);
+    const int ntiles_cab_max = std::max(cabaret_ctas(ii, jj, L, kMinBand), cabaret_tile_ctas(ii, jj, L));
 
     // Tables.
     std::vector<double2> tw(M), wsplit(M);
@@ -468,6 +472,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         s.ctas_tri = ntiles_tri;
         s.ctas_cab = ntiles_cab;
         s.dst_group = 0;
+        s.cab_kernel = cab_kernel;
         s.sm_count = sm_count;
         s.prefix_dst[0] = s.prefix_dst[1] = c->d_prefix;
         const int R = dst_rows_per_cta_host(N / 2, L, 0);
@@ -695,9 +700,12 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     if (t->cab_band < kMinBand || t->cab_band > kMaxBand) return fail(c, PQ_ERR_ARG, "cab_band out of range");
     CK(cudaStreamSynchronize(c->stream));
     if (t->dst_group < 0 || c->L * t->dst_group > 8) return fail(c, PQ_ERR_ARG, "dst_group out of range");
+    if (t->cab_kernel < 0 || t->cab_kernel > 1) return fail(c, PQ_ERR_ARG, "cab_kernel out of range");
     for (int p = 0; p < 2; ++p) {
         c->hm[p].cab_sh = t->cab_band;
-        c->hm[p].ntiles_cab = cabaret_ctas(c->ii, c->jj, c->L, t->cab_band);
+        c->hm[p].ntiles_cab = t->cab_kernel ? cabaret_ctas(c->ii, c->jj, c->L, t->cab_band)
+                                            : cabaret_tile_ctas(c->ii, c->jj, c->L);
+        c->ls[p].cab_kernel = t->cab_kernel;
         c->ls[p].ctas_cab = c->hm[p].ntiles_cab;
         c->ls[p].dst_group = t->dst_group;
         const int R = dst_rows_per_cta_host(c->hm[p].M, c->L, t->dst_group);
@@ -718,6 +726,7 @@ int pq_get_tuning(pq_ctx* c, pq_tuning* t) {
     if (!c || !t) return PQ_ERR_ARG;
     std::memset(t, 0, sizeof(*t));
     t->cab_band = c->hm[0].cab_sh;
+    t->cab_kernel = c->ls[0].cab_kernel;
     t->dst_group = c->ls[0].dst_group;
     return PQ_OK;
 }

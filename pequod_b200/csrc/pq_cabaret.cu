@@ -405,6 +405,38 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     return umax;
 }
 
+// Last CTA of a member: max |u| over the CTAs' partial maxima, the CFL
+// number, model time, and when adaptive stepping is on dt and the time
+// weights for the next step (cabaret_cfl / cabaret_adapt_dt,
+// qg3p_aux.F90:920-990).
+// Called by every thread of the last CTA; red: shared scratch of blockDim/32.
+__device__ void finish_step(const Member& Mb, double* red) {
+    __threadfence();
+    const double mu = block_max_l2(Mb.maxu_part, Mb.ntiles_cab, red);
+    if (threadIdx.x != 0) return;
+    Scalars* sc = Mb.sc;
+    sc->max_u = mu;
+    sc->cfl = mu * sc->dt;
+    sc->dt_last = sc->dt;
+    sc->tweight_a_last = sc->tweight_a;
+    sc->tweight_u_last = sc->tweight_u;
+    sc->model_time += sc->dt;
+    if (Mb.adapt_dt) {
+        const double old_dt = sc->dt;
+        double ndt = old_dt;
+        const double tol = 10.0 * fmax(fabs(mu) * 2.220446049250313e-16, 2.220446049250313e-16);
+        if (fabs(mu) > tol) {
+            ndt = Mb.target_cfl / mu;
+            ndt = fmin(fmin(ndt, old_dt * Mb.max_dt_increase), Mb.max_dt);
+        }
+        sc->dt = ndt;
+        sc->tweight_a = 0.5 * ndt / old_dt;
+        sc->tweight_u = ndt / (old_dt + ndt);
+        if (ndt < 1.0e-6) atomicOr(Mb.status, (int)ST_SMALL_DT);
+    }
+    Mb.counters[1] = 0u;
+}
+
 template <bool PRED, typename T>
 __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* __restrict__ mems,
                                                                     const int* __restrict__ prefix, int nmem) {
@@ -449,33 +481,461 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
         is_last = (prev == (unsigned)(Mb.ntiles_cab - 1));
     }
     __syncthreads();
-    if (is_last && threadIdx.x == 0) {
-        __threadfence();
-        const volatile double* part = Mb.maxu_part;
-        double mu = 0.0;
-        for (int q = 0; q < Mb.ntiles_cab; ++q) mu = fmax(mu, part[q]);
-        Scalars* sc = Mb.sc;
-        sc->max_u = mu;
-        sc->cfl = mu * sc->dt;
-        sc->dt_last = sc->dt;
-        sc->tweight_a_last = sc->tweight_a;
-        sc->tweight_u_last = sc->tweight_u;
-        sc->model_time += sc->dt;
-        if (Mb.adapt_dt) {
-            const double old_dt = sc->dt;
-            double ndt = old_dt;
-            const double tol = 10.0 * fmax(fabs(mu) * 2.220446049250313e-16, 2.220446049250313e-16);
-            if (fabs(mu) > tol) {
-                ndt = Mb.target_cfl / mu;
-                ndt = fmin(fmin(ndt, old_dt * Mb.max_dt_increase), Mb.max_dt);
-            }
-            sc->dt = ndt;
-            sc->tweight_a = 0.5 * ndt / old_dt;
-            sc->tweight_u = ndt / (old_dt + ndt);
-            if (ndt < 1.0e-6) atomicOr(Mb.status, (int)ST_SMALL_DT);
+    if (is_last) finish_step(Mb, red);
+}
+
+// ---------------------------------------------------------------------------
+// Tile formulation of the same fused step: one CTA (8 warps) per (layer,
+// CT_X x CT_Y tile of output nodes).  Every stage is computed once per node
+// or face of the tile's footprint into shared memory, stages separated by
+// block barriers; lane = column, warps stride over rows.  All footprint
+// arrays share one 32-column frame whose column 0 is node i0-2 and row 0 is
+// node j0-2 (a face a sits in the column of node a, a corner between columns
+// c-1 and c in column c).  For outputs i in [i0, i0+CT_X), j in [j0, j0+CT_Y):
+//   psi (3 layers), zeta, rel   nodes [i0-2, i0+CT_X+1] x [j0-2, j0+CT_Y+1]
+//   corner psi                  columns [i0-1, i0+CT_X+1], rows [j0-1, j0+CT_Y+1]
+//   zeta after forcing, zeta_old   nodes [i0-1, i0+CT_X] x [j0-1, j0+CT_Y]
+//   ui, zeta_fi (old)           faces a in [i0-1, i0+CT_X+1], rows [j0, j0+CT_Y)
+//   uj, zeta_fj (old)           faces b in [j0-1, j0+CT_Y+1], columns [i0, i0+CT_X)
+//   flux_i / flux_j             faces a in [i0, i0+CT_X] / b in [j0, j0+CT_Y]
+// Each output node owns face a = i (ui, uimo, zeta_fi) and face b = j (uj,
+// ujmo, zeta_fj), as in the sweep.  EDGE = false: the whole footprint is at
+// least one node inside the domain, so no bounds checks or boundary branches.
+constexpr int CT_X = 28, CT_Y = 16, CT_THREADS = 256, CT_W = 32, CT_H = CT_Y + 4;
+constexpr int CT_N = CT_W * CT_H;  // entries of one frame array
+
+template <typename T>
+struct TileSmem {
+    // doubles: psi, psi above, psi below, corner psi; T: zeta, rel, zf, zo,
+    // ui, fio, uj, fj.  The fluxes reuse the psi-above / psi-below space.
+    static constexpr size_t bytes() { return 4 * CT_N * sizeof(double) + 8 * CT_N * sizeof(T); }
+};
+
+// rows handled by a warp in a frame row range of length h: ceil(h / 8)
+__host__ __device__ constexpr int ct_rows(int h) { return (h + 7) / 8; }
+
+template <bool PRED, bool EDGE, typename T>
+__device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int j0, char* smem) {
+    const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
+    const long long ls = Mb.lstride;
+    const int cur = Mb.cur, nxt = cur ^ 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const T dt = (T)Mb.sc->dt, tu = (T)Mb.sc->tweight_u, ta = (T)Mb.sc->tweight_a;
+    const T hdt = (T)0.5 * dt;
+    const double s1 = Mb.s1[l], s2 = Mb.s2[l];
+    const int bc = Mb.bc_type;
+    const double cffbc = Mb.alpha / (Mb.alpha + 3.0);
+    const bool lim = Mb.limiter != 0;
+    const bool top = (l == 0), bottom = (l == L - 1);
+    const T nu = (T)Mb.viscosity, vb = (T)Mb.visc_bot, beta_l = (T)Mb.beta[l];
+    const long long lo = l * ls;
+    // This lane's column: node i0 - 2 + lane; the row of frame row r is j0 - 2 + r.
+    const int ic = i0 - 2 + lane;
+    const long long gcol = lo + ic;
+    auto grow = [&](int r) { return (long long)(j0 - 2 + r) * pitch; };
+    const bool col_in = !EDGE || (ic >= 0 && ic < ii);
+    const bool col_int = !EDGE || (ic > 0 && ic < ii - 1);
+    auto row_in = [&](int r) { return !EDGE || (j0 - 2 + r >= 0 && j0 - 2 + r < jj); };
+    auto row_int = [&](int r) { return !EDGE || (j0 - 2 + r > 0 && j0 - 2 + r < jj - 1); };
+    const bool ui_col = !EDGE || (ic >= 1 && ic <= ii - 1);   // face a = ic can exist
+    const bool uj_col = !EDGE || (ic >= 1 && ic <= ii - 2);   // column ic can carry j-faces
+    auto ui_row = [&](int r) { return !EDGE || (j0 - 2 + r >= 1 && j0 - 2 + r <= jj - 2); };
+    auto uj_row = [&](int r) { return !EDGE || (j0 - 2 + r >= 1 && j0 - 2 + r <= jj - 1); };
+
+    double* sPsi = reinterpret_cast<double*>(smem);
+    double* sPm = sPsi + CT_N;
+    double* sPp = sPm + CT_N;
+    double* sPe = sPp + CT_N;
+    T* sZpb = reinterpret_cast<T*>(sPe + CT_N);
+    T* sRel = sZpb + CT_N;
+    T* sZf = sRel + CT_N;
+    T* sZo = sZf + CT_N;
+    T* sUi = sZo + CT_N;
+    T* sFio = sUi + CT_N;
+    T* sUj = sFio + CT_N;
+    T* sFj = sUj + CT_N;
+    T* sFli = reinterpret_cast<T*>(sPm);  // after the face velocities
+    T* sFlj = sFli + CT_N;
+    auto X = [&](int r, int c) { return r * CT_W + c; };  // frame index
+
+    // Limited upwind extrapolation (cabaret_extrapolator, interior branch).
+    auto extrap = [&](T u1, T u2, T fi1, T fi2, T psi_n, T psi_o, bool pos) -> T {
+        const T v0 = (u1 + u2) / (T)2;
+        const T d_f = pos ? -(psi_n - psi_o) * (T)2 - dt * v0 * (fi1 - fi2)
+                          : -(psi_n - psi_o) * (T)2 - dt * v0 * (fi2 - fi1);
+        T v = (T)2 * psi_n - fi2;
+        if (lim) {
+            const T fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+            const T fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+            if (v > fmx) v = fmx;
+            if (v < fmn) v = fmn;
         }
-        Mb.counters[1] = 0u;
+        return v;
+    };
+    // The wall branch: upwind node on the boundary.
+    auto extrap_wall = [&](T fi1, T psi_n, T psi_o) -> T {
+        const T fi2 = psi_n;
+        const T d_f = -(psi_n - psi_o);
+        T v = (T)2 * psi_n - fi2;
+        if (lim) {
+            const T fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+            const T fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+            if (v > fmx) v = fmx;
+            if (v < fmn) v = fmn;
+        }
+        return v;
+    };
+
+    const T* zpb = reinterpret_cast<const T*>(Mb.zeta);
+    const double* wind = (top && Mb.wind) ? Mb.wind : nullptr;
+    // ---- loads used by later stages, issued first (held in registers) -----
+    // frame rows: zf 1..CT_Y+2, ui rows 2..CT_Y+1, uj rows 1..CT_Y+3, outputs 2..CT_Y+1
+    constexpr int NZ = ct_rows(CT_Y + 2), NU = ct_rows(CT_Y), NV = ct_rows(CT_Y + 3);
+    T rWind[NZ], rUimo[NU], rUjmo[NV], rRb[NU];
+    {
+        const T* uimo = reinterpret_cast<const T*>(Mb.uimo[cur]);
+        const T* ujmo = reinterpret_cast<const T*>(Mb.ujmo[cur]);
+        const T* rb = reinterpret_cast<const T*>(Mb.res_beta);
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) {
+            const int r = 1 + warp + 8 * k;
+            rWind[k] = (wind && r < CT_Y + 3 && lane >= 1 && lane <= CT_X + 2 && col_int && row_int(r))
+                           ? (T)wind[grow(r) + ic]
+                           : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NU; ++k) {
+            const int r = 2 + warp + 8 * k;
+            const bool ok = r < CT_Y + 2;
+            rUimo[k] = (ok && lane >= 1 && lane <= CT_X + 3 && ui_col && ui_row(r)) ? uimo[grow(r) + gcol] : (T)0;
+            rRb[k] = (PRED && ok && lane >= 2 && lane < CT_X + 2 && col_int && row_int(r)) ? rb[grow(r) + gcol] : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const int r = 1 + warp + 8 * k;
+            rUjmo[k] = (r < CT_Y + 4 && lane >= 2 && lane < CT_X + 2 && uj_col && uj_row(r)) ? ujmo[grow(r) + gcol]
+                                                                                             : (T)0;
+        }
     }
+
+    // ---- stage 1: psi (three layers), zeta, zeta_old, old face values ------
+    {
+        constexpr int NP = ct_rows(CT_H);
+        const double* psi = Mb.psi;
+        const long long om = (l > 0) ? -ls : 0, op = (l < L - 1) ? ls : 0;
+        const T* zold = reinterpret_cast<const T*>(Mb.zeta_old[cur]);
+        const T* fio = reinterpret_cast<const T*>(Mb.zfi[cur]);
+        const T* fjo = reinterpret_cast<const T*>(Mb.zfj[cur]);
+        double vP[NP], vM[NP], vQ[NP];
+        T vZ[NP], vO[NZ], vF[NU], vG[NV];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const int r = warp + 8 * k;
+            const bool ok = r < CT_H && col_in && row_in(r);
+            const long long o = grow(r) + gcol;
+            vP[k] = ok ? psi[o] : 0.0;
+            vM[k] = (ok && L > 1) ? psi[o + om] : 0.0;
+            vQ[k] = (ok && L > 1) ? psi[o + op] : 0.0;
+            vZ[k] = (ok && col_int && row_int(r)) ? zpb[o] : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) {
+            const int r = 1 + warp + 8 * k;
+            vO[k] = (r < CT_Y + 3 && lane >= 1 && lane <= CT_X + 2 && col_in && row_in(r)) ? zold[grow(r) + gcol]
+                                                                                           : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NU; ++k) {
+            const int r = 2 + warp + 8 * k;
+            vF[k] = (r < CT_Y + 2 && lane >= 1 && lane <= CT_X + 3 && ui_col && ui_row(r)) ? fio[grow(r) + gcol]
+                                                                                          : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const int r = 1 + warp + 8 * k;
+            vG[k] = (r < CT_Y + 4 && lane >= 2 && lane < CT_X + 2 && uj_col && uj_row(r)) ? fjo[grow(r) + gcol]
+                                                                                          : (T)0;
+        }
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const int r = warp + 8 * k;
+            if (r < CT_H) {
+                sPsi[X(r, lane)] = vP[k];
+                sPm[X(r, lane)] = vM[k];
+                sPp[X(r, lane)] = vQ[k];
+                sZpb[X(r, lane)] = vZ[k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) {
+            const int r = 1 + warp + 8 * k;
+            if (r < CT_Y + 3) sZo[X(r, lane)] = vO[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NU; ++k) {
+            const int r = 2 + warp + 8 * k;
+            if (r < CT_Y + 2) sFio[X(r, lane)] = vF[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const int r = 1 + warp + 8 * k;
+            if (r < CT_Y + 4) sFj[X(r, lane)] = vG[k];
+        }
+    }
+    __syncthreads();
+
+    // ---- stage 2: rel (rel_from_zeta_and_psi + apply_rel_bc), corner psi ---
+#pragma unroll
+    for (int k = 0; k < ct_rows(CT_H); ++k) {
+        const int r = warp + 8 * k;
+        if (r >= CT_H) break;
+        const int q = X(r, lane);
+        T rel = (T)0;
+        if (col_in && row_in(r)) {
+            const int j = j0 - 2 + r;
+            const double p = sPsi[q];
+            const bool bj = EDGE && (j == 0 || j == jj - 1), bi = EDGE && (ic == 0 || ic == ii - 1);
+            if (bj || bi) {
+                // Corners take the j-boundary formula, which the reference applies last.
+                if (bc != 3) {
+                    double q1, q2;
+                    if (bj) {
+                        const int d = (j == 0) ? CT_W : -CT_W;
+                        q1 = sPsi[q + d];
+                        q2 = sPsi[q + 2 * d];
+                    } else {
+                        const int d = (ic == 0) ? 1 : -1;
+                        q1 = sPsi[q + d];
+                        q2 = sPsi[q + 2 * d];
+                    }
+                    rel = (T)((bc == 1) ? cffbc * (-3.5 * p + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - p));
+                }
+            } else {
+                const T z = sZpb[q];
+                if (L == 1)
+                    rel = z;
+                else if (top)
+                    rel = (T)((double)z + s2 * (p - sPp[q]));
+                else if (bottom)
+                    rel = (T)((double)z + s1 * (p - sPm[q]));
+                else
+                    rel = (T)((double)z + s1 * (p - sPm[q]) + s2 * (p - sPp[q]));
+            }
+        }
+        sRel[q] = rel;
+    }
+#pragma unroll
+    for (int k = 0; k < ct_rows(CT_Y + 3); ++k) {
+        const int r = 1 + warp + 8 * k;  // corner between rows r-1 and r
+        if (r >= CT_H) break;
+        if (lane >= 1) {
+            const int q = X(r, lane);     // corner between columns lane-1 and lane
+            sPe[q] = 0.25 * (sPsi[q] + sPsi[q - CT_W] + sPsi[q - 1] + sPsi[q - CT_W - 1]);
+        }
+    }
+    __syncthreads();
+
+    // ---- stage 3: zeta after update_zeta_bc + forcing; face velocities -----
+    double umax = 0.0;
+#pragma unroll
+    for (int k = 0; k < NZ; ++k) {
+        const int r = 1 + warp + 8 * k;
+        if (r >= CT_Y + 3) break;
+        if (lane < 1 || lane > CT_X + 2) continue;
+        const int q = X(r, lane);
+        T zf = (T)0;
+        if (col_in && row_in(r)) {
+            const T R = sRel[q];
+            if (EDGE && !(col_int && row_int(r))) {
+                const double p = sPsi[q];
+                if (L == 1)
+                    zf = R;
+                else if (top)
+                    zf = (T)((double)R - s2 * (p - sPp[q]));
+                else if (bottom)
+                    zf = (T)((double)R - s1 * (p - sPm[q]));
+                else
+                    zf = (T)((double)R - s1 * (p - sPm[q]) - s2 * (p - sPp[q]));
+            } else {
+                const T lap = (T)-4 * R + sRel[q - 1] + sRel[q + 1] + sRel[q - CT_W] + sRel[q + CT_W];
+                const T w = rWind[k];
+                T rv;
+                if (L == 1)
+                    rv = dt * (w - vb * R + nu * lap);
+                else if (top)
+                    rv = dt * (w + nu * lap);
+                else if (bottom)
+                    rv = dt * (-vb * R + nu * lap);
+                else
+                    rv = dt * nu * lap;
+                zf = sZpb[q] + rv;
+            }
+        }
+        sZf[q] = zf;
+    }
+    T* ui_g = reinterpret_cast<T*>(Mb.ui);
+    T* uimo_n = reinterpret_cast<T*>(Mb.uimo[nxt]);
+    T* uj_g = reinterpret_cast<T*>(Mb.uj);
+    T* ujmo_n = reinterpret_cast<T*>(Mb.ujmo[nxt]);
+    const bool own_col = lane >= 2 && lane < CT_X + 2;  // columns of the tile's outputs
+#pragma unroll
+    for (int k = 0; k < NU; ++k) {
+        const int r = 2 + warp + 8 * k;  // face a = ic on row r
+        if (r >= CT_Y + 2) break;
+        if (lane < 1 || lane > CT_X + 3) continue;
+        const int q = X(r, lane);
+        T u = (T)0;
+        if (ui_col && ui_row(r)) {
+            // corners (a, rows r-1|r) and (a, rows r|r+1)
+            const T um = (T)(sPe[q] - sPe[q + CT_W]);
+            u = ((T)1 + tu) * um - tu * rUimo[k];
+            if (own_col) {
+                const long long o = grow(r) + gcol;
+                ui_g[o] = u;
+                uimo_n[o] = um;
+                umax = fmax(umax, (double)fabs(u));
+            }
+        }
+        sUi[q] = u;
+    }
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const int r = 1 + warp + 8 * k;  // face b = row r, column ic
+        if (r >= CT_Y + 4) break;
+        if (!own_col) continue;
+        const int q = X(r, lane);
+        T u = (T)0;
+        if (uj_col && uj_row(r)) {
+            // corners (columns ic|ic+1, rows r-1|r) and (ic-1|ic, r-1|r)
+            const T um = (T)(sPe[q + 1] - sPe[q]);
+            u = ((T)1 + tu) * um - tu * rUjmo[k];
+            if (r >= 2 && r < CT_Y + 2) {
+                const long long o = grow(r) + gcol;
+                uj_g[o] = u;
+                ujmo_n[o] = um;
+                umax = fmax(umax, (double)fabs(u));
+            }
+        }
+        sUj[q] = u;
+    }
+    __syncthreads();
+
+    // ---- stage 4: extrapolated face values (cabaret_extrapolator) and fluxes
+    T* fin_g = reinterpret_cast<T*>(Mb.zfi[nxt]);
+    T* fjn_g = reinterpret_cast<T*>(Mb.zfj[nxt]);
+#pragma unroll
+    for (int k = 0; k < NU; ++k) {
+        const int r = 2 + warp + 8 * k;  // face a = ic on row r, a in [i0, i0+CT_X]
+        if (r >= CT_Y + 2) break;
+        if (lane < 2 || lane > CT_X + 2) continue;
+        const int q = X(r, lane);
+        T flux = (T)0;
+        if (ui_col && ui_row(r)) {
+            const T u1 = sUi[q];
+            T f;
+            if (u1 >= (T)0)
+                f = (!EDGE || ic > 1) ? extrap(u1, sUi[q - 1], sFio[q], sFio[q - 1], sZf[q - 1], sZo[q - 1], true)
+                                      : extrap_wall(sFio[q], sZf[q - 1], sZo[q - 1]);
+            else
+                f = (!EDGE || ic < ii - 1) ? extrap(u1, sUi[q + 1], sFio[q], sFio[q + 1], sZf[q], sZo[q], false)
+                                           : extrap_wall(sFio[q], sZf[q], sZo[q]);
+            if (own_col) fin_g[grow(r) + gcol] = f;
+            flux = u1 * f;
+        }
+        sFli[q] = flux;
+    }
+#pragma unroll
+    for (int k = 0; k < ct_rows(CT_Y + 1); ++k) {
+        const int r = 2 + warp + 8 * k;  // face b = row r in [j0, j0+CT_Y], column ic
+        if (r >= CT_Y + 3) break;
+        if (!own_col) continue;
+        const int q = X(r, lane);
+        const int b = j0 - 2 + r;
+        T flux = (T)0;
+        if (uj_col && uj_row(r)) {
+            const T u1 = sUj[q];
+            T f;
+            if (u1 >= (T)0)
+                f = (!EDGE || b > 1)
+                        ? extrap(u1, sUj[q - CT_W], sFj[q], sFj[q - CT_W], sZf[q - CT_W], sZo[q - CT_W], true)
+                        : extrap_wall(sFj[q], sZf[q - CT_W], sZo[q - CT_W]);
+            else
+                f = (!EDGE || b < jj - 1) ? extrap(u1, sUj[q + CT_W], sFj[q], sFj[q + CT_W], sZf[q], sZo[q], false)
+                                          : extrap_wall(sFj[q], sZf[q], sZo[q]);
+            if (r < CT_Y + 2) fjn_g[grow(r) + gcol] = f;
+            flux = u1 * f;
+        }
+        sFlj[q] = flux;
+    }
+    __syncthreads();
+
+    // ---- stage 5: cabaret_corrector (+ the next step's predictor and beta) --
+    T* res_g = reinterpret_cast<T*>(Mb.res);
+    T* zn_g = reinterpret_cast<T*>(Mb.zeta_old[nxt]);
+    T* rbn_g = reinterpret_cast<T*>(Mb.res_beta_other);
+    T* zpn_g = reinterpret_cast<T*>(Mb.zeta_next);
+#pragma unroll
+    for (int k = 0; k < NU; ++k) {
+        const int r = 2 + warp + 8 * k;
+        if (r >= CT_Y + 2) break;
+        if (!own_col || !(col_in && row_in(r))) continue;
+        const int q = X(r, lane);
+        const long long o = grow(r) + gcol;
+        T z = sZf[q];
+        if (col_int && row_int(r)) {
+            const T rr = -(sFli[q + 1] - sFli[q] + sFlj[q + CT_W] - sFlj[q]);
+            res_g[o] = rr;
+            z = z + hdt * rr;
+            if (PRED) {
+                // cabaret_predictor (qg3p_aux.F90:1012-1018) and cabaret_beta
+                // (:1051-1059) of the next step with this step's ui.
+                T zz = z + hdt * rr;
+                const T rbn = dt * ((T)0.5 * (sUi[q + 1] + sUi[q]) * beta_l);
+                zz = zz + ((T)1 + ta) * rbn - ta * rRb[k];
+                rbn_g[o] = rbn;
+                zpn_g[o] = zz;
+            }
+        }
+        zn_g[o] = z;
+    }
+    return umax;
+}
+
+template <bool PRED, typename T>
+__global__ void __launch_bounds__(CT_THREADS) k_cabaret_tile(const Member* __restrict__ mems,
+                                                              const int* __restrict__ prefix, int nmem) {
+    __shared__ Member Mb;
+    __shared__ double red[CT_THREADS / 32];
+    __shared__ int is_last;
+    extern __shared__ __align__(16) char tsm[];
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
+    load_member_c(Mb, mems + mi);
+    __syncthreads();
+    const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
+    const int tx = (ii + CT_X - 1) / CT_X;
+    const int l = local % L;
+    const int tile = local / L;
+    const int i0 = (tile % tx) * CT_X, j0 = (tile / tx) * CT_Y;
+    // Interior tiles: footprint [i0-2, i0+CT_X+1] x [j0-2, j0+CT_Y+1] inside
+    // the interior nodes.
+    const bool inner = i0 - 2 >= 1 && i0 + CT_X + 1 <= ii - 2 && j0 - 2 >= 1 && j0 + CT_Y + 1 <= jj - 2;
+    double umax = inner ? cab_tile<PRED, false, T>(Mb, l, i0, j0, tsm) : cab_tile<PRED, true, T>(Mb, l, i0, j0, tsm);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    umax = warp_max(umax);
+    if (lane == 0) red[warp] = umax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < CT_THREADS / 32; ++w) t = fmax(t, red[w]);
+        Mb.maxu_part[local] = t;
+        __threadfence();
+        const unsigned prev = atomicAdd(&Mb.counters[1], 1u);
+        is_last = (prev == (unsigned)(Mb.ntiles_cab - 1));
+    }
+    __syncthreads();
+    if (is_last) finish_step(Mb, red);
 }
 
 int cabaret_ctas(int ii, int jj, int L, int sh) {
@@ -483,8 +943,20 @@ int cabaret_ctas(int ii, int jj, int L, int sh) {
     return (nstrips * nbands * L + CAB_WARPS - 1) / CAB_WARPS;
 }
 
+int cabaret_tile_ctas(int ii, int jj, int L) {
+    return ((ii + CT_X - 1) / CT_X) * ((jj + CT_Y - 1) / CT_Y) * L;
+}
+
 template <bool PRED, typename T>
 static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
+    if (ls.cab_kernel == 0) {
+        const size_t tb = TileSmem<T>::bytes();
+        cudaError_t e =
+            cudaFuncSetAttribute(k_cabaret_tile<PRED, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb);
+        if (e != cudaSuccess) return e;
+        k_cabaret_tile<PRED, T><<<ls.ctas_cab, CT_THREADS, tb, st>>>(ls.members, ls.prefix_cab, ls.nmem);
+        return cudaGetLastError();
+    }
     const size_t bytes = (size_t)CAB_WARPS * CAB_RING * sizeof(double);
     cudaError_t e =
         cudaFuncSetAttribute(k_cabaret_fused<PRED, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -614,13 +1086,11 @@ __global__ void __launch_bounds__(256) k_energy(const Member* __restrict__ mems,
         is_last = (prev == (unsigned)(jj - 1));
     }
     __syncthreads();
-    if (!is_last || threadIdx.x != 0) return;
+    if (!is_last) return;
     __threadfence();
-    const volatile double* part = Mb.partials;
     double tot[PQ_MAXL + 1];
-    for (int q = 0; q <= L; ++q) tot[q] = 0.0;
-    for (int r = 0; r < jj; ++r)
-        for (int q = 0; q <= L; ++q) tot[q] += part[(long long)r * (PQ_MAXL + 1) + q];
+    for (int q = 0; q <= L; ++q) tot[q] = block_sum_l2(Mb.partials + q, jj, PQ_MAXL + 1, &red[0][0]);
+    if (threadIdx.x != 0) return;
     Scalars* sc = Mb.sc;
     const double cff = Mb.mean_scale;
     const double epot = cff * tot[L];

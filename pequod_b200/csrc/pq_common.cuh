@@ -191,6 +191,38 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
+// Block-wide reductions of n partial results that other CTAs wrote (the
+// "last CTA finishes" pattern): every thread of the block takes part, the
+// values are read through L2 (__ldcg: written by other SMs after their
+// fence), and the result is valid in thread 0.  The sum has a fixed order
+// (per-thread strided sums, warp butterflies, warps in order), so it does not
+// depend on which CTA finished last.  red: shared scratch of blockDim/32.
+__device__ __forceinline__ double block_max_l2(const double* p, int n, double* red) {
+    double m = 0.0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) m = fmax(m, __ldcg(p + q));
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, red[w]);
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ double block_sum_l2(const double* p, int n, long long stride, double* red) {
+    double s = 0.0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) s += __ldcg(p + q * stride);
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += red[w];
+    __syncthreads();
+    return r;
+}
+
 // Relative vorticity at node (i, j) of layer l from zeta and psi
 // (rel_from_zeta_and_psi) with the boundary condition of apply_rel_bc.
 // ps(i, j, l) reads staged psi.  Corners take the j-boundary formula, which

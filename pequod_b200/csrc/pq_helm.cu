@@ -565,7 +565,10 @@ struct PivotRow {
 
 // S = float: the mixed form, whose baroclinic spectral rows are FP32 (staged
 // and solved in FP64); the barotropic mode (m = 0) comes from spec64.
-template <typename S>
+// GS = true: the reciprocal pivots of the strip are staged in shared memory
+// beside it (same layout), so the recurrences never wait on a global load;
+// used whenever both strips fit.
+template <typename S, bool GS>
 __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restrict__ mems,
                                                           const int* __restrict__ prefix, int nmem, int do_mean) {
     __shared__ Member Mb;
@@ -593,12 +596,35 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     // Asynchronous 8-byte copies (cp.async), so the loads of a thread do not
     // wait for one another; columns past n are zero-filled (source size 0).
     // FP32 rows are loaded and widened in registers.
+    double* gstrip = strip + TRI_KT * CS;  // pivots (GS)
     {
         const int c = threadIdx.x & 7, q = threadIdx.x >> 3;
         const bool colok = (k0 + c < n);
         const long long go = (long long)(q * R + 1) * pitch + (colok ? k0 + c : 0);
         double* sdst = strip + c * CS + q * RS;
         const int Rq = min(R, Mr - q * R);
+        if (GS) {
+            // g(p) for the rows p = q*R + 1 .. of this chunk: the stored
+            // reciprocal pivots up to len, then the fixed point.
+            double* gdst = gstrip + c * CS + q * RS;
+            if (colok) {
+                const int mk = m * n + k0 + c;
+                const int off = __ldg(&Mb.piv_off[mk]), len = __ldg(&Mb.piv_len[mk]);
+                const double fix = __ldg(&Mb.piv_fix[mk]);
+                const unsigned gbase = (unsigned)__cvta_generic_to_shared(gdst);
+                for (int t = 0; t < Rq; ++t) {
+                    const int pp = q * R + 1 + t;
+                    if (pp <= len)
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(gbase + 8u * t),
+                                     "l"(Mb.piv + off + pp - 1)
+                                     : "memory");
+                    else
+                        gdst[t] = fix;
+                }
+            } else {
+                for (int t = 0; t < Rq; ++t) gdst[t] = 0.0;
+            }
+        }
         if (!f32) {
             const double* g = spec + go;
             const unsigned sbase = (unsigned)__cvta_generic_to_shared(sdst);
@@ -613,6 +639,8 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
             const float* g = specf + go;
 #pragma unroll 4
             for (int t = 0; t < Rq; ++t) sdst[t] = colok ? (double)g[(long long)t * pitch] : 0.0;
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
     }
     __syncthreads();
@@ -628,14 +656,24 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         const int cnt = max(0, min(R, Mr - lane * R));
         const int b = a + cnt - 1;
         double* s = strip + c * CS + lane * RS;     // s[t] is position a + t
+        const double* gs = gstrip + c * CS + lane * RS;  // GS: gs[t] = g(a + t)
+        // g(p) for p in [a - 1, b]: g(a - 1) is the previous chunk's last pivot.
+        auto G = [&](int p) -> double {
+            if constexpr (GS) {
+                const int t = p - a;
+                return t >= 0 ? gs[t] : gstrip[c * CS + (lane - 1) * RS + (R - 1)];
+            } else {
+                return g(p);
+            }
+        };
         // Forward elimination, local: y~_a = f_a, y~_p = f_p - g_{p-1} y~_{p-1};
         // y_p = y~_p + A_p y_{a-1}, A_a = -g_{a-1}, A_p = -g_{p-1} A_{p-1}.
         double A = 1.0, cend = 0.0;
         if (cnt > 0) {
             double y = s[0];
-            A = (a > 1) ? -g(a - 1) : 0.0;
+            A = (a > 1) ? -G(a - 1) : 0.0;
             for (int t = 1; t < cnt; ++t) {
-                const double gp = g(a + t - 1);
+                const double gp = G(a + t - 1);
                 y = s[t] - gp * y;
                 s[t] = y;
                 A = -gp * A;
@@ -660,18 +698,18 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         // B_b = -g_b, B_p = -g_p B_{p+1}.
         double B = 1.0, cstart = 0.0;
         if (cnt > 0) {
-            double Ap = (a > 1) ? -g(a - 1) : 0.0;
+            double Ap = (a > 1) ? -G(a - 1) : 0.0;
             s[0] = s[0] + Ap * yin;
             for (int t = 1; t < cnt; ++t) {
-                Ap = -g(a + t - 1) * Ap;
+                Ap = -G(a + t - 1) * Ap;
                 s[t] = s[t] + Ap * yin;
             }
-            const double gb = g(b);
+            const double gb = G(b);
             double x = s[cnt - 1] * gb;
             s[cnt - 1] = x;
             B = -gb;
             for (int t = cnt - 2; t >= 0; --t) {
-                const double gp = g(a + t);
+                const double gp = G(a + t);
                 x = (s[t] - x) * gp;
                 s[t] = x;
                 B = -gp * B;
@@ -693,12 +731,12 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         if (lane == 31) xin = 0.0;
         double lsum = 0.0;
         if (cnt > 0) {
-            double Bp = -g(b);
+            double Bp = -G(b);
             double v = s[cnt - 1] + Bp * xin;
             s[cnt - 1] = v;
             lsum += v;
             for (int t = cnt - 2; t >= 0; --t) {
-                Bp = -g(a + t) * Bp;
+                Bp = -G(a + t) * Bp;
                 v = s[t] + Bp * xin;
                 s[t] = v;
                 lsum += v;
@@ -736,16 +774,15 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     if (!is_last) return;
     // Last CTA of this member: psiC_m = (sum of partials) / (g_ii_int g_jj_int),
     // summed in a fixed order so that the result is independent of CTA timing.
-    if (threadIdx.x < Mb.L) {
-        __threadfence();
-        const int mm = threadIdx.x;
-        const volatile double* part = Mb.partials;
-        double t = 0.0;
-        for (int q = 0; q < tiles_per_mode; ++q) t += part[mm * tiles_per_mode + q];
-        const double pc = t * Mb.mean_scale;
-        Mb.sc->psiC[mm] = pc;
-        if (pc != pc) atomicOr(Mb.status, (int)ST_NAN_PSIC);
-        else if (fabs(pc) > 1.0e100) atomicOr(Mb.status, (int)ST_LARGE_PSIC);
+    __threadfence();
+    for (int mm = 0; mm < Mb.L; ++mm) {
+        const double t = block_sum_l2(Mb.partials + (long long)mm * tiles_per_mode, tiles_per_mode, 1, wpart);
+        if (threadIdx.x == 0) {
+            const double pc = t * Mb.mean_scale;
+            Mb.sc->psiC[mm] = pc;
+            if (pc != pc) atomicOr(Mb.status, (int)ST_NAN_PSIC);
+            else if (fabs(pc) > 1.0e100) atomicOr(Mb.status, (int)ST_LARGE_PSIC);
+        }
     }
     if (threadIdx.x == 0) Mb.counters[0] = 0u;
 }
@@ -805,18 +842,21 @@ cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, int f32, cudaS
     return f32 ? launch_dst<float, PRO_PLAIN, EPI_PV>(ls, st) : launch_dst<double, PRO_PLAIN, EPI_PV>(ls, st);
 }
 
+template <typename S, bool GS>
+static cudaError_t launch_tri(const LaunchSet& ls, int do_mean, size_t bytes, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(k_tridiag<S, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    k_tridiag<S, GS><<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, int f32, cudaStream_t st) {
     const size_t bytes = tri_smem_bytes(ls.maxJ);
-    if (f32) {
-        cudaError_t e = cudaFuncSetAttribute(k_tridiag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        if (e != cudaSuccess) return e;
-        k_tridiag<float><<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
-    } else {
-        cudaError_t e = cudaFuncSetAttribute(k_tridiag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        if (e != cudaSuccess) return e;
-        k_tridiag<double><<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
-    }
-    return cudaGetLastError();
+    // Pivots staged beside the strip when both fit; the FP32 form (whose
+    // strip is loaded synchronously) only while two CTAs still fit an SM.
+    const bool gs = 2 * bytes <= (f32 ? 100 : 160) * 1024;
+    if (f32) return gs ? launch_tri<float, true>(ls, do_mean, 2 * bytes, st) : launch_tri<float, false>(ls, do_mean, bytes, st);
+    return gs ? launch_tri<double, true>(ls, do_mean, 2 * bytes, st) : launch_tri<double, false>(ls, do_mean, bytes, st);
 }
 
 }  // namespace pq

@@ -24,6 +24,7 @@ struct LaunchSet {
     const int* prefix_dst[2];         // DST CTAs per member, forward [0] and inverse [1]
     int ctas_dst[2];                  //   (ceil(rows / dst_rows_per_cta) per member)
     int dst_group;                    // row groups per DST CTA (0: automatic)
+    int cab_kernel;                   // CABARET formulation: 0 tiles, 1 warp sweeps
     int sm_count;                     // SMs of the device (persistent grids)
 };
 
@@ -39,7 +40,8 @@ cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, int f32, cudaStream
 // pq_cabaret.cu
 // predict_next: also apply the next step's predictor + beta (fixed dt only)
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, int f32, cudaStream_t st);
-int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of k_cabaret_fused per member (band height sh)
+int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of the sweep kernel per member (band height sh)
+int cabaret_tile_ctas(int ii, int jj, int L);     // CTAs of the tile kernel per member
 cudaError_t launch_rel(const LaunchSet& ls, int f32, cudaStream_t st);
 cudaError_t launch_init_finish(const LaunchSet& ls, int f32, cudaStream_t st);
 // pq_leapfrog.cu

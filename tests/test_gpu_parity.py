@@ -220,14 +220,15 @@ def test_energy_kats_gpu():
     assert abs(ep - ep_o) <= 1e-13 * abs(ep_o)
 
 
-@pytest.mark.parametrize("band,group", [(4, 0), (8, 1), (32, 2), (128, 1)])
-def test_tile_parameters_do_not_change_results(band, group):
-    """The CABARET band height and the DST CTA width are tuning knobs: results
-    must match the oracle for any choice."""
+@pytest.mark.parametrize("kernel,band,group", [(1, 4, 0), (1, 8, 1), (1, 32, 2), (1, 128, 1), (0, 16, 2)])
+def test_tile_parameters_do_not_change_results(kernel, band, group):
+    """The CABARET formulation (tiles or warp sweeps), the sweep's band height
+    and the DST CTA width are tuning knobs: results must match the oracle for
+    any choice."""
     cfg = double_gyre(129, 3)
     g, o = start(cfg, seed=5)
-    g.set_tuning(cab_band=band, dst_group=group)
-    assert g.get_tuning() == {"cab_band": band, "dst_group": group}
+    g.set_tuning(cab_kernel=kernel, cab_band=band, dst_group=group)
+    assert g.get_tuning() == {"cab_band": band, "dst_group": group, "cab_kernel": kernel}
     g.step(3)
     o.step(3)
     compare(g, o, TOL_STEP * 10)
