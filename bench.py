@@ -238,8 +238,19 @@ def run_ours(a, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    # ---- timed region: K steps, L2 flushed before each ----------------------
+    # ---- per-kernel times: eager launches with CUDA events between kernels --
     m.kernel_timing(True)
+    with torch.cuda.stream(stream):
+        for k in range(min(K, 200)):
+            flush.zero_()
+            m.step_async(1)
+    stream.synchronize()
+    m.check()
+    m.kernel_timing(False)
+    kt = m.kernel_times()
+    m.step(2)  # back to graph launches (one-step graphs of each parity)
+
+    # ---- timed region: K steps (one-step graphs), L2 flushed before each -----
     barrier()
     with ClockSampler(dev) as clk:
         with torch.cuda.stream(stream):
@@ -251,10 +262,8 @@ def run_ours(a, rank, world, local_rank):
         stream.synchronize()
     barrier()
     m.check()
-    m.kernel_timing(False)
     step_ms = [s.elapsed_time(e) for s, e in ev]
     total_ms = float(sum(step_ms))
-    kt = m.kernel_times()
     if dist:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

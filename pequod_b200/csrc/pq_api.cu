@@ -188,6 +188,8 @@ void pq_destroy(pq_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph2) cudaGraphExecDestroy(c->graph2);
+    for (auto& g : c->graph1)
+        if (g) cudaGraphExecDestroy(g);
     if (c->arena) cudaFree(c->arena);
     if (c->d_members) cudaFree(c->d_members);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
@@ -653,10 +655,34 @@ int pq_step_async(pq_ctx* c, int nsteps) {
     CK(cudaSetDevice(c->device));
     int done = 0;
     long launches = 0;
-    // Eager steps until the graph's entry state: parity 0 and, with the fused
-    // predictor, the next step's inversion input already computed.
+    // One step at parity par: a captured one-step graph once the step's
+    // variant is settled (fused predictor ready, or not fusing), else eager
+    // (also when per-kernel timing is on).
+    auto one = [&](int par) -> int {
+        if (c->timing || (c->fuse && !c->pred_ready)) return run_step(c, par);
+        if (!c->graph1[par]) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+            const int rc = run_step(c, par);
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (rc) return rc;
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&c->graph1[par], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+        } else {
+            CK(cudaGraphLaunch(c->graph1[par], c->stream));
+            c->pred_ready = c->fuse;
+            c->zpar = par;
+            return PQ_OK;
+        }
+        CK(cudaGraphLaunch(c->graph1[par], c->stream));
+        return PQ_OK;
+    };
+    // Single steps until the two-step graph's entry state: parity 0 and, with
+    // the fused predictor, the next step's inversion input already computed.
     while (done < nsteps && (c->cur == 1 || (c->fuse && !c->pred_ready))) {
-        int rc = run_step(c, c->cur);
+        int rc = one(c->cur);
         if (rc) return rc;
         c->cur ^= 1;
         ++done;
@@ -685,7 +711,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         }
     }
     if (done < nsteps) {
-        int rc = run_step(c, 0);
+        int rc = one(0);
         if (rc) return rc;
         c->cur = 1;
         ++done;
@@ -714,6 +740,11 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     }
     int rc = upload_members(c);
     if (rc) return rc;
+    for (auto& g : c->graph1)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
     if (c->graph2) {
         cudaGraphExecDestroy(c->graph2);
         c->graph2 = nullptr;

@@ -36,7 +36,8 @@ struct pq_ctx {
     bool leapfrog = false;    // PQ_SCHEME_LEAPFROG: cur is the level advanced next (lf - 1)
     bool pred_ready = false;  // zeta[cur] / res_beta[cur] already hold the next step's predictor
     int zpar = 0;             // parity whose zeta entered the last inversion
-    cudaGraphExec_t graph2 = nullptr;
+    cudaGraphExec_t graph2 = nullptr;     // two steps (parity 0, 1)
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step of each parity
     std::string err;
     long last_launches = 0;
     // Per-kernel CUDA-event timing of eagerly launched steps.
