@@ -206,7 +206,9 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     if (!out || !d) return PQ_ERR_ARG;
     *out = nullptr;
     const int ii = d->ii, jj = d->jj, L = d->layers;
-    if (ii < 5 || jj < 5 || !is_pow2(ii - 1) || L < 1 || L > PQ_MAX_LAYERS || d->periodic_j) return PQ_ERR_ARG;
+    if (ii < 5 || jj < 5 || !is_pow2(ii - 1) || L < 1 || L > PQ_MAX_LAYERS) return PQ_ERR_ARG;
+    // A channel periodic in j is supported by the Helmholtz solver (pq_helm);
+    // the time step of a channel (its momentum correction) is not built.
     if (d->precision != PQ_PREC_FP64 && d->precision != PQ_PREC_MIXED) return PQ_ERR_UNSUPPORTED;
     if (d->scheme != PQ_SCHEME_CABARET && d->scheme != PQ_SCHEME_LEAPFROG) return PQ_ERR_UNSUPPORTED;
     // The leapfrog scheme runs in FP64 with a fixed dt (the reference's
@@ -303,6 +305,54 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     const size_t o_plen = take(pv.len.size() * sizeof(int));
     const size_t o_piv = take(pv.piv.size() * sizeof(double));
     const size_t o_pfix = take(pv.fix.size() * sizeof(double));
+    // periodic_coefficients (qg3p_helmholtz.F90:473-559) of a channel: for
+    // each (mode, k) the vectors b, c over j = 1..jj, computed exactly as the
+    // reference does from the pivots e of poinit_j (:429-469).
+    std::vector<double> pbv, pcv;
+    if (d->periodic_j) {
+        pbv.assign((size_t)L * jj * n, 0.0);
+        pcv.assign((size_t)L * jj * n, 0.0);
+        const double cff = 3.14159265358979323846 / (2.0 * (double)(ii - 1));
+        std::vector<double> e(jj + 1), b(jj + 1), cc(jj + 1);
+        for (int mm = 0; mm < L; ++mm)
+            for (int k = 1; k <= n; ++k) {
+                const double sn = std::sin((double)k * cff);
+                const double v = -2.0 - d->ss[mm] - 4.0 * (sn * sn);
+                for (int j = 1; j <= jj; ++j) e[j] = v;
+                for (int j = 3; j <= jj - 1; ++j) e[j] = e[j] - 1.0 / e[j - 1];
+                for (int j = 2; j <= jj - 1; ++j) e[j] = 1.0 / e[j];
+                b[1] = v;
+                b[2] = 1.0;
+                for (int j = 3; j <= jj - 1; ++j) b[j] = 0.0;
+                b[jj] = 1.0;
+                cc[1] = 1.0;
+                for (int j = 2; j <= jj - 2; ++j) cc[j] = 0.0;
+                cc[jj - 1] = 1.0;
+                cc[jj] = v;
+                for (int j = 3; j <= jj - 1; ++j) {
+                    b[j] = b[j] - b[j - 1] * e[j - 1];
+                    cc[j] = cc[j] - cc[j - 1] * e[j - 1];
+                }
+                b[jj - 1] = b[jj - 1] * e[jj - 1];
+                cc[jj - 1] = cc[jj - 1] * e[jj - 1];
+                for (int j = jj - 2; j >= 2; --j) {
+                    b[j] = (b[j] - b[j + 1]) * e[j];
+                    cc[j] = (cc[j] - cc[j + 1]) * e[j];
+                }
+                b[1] = b[1] - b[2];
+                cc[1] = cc[1] - cc[2];
+                b[jj] = b[jj] - b[jj - 1];
+                cc[jj] = cc[jj] - cc[jj - 1];
+                cc[1] = cc[1] / b[1];
+                for (int j = 2; j <= jj; ++j) cc[j] = cc[j] - cc[1] * b[j];
+                for (int j = 1; j <= jj; ++j) {
+                    pbv[((size_t)mm * jj + (j - 1)) * n + (k - 1)] = b[j];
+                    pcv[((size_t)mm * jj + (j - 1)) * n + (k - 1)] = cc[j];
+                }
+            }
+    }
+    const size_t o_pb = take(pbv.size() * sizeof(double));
+    const size_t o_pc = take(pcv.size() * sizeof(double));
     const size_t npart = std::max((size_t)ntiles_tri, (size_t)jj * (PQ_MAXL + 1));
     const size_t o_part = take(npart * sizeof(double));
     const size_t o_maxu = take(ntiles_cab_max * sizeof(double));
@@ -325,6 +375,10 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     CK(cudaMemcpyAsync(A + o_plen, pv.len.data(), pv.len.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_piv, pv.piv.data(), pv.piv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_pfix, pv.fix.data(), pv.fix.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (!pbv.empty()) {
+        CK(cudaMemcpyAsync(A + o_pb, pbv.data(), pbv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(A + o_pc, pcv.data(), pcv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
     if (!c->wind.empty())
         CK(cudaMemcpy2DAsync(A + o_wind, (size_t)c->pitch * sizeof(double), c->wind.data(), (size_t)ii * sizeof(double),
                              (size_t)ii * sizeof(double), jj, cudaMemcpyHostToDevice, c->stream));
@@ -371,6 +425,10 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     m.piv_len = reinterpret_cast<const int*>(A + o_plen);
     m.piv = reinterpret_cast<const double*>(A + o_piv);
     m.piv_fix = reinterpret_cast<const double*>(A + o_pfix);
+    m.periodic = d->periodic_j ? 1 : 0;
+    m.pb = pbv.empty() ? nullptr : reinterpret_cast<const double*>(A + o_pb);
+    m.pc = pcv.empty() ? nullptr : reinterpret_cast<const double*>(A + o_pc);
+    c->periodic = d->periodic_j != 0;
     char* F = A + o_fields;
     int fi = 0;
     auto fld = [&]() { return (void*)(F + fb * (fi++)); };
@@ -477,8 +535,9 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         s.cab_kernel = cab_kernel;
         s.sm_count = sm_count;
         s.prefix_dst[0] = s.prefix_dst[1] = c->d_prefix;
+        s.periodic = c->periodic ? 1 : 0;
         const int R = dst_rows_per_cta_host(N / 2, L, 0);
-        s.ctas_dst[0] = (jj - 2 + R - 1) / R;
+        s.ctas_dst[0] = ((c->periodic ? jj : jj - 2) + R - 1) / R;
         s.ctas_dst[1] = (jj + R - 1) / R;
     }
     // Scalars: dt and the initial time weights.
@@ -493,7 +552,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     // (qg3p_aux.F90:196-230): solve with a unit right-hand side, Dirichlet 0,
     // then corr = (1 + ss psi) / (1 + ss mean(psi)) with the plain interior
     // mean the reference uses there.
-    if (!helm_only) {
+    if (!helm_only && !c->periodic) {
         std::vector<double> ones((size_t)ii * jj * L, 1.0);
         rc = copy_in(c, m.helm_io, ones.data(), PQ_PTR_HOST);
         if (rc) return rc;
@@ -539,6 +598,7 @@ int pq_helm(pq_ctx* c, double* zeta, int ptr_kind) {
 
 int pq_pv_inversion(pq_ctx* c, const double* zeta, double* psi, int ptr_kind) {
     if (!c || !zeta || !psi) return PQ_ERR_ARG;
+    if (c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "the channel (periodic j) time step is not built; pq_helm only");
     CK(cudaSetDevice(c->device));
     int rc = copy_in_state(c, c->hm[c->cur].zeta, zeta, ptr_kind);
     if (rc) return rc;
@@ -554,6 +614,7 @@ int pq_pv_inversion(pq_ctx* c, const double* zeta, double* psi, int ptr_kind) {
 
 int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     if (!c || !zeta_ic) return PQ_ERR_ARG;
+    if (c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "the channel (periodic j) time step is not built; pq_helm only");
     CK(cudaSetDevice(c->device));
     const int ii = c->ii, jj = c->jj, L = c->L;
     const int nlev = c->leapfrog ? 2 : 1;  // init_rand fills both leapfrog levels
@@ -735,7 +796,7 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
         c->ls[p].ctas_cab = c->hm[p].ntiles_cab;
         c->ls[p].dst_group = t->dst_group;
         const int R = dst_rows_per_cta_host(c->hm[p].M, c->L, t->dst_group);
-        c->ls[p].ctas_dst[0] = (c->jj - 2 + R - 1) / R;
+        c->ls[p].ctas_dst[0] = ((c->periodic ? c->jj : c->jj - 2) + R - 1) / R;
         c->ls[p].ctas_dst[1] = (c->jj + R - 1) / R;
     }
     int rc = upload_members(c);

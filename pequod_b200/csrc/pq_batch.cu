@@ -158,7 +158,7 @@ int pq_batch_create(pq_batch** out, int n, const int* ii, const int* jj, const i
     };
     std::vector<Pending> pd, pt;
     for (auto& kv : dk) {
-        pq_batch::Class cl;
+        pq_batch::Class cl{};
         cl.idx = kv.second;
         Pending p;
         p.mem_off = hd.size();
@@ -193,7 +193,7 @@ int pq_batch_create(pq_batch** out, int n, const int* ii, const int* jj, const i
         pd.push_back(p);
     }
     for (auto& kv : tk) {
-        pq_batch::Class cl;
+        pq_batch::Class cl{};
         cl.idx = kv.second;
         Pending p;
         p.mem_off = ht.size();

@@ -79,6 +79,9 @@ struct Member {
     const float2* tw_f;     // FP32 copies of tw, wsplit, was (mixed path)
     const float2* wsplit_f;
     const float* was_f;
+    int periodic;           // 1: channel periodic in j (helm only)
+    const double* pb;       // periodic_coefficients b, c of the channel,
+    const double* pc;       //   [(m * jj + j) * n + k-1], j 0-based
     int mixed;              // 1: FP32 storage of the CABARET fields and the
                             // baroclinic spectral rows (see spec64)
     // Compressed tridiagonal pivots, per (mode, k): piv[off + p - 1] for

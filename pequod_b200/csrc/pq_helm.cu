@@ -316,7 +316,8 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
     const int R = dst_rows_per_cta(M, L, c);
     const int U = dst_unit_len(N);
     const int j0 = row_offset + local * R;                 // first row of this CTA
-    const int jend = (EPI == EPI_SPEC) ? jj - 1 : jj;       // one past the last row
+    // one past the last row; a channel periodic in j transforms every row
+    const int jend = (EPI == EPI_SPEC && !Mb.periodic) ? jj - 1 : jj;
     const int nthr = blockDim.x;
     double* extra = sm + (size_t)L * R * U;                 // EPI_PV: corr rows [R][L-1][pitch];
                                                             // mixed forward: staged rows [R][L][N] (FP32)
@@ -439,7 +440,7 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
         for (int rm = warp; rm < R * L; rm += nwarp) {
             const int m = rm / R, r = rm - m * R;
             const int j = j0 + r;
-            const bool ok = j >= 1 && j <= jj - 2 && j < jend;
+            const bool ok = (Mb.periodic || (j >= 1 && j <= jj - 2)) && j < jend;
             if (fp64_mode(m)) {
                 const double* g = (MX ? Mb.spec64 : reinterpret_cast<const double*>(Mb.spec)) + m * ls +
                                   (long long)(ok ? j : 1) * pitch - 1;
@@ -472,7 +473,7 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
     const int um = u / R, ur = u - um * R;
     const int ju = j0 + ur;
     double* buf = ubuf(um, ur);
-    const bool interior = ju >= 1 && ju <= jj - 2 && ju < jend;
+    const bool interior = (Mb.periodic || (ju >= 1 && ju <= jj - 2)) && ju < jend;
     if (fp64_mode(um))
         dst_unit<V, double>(buf, p, P, N, M, logM, Mb.tw, Mb.wsplit, Mb.was);
     else
@@ -499,7 +500,7 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
             if (interior) {
                 for (int k = 1 + p; k <= n; k += P) io[k] = buf[xpad(k)];
                 if (p == 0) io[ii - 1] = 0.0;
-            } else if (ju == 0) {
+            } else if (ju == 0 && !Mb.periodic) {
                 for (int k = 1 + p; k <= n; k += P) io[k] = 0.0;
             }
         }
@@ -742,6 +743,31 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                 lsum += v;
             }
         }
+        if (Mb.periodic) {
+            // periodic_ge (qg3p_helmholtz.F90:565-610): the cyclic closure
+            // through the rows 1 and jj, which the Thomas solve above leaves
+            // out, as two rank-one corrections with the precomputed b, c.
+            __syncwarp();
+            const double* pb = Mb.pb + (long long)m * jj * n + kk;
+            const double* pc = Mb.pc + (long long)m * jj * n + kk;
+            double z1 = 0.0, zj = 0.0;
+            if (lane == 0) {
+                const int ql = (Mr - 1) / R, tl = (Mr - 1) - ql * R;
+                const double z2 = strip[c * CS];                 // row 2 (1-based) after the solve
+                const double zl = strip[c * CS + ql * RS + tl];  // row jj-1
+                const double z1i = spec[kk], zji = spec[(long long)(jj - 1) * pitch + kk];
+                z1 = (z1i - z2) / __ldg(&pb[0]);
+                zj = ((zji - zl) - z1 * __ldg(&pb[(long long)(jj - 1) * n])) / __ldg(&pc[(long long)(jj - 1) * n]);
+                spec[kk] = z1 - zj * __ldg(&pc[0]);
+                spec[(long long)(jj - 1) * pitch + kk] = zj;
+            }
+            z1 = __shfl_sync(0xffffffffu, z1, 0);
+            zj = __shfl_sync(0xffffffffu, zj, 0);
+            for (int t = 0; t < cnt; ++t) {
+                const long long row = a + t;  // 0-based grid row
+                s[t] = (s[t] - z1 * __ldg(&pb[row * n])) - zj * __ldg(&pc[row * n]);
+            }
+        }
         if (do_mean) colsum = warp_sum(lsum) * __ldg(&Mb.wmean[kk]);
     }
     if (lane == 0) wpart[warp] = colsum;
@@ -810,8 +836,8 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
         cudaFuncSetAttribute(k_dst<S, V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     const int dir = (EPI == EPI_SPEC) ? 0 : 1;
-    k_dst<S, V, PRO, EPI><<<ls.ctas_dst[dir], threads, bytes, st>>>(ls.members, ls.prefix_dst[dir], ls.nmem,
-                                                                  EPI == EPI_SPEC ? 1 : 0, ls.dst_group, corr_smem);
+    k_dst<S, V, PRO, EPI><<<ls.ctas_dst[dir], threads, bytes, st>>>(
+        ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0, ls.dst_group, corr_smem);
     return cudaGetLastError();
 }
 

@@ -25,6 +25,7 @@ struct LaunchSet {
     int ctas_dst[2];                  //   (ceil(rows / dst_rows_per_cta) per member)
     int dst_group;                    // row groups per DST CTA (0: automatic)
     int cab_kernel;                   // CABARET formulation: 0 tiles, 1 warp sweeps
+    int periodic;                     // channel periodic in j: every row is transformed
     int sm_count;                     // SMs of the device (persistent grids)
 };
 

@@ -24,11 +24,12 @@ def rel_l2(a, b):
     return np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0)
 
 
-def helm_cfg(ii, jj, ss):
+def helm_cfg(ii, jj, ss, periodic=False):
     """A context whose layers are Helmholtz problems with the given ss."""
     L = len(ss)
     d = pq.ModelDesc()
     d.ii, d.jj, d.layers = ii, jj, L
+    d.periodic_j = int(periodic)
     d.limiter, d.bc_type, d.dt = 1, pq.BC_FREE_SLIP, 1.0
     for k in range(L):
         d.ss[k] = ss[k]
@@ -82,6 +83,54 @@ def test_helm_convergence_gpu(ss, min_order):
         m = pq.Model(helm_cfg(g, g, [ss]))
         out = m.helm(np.asfortranarray(rhs[:, :, None]))
         out = O.apply_dirichlet_bc(out, 0.0)
+        errs.append(np.abs(out[:, :, 0] - exact).max())
+        m.close()
+    orders = [-math.log10(errs[n] / errs[n - 1]) / math.log10(sizes[n] / sizes[n - 1]) for n in range(1, len(errs))]
+    assert min(orders) >= min_order, orders
+
+
+@pytest.mark.parametrize("ii,jj,ss", [
+    (33, 64, [0.0]),
+    (65, 128, [0.0, 2.0]),
+    (129, 40, [0.5, 0.0, 7.0]),
+    (257, 512, [0.0, 1.07613857]),
+])
+def test_helm_periodic_matches_oracle(ii, jj, ss):
+    """The channel (periodic in j): Thomas solve plus periodic_ge's cyclic
+    closure, qg3p_helmholtz.F90:473-610, against the oracle."""
+    rng = np.random.default_rng(ii + 3 * jj)
+    L = len(ss)
+    rhs = np.asfortranarray(rng.standard_normal((ii, jj, L)))
+    g = pq.Model(helm_cfg(ii, jj, ss, periodic=True))
+    out = g.helm(rhs)
+    ref = O.Helm(ii, jj, L, ss, periodic_j=True)(rhs)
+    for l in range(L):
+        assert rel_l2(out[:, :, l], ref[:, :, l]) <= TOL_STEP, (l, rel_l2(out[:, :, l], ref[:, :, l]))
+    assert np.array_equal(out[0, :, :], rhs[0, :, :])
+    with pytest.raises(pq.PQError):
+        g.init_perturb(np.zeros((ii, jj, L)))
+
+
+@pytest.mark.parametrize("ss,min_order", [(0.0, 2.0), (0.5, 3.9)])
+def test_helm_periodic_convergence_gpu(ss, min_order):
+    """test_helmholtz.F90:249-357 (periodic channel) through the CUDA path."""
+    PI = math.pi
+    sizes = (33, 65, 129, 257, 513, 1025)
+    errs = []
+    for g in sizes:
+        ii, jj = g, (g - 1) * 2
+        i = np.arange(1, ii + 1)[:, None]
+        j = np.arange(1, jj + 1)[None, :]
+        x = (j - 1) / jj
+        y = (ii - i) / (ii - 1)
+        exact = np.cos(2.0 * PI * x) * np.sin(PI * y)
+        if ss == 0.0:
+            rhs = -PI * PI * exact * ((1.0 / (ii - 1) ** 2) + (4.0 / jj ** 2))
+        else:
+            rhs = -exact * ((PI * PI / (ii - 1) ** 2) + (4.0 * PI * PI / jj ** 2) + ss)
+        m = pq.Model(helm_cfg(ii, jj, [ss], periodic=True))
+        out = m.helm(np.asfortranarray(rhs[:, :, None]))
+        out = O.apply_dirichlet_bc(out, 0.0, periodic_j=True)
         errs.append(np.abs(out[:, :, 0] - exact).max())
         m.close()
     orders = [-math.log10(errs[n] / errs[n - 1]) / math.log10(sizes[n] / sizes[n - 1]) for n in range(1, len(errs))]
