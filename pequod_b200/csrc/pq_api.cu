@@ -245,7 +245,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     c->pitch = (ii + 31) & ~31;
     const size_t lstride = (size_t)c->pitch * jj;
     c->field_bytes = lstride * L * sizeof(double);
-    const int ntiles_tri = L * ((n + 7) / 8);
+    const int ntiles_tri = tri_ctas(n, jj, L);
     // Default CABARET band height by grid size (measured on B200: shorter
     // bands give small grids enough warps, taller ones cut halo rows on big ones).
     const int cab_sh = jj <= 300 ? 8 : jj <= 700 ? 32 : 64;

@@ -122,13 +122,24 @@ struct Member {
     unsigned int* counters;  // [4] last-block counters
     Scalars* sc;
     int* status;
-    int ntiles_tri;       // L * ceil(n / 8)
+    int ntiles_tri;       // tri_ctas(n, jj, L)
     int ntiles_cab;
     int cab_sh;           // output rows per warp of the fused CABARET sweep
     int cur;              // ping-pong parity for ui / zfi / zfj (host-managed)
     int adapt_dt;
     double target_cfl, max_dt, max_dt_increase;
 };
+
+// Tridiagonal solve geometry: W warps of row chunks per wavenumber column,
+// 8 / W columns per CTA of 256 threads (chosen so a lane's chunk stays short).
+__host__ __device__ inline int tri_warps(int jj) {
+    const int Mr = jj - 2;
+    return Mr > 1024 ? 4 : Mr > 128 ? 2 : 1;
+}
+__host__ __device__ inline int tri_ctas(int n, int jj, int L) {
+    const int KT = 8 / tri_warps(jj);
+    return L * ((n + KT - 1) / KT);
+}
 
 // Map a flat CTA index to (member, local CTA) given prefix sums.
 __device__ __forceinline__ int find_member(const int* __restrict__ prefix, int nmem, int cta, int* local) {

@@ -36,7 +36,6 @@ enum { PRO_PLAIN = 0, PRO_MODAL = 1, PRO_STEP = 2 };
 enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
 
 constexpr int TRI_THREADS = 256;
-constexpr int TRI_KT = 8;   // wavenumbers per tridiagonal CTA (one per warp)
 
 __device__ __forceinline__ void load_member(Member& dst, const Member* src) {
     const int n = sizeof(Member) / 4;
@@ -566,14 +565,24 @@ struct PivotRow {
 
 // S = float: the mixed form, whose baroclinic spectral rows are FP32 (staged
 // and solved in FP64); the barotropic mode (m = 0) comes from spec64.
-// GS = true: the reciprocal pivots of the strip are staged in shared memory
-// beside it (same layout), so the recurrences never wait on a global load;
-// used whenever both strips fit.
+// Tridiagonal solves along j.  A CTA of 256 threads solves KT = 8 / W
+// wavenumber columns of one mode, W warps per column: the column's rows are
+// split into 32 W chunks of R rows, one per lane, staged in shared memory
+// (chunk q of column c at c*CS + q*RS, RS = R | 1 odd, so a warp's 32 chunk
+// accesses hit 32 banks).  Each lane runs the forward and backward Thomas
+// recurrences of its chunk as first-order affine recurrences (local sweep,
+// scan of the affine chunk maps -- in the warp, then across the column's
+// warps through shared memory -- and a fix-up sweep).  GS = true: the
+// reciprocal pivots of the strip are staged beside it (same layout), so the
+// recurrences never wait on a global load; used whenever both strips fit.
+// The CTA also accumulates the domain mean of the solution in spectral space;
+// the last CTA of a member finishes psiC.
 template <typename S, bool GS>
 __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restrict__ mems,
                                                           const int* __restrict__ prefix, int nmem, int do_mean) {
     __shared__ Member Mb;
-    __shared__ double wpart[TRI_KT];
+    __shared__ double wpart[TRI_THREADS / 32];
+    __shared__ double tot[2][TRI_THREADS / 32][2];  // per-warp affine totals (forward, backward)
     __shared__ int is_last;
     extern __shared__ __align__(16) double strip[];
     int local;
@@ -581,25 +590,26 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     load_member(Mb, mems + mi);
     __syncthreads();
     const int n = Mb.n, jj = Mb.jj, pitch = Mb.pitch;
-    const int tiles_per_mode = (n + TRI_KT - 1) / TRI_KT;
+    const int W = tri_warps(jj), KT = 8 / W, NQ = 32 * W;
+    const int tiles_per_mode = (n + KT - 1) / KT;
     const int m = local / tiles_per_mode;
     const int tile = local - m * tiles_per_mode;
-    const int k0 = tile * TRI_KT;  // 0-based column (wavenumber k0+1)
+    const int k0 = tile * KT;  // 0-based column (wavenumber k0+1)
     const int Mr = jj - 2;
-    const int R = (Mr + 31) >> 5;
+    const int R = (Mr + NQ - 1) / NQ;
     const int RS = R | 1;
-    const int CS = 32 * RS + 1;
+    const int CS = NQ * RS + 1;
     const bool f32 = sizeof(S) == 4 && m > 0;  // this mode's rows are FP32
     double* spec = ((sizeof(S) == 4) ? Mb.spec64 : reinterpret_cast<double*>(Mb.spec)) + (long long)m * Mb.lstride;
     float* specf = reinterpret_cast<float*>(Mb.spec) + (long long)m * Mb.lstride;
+    double* gstrip = strip + KT * CS;  // pivots (GS)
 
-    // Stage: thread -> (column c = tid & 7, chunk q = tid >> 3); loop over t.
+    // Stage: thread -> (column c = tid % KT, chunk q = tid / KT); loop over t.
     // Asynchronous 8-byte copies (cp.async), so the loads of a thread do not
     // wait for one another; columns past n are zero-filled (source size 0).
     // FP32 rows are loaded and widened in registers.
-    double* gstrip = strip + TRI_KT * CS;  // pivots (GS)
     {
-        const int c = threadIdx.x & 7, q = threadIdx.x >> 3;
+        const int c = threadIdx.x % KT, q = threadIdx.x / KT;
         const bool colok = (k0 + c < n);
         const long long go = (long long)(q * R + 1) * pitch + (colok ? k0 + c : 0);
         double* sdst = strip + c * CS + q * RS;
@@ -634,123 +644,142 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sbase + 8u * t),
                              "l"(g + (long long)t * pitch), "r"(nbytes)
                              : "memory");
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         } else {
             const float* g = specf + go;
 #pragma unroll 4
             for (int t = 0; t < Rq; ++t) sdst[t] = colok ? (double)g[(long long)t * pitch] : 0.0;
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = warp;
-    const int kk = k0 + c;  // 0-based wavenumber index
-    double colsum = 0.0;
-    if (kk < n) {
+    const int c = warp % KT, h = warp / KT;  // column, and which W-th of it
+    const int q = h * 32 + lane;             // chunk
+    const int kk = k0 + c;                   // 0-based wavenumber index
+    const bool active = kk < n;
+    const int a = q * R + 1;                 // first row position (1-based) of the chunk
+    const int cnt = max(0, min(R, Mr - q * R));
+    const int b = a + cnt - 1;
+    double* s = strip + c * CS + q * RS;     // s[t] is position a + t
+    const double* gs = gstrip + c * CS + q * RS;  // GS: gs[t] = g(a + t)
+    PivotRow g{nullptr, 0, 0.0};
+    if (!GS && active) {
         const int mk = m * n + kk;
-        PivotRow g{Mb.piv + __ldg(&Mb.piv_off[mk]), __ldg(&Mb.piv_len[mk]), __ldg(&Mb.piv_fix[mk])};
-        const int a = lane * R + 1;                 // first row position (1-based) of the chunk
-        const int cnt = max(0, min(R, Mr - lane * R));
-        const int b = a + cnt - 1;
-        double* s = strip + c * CS + lane * RS;     // s[t] is position a + t
-        const double* gs = gstrip + c * CS + lane * RS;  // GS: gs[t] = g(a + t)
-        // g(p) for p in [a - 1, b]: g(a - 1) is the previous chunk's last pivot.
-        auto G = [&](int p) -> double {
-            if constexpr (GS) {
-                const int t = p - a;
-                return t >= 0 ? gs[t] : gstrip[c * CS + (lane - 1) * RS + (R - 1)];
-            } else {
-                return g(p);
-            }
-        };
-        // Forward elimination, local: y~_a = f_a, y~_p = f_p - g_{p-1} y~_{p-1};
-        // y_p = y~_p + A_p y_{a-1}, A_a = -g_{a-1}, A_p = -g_{p-1} A_{p-1}.
-        double A = 1.0, cend = 0.0;
-        if (cnt > 0) {
-            double y = s[0];
-            A = (a > 1) ? -G(a - 1) : 0.0;
-            for (int t = 1; t < cnt; ++t) {
-                const double gp = G(a + t - 1);
-                y = s[t] - gp * y;
-                s[t] = y;
-                A = -gp * A;
-            }
-            cend = y;
+        g = PivotRow{Mb.piv + __ldg(&Mb.piv_off[mk]), __ldg(&Mb.piv_len[mk]), __ldg(&Mb.piv_fix[mk])};
+    }
+    // g(p) for p in [a - 1, b]: g(a - 1) is the previous chunk's last pivot.
+    auto G = [&](int p) -> double {
+        if constexpr (GS) {
+            const int t = p - a;
+            return t >= 0 ? gs[t] : gstrip[c * CS + (q - 1) * RS + (R - 1)];
+        } else {
+            return g(p);
         }
-        // Inclusive scan of the affine chunk maps y_out = c + A y_in.
-        double sA = A, sc = cend;
+    };
+
+    // Forward elimination, local: y~_a = f_a, y~_p = f_p - g_{p-1} y~_{p-1};
+    // y_p = y~_p + A_p y_{a-1}, A_a = -g_{a-1}, A_p = -g_{p-1} A_{p-1}.
+    double A = 1.0, cend = 0.0;
+    if (active && cnt > 0) {
+        double y = s[0];
+        A = (a > 1) ? -G(a - 1) : 0.0;
+        for (int t = 1; t < cnt; ++t) {
+            const double gp = G(a + t - 1);
+            y = s[t] - gp * y;
+            s[t] = y;
+            A = -gp * A;
+        }
+        cend = y;
+    }
+    // Inclusive scan of the affine chunk maps y_out = c + A y_in in the warp,
+    // then the column's earlier warps' totals composed in order.
+    double sA = A, sc = cend;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const double pA = __shfl_up_sync(0xffffffffu, sA, o);
-            const double pc = __shfl_up_sync(0xffffffffu, sc, o);
-            if (lane >= o) {
-                sc = sc + sA * pc;
-                sA = sA * pA;
-            }
+    for (int o = 1; o < 32; o <<= 1) {
+        const double pA = __shfl_up_sync(0xffffffffu, sA, o);
+        const double pc = __shfl_up_sync(0xffffffffu, sc, o);
+        if (lane >= o) {
+            sc = sc + sA * pc;
+            sA = sA * pA;
         }
-        double yin = __shfl_up_sync(0xffffffffu, sc, 1);
-        if (lane == 0) yin = 0.0;
-        // Fix-up of y, then the local back substitution from the chunk end:
-        // x~_b = y_b g_b, x~_p = (y_p - x~_{p+1}) g_p; x_p = x~_p + B_p x_{b+1},
-        // B_b = -g_b, B_p = -g_p B_{p+1}.
-        double B = 1.0, cstart = 0.0;
-        if (cnt > 0) {
-            double Ap = (a > 1) ? -G(a - 1) : 0.0;
-            s[0] = s[0] + Ap * yin;
-            for (int t = 1; t < cnt; ++t) {
-                Ap = -G(a + t - 1) * Ap;
-                s[t] = s[t] + Ap * yin;
-            }
-            const double gb = G(b);
-            double x = s[cnt - 1] * gb;
-            s[cnt - 1] = x;
-            B = -gb;
-            for (int t = cnt - 2; t >= 0; --t) {
-                const double gp = G(a + t);
-                x = (s[t] - x) * gp;
-                s[t] = x;
-                B = -gp * B;
-            }
-            cstart = x;
+    }
+    if (lane == 31) {
+        tot[0][warp][0] = sA;
+        tot[0][warp][1] = sc;
+    }
+    __syncthreads();
+    double y0 = 0.0;  // y entering this warp's first chunk
+    for (int hh = 0; hh < h; ++hh) y0 = tot[0][hh * KT + c][1] + tot[0][hh * KT + c][0] * y0;
+    const double eA = __shfl_up_sync(0xffffffffu, sA, 1), ec = __shfl_up_sync(0xffffffffu, sc, 1);
+    const double yin = (lane == 0) ? y0 : ec + eA * y0;
+    // Fix-up of y, then the local back substitution from the chunk end:
+    // x~_b = y_b g_b, x~_p = (y_p - x~_{p+1}) g_p; x_p = x~_p + B_p x_{b+1},
+    // B_b = -g_b, B_p = -g_p B_{p+1}.
+    double B = 1.0, cstart = 0.0;
+    if (active && cnt > 0) {
+        double Ap = (a > 1) ? -G(a - 1) : 0.0;
+        s[0] = s[0] + Ap * yin;
+        for (int t = 1; t < cnt; ++t) {
+            Ap = -G(a + t - 1) * Ap;
+            s[t] = s[t] + Ap * yin;
         }
-        // Reverse inclusive scan of x_start = c + B x_next.
-        double rB = B, rc = cstart;
+        const double gb = G(b);
+        double x = s[cnt - 1] * gb;
+        s[cnt - 1] = x;
+        B = -gb;
+        for (int t = cnt - 2; t >= 0; --t) {
+            const double gp = G(a + t);
+            x = (s[t] - x) * gp;
+            s[t] = x;
+            B = -gp * B;
+        }
+        cstart = x;
+    }
+    // Reverse inclusive scan of x_start = c + B x_next, then the column's
+    // later warps' totals composed in order.
+    double rB = B, rc = cstart;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const double nB = __shfl_down_sync(0xffffffffu, rB, o);
-            const double nc = __shfl_down_sync(0xffffffffu, rc, o);
-            if (lane + o < 32) {
-                rc = rc + rB * nc;
-                rB = rB * nB;
-            }
+    for (int o = 1; o < 32; o <<= 1) {
+        const double nB = __shfl_down_sync(0xffffffffu, rB, o);
+        const double nc = __shfl_down_sync(0xffffffffu, rc, o);
+        if (lane + o < 32) {
+            rc = rc + rB * nc;
+            rB = rB * nB;
         }
-        double xin = __shfl_down_sync(0xffffffffu, rc, 1);
-        if (lane == 31) xin = 0.0;
-        double lsum = 0.0;
-        if (cnt > 0) {
-            double Bp = -G(b);
-            double v = s[cnt - 1] + Bp * xin;
-            s[cnt - 1] = v;
+    }
+    if (lane == 0) {
+        tot[1][warp][0] = rB;
+        tot[1][warp][1] = rc;
+    }
+    __syncthreads();
+    double x0 = 0.0;  // x entering this warp's last chunk from above
+    for (int hh = W - 1; hh > h; --hh) x0 = tot[1][hh * KT + c][1] + tot[1][hh * KT + c][0] * x0;
+    const double nB = __shfl_down_sync(0xffffffffu, rB, 1), nc = __shfl_down_sync(0xffffffffu, rc, 1);
+    const double xin = (lane == 31) ? x0 : nc + nB * x0;
+    double lsum = 0.0;
+    if (active && cnt > 0) {
+        double Bp = -G(b);
+        double v = s[cnt - 1] + Bp * xin;
+        s[cnt - 1] = v;
+        lsum += v;
+        for (int t = cnt - 2; t >= 0; --t) {
+            Bp = -G(a + t) * Bp;
+            v = s[t] + Bp * xin;
+            s[t] = v;
             lsum += v;
-            for (int t = cnt - 2; t >= 0; --t) {
-                Bp = -G(a + t) * Bp;
-                v = s[t] + Bp * xin;
-                s[t] = v;
-                lsum += v;
-            }
         }
-        if (Mb.periodic) {
-            // periodic_ge (qg3p_helmholtz.F90:565-610): the cyclic closure
-            // through the rows 1 and jj, which the Thomas solve above leaves
-            // out, as two rank-one corrections with the precomputed b, c.
-            __syncwarp();
+    }
+    if (Mb.periodic) {
+        // periodic_ge (qg3p_helmholtz.F90:565-610): the cyclic closure
+        // through the rows 1 and jj, which the Thomas solve above leaves
+        // out, as two rank-one corrections with the precomputed b, c.
+        __syncthreads();
+        double z1 = 0.0, zj = 0.0;
+        if (active) {
             const double* pb = Mb.pb + (long long)m * jj * n + kk;
             const double* pc = Mb.pc + (long long)m * jj * n + kk;
-            double z1 = 0.0, zj = 0.0;
             if (lane == 0) {
                 const int ql = (Mr - 1) / R, tl = (Mr - 1) - ql * R;
                 const double z2 = strip[c * CS];                 // row 2 (1-based) after the solve
@@ -758,26 +787,31 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                 const double z1i = spec[kk], zji = spec[(long long)(jj - 1) * pitch + kk];
                 z1 = (z1i - z2) / __ldg(&pb[0]);
                 zj = ((zji - zl) - z1 * __ldg(&pb[(long long)(jj - 1) * n])) / __ldg(&pc[(long long)(jj - 1) * n]);
-                spec[kk] = z1 - zj * __ldg(&pc[0]);
-                spec[(long long)(jj - 1) * pitch + kk] = zj;
             }
             z1 = __shfl_sync(0xffffffffu, z1, 0);
             zj = __shfl_sync(0xffffffffu, zj, 0);
+        }
+        __syncthreads();  // every warp has read rows 1 and jj before they are written
+        if (active && h == 0 && lane == 0) {
+            spec[kk] = z1 - zj * __ldg(&Mb.pc[(long long)m * jj * n + kk]);
+            spec[(long long)(jj - 1) * pitch + kk] = zj;
+        }
+        if (active)
             for (int t = 0; t < cnt; ++t) {
                 const long long row = a + t;  // 0-based grid row
-                s[t] = (s[t] - z1 * __ldg(&pb[row * n])) - zj * __ldg(&pc[row * n]);
+                s[t] = (s[t] - z1 * __ldg(&Mb.pb[((long long)m * jj + row) * n + kk])) -
+                       zj * __ldg(&Mb.pc[((long long)m * jj + row) * n + kk]);
             }
-        }
-        if (do_mean) colsum = warp_sum(lsum) * __ldg(&Mb.wmean[kk]);
     }
+    const double colsum = (active && do_mean) ? warp_sum(lsum) * __ldg(&Mb.wmean[kk]) : 0.0;
     if (lane == 0) wpart[warp] = colsum;
     __syncthreads();
     {
-        const int cc = threadIdx.x & 7, q = threadIdx.x >> 3;
+        const int cc = threadIdx.x % KT, qq = threadIdx.x / KT;
         if (k0 + cc < n) {
-            const long long go = (long long)(q * R + 1) * pitch + k0 + cc;
-            const double* ssrc = strip + cc * CS + q * RS;
-            const int Rq = min(R, Mr - q * R);
+            const long long go = (long long)(qq * R + 1) * pitch + k0 + cc;
+            const double* ssrc = strip + cc * CS + qq * RS;
+            const int Rq = min(R, Mr - qq * R);
             if (!f32) {
                 double* gdst = spec + go;
                 for (int t = 0; t < Rq; ++t) gdst[(long long)t * pitch] = ssrc[t];
@@ -790,7 +824,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     if (!do_mean) return;
     if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int w = 0; w < TRI_KT; ++w) t += wpart[w];
+        for (int w = 0; w < TRI_THREADS / 32; ++w) t += wpart[w];
         Mb.partials[local] = t;
         __threadfence();
         const unsigned prev = atomicAdd(&Mb.counters[0], 1u);
@@ -814,8 +848,9 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
 }
 
 __host__ __device__ inline size_t tri_smem_bytes(int jj) {
-    const int Mr = jj - 2, R = (Mr + 31) >> 5, RS = R | 1;
-    return (size_t)TRI_KT * (32 * RS + 1) * sizeof(double);
+    const int W = tri_warps(jj), KT = 8 / W, NQ = 32 * W;
+    const int Mr = jj - 2, R = (Mr + NQ - 1) / NQ, RS = R | 1;
+    return (size_t)KT * (NQ * RS + 1) * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
