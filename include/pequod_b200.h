@@ -222,6 +222,35 @@ PQ_API int pq_set_field(pq_ctx* ctx, int field, const double* in);
  * start of the next one, qg3.F90 timestep loop). */
 PQ_API int pq_get_scalars(pq_ctx* ctx, double* out4);
 
+/* ---- checkpoint dump and pickup ------------------------------------------
+ * The reference's checkpoint files, byte for byte: Fortran unformatted stream
+ * records (4-byte byte count, REAL(8) data column-major, byte count;
+ * qg3p_io.F90:574-760), native byte order.
+ *   s_path     qg<L>_<ii>_s.d: model_time_day, total_time_day, L x psi sdata,
+ *              L x zeta sdata (qg3.F90:836-856); leapfrog records hold both
+ *              time levels.
+ *   supp_path  qg<L>_<ii>_s_supp.d (CABARET only, qg3.F90:858-881):
+ *              model_time_day, total_time_day, dt, L x ui, L x uj,
+ *              L x zeta_fi, L x zeta_fj (interior faces), L x res,
+ *              L x res_beta.
+ * pq_write_checkpoint writes the current state; model_time_day =
+ * model_time * t_scale / 86400 and total_time_day = start_time_day +
+ * model_time_day (qg3.F90:661, 844-845).  supp_path may be NULL to write the
+ * _s file alone (the reference writes _s_supp every k_cp dumps).
+ * pq_read_checkpoint is START_PICKUP (read_parallel_checkpoint,
+ * qg3p_io.F90:202-314, then qg3.F90:316-363 and :448-497): CABARET takes dt
+ * from the file, sets uimo / ujmo to the face velocities of psi, advances
+ * zeta half a step with the stored fluxes, zeta_old = zeta, model_time =
+ * dt / 2; leapfrog sets rel from psi on both levels, zeta_old = zeta,
+ * model_time = 0 and skips the forward-Euler start.  The file times must
+ * agree (PQ_ERR_ARG "Input times do not match", as the reference aborts);
+ * total_time_day receives the checkpoint's total time (the new run's
+ * start_time_day) and may be NULL.  Not for periodic-channel contexts
+ * (PQ_ERR_UNSUPPORTED). */
+PQ_API int pq_write_checkpoint(pq_ctx* ctx, const char* s_path, const char* supp_path, double t_scale,
+                               double start_time_day);
+PQ_API int pq_read_checkpoint(pq_ctx* ctx, const char* s_path, const char* supp_path, double* total_time_day);
+
 /* Block until the context's queued device work is complete. */
 PQ_API int pq_sync(pq_ctx* ctx);
 

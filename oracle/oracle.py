@@ -74,6 +74,7 @@ def lib():
         L.or_model_cfl.restype = C.c_double
         L.or_model_cfl.argtypes = [C.c_void_p]
         L.or_pv_inversion.argtypes = [C.c_void_p, _dp, _dp]
+        L.or_model_pickup.argtypes = [C.c_void_p, C.c_double]
         _lib = L
     return _lib
 
@@ -298,6 +299,18 @@ class Model:
         a = self.get(name)
         return np.asfortranarray(a[1:-1, 1:-1, :])
 
+    def pickup(self, ckpt: dict) -> None:
+        """START_PICKUP from a checkpoint dictionary (read_checkpoint's
+        output): load its fields, then or_model_pickup."""
+        leap = self.cfg.get("scheme", 0) == 1
+        names = (["psi", "zeta", "ui", "uj", "zeta_fi", "zeta_fj", "res", "res_beta"] if not leap else
+                 ["psi", "psi2", "zeta", "zeta2"])
+        for n in names:
+            self.set(n, ckpt[n])
+        rc = lib().or_model_pickup(self.m, float(ckpt.get("dt", self.cfg["dt"])))
+        if rc:
+            raise RuntimeError(f"or_model_pickup rc={rc}")
+
     def scalars(self):
         out = np.zeros(4)
         lib().or_model_scalars(self.m, _p(out))
@@ -327,3 +340,111 @@ class Model:
         if getattr(self, "m", None):
             lib().or_model_destroy(self.m)
             self.m = None
+
+
+# ---------------------------------------------------------------------------
+# Checkpoint files (qg3.F90:836-878 write, qg3p_io.F90:202-314 read).  Each
+# record is Fortran unformatted stream output: a 4-byte byte count, the REAL(8)
+# data column-major, the byte count again (qg3p_io.F90:574-651).
+#   _s.d       model_time_day, total_time_day, L x psi sdata (ii, jj),
+#              L x zeta sdata; leapfrog records hold level 1 then level 2.
+#   _s_supp.d  (CABARET) model_time_day, total_time_day, dt,
+#              L x ui   data(fa_i_min+1:fa_i_max,   fa_j_min+1:fa_j_max-1),
+#              L x uj   data(fa_i_min+1:fa_i_max-1, fa_j_min+1:fa_j_max),
+#              L x zeta_fi, L x zeta_fj (same ranges), L x res, L x res_beta.
+# With one process and no neighbours the ranges are, in the 1-based indexes
+# of the reference-layout arrays used here, ui / zeta_fi i in [3, ii+1],
+# j in [3, jj]; uj / zeta_fj i in [3, ii], j in [3, jj+1].
+
+def _records(path):
+    raw = open(path, "rb").read()
+    out, k = [], 0
+    while k < len(raw):
+        n = int(np.frombuffer(raw, "<i4", 1, k)[0])
+        data = np.frombuffer(raw, "<f8", n // 8, k + 4).copy()
+        m = int(np.frombuffer(raw, "<i4", 1, k + 4 + n)[0])
+        if m != n or n % 8:
+            raise ValueError(f"{path}: bad record framing at byte {k}")
+        out.append(data)
+        k += 8 + n
+    return out
+
+
+def _write_records(path, recs):
+    with open(path, "wb") as f:
+        for r in recs:
+            r = np.asarray(r, dtype="<f8").ravel(order="F")
+            n = np.array([r.size * 8], dtype="<i4")
+            f.write(n.tobytes() + r.tobytes() + n.tobytes())
+
+
+def _face_ranges(ii, jj):
+    # 0-based slices of the FLUX_II / FLUX_JJ reference-layout arrays.
+    return (slice(2, ii + 1), slice(2, jj)), (slice(2, ii), slice(2, jj + 1))
+
+
+def read_checkpoint(s_path, supp_path, ii, jj, L, leapfrog=False):
+    """Parse a checkpoint into reference-layout arrays and the three times."""
+    rs = _records(s_path)
+    out = {"model_time_day": float(rs[0][0]), "total_time_day": float(rs[1][0])}
+    nlev = 2 if leapfrog else 1
+    if len(rs) != 2 + 2 * L or any(r.size != ii * jj * nlev for r in rs[2:]):
+        raise ValueError("unexpected _s record layout")
+    for k, name in enumerate(("psi", "zeta")):
+        for lv in range(nlev):
+            a = np.zeros((ii + 2, jj + 2, L), order="F")
+            for l in range(L):
+                r = rs[2 + k * L + l]
+                a[1:-1, 1:-1, l] = r[lv * ii * jj:(lv + 1) * ii * jj].reshape((ii, jj), order="F")
+            out[name + ("2" if lv else "")] = a
+    if leapfrog or supp_path is None:
+        return out
+    rp = _records(supp_path)
+    if len(rp) != 3 + 6 * L:
+        raise ValueError("unexpected _s_supp record layout")
+    if rp[0][0] != out["model_time_day"] or rp[1][0] != out["total_time_day"]:
+        raise ValueError("Input times do not match in CABARET checkpoint data")
+    out["dt"] = float(rp[2][0])
+    (fi_i, fi_j), (fj_i, fj_j) = _face_ranges(ii, jj)
+    k = 3
+    for name, shape, (si, sj) in (("ui", (ii + 3, jj + 2), (fi_i, fi_j)), ("uj", (ii + 2, jj + 3), (fj_i, fj_j)),
+                                  ("zeta_fi", (ii + 3, jj + 2), (fi_i, fi_j)),
+                                  ("zeta_fj", (ii + 2, jj + 3), (fj_i, fj_j))):
+        a = np.zeros(shape + (L,), order="F")
+        for l in range(L):
+            a[si, sj, l] = rp[k].reshape((si.stop - si.start, sj.stop - sj.start), order="F")
+            k += 1
+        out[name] = a
+    for name in ("res", "res_beta"):
+        a = np.zeros((ii, jj, L), order="F")
+        for l in range(L):
+            a[:, :, l] = rp[k].reshape((ii, jj), order="F")
+            k += 1
+        out[name] = a
+    return out
+
+
+def write_checkpoint(s_path, supp_path, fields, model_time_day, total_time_day, dt=None, leapfrog=False):
+    """Write reference-layout arrays as a checkpoint (the reference's writer)."""
+    L = fields["psi"].shape[2]
+    recs = [[model_time_day], [total_time_day]]
+    for name in ("psi", "zeta"):
+        for l in range(L):
+            r = fields[name][1:-1, 1:-1, l].ravel(order="F")
+            if leapfrog:
+                r = np.concatenate([r, fields[name + "2"][1:-1, 1:-1, l].ravel(order="F")])
+            recs.append(r)
+    _write_records(s_path, recs)
+    if leapfrog or supp_path is None:
+        return
+    ii, jj = fields["psi"].shape[0] - 2, fields["psi"].shape[1] - 2
+    (fi_i, fi_j), (fj_i, fj_j) = _face_ranges(ii, jj)
+    recs = [[model_time_day], [total_time_day], [dt]]
+    for name, (si, sj) in (("ui", (fi_i, fi_j)), ("uj", (fj_i, fj_j)), ("zeta_fi", (fi_i, fi_j)),
+                           ("zeta_fj", (fj_i, fj_j))):
+        for l in range(L):
+            recs.append(fields[name][si, sj, l].ravel(order="F"))
+    for name in ("res", "res_beta"):
+        for l in range(L):
+            recs.append(fields[name][:, :, l].ravel(order="F"))
+    _write_records(supp_path, recs)

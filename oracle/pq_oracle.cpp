@@ -998,6 +998,19 @@ void apply_rel_bc(or_model& m, std::vector<double>& psi_v, std::vector<double>& 
     }
 }
 
+// rel_from_psi, qg3p_aux.F90:579-603: the five-point Laplacian of psi on
+// the interior nodes, then apply_rel_bc on the boundary.
+void rel_from_psi(or_model& m, std::vector<double>& psi_v, std::vector<double>& rel_v) {
+    const Decomp& d = m.d;
+    V3 psi = m.full(psi_v), rel = m.full(rel_v);
+    for (int l = 1; l <= d.layers; ++l)
+        for (int j = d.f_j_min; j <= d.f_j_max; ++j)
+            for (int i = d.f_i_min; i <= d.f_i_max; ++i)
+                rel(i, j, l) = -4.0 * psi(i, j, l) + psi(i - 1, j, l) + psi(i, j + 1, l) + psi(i + 1, j, l) +
+                               psi(i, j - 1, l);
+    apply_rel_bc(m, psi_v, rel_v);
+}
+
 // rel_from_zeta_and_psi, qg3p_aux.F90:738-775.
 void rel_from_zeta_and_psi(or_model& m, std::vector<double>& zeta_v, std::vector<double>& psi_v,
                            std::vector<double>& rel_v) {
@@ -1180,6 +1193,27 @@ void cabaret_cell_boundaries(or_model& m) {
                 uj(i, j, l) = (1.0 + tu) * ujm - tu * ujmo(i, j, l);
                 ujmo(i, j, l) = ujm;
             }
+}
+
+// cabaret_cell_boundaries_velocity, qg3p_aux.F90:1168-1231: the face
+// velocities of psi itself, without time weighting, into uimo / ujmo (the
+// checkpoint pickup's use, qg3.F90:326).
+void cabaret_cell_boundaries_velocity(or_model& m) {
+    const Decomp& d = m.d;
+    int L = d.layers;
+    V3 psi = m.full(m.psi[0]), uimo = m.fi(m.uimo), ujmo = m.fj(m.ujmo);
+    m.psi_edge.assign(m.nfull(), 0.0);
+    V3 pe = m.full(m.psi_edge);
+    for (int l = 1; l <= L; ++l)
+        for (int j = d.fa_j_min + 1; j <= d.fa_j_max; ++j)
+            for (int i = d.fa_i_min + 1; i <= d.fa_i_max; ++i)
+                pe(i, j, l) = 0.25 * (psi(i, j, l) + psi(i, j - 1, l) + psi(i - 1, j, l) + psi(i - 1, j - 1, l));
+    for (int l = 1; l <= L; ++l)
+        for (int j = d.fa_j_min + 1; j <= d.fa_j_max - 1; ++j)
+            for (int i = d.fa_i_min + 1; i <= d.fa_i_max; ++i) uimo(i, j, l) = -pe(i, j + 1, l) + pe(i, j, l);
+    for (int l = 1; l <= L; ++l)
+        for (int j = d.fa_j_min + 1; j <= d.fa_j_max; ++j)
+            for (int i = d.fa_i_min + 1; i <= d.fa_i_max - 1; ++i) ujmo(i, j, l) = pe(i + 1, j, l) - pe(i, j, l);
 }
 
 // cabaret_extrapolator, qg3p_aux.F90:1317-1544.
@@ -1663,6 +1697,36 @@ int or_model_step(or_model* m, int nsteps) {
             if (rc) return rc;
             m->model_time += m->dt;
         }
+    }
+    return 0;
+}
+
+// START_PICKUP (qg3.F90:314-363) and the common timestep initialisation
+// (:448-462) on fields already loaded with or_model_set from a checkpoint:
+// CABARET: psi, zeta, ui, uj, zeta_fi, zeta_fj, res, res_beta (read by
+// read_parallel_checkpoint, qg3p_io.F90:202-314) and the checkpoint's dt;
+// the face velocities of psi become uimo / ujmo, flux = u * zeta_f, and the
+// corrector takes zeta half a step forwards.  Leapfrog: psi, zeta of both
+// levels; rel = rel_from_psi of each level.  Then zeta_old = zeta, and
+// model_time = dt / 2 with tweights 0.5 (CABARET) or model_time = 0 with the
+// forward-Euler start skipped (leapfrog, :461-497).
+int or_model_pickup(or_model* m, double dt) {
+    if (m->p.scheme == 0) {
+        m->dt = dt;
+        cabaret_cell_boundaries_velocity(*m);
+        cabaret_flux(*m);
+        cabaret_corrector(*m);
+        m->zeta_old[0] = m->zeta[0];
+        m->model_time = m->dt / 2.0;
+        m->tweight_a = 0.5;
+        m->tweight_u = 0.5;
+    } else {
+        for (int lv = 0; lv < 2; ++lv) {
+            rel_from_psi(*m, m->psi[lv], m->rel[lv]);
+            m->zeta_old[lv] = m->zeta[lv];
+        }
+        m->model_time = 0.0;
+        m->lf_count = 0;
     }
     return 0;
 }

@@ -118,6 +118,9 @@ int or_model_step(or_model* m, int nsteps);
  * to query the size. */
 long or_model_get(or_model* m, const char* name, double* out);
 long or_model_set(or_model* m, const char* name, const double* in);
+/* Checkpoint pickup (qg3.F90:314-363, :448-497) on fields loaded with
+ * or_model_set; dt is the checkpoint's (CABARET; ignored for leapfrog). */
+int or_model_pickup(or_model* m, double dt);
 /* Scalars: dt, tweight_a, tweight_u, model_time. */
 void or_model_scalars(or_model* m, double* out4);
 int or_model_energy(or_model* m, double* ekin, double* epot);

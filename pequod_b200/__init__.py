@@ -98,6 +98,8 @@ SIGNATURES = {
     "pq_set_field": (C.c_int, [C.c_void_p, C.c_int, _dp]),
     "pq_get_scalars": (C.c_int, [C.c_void_p, _dp]),
     "pq_sync": (C.c_int, [C.c_void_p]),
+    "pq_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_double]),
+    "pq_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, _dp]),
     "pq_stream": (C.c_void_p, [C.c_void_p]),
     "pq_last_launch_count": (C.c_long, [C.c_void_p]),
     "pq_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
@@ -358,6 +360,19 @@ class Model:
         out = np.zeros(4)
         _check(lib().pq_get_scalars(self.ctx, _p(out)), self.ctx)
         return dict(dt=out[0], tweight_a=out[1], tweight_u=out[2], model_time=out[3])
+
+    def write_checkpoint(self, s_path: str, supp_path: str | None = None, t_scale: float = 1.0,
+                         start_time_day: float = 0.0) -> None:
+        """Dump the state as the reference's qg<L>_<ii>_s.d / _s_supp.d pair."""
+        supp = supp_path.encode() if supp_path else None
+        _check(lib().pq_write_checkpoint(self.ctx, s_path.encode(), supp, t_scale, start_time_day), self.ctx)
+
+    def read_checkpoint(self, s_path: str, supp_path: str | None = None) -> float:
+        """START_PICKUP from a checkpoint pair; returns its total_time_day."""
+        ttd = np.zeros(1)
+        supp = supp_path.encode() if supp_path else None
+        _check(lib().pq_read_checkpoint(self.ctx, s_path.encode(), supp, _p(ttd)), self.ctx)
+        return float(ttd[0])
 
     def device_bytes(self) -> int:
         return int(lib().pq_device_bytes(self.ctx))

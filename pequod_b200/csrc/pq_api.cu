@@ -878,6 +878,37 @@ int pq_cfl(pq_ctx* c, double* cfl) {
     return PQ_OK;
 }
 
+}  // extern "C"
+
+namespace pq {
+
+// Clears the CABARET fields of both parities (as pq_init_perturb does),
+// installs `sc` and the status word, and resets the step parity; the caller
+// then writes the prognostic fields with pq_set_field.  Used by the
+// checkpoint pickup.
+int reset_prognostic(pq_ctx* c, const Scalars& sc) {
+    CK(cudaSetDevice(c->device));
+    if (!c->leapfrog) CK(cudaMemsetAsync(c->hm[0].zeta_old[0], 0, align256(c->field_bytes) * 18, c->stream));
+    CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->cur = 0;
+    c->zpar = 0;
+    c->pred_ready = false;
+    return PQ_OK;
+}
+
+int read_scalars(pq_ctx* c, Scalars* sc) {
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemcpyAsync(sc, c->d_sc, sizeof(*sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PQ_OK;
+}
+
+}  // namespace pq
+
+extern "C" {
+
 int pq_get_scalars(pq_ctx* c, double* out4) {
     if (!c || !out4) return PQ_ERR_ARG;
     Scalars sc;

@@ -81,6 +81,10 @@ int check_status(pq_ctx* c);
 int upload_members(pq_ctx* c);
 int run_helm(pq_ctx* c, int par, int prologue, int epilogue, int mean);
 int run_step(pq_ctx* c, int par);
+// Checkpoint pickup support: clear the prognostic fields and install the
+// scalars (reset_prognostic); copy the device scalars to the host.
+int reset_prognostic(pq_ctx* c, const Scalars& sc);
+int read_scalars(pq_ctx* c, Scalars* sc);
 // pq_create's body.  helm_only: allocate only the Helmholtz fields (helm_io,
 // spec) -- the batched solver's members; stream: use this stream instead of
 // creating one (not owned).

@@ -1,0 +1,174 @@
+"""Checkpoint files and the pickup, on the CPU: the oracle's record format
+(qg3p_io.F90:574-760) and its START_PICKUP (qg3.F90:314-363, :448-497)
+against a separate numpy statement of the same steps."""
+import os
+
+import numpy as np
+import pytest
+
+import pequod_b200 as pq
+from oracle import oracle as O
+
+
+def double_gyre(ii, layers=2, dt=1800.0, **kw):
+    H = {2: (1.0e5, 3.0e5), 3: (3.0e4, 7.0e4, 3.0e5)}[layers]
+    gp = {2: (1.5,), 3: (1.5, 0.75)}[layers]
+    p = pq.double_gyre_physical(ii, layers=layers, dt=dt, dx=3.84e8 / (ii - 1), H=H, gprime=gp, **kw)
+    return pq.Config.from_physical(p)
+
+
+def run_oracle(cfg, steps, seed):
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    if cfg.oracle_cfg().get("scheme", 0) == 1:
+        ic2 = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed + 1000, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+        ic = np.asfortranarray(np.stack([ic, ic2], axis=3))
+    o = O.Model(cfg.oracle_cfg())
+    o.init(ic)
+    o.step(steps)
+    return o
+
+
+CAB = ["psi", "zeta", "ui", "uj", "zeta_fi", "zeta_fj", "res", "res_beta"]
+
+
+def test_record_framing(tmp_path):
+    """Each record: int32 byte count, REAL(8) data, the same count."""
+    s = str(tmp_path / "qg2_17_s.d")
+    supp = str(tmp_path / "qg2_17_s_supp.d")
+    cfg = double_gyre(17)
+    o = run_oracle(cfg, 3, seed=1)
+    fields = {n: o.get(n) for n in CAB}
+    O.write_checkpoint(s, supp, fields, 1.25, 11.25, dt=0.5)
+    ii = jj = 17
+    L = 2
+    raw = open(s, "rb").read()
+    assert len(raw) == 2 * (8 + 8) + 2 * L * (8 + 8 * ii * jj)
+    assert np.frombuffer(raw, "<i4", 1, 0)[0] == 8
+    assert np.frombuffer(raw, "<f8", 1, 4)[0] == 1.25
+    assert np.frombuffer(raw, "<i4", 1, 12)[0] == 8
+    assert np.frombuffer(raw, "<i4", 1, 32)[0] == 8 * ii * jj
+    nfi = (ii - 1) * (jj - 2)
+    nfj = (ii - 2) * (jj - 1)
+    assert os.path.getsize(supp) == 3 * 16 + L * (6 * 8 + 8 * (2 * nfi + 2 * nfj + 2 * ii * jj))
+    back = O.read_checkpoint(s, supp, ii, jj, L)
+    assert back["model_time_day"] == 1.25 and back["total_time_day"] == 11.25 and back["dt"] == 0.5
+    # The saved ranges come back exactly; the unsaved boundary faces as zero.
+    for n in CAB:
+        a, b = back[n], fields[n]
+        if n in ("psi", "zeta"):
+            np.testing.assert_array_equal(a[1:-1, 1:-1], b[1:-1, 1:-1])
+        elif n in ("ui", "zeta_fi"):
+            np.testing.assert_array_equal(a[2:ii + 1, 2:jj], b[2:ii + 1, 2:jj])
+            assert not a[:2].any() and not a[ii + 1:].any()
+        elif n in ("uj", "zeta_fj"):
+            np.testing.assert_array_equal(a[2:ii, 2:jj + 1], b[2:ii, 2:jj + 1])
+        else:
+            np.testing.assert_array_equal(a, b)
+
+
+def test_mismatched_times_are_rejected(tmp_path):
+    s, supp = str(tmp_path / "a_s.d"), str(tmp_path / "a_s_supp.d")
+    cfg = double_gyre(9)
+    o = run_oracle(cfg, 1, seed=2)
+    fields = {n: o.get(n) for n in CAB}
+    O.write_checkpoint(s, supp, fields, 1.0, 2.0, dt=0.5)
+    s2 = str(tmp_path / "b_s.d")
+    O.write_checkpoint(s2, None, fields, 1.0, 3.0)
+    with pytest.raises(ValueError, match="do not match"):
+        O.read_checkpoint(s2, supp, 9, 9, 2)
+
+
+def numpy_cabaret_pickup(ck, dt):
+    """qg3.F90:316-340 in numpy, 0-based reference-layout indexes."""
+    psi, zeta = ck["psi"], ck["zeta"].copy(order="F")
+    ui, uj, zfi, zfj = ck["ui"], ck["uj"], ck["zeta_fi"], ck["zeta_fj"]
+    ii, jj = psi.shape[0] - 2, psi.shape[1] - 2
+    pe = np.zeros_like(psi)
+    # psi_edge at 1-based (i, j), i in [3, ii+1], j in [3, jj+1].
+    pe[2:ii + 1, 2:jj + 1] = 0.25 * (((psi[2:ii + 1, 2:jj + 1] + psi[2:ii + 1, 1:jj]) + psi[1:ii, 2:jj + 1])
+                                     + psi[1:ii, 1:jj])
+    uimo = np.zeros_like(ui)
+    uimo[2:ii + 1, 2:jj] = -pe[2:ii + 1, 3:jj + 1] + pe[2:ii + 1, 2:jj]
+    ujmo = np.zeros_like(uj)
+    ujmo[2:ii, 2:jj + 1] = pe[3:ii + 1, 2:jj + 1] - pe[2:ii, 2:jj + 1]
+    fli = ui * zfi
+    flj = uj * zfj
+    res = ck["res"].copy(order="F")
+    # corrector on nodes 1-based i, j in [3, ii] x [3, jj]
+    r = -(((fli[3:ii + 1, 2:jj] - fli[2:ii, 2:jj]) + flj[2:ii, 3:jj + 1]) - flj[2:ii, 2:jj])
+    res[1:ii - 1, 1:jj - 1] = r
+    zeta[2:ii, 2:jj] = zeta[2:ii, 2:jj] + 0.5 * dt * r
+    return dict(uimo=uimo, ujmo=ujmo, res=res, zeta=zeta, zeta_old=zeta, flux_i=fli, flux_j=flj)
+
+
+def test_cabaret_pickup_matches_numpy(tmp_path):
+    s, supp = str(tmp_path / "c_s.d"), str(tmp_path / "c_s_supp.d")
+    cfg = double_gyre(17, 3)
+    o = run_oracle(cfg, 5, seed=3)
+    fields = {n: o.get(n) for n in CAB}
+    dt = o.scalars()["dt"]
+    O.write_checkpoint(s, supp, fields, 0.1, 0.1, dt=dt)
+    ck = O.read_checkpoint(s, supp, 17, 17, 3)
+    p = O.Model(cfg.oracle_cfg())
+    p.pickup(ck)
+    want = numpy_cabaret_pickup(ck, dt)
+    ii = jj = 17
+    for n in ("uimo", "ujmo", "res", "zeta", "zeta_old"):
+        got = p.get(n)
+        if n == "uimo":
+            got, w = got[2:ii + 1, 2:jj], want[n][2:ii + 1, 2:jj]
+        elif n == "ujmo":
+            got, w = got[2:ii, 2:jj + 1], want[n][2:ii, 2:jj + 1]
+        else:
+            w = want[n]
+        np.testing.assert_array_equal(got, w, err_msg=n)
+    fl = p.get("flux_i")
+    np.testing.assert_array_equal(fl[2:ii + 1, 2:jj], want["flux_i"][2:ii + 1, 2:jj])
+    sc = p.scalars()
+    assert sc["dt"] == dt and sc["model_time"] == dt / 2 and sc["tweight_a"] == 0.5 and sc["tweight_u"] == 0.5
+    # The pickup differs from continuing the run: zeta_old is the corrected
+    # zeta, not the dumped one, so the next predictor applies res again.
+    assert not np.array_equal(p.get("zeta"), fields["zeta"])
+    p.step(2)
+    assert np.isfinite(p.get("psi")).all()
+
+
+@pytest.mark.parametrize("bc", [pq.BC_PARTIAL_SLIP, pq.BC_NO_SLIP, pq.BC_FREE_SLIP])
+def test_leapfrog_pickup_rel_from_psi(tmp_path, bc):
+    """rel_from_psi (qg3p_aux.F90:579-603) + apply_rel_bc on both levels."""
+    s = str(tmp_path / "lf_s.d")
+    cfg = double_gyre(17, 2, scheme=pq.SCHEME_LEAPFROG, partial_slip=int(bc == pq.BC_PARTIAL_SLIP))
+    oc = cfg.oracle_cfg()
+    oc["bc_type"] = bc
+    ic = pq.make_ic(17, 17, 2, seed=4, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    o = O.Model(oc)
+    o.init(np.asfortranarray(np.stack([ic, 0.5 * ic], axis=3)))
+    o.step(3)
+    fields = {n: o.get(n) for n in ("psi", "zeta", "psi2", "zeta2")}
+    O.write_checkpoint(s, None, fields, 0.2, 0.2, leapfrog=True)
+    ck = O.read_checkpoint(s, None, 17, 17, 2, leapfrog=True)
+    for n in fields:
+        np.testing.assert_array_equal(ck[n][1:-1, 1:-1], fields[n][1:-1, 1:-1])
+    p = O.Model(oc)
+    p.pickup(ck)
+    alpha = oc.get("alpha", 0.0)
+    for lv, suf in ((0, ""), (1, "2")):
+        psi = ck["psi" + suf]
+        rel = np.zeros_like(psi)
+        rel[2:-2, 2:-2] = ((((-4.0 * psi[2:-2, 2:-2] + psi[1:-3, 2:-2]) + psi[2:-2, 3:-1]) + psi[3:-1, 2:-2])
+                           + psi[2:-2, 1:-3])
+
+        def edge(p0, p1, p2):
+            if bc == pq.BC_PARTIAL_SLIP:
+                return alpha / (alpha + 3.0) * ((-3.5 * p0 + 4.0 * p1) - 0.5 * p2)
+            if bc == pq.BC_NO_SLIP:
+                return 2.0 * (p1 - p0)
+            return 0.0 * p0
+
+        rel[1, 1:-1] = edge(psi[1, 1:-1], psi[2, 1:-1], psi[3, 1:-1])
+        rel[-2, 1:-1] = edge(psi[-2, 1:-1], psi[-3, 1:-1], psi[-4, 1:-1])
+        rel[1:-1, 1] = edge(psi[1:-1, 1], psi[1:-1, 2], psi[1:-1, 3])
+        rel[1:-1, -2] = edge(psi[1:-1, -2], psi[1:-1, -3], psi[1:-1, -4])
+        np.testing.assert_allclose(p.get("rel" + suf), rel, rtol=0, atol=1e-15 * np.abs(rel).max())
+        np.testing.assert_array_equal(p.get("zeta_old" + suf), ck["zeta" + suf])
+    assert p.scalars()["model_time"] == 0.0
