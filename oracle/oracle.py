@@ -75,6 +75,8 @@ def lib():
         L.or_model_cfl.argtypes = [C.c_void_p]
         L.or_pv_inversion.argtypes = [C.c_void_p, _dp, _dp]
         L.or_model_pickup.argtypes = [C.c_void_p, C.c_double]
+        L.or_model_step_to_dump.argtypes = [C.c_void_p]
+        L.or_model_finish_step.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -298,6 +300,25 @@ class Model:
     def sdata(self, name: str) -> np.ndarray:
         a = self.get(name)
         return np.asfortranarray(a[1:-1, 1:-1, :])
+
+    def step_to_dump(self) -> None:
+        """One CABARET step up to the reference's checkpoint point."""
+        rc = lib().or_model_step_to_dump(self.m)
+        if rc:
+            raise RuntimeError(f"or_model_step_to_dump rc={rc}")
+
+    def finish_step(self) -> None:
+        """The rest of that step: corrector, zeta_old = zeta, time."""
+        rc = lib().or_model_finish_step(self.m)
+        if rc:
+            raise RuntimeError(f"or_model_finish_step rc={rc}")
+
+    def dump_fields(self) -> dict:
+        """The fields a checkpoint holds, in reference layout."""
+        names = ["psi", "zeta", "ui", "uj", "zeta_fi", "zeta_fj", "res", "res_beta"]
+        if self.cfg.get("scheme", 0) == 1:
+            names = ["psi", "zeta", "psi2", "zeta2"]
+        return {n: self.get(n) for n in names}
 
     def pickup(self, ckpt: dict) -> None:
         """START_PICKUP from a checkpoint dictionary (read_checkpoint's

@@ -1668,23 +1668,42 @@ int or_model_init(or_model* m, const double* zeta_ic) {
     return 0;
 }
 
+// The CABARET timestep_loop body (qg3.F90:590-967) up to its data output
+// and exit point (:807-934): adapt_dt, predictor, beta, inversion, rel and
+// boundary PV, half the time increment, forcing, cell boundaries,
+// extrapolator, flux.  The state here is what the reference's checkpoint
+// holds.
+int or_model_step_to_dump(or_model* m) {
+    if (m->p.scheme != 0) return -1;
+    if (m->p.adapt_dt) cabaret_adapt_dt(*m);
+    cabaret_predictor(*m);
+    cabaret_beta(*m);
+    int rc = invert_level(*m, 0);
+    if (rc) return rc;
+    m->model_time += 0.5 * m->dt;
+    cabaret_forcing(*m);
+    cabaret_cell_boundaries(*m);
+    cabaret_extrapolator(*m);
+    cabaret_flux(*m);
+    return 0;
+}
+
+// The rest of the body after the exit point (qg3.F90:940-956): corrector,
+// zeta_old = zeta, the second half of the time increment.
+int or_model_finish_step(or_model* m) {
+    if (m->p.scheme != 0) return -1;
+    cabaret_corrector(*m);
+    m->zeta_old[0] = m->zeta[0];
+    m->model_time += 0.5 * m->dt;
+    return 0;
+}
+
 int or_model_step(or_model* m, int nsteps) {
     for (int s = 0; s < nsteps; ++s) {
         if (m->p.scheme == 0) {
-            // timestep_loop body, CABARET branch, qg3.F90:590-967.
-            if (m->p.adapt_dt) cabaret_adapt_dt(*m);
-            cabaret_predictor(*m);
-            cabaret_beta(*m);
-            int rc = invert_level(*m, 0);
+            int rc = or_model_step_to_dump(m);
             if (rc) return rc;
-            m->model_time += 0.5 * m->dt;
-            cabaret_forcing(*m);
-            cabaret_cell_boundaries(*m);
-            cabaret_extrapolator(*m);
-            cabaret_flux(*m);
-            cabaret_corrector(*m);
-            m->zeta_old[0] = m->zeta[0];
-            m->model_time += 0.5 * m->dt;
+            or_model_finish_step(m);
         } else {
             // One DOLEAPFROG sub-step, qg3.F90:615-651.  The sub-step index
             // alternates 1, 2, 1, 2, ... from the first step after the

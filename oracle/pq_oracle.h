@@ -118,6 +118,11 @@ int or_model_step(or_model* m, int nsteps);
  * to query the size. */
 long or_model_get(or_model* m, const char* name, double* out);
 long or_model_set(or_model* m, const char* name, const double* in);
+/* One CABARET step split at the reference's data output / exit point:
+ * or_model_step_to_dump leaves the state its checkpoint holds,
+ * or_model_finish_step completes the step (corrector, zeta_old, time). */
+int or_model_step_to_dump(or_model* m);
+int or_model_finish_step(or_model* m);
 /* Checkpoint pickup (qg3.F90:314-363, :448-497) on fields loaded with
  * or_model_set; dt is the checkpoint's (CABARET; ignored for leapfrog). */
 int or_model_pickup(or_model* m, double dt);

@@ -274,7 +274,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
 
     // Arena layout.
     const int nfields = helm_only ? 2 /*helm_io, spec*/
-                                  : 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 1 /*res*/ + 2 /*res_beta*/ +
+                                  : 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 2 /*res*/ + 2 /*res_beta*/ +
                                         1 /*ui*/ + 1 /*uj*/ + 2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ +
                                         1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ + 1 /*corr*/ + 1 /*spec64*/ +
                                         2 /*leapfrog psi(2), rel(2)*/;
@@ -432,7 +432,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     char* F = A + o_fields;
     int fi = 0;
     auto fld = [&]() { return (void*)(F + fb * (fi++)); };
-    void *zpb0 = nullptr, *zpb1 = nullptr, *rb0 = nullptr, *rb1 = nullptr, *rel2 = nullptr;
+    void *zpb0 = nullptr, *zpb1 = nullptr, *rb0 = nullptr, *rb1 = nullptr, *rel2 = nullptr, *rs1 = nullptr;
     double* psi2 = nullptr;
     if (helm_only) {
         m.helm_io = fld();
@@ -456,6 +456,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         m.zfj[1] = fld();
         zpb1 = fld();
         rb1 = fld();
+        rs1 = fld();
         m.rel = fld();
         m.helm_io = fld();
         m.spec = fld();
@@ -489,6 +490,10 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     c->hm[1].zeta = c->hm[0].zeta_next = zpb1;
     c->hm[0].res_beta = c->hm[1].res_beta_other = rb0;
     c->hm[1].res_beta = c->hm[0].res_beta_other = rb1;
+    // The corrector writes the other parity's res: a step of parity p reads
+    // res[p] (the previous step's) and writes res[p ^ 1].
+    c->hm[0].res = c->hm[1].res_out = m.res;
+    c->hm[1].res = c->hm[0].res_out = rs1;
     c->fuse = !d->adapt_dt;
     c->leapfrog = d->scheme == PQ_SCHEME_LEAPFROG;
     if (c->leapfrog) {
@@ -632,10 +637,10 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     const Member& m = c->hm[0];
     // Zero all CABARET fields and both parities (qg3.F90:393-404).
     const size_t fb = align256(c->field_bytes);
-    // Fields 0..17 of the arena: zeta_old[2], zeta[0], psi, res, res_beta[0],
-    // ui, uj, uimo[2], ujmo[2], zeta_fi[2], zeta_fj[2], zeta[1], res_beta[1]
-    // (corr is kept).
-    CK(cudaMemsetAsync(m.zeta_old[0], 0, fb * 18, c->stream));
+    // Fields 0..18 of the arena: zeta_old[2], zeta[0], psi, res[0], res_beta[0],
+    // ui, uj, uimo[2], ujmo[2], zeta_fi[2], zeta_fj[2], zeta[1], res_beta[1],
+    // res[1] (corr is kept).
+    CK(cudaMemsetAsync(m.zeta_old[0], 0, fb * 19, c->stream));
     int rc = copy_in_state(c, m.zeta, z.data(), PQ_PTR_HOST);
     if (rc) return rc;
     Scalars sc;
@@ -888,7 +893,7 @@ namespace pq {
 // checkpoint pickup.
 int reset_prognostic(pq_ctx* c, const Scalars& sc) {
     CK(cudaSetDevice(c->device));
-    if (!c->leapfrog) CK(cudaMemsetAsync(c->hm[0].zeta_old[0], 0, align256(c->field_bytes) * 18, c->stream));
+    if (!c->leapfrog) CK(cudaMemsetAsync(c->hm[0].zeta_old[0], 0, align256(c->field_bytes) * 19, c->stream));
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
     CK(cudaStreamSynchronize(c->stream));

@@ -83,7 +83,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const int o_zpb = ofst(Mb.zeta) + lo;
     const int o_zo = ofst(Mb.zeta_old[cur]) + lo;
     const int o_zn = ofst(Mb.zeta_old[nxt]) + lo;
-    const int o_res = ofst(Mb.res) + lo;
+    const int o_res = ofst(Mb.res_out) + lo;
     const int o_ui = ofst(Mb.ui) + lo;
     const int o_uj = ofst(Mb.uj) + lo;
     const int o_uimo = ofst(Mb.uimo[cur]) + lo;
@@ -870,7 +870,7 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
     __syncthreads();
 
     // ---- stage 5: cabaret_corrector (+ the next step's predictor and beta) --
-    T* res_g = reinterpret_cast<T*>(Mb.res);
+    T* res_g = reinterpret_cast<T*>(Mb.res_out);
     T* zn_g = reinterpret_cast<T*>(Mb.zeta_old[nxt]);
     T* rbn_g = reinterpret_cast<T*>(Mb.res_beta_other);
     T* zpn_g = reinterpret_cast<T*>(Mb.zeta_next);

@@ -12,6 +12,15 @@
 //              L x uj%data(fa_i_min+1:fa_i_max-1, fa_j_min+1:fa_j_max, l),
 //              L x zeta_fi, L x zeta_fj (the same ranges),
 //              L x res(:ii, :jj, l), L x res_beta(:ii, :jj, l).
+// The reference writes its checkpoint inside a step, after the flux and
+// before the corrector (qg3.F90:807-934 precede the exit point and the
+// corrector :940-956): psi, ui, uj, zeta_fi, zeta_fj and res_beta of the
+// step, zeta before the corrector, res of the step before, and model_time
+// half a step short.  The device stops after whole steps, so the dump
+// rebuilds that state: zeta - dt/2 res on the interior nodes, the previous
+// step's res (kept by the step's res ping-pong), model_time - dt/2.  A pickup
+// then finishes the step with the corrector and carries on exactly as the
+// uninterrupted run.
 // The state moves through pq_get_field / pq_set_field in the reference's
 // array layouts, so the device layout (pitched, FP32 state in the mixed form)
 // never shows here.  Reference-layout arrays are indexed below with the
@@ -147,15 +156,30 @@ int pq_write_checkpoint(pq_ctx* c, const char* s_path, const char* supp_path, do
     if (!supported(c)) return PQ_ERR_UNSUPPORTED;
     if (!c->initialized) return fail(c, PQ_ERR_STATE, "pq_write_checkpoint before the state is initialised");
     const int ii = c->ii, jj = c->jj, L = c->L;
+    const bool lf = c->leapfrog;
+    if (lf && c->cur != 0)
+        return fail(c, PQ_ERR_STATE, "the leapfrog state is dumped after the second sub-step of a pair (qg3.F90:823)");
     double sc4[4];
     int rc = pq_get_scalars(c, sc4);
     if (rc) return rc;
-    const double model_time_day = sc4[3] * t_scale / kDayS;  // qg3.F90:661
+    const double dt = sc4[0];  // the dt the last step ran with
+    // qg3.F90:661; CABARET dumps half a step before the step's end.
+    const double model_time_day = (lf ? sc4[3] : sc4[3] - 0.5 * dt) * t_scale / kDayS;
     const double total_time_day = start_time_day + model_time_day;
-    const bool lf = c->leapfrog;
     Ref psi(ii + 2, jj + 2, L), zeta(ii + 2, jj + 2, L), psi2(ii + 2, jj + 2, L), zeta2(ii + 2, jj + 2, L);
     if ((rc = get_ref(c, PQ_F_PSI, psi)) || (rc = get_ref(c, PQ_F_ZETA, zeta))) return rc;
     if (lf && ((rc = get_ref(c, PQ_F_PSI2, psi2)) || (rc = get_ref(c, PQ_F_ZETA2, zeta2)))) return rc;
+    Ref res(ii, jj, L), res_prev(ii, jj, L);
+    if (!lf) {
+        // zeta before the corrector (cabaret_corrector, qg3p_aux.F90:1630-1638,
+        // touches interior nodes only) and the res the reference still holds.
+        if ((rc = get_ref(c, PQ_F_RES, res))) return rc;
+        if ((rc = copy_out_state(c, res_prev.v.data(), c->hm[c->cur].res_out, PQ_PTR_HOST))) return rc;
+        CK(cudaStreamSynchronize(c->stream));
+        for (int l = 1; l <= L; ++l)
+            for (int j = 3; j <= jj; ++j)
+                for (int i = 3; i <= ii; ++i) zeta(i, j, l) = zeta(i, j, l) - 0.5 * dt * res(i - 1, j - 1, l);
+    }
     {
         File out;
         out.f = std::fopen(s_path, "wb");
@@ -176,20 +200,19 @@ int pq_write_checkpoint(pq_ctx* c, const char* s_path, const char* supp_path, do
     }
     if (lf || !supp_path) return PQ_OK;
     Ref ui(ii + 3, jj + 2, L), uj(ii + 2, jj + 3, L), zfi(ii + 3, jj + 2, L), zfj(ii + 2, jj + 3, L);
-    Ref res(ii, jj, L), rb(ii, jj, L);
+    Ref rb(ii, jj, L);
     if ((rc = get_ref(c, PQ_F_UI, ui)) || (rc = get_ref(c, PQ_F_UJ, uj)) || (rc = get_ref(c, PQ_F_ZETA_FI, zfi)) ||
-        (rc = get_ref(c, PQ_F_ZETA_FJ, zfj)) || (rc = get_ref(c, PQ_F_RES, res)) ||
-        (rc = get_ref(c, PQ_F_RES_BETA, rb)))
+        (rc = get_ref(c, PQ_F_ZETA_FJ, zfj)) || (rc = get_ref(c, PQ_F_RES_BETA, rb)))
         return rc;
     File out;
     out.f = std::fopen(supp_path, "wb");
     if (!out.f) return fail(c, PQ_ERR_ARG, std::string("Failed to open output file ") + supp_path);
-    const double dt = sc4[0];  // the dt the last step ran with
     bool ok = put_record(out.f, &model_time_day, 1) && put_record(out.f, &total_time_day, 1) &&
               put_record(out.f, &dt, 1);
     const Range ri = fi_range(ii, jj), rj = fj_range(ii, jj), rs{1, ii, 1, jj};
     std::vector<double> rec;
-    const std::pair<Ref*, Range> order[] = {{&ui, ri}, {&uj, rj}, {&zfi, ri}, {&zfj, rj}, {&res, rs}, {&rb, rs}};
+    const std::pair<Ref*, Range> order[] = {{&ui, ri},  {&uj, rj},       {&zfi, ri},
+                                            {&zfj, rj}, {&res_prev, rs}, {&rb, rs}};
     for (const auto& fr : order)
         for (int l = 1; l <= L && ok; ++l) {
             pack(*fr.first, fr.second, l, rec);

@@ -97,7 +97,9 @@ struct Member {
     void* zeta;       // zeta after predictor and beta (input of the inversion)
     void* zeta_next;  // the same for the next step (written by the fused step)
     double* psi;
-    void* res;
+    void* res;             // corrector residual of the previous step (read by the predictor)
+    void* res_out;         // this step's residual (written by the corrector); ping-ponged
+                           // so that the previous step's stays readable
     void* res_beta;        // res_beta of this step
     void* res_beta_other;  // of the previous step (read by the predictor) or
                            // of the next step (written by the fused step)

@@ -94,11 +94,11 @@ std::string config_key(const pq_model_desc& d, const std::vector<double>& wind) 
 }
 
 // Device bytes a context of this description takes before one exists: its
-// 27 fields, the uncompressed pivot tables as a bound, and 1 MB for the rest.
+// 28 fields, the uncompressed pivot tables as a bound, and 1 MB for the rest.
 size_t estimate_bytes(const pq_model_desc& d) {
     const size_t pitch = (size_t)((d.ii + 31) & ~31);
     const size_t field = align256(pitch * d.jj * d.layers * sizeof(double));
-    return 27 * field + (size_t)d.layers * (d.ii - 2) * d.jj * sizeof(double) + ((size_t)1 << 20);
+    return 28 * field + (size_t)d.layers * (d.ii - 2) * d.jj * sizeof(double) + ((size_t)1 << 20);
 }
 
 void release_ctx(pq_server* s, pq_server::Run& r) {

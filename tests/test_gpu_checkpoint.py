@@ -1,10 +1,11 @@
 """Checkpoint dump and pickup through the C ABI against the oracle.
 
-The device writes the reference's _s.d / _s_supp.d records from its state;
-the files parse with the oracle's reader into the oracle's own fields.  A
-pickup from those files on the device and in the oracle then runs on in
-step.  FP64 bar: relative L2 <= 1e-12 per field after the pickup and after
-a few steps."""
+The device writes the reference's _s.d / _s_supp.d records: the state the
+reference holds at its data output, inside a step before the corrector.
+The files parse with the oracle's reader and match the oracle stopped at
+that point.  A pickup from those files on the device and in the oracle then
+runs on in step, and as the uninterrupted run.  FP64 bar: relative L2
+<= 1e-12 per field."""
 import numpy as np
 import pytest
 
@@ -66,7 +67,8 @@ def test_cabaret_dump_matches_oracle_state(tmp_path, ii, layers):
     cfg = double_gyre(ii, layers)
     g, o = start(cfg, seed=31)
     g.step(7)
-    o.step(7)
+    o.step(6)
+    o.step_to_dump()
     s, supp = str(tmp_path / f"qg{layers}_{ii}_s.d"), str(tmp_path / f"qg{layers}_{ii}_s_supp.d")
     g.write_checkpoint(s, supp, t_scale=cfg.t_scale, start_time_day=10.0)
     ck = O.read_checkpoint(s, supp, ii, ii, layers)
@@ -87,7 +89,8 @@ def test_cabaret_pickup_matches_oracle(tmp_path, adapt):
     cfg = double_gyre(129, 3, **kw)
     g, o = start(cfg, seed=32)
     g.step(9)
-    o.step(9)
+    o.step(8)
+    o.step_to_dump()
     s, supp = str(tmp_path / "qg3_129_s.d"), str(tmp_path / "qg3_129_s_supp.d")
     g.write_checkpoint(s, supp, t_scale=cfg.t_scale, start_time_day=3.5)
     ck = O.read_checkpoint(s, supp, 129, 129, 3)
@@ -99,10 +102,16 @@ def test_cabaret_pickup_matches_oracle(tmp_path, adapt):
     # Both pick up from the same file: the set-up arithmetic is the same.
     compare(g2, o2, AFTER, 1e-15)
     assert g2.scalars()["model_time"] == o2.scalars()["model_time"]
+    # The resumed runs continue the uninterrupted ones.
+    o.finish_step()
+    compare(g2, o, AFTER, TOL)
+    compare(g, o, AFTER, TOL)
     for n in (1, 2, 5):
-        g2.step(n)
-        o2.step(n)
+        for m in (g, g2, o, o2):
+            m.step(n)
         compare(g2, o2, AFTER, TOL * 10)
+        compare(g2, o, AFTER, TOL * 10)
+        assert max(rel_l2(g2.get(f), g.get(f)) for f in ("psi", "zeta")) <= TOL
     sg, so = g2.scalars(), o2.scalars()
     for k in ("dt", "tweight_a", "tweight_u", "model_time"):
         assert abs(sg[k] - so[k]) <= 1e-12 * abs(so[k]), (k, sg[k], so[k])
@@ -128,7 +137,11 @@ def test_pickup_into_a_context_that_has_run(tmp_path):
 def test_leapfrog_checkpoint_round_trip(tmp_path):
     cfg = double_gyre(65, 2, scheme=pq.SCHEME_LEAPFROG)
     g, o = start(cfg, seed=34)
-    g.step(4)
+    g.step(3)
+    with pytest.raises(pq.PQError) as e:   # mid-pair: the reference never dumps here
+        g.write_checkpoint(str(tmp_path / "odd_s.d"))
+    assert e.value.code == pq.PQ_ERR_STATE
+    g.step(1)
     o.step(4)
     s = str(tmp_path / "qg2_65_s.d")
     g.write_checkpoint(s, None, t_scale=cfg.t_scale)
