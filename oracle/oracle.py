@@ -76,6 +76,9 @@ def lib():
         L.or_pv_inversion.argtypes = [C.c_void_p, _dp, _dp]
         L.or_model_pickup.argtypes = [C.c_void_p, C.c_double]
         L.or_model_step_to_dump.argtypes = [C.c_void_p]
+        L.or_model_average.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.or_model_get_average.restype = C.c_double
+        L.or_model_get_average.argtypes = [C.c_void_p, _dp]
         L.or_model_finish_step.argtypes = [C.c_void_p]
         _lib = L
     return _lib
@@ -300,6 +303,16 @@ class Model:
     def sdata(self, name: str) -> np.ndarray:
         a = self.get(name)
         return np.asfortranarray(a[1:-1, 1:-1, :])
+
+    def average(self, enable: bool = True, threshold: float = 0.0) -> None:
+        """Start (clearing) or stop the time average of psi."""
+        lib().or_model_average(self.m, int(enable), float(threshold))
+
+    def get_average(self):
+        """(psi_av / diagnostic_time as (ii, jj, L), diagnostic_time)."""
+        s = np.zeros((self.cfg["ii"], self.cfg["jj"], self.cfg["layers"]), order="F")
+        t = lib().or_model_get_average(self.m, _p(s))
+        return (s * (1.0 / t) if t > 0 else s), t
 
     def step_to_dump(self) -> None:
         """One CABARET step up to the reference's checkpoint point."""

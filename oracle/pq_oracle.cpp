@@ -852,6 +852,10 @@ struct or_model {
     std::vector<double> res, res_beta;  // (ii, jj, L) sized as ii_m x jj_m x layers
     double dt = 0, tweight_a = 0.5, tweight_u = 0.5, model_time = 0;
     int lf_count = 0;  // leapfrog sub-steps taken since initialisation
+    // Time average (qg3.F90:93, 502-503, 672-680, 725): sum of dt * psi sdata.
+    std::vector<double> psi_av;  // (ii, jj, L)
+    double diag_time = 0, av_threshold = 0;
+    bool av_on = false;
     std::vector<double> p_beta_y;  // (ii+2, L)
     // Scratch arrays the reference keeps as module-level `save` arrays.
     std::vector<double> psi_edge, zeta_fin, zeta_fjn, res_visc;
@@ -1668,6 +1672,33 @@ int or_model_init(or_model* m, const double* zeta_ic) {
     return 0;
 }
 
+// psi_av += dt * psi%sdata and diagnostic_time += dt once start_time +
+// model_time > max_spin (qg3.F90:672-680, 725); av_threshold holds
+// max_spin - start_time.  lv: the time level just inverted (psi BLEAPFROG).
+static void accumulate_average(or_model& m, int lv) {
+    if (!m.av_on || !(m.model_time > m.av_threshold)) return;
+    V3 psi = m.full(m.psi[lv]), av = m.sdv(m.psi_av);
+    const Decomp& d = m.d;
+    for (int l = 1; l <= d.layers; ++l)
+        for (int j = 1; j <= d.jj; ++j)
+            for (int i = 1; i <= d.ii; ++i) av(i, j, l) = av(i, j, l) + m.dt * psi(i + 1, j + 1, l);
+    m.diag_time = m.diag_time + m.dt;
+}
+
+// Start (clearing the sum, qg3.F90:502-503) or stop the time average.
+void or_model_average(or_model* m, int enable, double threshold) {
+    m->av_on = enable != 0;
+    m->av_threshold = threshold;
+    m->diag_time = 0.0;
+    m->psi_av.assign(m->nsd(), 0.0);
+}
+
+// The summed dt * psi (ii, jj, L) and diagnostic_time.
+double or_model_get_average(or_model* m, double* sum) {
+    if (sum) std::memcpy(sum, m->psi_av.data(), m->psi_av.size() * sizeof(double));
+    return m->diag_time;
+}
+
 // The CABARET timestep_loop body (qg3.F90:590-967) up to its data output
 // and exit point (:807-934): adapt_dt, predictor, beta, inversion, rel and
 // boundary PV, half the time increment, forcing, cell boundaries,
@@ -1681,6 +1712,7 @@ int or_model_step_to_dump(or_model* m) {
     int rc = invert_level(*m, 0);
     if (rc) return rc;
     m->model_time += 0.5 * m->dt;
+    accumulate_average(*m, 0);
     cabaret_forcing(*m);
     cabaret_cell_boundaries(*m);
     cabaret_extrapolator(*m);
@@ -1715,6 +1747,7 @@ int or_model_step(or_model* m, int nsteps) {
             int rc = invert_level(*m, lf - 1);
             if (rc) return rc;
             m->model_time += m->dt;
+            accumulate_average(*m, lf - 1);
         }
     }
     return 0;

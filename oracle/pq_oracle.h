@@ -123,6 +123,12 @@ long or_model_set(or_model* m, const char* name, const double* in);
  * or_model_finish_step completes the step (corrector, zeta_old, time). */
 int or_model_step_to_dump(or_model* m);
 int or_model_finish_step(or_model* m);
+/* Time average of psi (qg3.F90:502-503, 672-680, 725): enable clears the
+ * sum; steps whose model time (after the first half increment) exceeds
+ * threshold = max_spin - start_time add dt * psi.  get returns
+ * diagnostic_time and copies the sum (ii, jj, L). */
+void or_model_average(or_model* m, int enable, double threshold);
+double or_model_get_average(or_model* m, double* sum);
 /* Checkpoint pickup (qg3.F90:314-363, :448-497) on fields loaded with
  * or_model_set; dt is the checkpoint's (CABARET; ignored for leapfrog). */
 int or_model_pickup(or_model* m, double dt);

@@ -153,6 +153,7 @@ int run_step(pq_ctx* c, int par) {
         if (ev) CK(cudaEventRecord(ev[3], c->stream));
         CK(launch_lf_rel_bc(c->ls[par], 0, 1, c->stream));
         if (ev) CK(cudaEventRecord(ev[4], c->stream));
+        if (c->psi_av) CK(launch_lf_average(c->ls[par], c->stream));
         c->zpar = par;
         return PQ_OK;
     }
@@ -191,6 +192,7 @@ void pq_destroy(pq_ctx* c) {
     for (auto& g : c->graph1)
         if (g) cudaGraphExecDestroy(g);
     if (c->arena) cudaFree(c->arena);
+    if (c->psi_av) cudaFree(c->psi_av);
     if (c->d_members) cudaFree(c->d_members);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -654,6 +656,8 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     sc.tweight_u_last = sc.tweight_u;
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    // diagnostic_time = 0, psi_av = 0 (qg3.F90:502-503)
+    if (c->psi_av) CK(cudaMemsetAsync(c->psi_av, 0, c->field_bytes, c->stream));
     // zeta was cleared together with the other fields; upload it again.
     rc = copy_in_state(c, m.zeta, z.data(), PQ_PTR_HOST);
     if (rc) return rc;
@@ -752,7 +756,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         if (rc) return rc;
         c->cur ^= 1;
         ++done;
-        launches += c->leapfrog ? 5 : 4;
+        launches += step_launches(c);
     }
     if (nsteps - done >= 2) {
         if (!c->graph2) {
@@ -773,7 +777,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         while (nsteps - done >= 2) {
             CK(cudaGraphLaunch(c->graph2, c->stream));
             done += 2;
-            launches += c->leapfrog ? 10 : 8;
+            launches += 2 * step_launches(c);
         }
     }
     if (done < nsteps) {
@@ -781,7 +785,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
         if (rc) return rc;
         c->cur = 1;
         ++done;
-        launches += c->leapfrog ? 5 : 4;
+        launches += step_launches(c);
     }
     c->last_launches = launches;
     return PQ_OK;
@@ -896,12 +900,15 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc) {
     if (!c->leapfrog) CK(cudaMemsetAsync(c->hm[0].zeta_old[0], 0, align256(c->field_bytes) * 19, c->stream));
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    if (c->psi_av) CK(cudaMemsetAsync(c->psi_av, 0, c->field_bytes, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->cur = 0;
     c->zpar = 0;
     c->pred_ready = false;
     return PQ_OK;
 }
+
+int step_launches(const pq_ctx* c) { return c->leapfrog ? (c->psi_av ? 6 : 5) : 4; }
 
 int read_scalars(pq_ctx* c, Scalars* sc) {
     CK(cudaSetDevice(c->device));

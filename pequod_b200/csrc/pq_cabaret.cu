@@ -67,6 +67,8 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const int cur = Mb.cur, nxt = cur ^ 1;
     const double dt64 = Mb.sc->dt;
     const T dt = (T)dt64, tu = (T)Mb.sc->tweight_u;
+    const bool avg = cab_average_gate(Mb);
+    double* const psi_av = Mb.psi_av;
     const T hdt = (T)0.5 * dt;
     const int SH = Mb.cab_sh;
     // All fields of a member live in one allocation: address them by 32-bit
@@ -369,6 +371,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
                 }
             }
             W[o_zn + o * pitch] = z;
+            if (avg) psi_av[o_psil + o * pitch] += dt64 * B[o_psil + o * pitch];
         }
         // ---- owned face writes ---------------------------------------------------
         if (out_i) {
@@ -415,6 +418,7 @@ __device__ void finish_step(const Member& Mb, double* red) {
     const double mu = block_max_l2(Mb.maxu_part, Mb.ntiles_cab, red);
     if (threadIdx.x != 0) return;
     Scalars* sc = Mb.sc;
+    if (cab_average_gate(Mb)) sc->diag_time += sc->dt;
     sc->max_u = mu;
     sc->cfl = mu * sc->dt;
     sc->dt_last = sc->dt;
@@ -874,6 +878,8 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
     T* zn_g = reinterpret_cast<T*>(Mb.zeta_old[nxt]);
     T* rbn_g = reinterpret_cast<T*>(Mb.res_beta_other);
     T* zpn_g = reinterpret_cast<T*>(Mb.zeta_next);
+    const bool avg = cab_average_gate(Mb);
+    const double dt64 = Mb.sc->dt;
 #pragma unroll
     for (int k = 0; k < NU; ++k) {
         const int r = 2 + warp + 8 * k;
@@ -881,6 +887,7 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
         if (!own_col || !(col_in && row_in(r))) continue;
         const int q = X(r, lane);
         const long long o = grow(r) + gcol;
+        if (avg) Mb.psi_av[o] += dt64 * sPsi[q];
         T z = sZf[q];
         if (col_int && row_int(r)) {
             const T rr = -(sFli[q + 1] - sFli[q] + sFlj[q + CT_W] - sFlj[q]);

@@ -41,7 +41,7 @@ struct Scalars {
     // next step's when adaptive stepping is on); what the reference's state
     // holds after a step, since it adapts at the start of the next one.
     double dt_last, tweight_a_last, tweight_u_last;
-    double pad;
+    double diag_time;  // diagnostic_time: the summed dt of the steps in psi_av
 };
 
 // Device status bits (read by the host after a step).
@@ -130,7 +130,20 @@ struct Member {
     int cur;              // ping-pong parity for ui / zfi / zfj (host-managed)
     int adapt_dt;
     double target_cfl, max_dt, max_dt_increase;
+    // Time average of psi (qg3.F90:672-680, 725): when psi_av is set, a step
+    // whose model time after its first half increment exceeds av_threshold
+    // (max_spin - start_time) adds dt * psi to psi_av (node-shaped like psi)
+    // and dt to the scalars' diag_time.
+    double* psi_av;
+    double av_threshold;
 };
+
+// Whether the CABARET step now running accumulates the time average (model
+// time after the step's first half increment, qg3.F90:656, 672).  Read by
+// every CTA before the last one advances model_time.
+__device__ __forceinline__ bool cab_average_gate(const Member& Mb) {
+    return Mb.psi_av != nullptr && Mb.sc->model_time + 0.5 * Mb.sc->dt > Mb.av_threshold;
+}
 
 // Tridiagonal solve geometry: W warps of row chunks per wavenumber column,
 // 8 / W columns per CTA of 256 threads (chosen so a lane's chunk stays short).

@@ -50,6 +50,7 @@ struct pq_ctx {
     // host copies of layout facts
     int ii = 0, jj = 0, L = 0, pitch = 0;
     size_t field_bytes = 0;  // bytes of one L-layer field
+    double* psi_av = nullptr;  // time average of psi (pq_average), FP64, node-shaped like psi
 };
 
 namespace pq {
@@ -85,6 +86,8 @@ int run_step(pq_ctx* c, int par);
 // scalars (reset_prognostic); copy the device scalars to the host.
 int reset_prognostic(pq_ctx* c, const Scalars& sc);
 int read_scalars(pq_ctx* c, Scalars* sc);
+// Kernel launches of one step (the leapfrog time average adds one).
+int step_launches(const pq_ctx* c);
 // pq_create's body.  helm_only: allocate only the Helmholtz fields (helm_io,
 // spec) -- the batched solver's members; stream: use this stream instead of
 // creating one (not owned).

@@ -49,6 +49,7 @@ cudaError_t launch_init_finish(const LaunchSet& ls, int f32, cudaStream_t st);
 cudaError_t launch_lf_step(const LaunchSet& ls, double ra_nu, double ra_alpha, cudaStream_t st);
 cudaError_t launch_lf_forward_euler(const LaunchSet& ls, cudaStream_t st);
 cudaError_t launch_lf_rel_bc(const LaunchSet& ls, int copy_old, int advance_time, cudaStream_t st);
+cudaError_t launch_lf_average(const LaunchSet& ls, cudaStream_t st);
 // Elementwise FP64 <-> FP32 copy of `count` values (to_f32: double -> float).
 cudaError_t launch_convert(void* dst, const void* src, size_t count, int to_f32, cudaStream_t st);
 cudaError_t launch_energy(const LaunchSet& ls, cudaStream_t st);

@@ -142,6 +142,26 @@ __global__ void k_lf_rel_bc(const Member* __restrict__ mems, const int* __restri
     }
 }
 
+// psi_av += dt * psi of the level just advanced and diagnostic_time += dt
+// (qg3.F90:672-680, 725) once model_time, already advanced by this
+// sub-step, exceeds the threshold.  Launched after k_lf_rel_bc only while
+// the time average is on; no thread of this kernel writes model_time.
+__global__ void k_lf_average(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.y, &local);
+    const Member& Mb = mems[mi];
+    if (Mb.psi_av == nullptr || !(Mb.sc->model_time > Mb.av_threshold)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = local;
+    const double dt = Mb.sc->dt;
+    if (i == 0 && j == 0) Mb.sc->diag_time += dt;
+    if (i >= Mb.ii) return;
+    for (int l = 0; l < Mb.L; ++l) {
+        const long long o = (long long)j * Mb.pitch + i + l * Mb.lstride;
+        Mb.psi_av[o] += dt * Mb.psi[o];
+    }
+}
+
 static dim3 node_grid(const LaunchSet& ls) { return dim3((ls.maxI + 127) / 128, ls.maxJ * ls.nmem); }
 
 cudaError_t launch_lf_step(const LaunchSet& ls, double ra_nu, double ra_alpha, cudaStream_t st) {
@@ -151,6 +171,11 @@ cudaError_t launch_lf_step(const LaunchSet& ls, double ra_nu, double ra_alpha, c
 
 cudaError_t launch_lf_forward_euler(const LaunchSet& ls, cudaStream_t st) {
     k_lf_forward_euler<<<node_grid(ls), 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lf_average(const LaunchSet& ls, cudaStream_t st) {
+    k_lf_average<<<node_grid(ls), 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
     return cudaGetLastError();
 }
 
