@@ -251,6 +251,25 @@ PQ_API int pq_write_checkpoint(pq_ctx* ctx, const char* s_path, const char* supp
                                double start_time_day);
 PQ_API int pq_read_checkpoint(pq_ctx* ctx, const char* s_path, const char* supp_path, double* total_time_day);
 
+/* ---- time-averaged streamfunction ----------------------------------------
+ * psi_av (qg3.F90:93, 502-503, 672-680, 725): while on, every step whose
+ * model time (after the CABARET step's first half increment, after the
+ * leapfrog sub-step) exceeds `threshold` = max_spin - start_time
+ * (non-dimensional) adds dt * psi (the step's inversion result, every node)
+ * to the sum and dt to diagnostic_time.  The sum is added to inside the fused
+ * CABARET kernel.  pq_average(ctx, 1, threshold) allocates (first time) and
+ * clears the sum, as initialisation does (pq_init_perturb and
+ * pq_read_checkpoint clear it too); pq_average(ctx, 0, 0) frees it.  Call it
+ * between steps, not while a stream capture is in progress.
+ * pq_get_average: psi_av / diagnostic_time as sdata (ii, jj, L), the field
+ * the reference writes to qg<L>_<ii>_s_av.d (:886-899), and diagnostic_time
+ * (either pointer may be NULL; PQ_ERR_STATE before any step was averaged).
+ * pq_write_average writes that file: model_time_day, total_time_day, L x
+ * the averaged sdata, in the checkpoint's record format. */
+PQ_API int pq_average(pq_ctx* ctx, int enable, double threshold);
+PQ_API int pq_get_average(pq_ctx* ctx, double* psi_av, double* diagnostic_time);
+PQ_API int pq_write_average(pq_ctx* ctx, const char* path, double t_scale, double start_time_day);
+
 /* Block until the context's queued device work is complete. */
 PQ_API int pq_sync(pq_ctx* ctx);
 

@@ -99,6 +99,9 @@ SIGNATURES = {
     "pq_get_scalars": (C.c_int, [C.c_void_p, _dp]),
     "pq_sync": (C.c_int, [C.c_void_p]),
     "pq_write_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_double]),
+    "pq_average": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "pq_get_average": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "pq_write_average": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double]),
     "pq_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, _dp]),
     "pq_stream": (C.c_void_p, [C.c_void_p]),
     "pq_last_launch_count": (C.c_long, [C.c_void_p]),
@@ -373,6 +376,21 @@ class Model:
         supp = supp_path.encode() if supp_path else None
         _check(lib().pq_read_checkpoint(self.ctx, s_path.encode(), supp, _p(ttd)), self.ctx)
         return float(ttd[0])
+
+    def average(self, enable: bool = True, threshold: float = 0.0) -> None:
+        """Start (clearing) or stop the time average of psi (psi_av)."""
+        _check(lib().pq_average(self.ctx, int(enable), float(threshold)), self.ctx)
+
+    def get_average(self):
+        """(psi_av / diagnostic_time as sdata (ii, jj, L), diagnostic_time)."""
+        out = np.zeros((self.cfg.ii, self.cfg.jj, self.cfg.layers), order="F")
+        t = np.zeros(1)
+        _check(lib().pq_get_average(self.ctx, _p(out), _p(t)), self.ctx)
+        return out, float(t[0])
+
+    def write_average(self, path: str, t_scale: float = 1.0, start_time_day: float = 0.0) -> None:
+        """The reference's qg<L>_<ii>_s_av.d file of the current average."""
+        _check(lib().pq_write_average(self.ctx, path.encode(), t_scale, start_time_day), self.ctx)
 
     def device_bytes(self) -> int:
         return int(lib().pq_device_bytes(self.ctx))

@@ -180,3 +180,32 @@ def test_leapfrog_pickup_rel_from_psi(tmp_path, bc):
         np.testing.assert_allclose(p.get("rel" + suf), rel, rtol=0, atol=1e-15 * np.abs(rel).max())
         np.testing.assert_array_equal(p.get("zeta_old" + suf), ck["zeta" + suf])
     assert p.scalars()["model_time"] == 0.0
+
+
+@pytest.mark.parametrize("scheme", [pq.SCHEME_CABARET, pq.SCHEME_LEAPFROG])
+def test_oracle_time_average(scheme):
+    """psi_av (qg3.F90:672-680, 725): the sum of dt * psi over the steps whose
+    model time passed the threshold, restated step by step in numpy."""
+    cfg = double_gyre(17, 2, scheme=scheme)
+    o = run_oracle(cfg, 0, seed=5)
+    dt = cfg.oracle_cfg()["dt"]
+    t0 = o.scalars()["model_time"]
+    thr = t0 + 3.2 * dt          # the first steps are not averaged
+    o.average(True, thr)
+    want = np.zeros((17, 17, 2), order="F")
+    dtime = 0.0
+    for k in range(7):
+        if scheme == pq.SCHEME_CABARET:
+            o.step_to_dump()
+            psi, t = o.get("psi"), o.scalars()["model_time"]
+            o.finish_step()
+        else:
+            o.step(1)
+            t = o.scalars()["model_time"]
+            psi = o.get("psi" if k % 2 == 0 else "psi2")   # sub-steps alternate levels 1, 2
+        if t > thr:
+            want += dt * psi[1:-1, 1:-1]
+            dtime += dt
+    got, t = o.get_average()
+    assert t == dtime and dtime > 0 and dtime < 7 * dt
+    np.testing.assert_allclose(got, want / dtime, rtol=1e-14, atol=0)

@@ -1,0 +1,108 @@
+"""Time-averaged streamfunction (psi_av, qg3.F90:672-680, 725, 886-899) on
+the device against the oracle: the sum accumulated inside the fused CABARET
+kernel (tile and warp-sweep forms) and by the leapfrog sub-step, the
+threshold on model time, diagnostic_time, and the _s_av file."""
+import numpy as np
+import pytest
+
+import pequod_b200 as pq
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b.ravel())
+    return np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0)
+
+
+def double_gyre(ii, layers=3, dt=1800.0, **kw):
+    H = {2: (1.0e5, 3.0e5), 3: (3.0e4, 7.0e4, 3.0e5)}[layers]
+    gp = {2: (1.5,), 3: (1.5, 0.75)}[layers]
+    p = pq.double_gyre_physical(ii, layers=layers, dt=dt, dx=3.84e8 / (ii - 1), H=H, gprime=gp, **kw)
+    return pq.Config.from_physical(p)
+
+
+def start(cfg, seed):
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    if cfg.desc.scheme == pq.SCHEME_LEAPFROG:
+        ic2 = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed + 1000, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+        ic = np.asfortranarray(np.stack([ic, ic2], axis=3))
+    g = pq.Model(cfg)
+    g.init_perturb(ic)
+    o = O.Model(cfg.oracle_cfg())
+    o.init(ic)
+    return g, o
+
+
+@pytest.mark.parametrize("kernel,adapt,prec", [(0, 0, pq.PREC_FP64), (1, 0, pq.PREC_FP64), (0, 1, pq.PREC_FP64),
+                                               (0, 0, pq.PREC_MIXED)])
+def test_cabaret_average_matches_oracle(kernel, adapt, prec):
+    kw = dict(adapt_dt=1, target_cfl=0.1, max_dt=86400.0) if adapt else {}
+    cfg = double_gyre(129, 3, precision=prec, **kw)
+    g, o = start(cfg, seed=41)
+    g.set_tuning(cab_kernel=kernel, cab_band=16, dst_group=0)
+    g.step(2)
+    o.step(2)
+    dt = cfg.desc.dt
+    thr = o.scalars()["model_time"] + 2.6 * dt   # steps 1-2 after this point are not averaged
+    g.average(True, thr)
+    o.average(True, thr)
+    for n in (1, 2, 3, 5):   # eager steps, one-step and two-step graphs
+        g.step(n)
+        o.step(n)
+    a_g, t_g = g.get_average()
+    a_o, t_o = o.get_average()
+    assert t_o > 0 and abs(t_g - t_o) <= 1e-12 * t_o, (t_g, t_o)
+    tol = 1e-12 if prec == pq.PREC_FP64 else 1e-6
+    assert rel_l2(a_g, a_o) <= tol, rel_l2(a_g, a_o)
+
+
+def test_average_off_then_on_and_file(tmp_path):
+    cfg = double_gyre(65, 2)
+    g, o = start(cfg, seed=42)
+    g.step(3)
+    o.step(3)
+    with pytest.raises(pq.PQError) as e:
+        g.get_average()
+    assert e.value.code == pq.PQ_ERR_STATE
+    g.average(True, 0.0)
+    o.average(True, 0.0)
+    g.step(4)
+    o.step(4)
+    a_g, t_g = g.get_average()
+    path = str(tmp_path / "qg2_65_s_av.d")
+    g.write_average(path, t_scale=cfg.t_scale, start_time_day=2.0)
+    recs = O._records(path)
+    assert len(recs) == 2 + 2
+    want_day = (o.scalars()["model_time"] - 0.5 * cfg.desc.dt) * cfg.t_scale / 86400.0
+    assert abs(recs[0][0] - want_day) <= 1e-13 * want_day
+    assert abs(recs[1][0] - (2.0 + want_day)) <= 1e-13 * recs[1][0]
+    a_o, _ = o.get_average()
+    for l in range(2):
+        assert rel_l2(recs[2 + l].reshape((65, 65), order="F"), a_o[:, :, l]) <= 1e-12
+    # Stopping the average leaves the run untouched.
+    g.average(False)
+    g.step(2)
+    o.step(2)
+    assert rel_l2(g.get("psi"), o.get("psi")) <= 1e-11
+
+
+def test_leapfrog_average_matches_oracle():
+    cfg = double_gyre(65, 2, scheme=pq.SCHEME_LEAPFROG)
+    g, o = start(cfg, seed=43)
+    g.step(2)
+    o.step(2)
+    thr = o.scalars()["model_time"] + 1.5 * cfg.desc.dt
+    g.average(True, thr)
+    o.average(True, thr)
+    for n in (1, 2, 3):
+        g.step(n)
+        o.step(n)
+    assert g.last_launch_count() == 3 * 6    # the average adds one kernel per sub-step
+    a_g, t_g = g.get_average()
+    a_o, t_o = o.get_average()
+    assert abs(t_g - t_o) <= 1e-12 * t_o
+    assert rel_l2(a_g, a_o) <= 1e-12
