@@ -307,19 +307,29 @@ PQ_API int pq_kernel_times(pq_ctx* ctx, double* ms4, long* launches4);
 PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int ld, const double* h,
                              const double* s2, double* out, void* stream);
 
-/* Tile parameters of the step kernels (chosen per grid size by the
- * autotuner, pequod_b200/autotune.py; defaults are set by pq_create).
+/* Tile parameters of the step kernels (defaults per grid size are set by
+ * pq_create; results do not depend on them).
  *   cab_kernel CABARET step formulation: 0 one CTA per 28 x 16 tile and
  *              layer, 1 warp sweeps down bands of cab_band rows (default:
  *              tiles up to jj = 700, sweeps above)
  *   cab_band   output rows per warp of the sweep formulation, 4..128
  *   dst_group  row groups per DST CTA: a CTA holds dst_group * layers
- *              warps (0: automatic, 1); layers * dst_group <= 8 */
+ *              warps (0: automatic, 1); layers * dst_group <= 8
+ *   dst_lanes, dst_lanes_inv  lanes per (row, mode) unit of the forward
+ *              and the inverse row DSTs, a power of two up to 64 with
+ *              (ii - 1) / 2 / lanes values per lane in 2..32 (0: default,
+ *              one warp up to ii = 513, two warps from ii = 1025 forward and
+ *              ii = 2049 inverse where the layers fit); units wider than a
+ *              warp synchronise by named barriers.  A CTA (layers * rows *
+ *              lanes threads) must stay within 320 threads with 16 values
+ *              per lane, 256 otherwise. */
 typedef struct pq_tuning {
     int cab_band;
     int dst_group;
     int cab_kernel;
-    int reserved[5];
+    int dst_lanes;
+    int dst_lanes_inv;
+    int reserved[3];
 } pq_tuning;
 PQ_API int pq_set_tuning(pq_ctx* ctx, const pq_tuning* t);
 PQ_API int pq_get_tuning(pq_ctx* ctx, pq_tuning* t);

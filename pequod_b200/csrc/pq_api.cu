@@ -125,11 +125,23 @@ int upload_members(pq_ctx* c) {
 
 // The three Helmholtz kernels.
 int run_helm(pq_ctx* c, int par, int prologue, int epilogue, int mean) {
-    // The stand-alone helm entry (PRO_PLAIN / EPI_HELM) is always FP64.
+    // The stand-alone helm entry (PRO_PLAIN / EPI_HELM) is always FP64, and
+    // runs the row DSTs with the batched solver's geometry, so that a batch
+    // member and the same problem through pq_helm agree bit for bit.
     const int f32 = (c->mixed && epilogue == EPI_PV) ? 1 : 0;
-    CK(launch_dst_forward(c->ls[par], prologue, f32, c->stream));
-    CK(launch_tridiag(c->ls[par], mean, f32, c->stream));
-    CK(launch_dst_inverse(c->ls[par], epilogue, f32, c->stream));
+    LaunchSet ls = c->ls[par];
+    if (prologue == PRO_PLAIN) {
+        ls.dst_group = 0;
+        for (int dir = 0; dir < 2; ++dir) {
+            ls.dst_lanes[dir] = dst_lanes_batched(c->hm[par].M);
+            const int R = dst_rows_per_cta_host(ls.dst_lanes[dir], 0);
+            const int rows = dir == 1 ? c->jj : (c->periodic ? c->jj : c->jj - 2);
+            ls.ctas_dst[dir] = (rows + R - 1) / R;
+        }
+    }
+    CK(launch_dst_forward(ls, prologue, f32, c->stream));
+    CK(launch_tridiag(ls, mean, f32, c->stream));
+    CK(launch_dst_inverse(ls, epilogue, f32, c->stream));
     return PQ_OK;
 }
 
@@ -539,13 +551,15 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         s.ctas_tri = ntiles_tri;
         s.ctas_cab = ntiles_cab;
         s.dst_group = 0;
+        s.dst_lanes[0] = dst_lanes_default(N / 2, L, 0);
+        s.dst_lanes[1] = dst_lanes_default(N / 2, L, 1);
         s.cab_kernel = cab_kernel;
         s.sm_count = sm_count;
         s.prefix_dst[0] = s.prefix_dst[1] = c->d_prefix;
         s.periodic = c->periodic ? 1 : 0;
-        const int R = dst_rows_per_cta_host(N / 2, L, 0);
-        s.ctas_dst[0] = ((c->periodic ? jj : jj - 2) + R - 1) / R;
-        s.ctas_dst[1] = (jj + R - 1) / R;
+        const int R0 = dst_rows_per_cta_host(s.dst_lanes[0], 0), R1 = dst_rows_per_cta_host(s.dst_lanes[1], 0);
+        s.ctas_dst[0] = ((c->periodic ? jj : jj - 2) + R0 - 1) / R0;
+        s.ctas_dst[1] = (jj + R1 - 1) / R1;
     }
     // Scalars: dt and the initial time weights.
     Scalars sc;
@@ -797,6 +811,17 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     CK(cudaStreamSynchronize(c->stream));
     if (t->dst_group < 0 || c->L * t->dst_group > 8) return fail(c, PQ_ERR_ARG, "dst_group out of range");
     if (t->cab_kernel < 0 || t->cab_kernel > 1) return fail(c, PQ_ERR_ARG, "cab_kernel out of range");
+    const int M = c->hm[0].M;
+    int P[2];
+    for (int dir = 0; dir < 2; ++dir) {
+        const int want = dir == 0 ? t->dst_lanes : t->dst_lanes_inv;
+        P[dir] = want > 0 ? want : dst_lanes_default(M, c->L, dir);
+        const int V = M / P[dir];
+        const int R = dst_rows_per_cta_host(P[dir], t->dst_group);
+        if (!is_pow2(P[dir]) || P[dir] > 64 || V * P[dir] != M || V < 2 || V > 32 ||
+            c->L * R * P[dir] > dst_max_threads_host(V))
+            return fail(c, PQ_ERR_ARG, "dst_lanes out of range for this grid and dst_group");
+    }
     for (int p = 0; p < 2; ++p) {
         c->hm[p].cab_sh = t->cab_band;
         c->hm[p].ntiles_cab = t->cab_kernel ? cabaret_ctas(c->ii, c->jj, c->L, t->cab_band)
@@ -804,9 +829,11 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
         c->ls[p].cab_kernel = t->cab_kernel;
         c->ls[p].ctas_cab = c->hm[p].ntiles_cab;
         c->ls[p].dst_group = t->dst_group;
-        const int R = dst_rows_per_cta_host(c->hm[p].M, c->L, t->dst_group);
-        c->ls[p].ctas_dst[0] = ((c->periodic ? c->jj : c->jj - 2) + R - 1) / R;
-        c->ls[p].ctas_dst[1] = (c->jj + R - 1) / R;
+        c->ls[p].dst_lanes[0] = P[0];
+        c->ls[p].dst_lanes[1] = P[1];
+        const int R0 = dst_rows_per_cta_host(P[0], t->dst_group), R1 = dst_rows_per_cta_host(P[1], t->dst_group);
+        c->ls[p].ctas_dst[0] = ((c->periodic ? c->jj : c->jj - 2) + R0 - 1) / R0;
+        c->ls[p].ctas_dst[1] = (c->jj + R1 - 1) / R1;
     }
     int rc = upload_members(c);
     if (rc) return rc;
@@ -829,6 +856,8 @@ int pq_get_tuning(pq_ctx* c, pq_tuning* t) {
     t->cab_band = c->hm[0].cab_sh;
     t->cab_kernel = c->ls[0].cab_kernel;
     t->dst_group = c->ls[0].dst_group;
+    t->dst_lanes = c->ls[0].dst_lanes[0];
+    t->dst_lanes_inv = c->ls[0].dst_lanes[1];
     return PQ_OK;
 }
 

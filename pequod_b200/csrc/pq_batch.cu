@@ -163,9 +163,10 @@ int pq_batch_create(pq_batch** out, int n, const int* ii, const int* jj, const i
         Pending p;
         p.mem_off = hd.size();
         const int I = kv.first.first, L = kv.first.second, N = I - 1;
-        const int R = dst_rows_per_cta_host(N / 2, L, 0);
         int maxJ = 0, maxPitch = 0;
         for (int dir = 0; dir < 2; ++dir) {
+            cl.ls.dst_lanes[dir] = dst_lanes_batched(N / 2);
+            const int R = dst_rows_per_cta_host(cl.ls.dst_lanes[dir], 0);
             p.pref_off[dir] = pref.size();
             int acc = 0;
             for (int k : cl.idx) {

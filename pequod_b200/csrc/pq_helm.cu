@@ -110,14 +110,23 @@ template <int R, typename T2> __device__ __forceinline__ void dft_reg(T2* v) {
     }
 }
 
+// Barrier of one unit's P lanes: the warp (P <= 32) or the unit's warps by a
+// named barrier (P > 32; id 1 + uid, never 0, which __syncthreads uses).
+__device__ __forceinline__ void unit_sync(int P, int uid) {
+    if (P <= 32)
+        __syncwarp();
+    else
+        asm volatile("bar.sync %0, %1;\n" ::"r"(1 + uid), "r"(P) : "memory");
+}
+
 // One radix-R Stockham pass over the unit's M values (Ns = length of the
 // sub-transforms already done).  Lane p owns butterflies j = p + P*b; its
 // values v[b*R + r] are the butterfly inputs j + r*(M/R).  With `load` false
 // the inputs are already in registers (first pass).  Output is stored to the
 // unit's padded complex row.
 template <int V, int R, typename T2>
-__device__ __forceinline__ void fft_pass(T2 (&v)[V], T2* z, int p, int P, int M, int logM, int Ns, int logNs,
-                                         const T2* __restrict__ tw, bool load) {
+__device__ __forceinline__ void fft_pass(T2 (&v)[V], T2* z, int p, int P, int uid, int M, int logM, int Ns,
+                                         int logNs, const T2* __restrict__ tw, bool load) {
     constexpr int logR = (R == 8) ? 3 : (R == 4) ? 2 : 1;
     const int MR = M >> logR;
     if (load) {
@@ -136,7 +145,7 @@ __device__ __forceinline__ void fft_pass(T2 (&v)[V], T2* z, int p, int P, int M,
         }
         dft_reg<R>(&v[b * R]);
     }
-    __syncwarp();
+    unit_sync(P, uid);
 #pragma unroll
     for (int b = 0; b < V / R; ++b) {
         const int j = p + P * b, k = j & (Ns - 1);
@@ -144,14 +153,16 @@ __device__ __forceinline__ void fft_pass(T2 (&v)[V], T2* z, int p, int P, int M,
 #pragma unroll
         for (int r = 0; r < R; ++r) z[cpad(o + r * Ns)] = v[b * R + r];
     }
-    __syncwarp();
+    unit_sync(P, uid);
 }
 
 // DST-I (FFTPACK sint convention, qg3p_helmholtz.F90:1370-1426) of the real
 // row held in the unit buffer (x_k at buf[k], k = 1..N-1), output X_k at
-// buf[xpad(k)], k = 1..N-1.  Every lane of the warp must call this.
+// buf[xpad(k)], k = 1..N-1.  Every lane of the unit must call this; uid
+// names the unit's barrier, utot is P/32 scalars of scratch for units wider
+// than a warp.
 template <int V, typename T>
-__device__ __forceinline__ void dst_unit(T* buf, int p, int P, int N, int M, int logM,
+__device__ __forceinline__ void dst_unit(T* buf, int p, int P, int uid, T* utot, int N, int M, int logM,
                                          const typename Cplx<T>::type* __restrict__ tw,
                                          const typename Cplx<T>::type* __restrict__ wsp,
                                          const T* __restrict__ was) {
@@ -187,7 +198,7 @@ __device__ __forceinline__ void dst_unit(T* buf, int p, int P, int N, int M, int
             const int rem = M >> logNs;
             if constexpr (V >= 8) {
                 if (rem >= 8) {
-                    fft_pass<V, 8>(v, z, p, P, M, logM, Ns, logNs, tw, !first);
+                    fft_pass<V, 8>(v, z, p, P, uid, M, logM, Ns, logNs, tw, !first);
                     Ns <<= 3;
                     logNs += 3;
                     first = false;
@@ -195,15 +206,15 @@ __device__ __forceinline__ void dst_unit(T* buf, int p, int P, int N, int M, int
                 }
             }
             if constexpr (V >= 4) {
-                if (rem == 4) {
-                    fft_pass<V, 4>(v, z, p, P, M, logM, Ns, logNs, tw, !first);
+                if (rem >= 4) {
+                    fft_pass<V, 4>(v, z, p, P, uid, M, logM, Ns, logNs, tw, !first);
                     Ns <<= 2;
                     logNs += 2;
                     first = false;
                     continue;
                 }
             }
-            fft_pass<V, 2>(v, z, p, P, M, logM, Ns, logNs, tw, !first);
+            fft_pass<V, 2>(v, z, p, P, uid, M, logM, Ns, logNs, tw, !first);
             Ns <<= 1;
             logNs += 1;
             first = false;
@@ -231,14 +242,23 @@ __device__ __forceinline__ void dst_unit(T* buf, int p, int P, int N, int M, int
         run += (q == 0) ? (T)0.5 * cx : cx;
         Xo[e] = run;
     }
-    // Segmented (width P) exclusive scan of the lanes' totals.
+    // Segmented (width P) exclusive scan of the lanes' totals: in the warp
+    // (or P-lane segment), then across the unit's warps.
     T incl = run;
-    for (int d = 1; d < P; d <<= 1) {
-        const T y = __shfl_up_sync(0xffffffffu, incl, d, P);
-        if (p >= d) incl += y;
+    const int PW = P < 32 ? P : 32;
+    for (int d = 1; d < PW; d <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, incl, d, PW);
+        if ((p & (PW - 1)) >= d) incl += y;
+    }
+    if (P > 32) {
+        if ((p & 31) == 31) utot[p >> 5] = incl;
+        unit_sync(P, uid);
+        T add = (T)0;
+        for (int w = 0; w < (p >> 5); ++w) add += utot[w];
+        incl += add;
     }
     const T excl = incl - run;
-    __syncwarp();
+    unit_sync(P, uid);
 #pragma unroll
     for (int e = 0; e < V; ++e) {
         const int q = p * V + e;
@@ -247,16 +267,28 @@ __device__ __forceinline__ void dst_unit(T* buf, int p, int P, int N, int M, int
         pr.y = Xo[e] + excl;
         *reinterpret_cast<T2*>(buf + xpad(2 * q)) = pr;
     }
-    __syncwarp();
+    unit_sync(P, uid);
 }
 
-// Launch geometry shared by host and device: V per M, rows per CTA, scalars
-// per unit buffer.
-__host__ __device__ inline int dst_v(int M) { return M <= 2 ? 2 : M == 4 ? 4 : M <= 256 ? 8 : M / 32; }
-__host__ __device__ inline int dst_rows_per_cta(int M, int L, int c) {
-    const int P = M / dst_v(M);
+// Launch geometry shared by host and device: lanes P and values V = M / P
+// per unit, rows per CTA (whole warps: 32 / P rows per group for P < 32),
+// scalars per unit buffer.  Default P (measured per grid size on B200): one
+// warp per unit up to M = 256 (fewer values per lane, more warps in flight,
+// shorter dependent chains), two warps (a named barrier between passes) from
+// M = 512 for the forward and M = 1024 for the inverse transform (whose
+// back-projection epilogue favours one warp at M = 512), when a row's L units
+// fit the kernel's thread bound.
+// Threads a DST CTA may have: 320 for 16 values per lane (five layers of
+// two-warp units at M = 1024), else 256, the bound the others' register
+// use was tuned for.
+__host__ __device__ constexpr int dst_max_threads(int V) { return V == 16 ? 320 : 256; }
+__host__ __device__ inline int dst_lanes_default_hd(int M, int L, int dir) {
+    if (M <= 256 || (dir == 1 && M <= 512)) return M / 2 < 32 ? (M / 2 < 1 ? 1 : M / 2) : 32;
+    return L * 64 <= dst_max_threads(M / 64) ? 64 : 32;
+}
+__host__ __device__ inline int dst_rows_per_cta(int P, int c) {
     if (c <= 0) c = 1;  // one row group per CTA: the most CTAs, measured fastest
-    return c * (32 / P);
+    return c * (P >= 32 ? 1 : 32 / P);
 }
 __host__ __device__ inline int dst_unit_len(int N) { return (N + N / 8 + 2 + 1) & ~1; }
 
@@ -300,7 +332,7 @@ __device__ __forceinline__ void cp4z(void* dst, const void* src, bool ok) {
 // transformed in FP32, while the barotropic mode (m = 0) is kept in FP64
 // end to end (spec64), as are the projection, the back-projection and psi.
 template <typename S, int V, int PRO, int EPI>
-__global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
+__global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
                                              int nmem, int row_offset, int c, int corr_smem) {
     constexpr bool MX = sizeof(S) == 4;
     __shared__ Member Mb;
@@ -312,7 +344,7 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
     const int L = Mb.L, N = Mb.N, M = Mb.M, logM = Mb.logM, n = Mb.n, ii = Mb.ii, jj = Mb.jj, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
     const int P = M / V;
-    const int R = dst_rows_per_cta(M, L, c);
+    const int R = dst_rows_per_cta(P, c);
     const int U = dst_unit_len(N);
     const int j0 = row_offset + local * R;                 // first row of this CTA
     // one past the last row; a channel periodic in j transforms every row
@@ -473,10 +505,12 @@ __global__ void __launch_bounds__(256) k_dst(const Member* __restrict__ mems, co
     const int ju = j0 + ur;
     double* buf = ubuf(um, ur);
     const bool interior = (Mb.periodic || (ju >= 1 && ju <= jj - 2)) && ju < jend;
+    __shared__ double utot[8][2];  // cross-warp scan totals of units wider than a warp
     if (fp64_mode(um))
-        dst_unit<V, double>(buf, p, P, N, M, logM, Mb.tw, Mb.wsplit, Mb.was);
+        dst_unit<V, double>(buf, p, P, u, utot[u & 7], N, M, logM, Mb.tw, Mb.wsplit, Mb.was);
     else
-        dst_unit<V, float>(reinterpret_cast<float*>(buf), p, P, N, M, logM, Mb.tw_f, Mb.wsplit_f, Mb.was_f);
+        dst_unit<V, float>(reinterpret_cast<float*>(buf), p, P, u, reinterpret_cast<float*>(utot[u & 7]), N, M, logM,
+                           Mb.tw_f, Mb.wsplit_f, Mb.was_f);
 
     if (EPI == EPI_SPEC) {
         if (ju < jend) {
@@ -855,12 +889,21 @@ __host__ __device__ inline size_t tri_smem_bytes(int jj) {
 
 // ---------------------------------------------------------------------------
 // Host launchers.
-int dst_rows_per_cta_host(int M, int L, int c) { return dst_rows_per_cta(M, L, c); }
+int dst_lanes_default(int M, int L, int dir) { return dst_lanes_default_hd(M, L, dir); }
+// Batched solves fill the GPU with many members' rows: throughput, not one
+// row's latency, bounds them, so units keep 8 values per lane (fewer passes
+// and shared-memory round trips per value) up to M = 256, then one warp.
+int dst_lanes_batched(int M) {
+    const int V = M <= 2 ? 2 : M == 4 ? 4 : M <= 256 ? 8 : M / 32;
+    return M / V;
+}
+int dst_max_threads_host(int V) { return dst_max_threads(V); }
+int dst_rows_per_cta_host(int P, int c) { return dst_rows_per_cta(P, c); }
 
 template <typename S, int V, int PRO, int EPI>
 static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const int M = ls.maxN / 2, L = ls.maxL;
-    const int R = dst_rows_per_cta(M, L, ls.dst_group);
+    const int R = dst_rows_per_cta(M / V, ls.dst_group);
     const int threads = L * R * (M / V);
     size_t bytes = (size_t)L * R * dst_unit_len(ls.maxN) * sizeof(double);
     const size_t cbytes = (size_t)R * (L - 1) * ls.maxPitch * sizeof(double);
@@ -878,7 +921,7 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
 
 template <typename S, int PRO, int EPI>
 static cudaError_t launch_dst(const LaunchSet& ls, cudaStream_t st) {
-    switch (dst_v(ls.maxN / 2)) {
+    switch (ls.maxN / 2 / ls.dst_lanes[EPI == EPI_SPEC ? 0 : 1]) {
         case 2: return launch_dst_v<S, 2, PRO, EPI>(ls, st);
         case 4: return launch_dst_v<S, 4, PRO, EPI>(ls, st);
         case 8: return launch_dst_v<S, 8, PRO, EPI>(ls, st);

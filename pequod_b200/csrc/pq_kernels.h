@@ -24,6 +24,7 @@ struct LaunchSet {
     const int* prefix_dst[2];         // DST CTAs per member, forward [0] and inverse [1]
     int ctas_dst[2];                  //   (ceil(rows / dst_rows_per_cta) per member)
     int dst_group;                    // row groups per DST CTA (0: automatic)
+    int dst_lanes[2];                 // lanes P per DST unit (values per lane M / P), forward [0] / inverse [1]
     int cab_kernel;                   // CABARET formulation: 0 tiles, 1 warp sweeps
     int periodic;                     // channel periodic in j: every row is transformed
     int sm_count;                     // SMs of the device (persistent grids)
@@ -31,8 +32,13 @@ struct LaunchSet {
 
 
 // pq_helm.cu
-// Rows per DST CTA for complex length M = N/2, L modes, row-group setting c.
-int dst_rows_per_cta_host(int M, int L, int c);
+// Lanes per DST unit for complex length M = N/2 and L modes by default
+// (dir 0 forward, 1 inverse), and rows per DST CTA for P lanes per unit and
+// row-group setting c.
+int dst_lanes_default(int M, int L, int dir);
+int dst_lanes_batched(int M);
+int dst_max_threads_host(int V);
+int dst_rows_per_cta_host(int P, int c);
 // f32: the mixed form (FP32 layer fields and baroclinic spectral rows)
 cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, int f32, cudaStream_t st);
 cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, int f32, cudaStream_t st);

@@ -49,6 +49,8 @@ def helm_cfg(ii, jj, ss, periodic=False):
     (129, 257, [0.0, 0.7]),
     (257, 129, [0.0, 3.0, 11.0]),
     (1025, 1025, [0.0, 1.07613857, 3.31661571]),
+    (1025, 1025, [0.0, 0.4, 1.1, 2.5, 6.0]),
+    (2049, 2049, [0.0, 0.3, 1.2, 4.0, 9.5]),
 ])
 def test_helm_matches_oracle(ii, jj, ss):
     rng = np.random.default_rng(ii * 7 + jj)
@@ -269,15 +271,17 @@ def test_energy_kats_gpu():
     assert abs(ep - ep_o) <= 1e-13 * abs(ep_o)
 
 
-@pytest.mark.parametrize("kernel,band,group", [(1, 4, 0), (1, 8, 1), (1, 32, 2), (1, 128, 1), (0, 16, 2)])
-def test_tile_parameters_do_not_change_results(kernel, band, group):
-    """The CABARET formulation (tiles or warp sweeps), the sweep's band height
-    and the DST CTA width are tuning knobs: results must match the oracle for
-    any choice."""
+@pytest.mark.parametrize("kernel,band,group,lanes", [(1, 4, 0, 0), (1, 8, 1, 16), (1, 32, 2, 0), (1, 128, 1, 32),
+                                                     (0, 16, 2, 0), (0, 16, 1, 32)])
+def test_tile_parameters_do_not_change_results(kernel, band, group, lanes):
+    """The CABARET formulation (tiles or warp sweeps), the sweep's band height,
+    the DST CTA width and the DST lanes per unit are tuning knobs: results
+    must match the oracle for any choice."""
     cfg = double_gyre(129, 3)
     g, o = start(cfg, seed=5)
-    g.set_tuning(cab_kernel=kernel, cab_band=band, dst_group=group)
-    assert g.get_tuning() == {"cab_band": band, "dst_group": group, "cab_kernel": kernel}
+    g.set_tuning(cab_kernel=kernel, cab_band=band, dst_group=group, dst_lanes=lanes, dst_lanes_inv=lanes)
+    assert g.get_tuning() == {"cab_band": band, "dst_group": group, "cab_kernel": kernel,
+                              "dst_lanes": lanes if lanes else 32, "dst_lanes_inv": lanes if lanes else 32}
     g.step(3)
     o.step(3)
     compare(g, o, TOL_STEP * 10)
@@ -307,3 +311,17 @@ def test_odd_step_counts_match_oracle():
         g.step(n)
         o.step(n)
     compare(g, o, TOL_STEP * 10)
+
+
+@pytest.mark.parametrize("ii,lanes", [(257, 64), (513, 64), (513, 16)])
+def test_dst_units_of_two_warps_match_oracle(ii, lanes):
+    """Row DST units spread over two warps (named barriers between the
+    passes, a two-level scan) or over half warps give the oracle's results."""
+    cfg = double_gyre(ii, 3)
+    g, o = start(cfg, seed=8)
+    g.set_tuning(dst_lanes=lanes, dst_lanes_inv=lanes)
+    g.step(3)
+    o.step(3)
+    compare(g, o, TOL_STEP * 10)
+    with pytest.raises(pq.PQError):
+        g.set_tuning(dst_lanes=128)
