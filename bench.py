@@ -230,6 +230,8 @@ def run_ours(a, rank, world, local_rank):
     cfg = make_config(a.size, a.layers, a.dt, precision=0 if a.precision == "fp64" else 1)
     units = cfg.ii * cfg.jj * cfg.layers
     m = pq.Model(cfg, device=dev)
+    if getattr(a, "pdl", False):
+        m.set_tuning(pdl=1)
     ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=1 + rank, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     m.init_perturb(ic)
     m.step(max(3, a.warmup))
@@ -343,7 +345,8 @@ def run_ours(a, rank, world, local_rank):
         "dtype": "f64" if a.precision == "fp64" else "f32/f64", "data": "synthetic",
         "config": {"workload": workload, "ii": cfg.ii, "jj": cfg.jj, "layers": cfg.layers, "dt_s": a.dt,
                    "precision": a.precision, "l2": "flushed before every timed step (256 MiB memset)",
-                   "parallelism": f"replicas{world}"},
+                   "parallelism": f"replicas{world}",
+                   "launch": "programmatic dependent launch" if a.pdl else "serial"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "alg_bytes_per_launch": alg, "ms_per_launch": dom_ms},
@@ -545,6 +548,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=513)
+    ap.add_argument("--pdl", action="store_true",
+                    help="launch the step kernels with programmatic dependent launch")
     ap.add_argument("--layers", type=int, default=3)
     ap.add_argument("--dt", type=float, default=900.0)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])

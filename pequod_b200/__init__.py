@@ -61,7 +61,7 @@ class ModelDesc(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("cab_band", C.c_int), ("dst_group", C.c_int), ("cab_kernel", C.c_int), ("dst_lanes", C.c_int),
-                ("dst_lanes_inv", C.c_int), ("reserved", C.c_int * 3)]
+                ("dst_lanes_inv", C.c_int), ("pdl", C.c_int), ("reserved", C.c_int * 2)]
 
 
 class Physical(C.Structure):
@@ -410,7 +410,7 @@ class Model:
         t = Tuning()
         _check(lib().pq_get_tuning(self.ctx, C.byref(t)), self.ctx)
         return {"cab_band": t.cab_band, "dst_group": t.dst_group, "cab_kernel": t.cab_kernel, "dst_lanes": t.dst_lanes,
-                "dst_lanes_inv": t.dst_lanes_inv}
+                "dst_lanes_inv": t.dst_lanes_inv, "pdl": t.pdl}
 
     def kernel_timing(self, enable: bool) -> None:
         _check(lib().pq_kernel_timing(self.ctx, int(enable)), self.ctx)

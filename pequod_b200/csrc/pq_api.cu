@@ -551,6 +551,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         s.ctas_tri = ntiles_tri;
         s.ctas_cab = ntiles_cab;
         s.dst_group = 0;
+        s.pdl = 0;
         s.dst_lanes[0] = dst_lanes_default(N / 2, L, 0);
         s.dst_lanes[1] = dst_lanes_default(N / 2, L, 1);
         s.cab_kernel = cab_kernel;
@@ -811,6 +812,7 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     CK(cudaStreamSynchronize(c->stream));
     if (t->dst_group < 0 || c->L * t->dst_group > 8) return fail(c, PQ_ERR_ARG, "dst_group out of range");
     if (t->cab_kernel < 0 || t->cab_kernel > 1) return fail(c, PQ_ERR_ARG, "cab_kernel out of range");
+    if (t->pdl < 0 || t->pdl > 1) return fail(c, PQ_ERR_ARG, "pdl is 0 or 1");
     const int M = c->hm[0].M;
     int P[2];
     for (int dir = 0; dir < 2; ++dir) {
@@ -829,6 +831,7 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
         c->ls[p].cab_kernel = t->cab_kernel;
         c->ls[p].ctas_cab = c->hm[p].ntiles_cab;
         c->ls[p].dst_group = t->dst_group;
+        c->ls[p].pdl = t->pdl;
         c->ls[p].dst_lanes[0] = P[0];
         c->ls[p].dst_lanes[1] = P[1];
         const int R0 = dst_rows_per_cta_host(P[0], t->dst_group), R1 = dst_rows_per_cta_host(P[1], t->dst_group);
@@ -858,6 +861,7 @@ int pq_get_tuning(pq_ctx* c, pq_tuning* t) {
     t->dst_group = c->ls[0].dst_group;
     t->dst_lanes = c->ls[0].dst_lanes[0];
     t->dst_lanes_inv = c->ls[0].dst_lanes[1];
+    t->pdl = c->ls[0].pdl;
     return PQ_OK;
 }
 

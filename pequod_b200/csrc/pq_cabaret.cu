@@ -448,6 +448,7 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
     __shared__ double red[CAB_WARPS];
     __shared__ int is_last;
     extern __shared__ __align__(16) double cab_ring[];  // [CAB_WARPS][CAB_RING]
+    pdl_wait();
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
     load_member_c(Mb, mems + mi);
@@ -468,6 +469,7 @@ __global__ void __launch_bounds__(CAB_WARPS * 32) k_cabaret_fused(const Member* 
         umax = interior ? cab_sweep<false, PRED, T>(Mb, l, i0, j0, lane, ring)
                         : cab_sweep<true, PRED, T>(Mb, l, i0, j0, lane, ring);
     }
+    pdl_release();
 
     // Max |u| of the new face velocities (cabaret_cfl / cabaret_adapt_dt);
     // the last CTA of the member finishes the reduction and, when adaptive
@@ -915,6 +917,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_cabaret_tile(const Member* __res
     __shared__ double red[CT_THREADS / 32];
     __shared__ int is_last;
     extern __shared__ __align__(16) char tsm[];
+    pdl_wait();
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
     load_member_c(Mb, mems + mi);
@@ -928,6 +931,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_cabaret_tile(const Member* __res
     // the interior nodes.
     const bool inner = i0 - 2 >= 1 && i0 + CT_X + 1 <= ii - 2 && j0 - 2 >= 1 && j0 + CT_Y + 1 <= jj - 2;
     double umax = inner ? cab_tile<PRED, false, T>(Mb, l, i0, j0, tsm) : cab_tile<PRED, true, T>(Mb, l, i0, j0, tsm);
+    pdl_release();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     umax = warp_max(umax);
@@ -961,14 +965,16 @@ static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
         cudaError_t e =
             cudaFuncSetAttribute(k_cabaret_tile<PRED, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb);
         if (e != cudaSuccess) return e;
-        k_cabaret_tile<PRED, T><<<ls.ctas_cab, CT_THREADS, tb, st>>>(ls.members, ls.prefix_cab, ls.nmem);
-        return cudaGetLastError();
+        return launch_step_kernel(ls.pdl, k_cabaret_tile<PRED, T>, dim3(ls.ctas_cab), dim3(CT_THREADS), tb, st,
+                                  ls.members, ls.prefix_cab, ls.nmem);
     }
     const size_t bytes = (size_t)CAB_WARPS * CAB_RING * sizeof(double);
     cudaError_t e =
         cudaFuncSetAttribute(k_cabaret_fused<PRED, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    k_cabaret_fused<PRED, T><<<ls.ctas_cab, CAB_WARPS * 32, bytes, st>>>(ls.members, ls.prefix_cab, ls.nmem);
+    cudaError_t le = launch_step_kernel(ls.pdl, k_cabaret_fused<PRED, T>, dim3(ls.ctas_cab), dim3(CAB_WARPS * 32),
+                                        bytes, st, ls.members, ls.prefix_cab, ls.nmem);
+    if (le != cudaSuccess) return le;
     return cudaGetLastError();
 }
 

@@ -138,6 +138,16 @@ struct Member {
     double av_threshold;
 };
 
+// Programmatic dependent launch: the step kernels are launched so that the
+// next one may be scheduled while this one finishes.  pdl_wait() first waits
+// until the predecessor has completed and its writes are visible (a no-op
+// without the launch attribute); nothing is read or written before it.
+// pdl_release() lets the successor be scheduled once every CTA of this grid
+// has passed it: called after a CTA's main work, so that the successor's
+// CTAs overlap only this grid's tail.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // Whether the CABARET step now running accumulates the time average (model
 // time after the step's first half increment, qg3.F90:656, 672).  Read by
 // every CTA before the last one advances model_time.

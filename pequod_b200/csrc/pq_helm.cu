@@ -337,6 +337,7 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
     constexpr bool MX = sizeof(S) == 4;
     __shared__ Member Mb;
     extern __shared__ __align__(16) double sm[];
+    pdl_wait();
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
     load_member(Mb, mems + mi);
@@ -511,6 +512,7 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
     else
         dst_unit<V, float>(reinterpret_cast<float*>(buf), p, P, u, reinterpret_cast<float*>(utot[u & 7]), N, M, logM,
                            Mb.tw_f, Mb.wsplit_f, Mb.was_f);
+    pdl_release();
 
     if (EPI == EPI_SPEC) {
         if (ju < jend) {
@@ -619,6 +621,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     __shared__ double tot[2][TRI_THREADS / 32][2];  // per-warp affine totals (forward, backward)
     __shared__ int is_last;
     extern __shared__ __align__(16) double strip[];
+    pdl_wait();
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.x, &local);
     load_member(Mb, mems + mi);
@@ -839,6 +842,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     }
     const double colsum = (active && do_mean) ? warp_sum(lsum) * __ldg(&Mb.wmean[kk]) : 0.0;
     if (lane == 0) wpart[warp] = colsum;
+    pdl_release();
     __syncthreads();
     {
         const int cc = threadIdx.x % KT, qq = threadIdx.x / KT;
@@ -914,9 +918,9 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
         cudaFuncSetAttribute(k_dst<S, V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     const int dir = (EPI == EPI_SPEC) ? 0 : 1;
-    k_dst<S, V, PRO, EPI><<<ls.ctas_dst[dir], threads, bytes, st>>>(
-        ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0, ls.dst_group, corr_smem);
-    return cudaGetLastError();
+    return launch_step_kernel(ls.pdl, k_dst<S, V, PRO, EPI>, dim3(ls.ctas_dst[dir]), dim3(threads), bytes, st,
+                              ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0,
+                              ls.dst_group, corr_smem);
 }
 
 template <typename S, int PRO, int EPI>
@@ -950,7 +954,9 @@ template <typename S, bool GS>
 static cudaError_t launch_tri(const LaunchSet& ls, int do_mean, size_t bytes, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(k_tridiag<S, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    k_tridiag<S, GS><<<ls.ctas_tri, TRI_THREADS, bytes, st>>>(ls.members, ls.prefix_tri, ls.nmem, do_mean);
+    cudaError_t le = launch_step_kernel(ls.pdl, k_tridiag<S, GS>, dim3(ls.ctas_tri), dim3(TRI_THREADS), bytes, st,
+                                        ls.members, ls.prefix_tri, ls.nmem, do_mean);
+    if (le != cudaSuccess) return le;
     return cudaGetLastError();
 }
 

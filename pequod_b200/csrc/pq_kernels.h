@@ -28,7 +28,27 @@ struct LaunchSet {
     int cab_kernel;                   // CABARET formulation: 0 tiles, 1 warp sweeps
     int periodic;                     // channel periodic in j: every row is transformed
     int sm_count;                     // SMs of the device (persistent grids)
+    int pdl;                          // launch the step kernels with programmatic dependent launch
 };
+
+// Launch `kernel` on `st`, with programmatic stream serialisation when pdl
+// is set: the kernel may be scheduled before its predecessor in the stream
+// has finished, and waits for it in pdl_wait_then_release().
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_step_kernel(int pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                      cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 
 
 // pq_helm.cu

@@ -109,12 +109,15 @@ def main(argv=None) -> None:
     ap.add_argument("--steps", type=int, default=6)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--dst-lanes", type=int, default=0, help="lanes per row-DST unit, both directions (0: default)")
+    ap.add_argument("--pdl", action="store_true", help="programmatic dependent launch of the step kernels")
     a = ap.parse_args(argv)
     cfg = double_gyre(a.size, a.layers, a.dt, pq.PREC_FP64 if a.precision == "fp64" else pq.PREC_MIXED)
     m = pq.Model(cfg)
     m.init_perturb(initial_condition(cfg))
     if a.dst_lanes:
         m.set_tuning(dst_lanes=a.dst_lanes, dst_lanes_inv=a.dst_lanes)
+    if a.pdl:
+        m.set_tuning(pdl=1)
     m.step(4)
     m.kernel_timing(True)  # eager: one launch per kernel
     for _ in range(a.steps):

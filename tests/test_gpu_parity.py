@@ -281,7 +281,8 @@ def test_tile_parameters_do_not_change_results(kernel, band, group, lanes):
     g, o = start(cfg, seed=5)
     g.set_tuning(cab_kernel=kernel, cab_band=band, dst_group=group, dst_lanes=lanes, dst_lanes_inv=lanes)
     assert g.get_tuning() == {"cab_band": band, "dst_group": group, "cab_kernel": kernel,
-                              "dst_lanes": lanes if lanes else 32, "dst_lanes_inv": lanes if lanes else 32}
+                              "dst_lanes": lanes if lanes else 32, "dst_lanes_inv": lanes if lanes else 32,
+                              "pdl": 0}
     g.step(3)
     o.step(3)
     compare(g, o, TOL_STEP * 10)
@@ -325,3 +326,16 @@ def test_dst_units_of_two_warps_match_oracle(ii, lanes):
     compare(g, o, TOL_STEP * 10)
     with pytest.raises(pq.PQError):
         g.set_tuning(dst_lanes=128)
+
+
+@pytest.mark.parametrize("ii,kernel", [(129, 0), (129, 1), (513, 0)])
+def test_programmatic_dependent_launch_matches_oracle(ii, kernel):
+    """With pdl on, each step kernel may be scheduled before its predecessor
+    ends and waits for it on the device: same results, graphs included."""
+    cfg = double_gyre(ii, 3)
+    g, o = start(cfg, seed=9)
+    g.set_tuning(pdl=1, cab_kernel=kernel)
+    for n in (1, 2, 3):
+        g.step(n)
+        o.step(n)
+    compare(g, o, TOL_STEP * 10)
