@@ -914,9 +914,9 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
 }
 
 // MINB: CTAs per SM the register allocation must allow.  Three (80
-// registers) for FP64 grids of many waves, where the extra resident CTA
-// hides more latency than the tighter allocation costs (measured -8 % at
-// 513 x 513 x 3); one for short grids.
+// registers): the FP32 form always, FP64 on grids of many waves, where the
+// extra resident CTA hides more latency than the tighter allocation costs
+// (measured -8 % at 513 x 513 x 3); one for short FP64 grids.
 template <bool PRED, typename T, int MINB>
 __global__ void __launch_bounds__(CT_THREADS, MINB) k_cabaret_tile(const Member* __restrict__ mems,
                                                               const int* __restrict__ prefix, int nmem) {
@@ -969,8 +969,9 @@ template <bool PRED, typename T>
 static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
     if (ls.cab_kernel == 0) {
         const size_t tb = TileSmem<T>::bytes();
-        const bool many_waves = sizeof(T) == 8 && ls.ctas_cab > 4 * ls.sm_count;
-        auto kern = many_waves ? k_cabaret_tile<PRED, T, 3> : k_cabaret_tile<PRED, T, 1>;
+        // FP32 fits three CTAs per SM at any size; FP64 only on many-wave grids.
+        auto kern = (sizeof(T) == 4 || ls.ctas_cab > 4 * ls.sm_count) ? k_cabaret_tile<PRED, T, 3>
+                                                                       : k_cabaret_tile<PRED, T, 1>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb);
         if (e != cudaSuccess) return e;
         return launch_step_kernel(ls.pdl, kern, dim3(ls.ctas_cab), dim3(CT_THREADS), tb, st, ls.members,
