@@ -244,7 +244,7 @@ class Model:
 
         P = _Params()
         P.ii, P.jj, P.layers = cfg["ii"], cfg["jj"], L
-        P.periodic_j = 0
+        P.periodic_j = int(cfg.get("periodic_j", 0))
         P.scheme = cfg.get("scheme", 0)
         P.limiter = cfg.get("limiter", 1)
         P.bc_type = cfg.get("bc_type", BC_PARTIAL_SLIP)
@@ -284,6 +284,8 @@ class Model:
             return (ii + 3, jj + 2, L)
         if name in ("uj", "ujmo", "zeta_fj", "flux_j"):
             return (ii + 2, jj + 3, L)
+        if name == "corr" and self.cfg.get("periodic_j", 0):
+            return (ii, jj, L, 2)
         if name in ("res", "res_beta", "corr"):
             return (ii, jj, L)
         return (ii + 2, jj + 2, L)

@@ -843,7 +843,8 @@ struct or_model {
     or_params p;
     std::vector<double> beta, h, s1, s2, ss, m2z, z2m, wind;
     HelmCache hc;
-    std::vector<double> corr;  // (ii, jj, L), correction_function_mass
+    std::vector<double> corr;  // (ii, jj, L, 1) correction_function_mass; (ii, jj, L, 2) channel
+    std::vector<double> inv_corr_a;  // channel: (2, 2, L - 1), correction_function_momentum
     std::vector<double> phi;   // working memory (ii, jj, L)
     // Prognostic fields, full data arrays (ii+2, jj+2, L); [1] is leapfrog level 2.
     std::vector<double> psi[2], rel[2], zeta[2], zeta_old[2];
@@ -910,6 +911,112 @@ void correction_function_mass(or_model& m) {
     }
 }
 
+// update_pdata (qg3p_base.F90:1887-1956) for one rank: only a channel
+// (periodic j) has a halo to fill, its own first / last sdata row: halo row
+// 1 <- row jj+1, halo row jj+2 <- row 2, columns 2..ii+1.
+void update_pdata(or_model& m, std::vector<double>& v) {
+    const Decomp& d = m.d;
+    if (!d.periodic_j) return;
+    V3 a = m.full(v);
+    for (int l = 1; l <= d.layers; ++l)
+        for (int i = 2; i <= d.ii + 1; ++i) {
+            a(i, 1, l) = a(i, d.jj + 1, l);
+            a(i, d.jj + 2, l) = a(i, 2, l);
+        }
+}
+
+// update_flux_j (qg3p_base.F90:2964-3003) for one rank of a channel: faces
+// fa_j_min <- fa_j_max - 1 and fa_j_max + 1 <- fa_j_min + 2, and with
+// level_1 also fa_j_max <- fa_j_min + 1, over columns fa_i_min+1 ..
+// fa_i_min+ii2.  update_flux_i has nothing to do on one rank.
+void update_flux_j(or_model& m, std::vector<double>& v, bool level_1) {
+    const Decomp& d = m.d;
+    if (!d.periodic_j) return;
+    V3 a = m.fj(v);
+    for (int l = 1; l <= d.layers; ++l)
+        for (int i = d.fa_i_min + 1; i <= d.fa_i_min + d.ii2; ++i) {
+            a(i, d.fa_j_min, l) = a(i, d.fa_j_max - 1, l);
+            a(i, d.fa_j_max + 1, l) = a(i, d.fa_j_min + 2, l);
+            if (level_1) a(i, d.fa_j_max, l) = a(i, d.fa_j_min + 1, l);
+        }
+}
+
+// zeta_boundary, qg3p_aux.F90:289-379: the mean relative PV of the modal
+// field psi (sdata (ii, jj, L)) along the two walls i = 1 (z_b) and i = ii
+// (z_d) of a channel: the wall relative vorticity of the velocity boundary
+// condition and the thickness term -ss psi.
+void zeta_boundary(const or_model& m, const double* psi_p, double* z_b, double* z_d) {
+    const Decomp& d = m.d;
+    const int L = d.layers, ii = d.ii;
+    V3 psi{const_cast<double*>(psi_p), d.ii, d.jj, L};
+    for (int l = 0; l < L; ++l) z_b[l] = z_d[l] = 0.0;
+    switch (m.p.bc_type) {
+        case OR_BC_PARTIAL_SLIP: {
+            const double cff = m.p.alpha / (m.p.alpha + 3.0);
+            if (d.p_b == -1)
+                for (int l = 1; l <= L; ++l)
+                    for (int j = d.l_j_min; j <= d.l_j_max; ++j)
+                        z_b[l - 1] = z_b[l - 1] + cff * (-3.5 * psi(1, j, l) + 4.0 * psi(2, j, l) - 0.5 * psi(3, j, l));
+            if (d.p_d == -1)
+                for (int l = 1; l <= L; ++l)
+                    for (int j = d.l_j_min; j <= d.l_j_max; ++j)
+                        z_d[l - 1] = z_d[l - 1] +
+                                     cff * (-3.5 * psi(ii, j, l) + 4.0 * psi(ii - 1, j, l) - 0.5 * psi(ii - 2, j, l));
+            break;
+        }
+        case OR_BC_NO_SLIP: {
+            if (d.p_b == -1)
+                for (int l = 1; l <= L; ++l)
+                    for (int j = d.l_j_min; j <= d.l_j_max; ++j)
+                        z_b[l - 1] = z_b[l - 1] + 2.0 * (psi(2, j, l) - psi(1, j, l));
+            if (d.p_d == -1)
+                for (int l = 1; l <= L; ++l)
+                    for (int j = d.l_j_min; j <= d.l_j_max; ++j)
+                        z_d[l - 1] = z_d[l - 1] + 2.0 * (psi(ii - 1, j, l) - psi(ii, j, l));
+            break;
+        }
+        default:  // free slip: no vorticity term
+            break;
+    }
+    if (d.p_b == -1)
+        for (int l = 1; l <= L; ++l)
+            for (int j = d.l_j_min; j <= d.l_j_max; ++j) z_b[l - 1] = z_b[l - 1] - m.ss[l - 1] * psi(1, j, l);
+    if (d.p_d == -1)
+        for (int l = 1; l <= L; ++l)
+            for (int j = d.l_j_min; j <= d.l_j_max; ++j) z_d[l - 1] = z_d[l - 1] - m.ss[l - 1] * psi(ii, j, l);
+    for (int l = 0; l < L; ++l) {
+        z_b[l] = z_b[l] / (double)d.g_jj_int;
+        z_d[l] = z_d[l] / (double)d.g_jj_int;
+    }
+}
+
+// correction_function_momentum, qg3p_aux.F90:233-285: the two channel
+// correction functions (homogeneous Helmholtz solutions with psi = 1 on one
+// wall and 0 on the other) and, per baroclinic mode, the inverse of the 2 x 2
+// matrix of their wall PV means.
+void correction_function_momentum(or_model& m) {
+    const Decomp& d = m.d;
+    const int L = d.layers;
+    const size_t n = m.nsd();
+    m.corr.assign(2 * n, 0.0);
+    for (int w = 0; w < 2; ++w) {
+        double* c = m.corr.data() + (size_t)w * n;
+        const double bb = w == 0 ? 1.0 : 0.0, bd = w == 0 ? 0.0 : 1.0;
+        for (int l = 0; l < L; ++l) add_laplace_bc_rhs_layer(d, bb, bd, c + (size_t)l * d.ii * d.jj);
+        helm(m.hc, c);
+        for (int l = 0; l < L; ++l) apply_dirichlet_bc_layer(d, bb, bd, c + (size_t)l * d.ii * d.jj);
+    }
+    std::vector<double> zb1(L), zd1(L), zb2(L), zd2(L);
+    zeta_boundary(m, m.corr.data(), zb1.data(), zd1.data());
+    zeta_boundary(m, m.corr.data() + n, zb2.data(), zd2.data());
+    m.inv_corr_a.assign((size_t)4 * (L > 1 ? L - 1 : 1), 0.0);
+    for (int mode = 2; mode <= L; ++mode) {
+        // z_b(mode, :, :): rows (z_b, z_d), columns (corr 1, corr 2), column-major
+        const double a[4] = {zb1[mode - 1], zd1[mode - 1], zb2[mode - 1], zd2[mode - 1]};
+        inverse(2, a, m.inv_corr_a.data() + (size_t)4 * (mode - 2));
+    }
+}
+
 // pv_inversion + modes_to_z_correct_mass + modes_to_z_btcu,
 // qg3p_aux.F90:452-521 and qg3p_diagnostics.F90:615-635.  zeta/psi are full
 // data arrays; only their sdata parts are read / written.
@@ -926,6 +1033,32 @@ int pv_inversion(or_model& m, std::vector<double>& zeta, std::vector<double>& ps
     z_to_modes(m, zs.data(), m.phi.data());
     if (helm(m.hc, m.phi.data()) != 0) return -3;
     apply_dirichlet_bc(d, 0.0, m.phi.data());
+    if (d.periodic_j) {
+        // modes_to_z_correct_momentum, qg3p_aux.F90:524-575, then modes_to_z
+        // (qg3p_diagnostics.F90:570-612).
+        std::vector<double> cb(L), cd(L);
+        zeta_boundary(m, m.phi.data(), cb.data(), cd.data());
+        V3 ph = m.sdv(m.phi);
+        const size_t n = m.nsd();
+        V3 c1{m.corr.data(), ii, jj, L}, c2{m.corr.data() + n, ii, jj, L};
+        for (int layer = 2; layer <= L; ++layer) {
+            const double* A = m.inv_corr_a.data() + (size_t)4 * (layer - 2);
+            const double p1 = A[0] * cb[layer - 1] + A[2] * cd[layer - 1];
+            const double p2 = A[1] * cb[layer - 1] + A[3] * cd[layer - 1];
+            if (p1 != p1 || p2 != p2) return -2;  // labort("NaN psiC encountered")
+            for (int j = 1; j <= jj; ++j)
+                for (int i = 1; i <= ii; ++i)
+                    ph(i, j, layer) = ph(i, j, layer) - p1 * c1(i, j, layer) - p2 * c2(i, j, layer);
+        }
+        for (int j = 1; j <= jj; ++j)
+            for (int i = 1; i <= ii; ++i)
+                for (int layer = 1; layer <= L; ++layer) {
+                    double s = 0.0;
+                    for (int mm = 1; mm <= L; ++mm) s += m.m2z[(layer - 1) + L * (mm - 1)] * ph(i, j, mm);
+                    pf(i + 1, j + 1, layer) = s;
+                }
+        return 0;
+    }
     std::vector<double> psiC(L);
     for (int l = 1; l <= L; ++l) psiC[l - 1] = mean_layer(d, m.phi.data() + (size_t)(l - 1) * ii * jj);
     for (int l = 0; l < L; ++l)
@@ -1449,6 +1582,7 @@ void raw_filter(or_model& m, int lf) {
 int invert_level(or_model& m, int lv) {
     int rc = pv_inversion(m, m.zeta[lv], m.psi[lv]);
     if (rc) return rc;
+    update_pdata(m, m.psi[lv]);  // qg3.F90:642-643
     rel_from_zeta_and_psi(m, m.zeta[lv], m.psi[lv], m.rel[lv]);
     update_zeta_bc(m, m.rel[lv], m.psi[lv], m.zeta[lv]);
     return 0;
@@ -1582,11 +1716,12 @@ void or_energy(int ii, int jj, int layers, int periodic_j, const double* h, cons
 }
 
 or_model* or_model_create(const or_params* p) {
-    if (!p || p->ii < 5 || p->jj < 5 || p->layers < 1 || p->periodic_j) return nullptr;
+    if (!p || p->ii < 5 || p->jj < 5 || p->layers < 1) return nullptr;
+    if (p->periodic_j && p->scheme != 0) return nullptr;  // the leapfrog channel is not restated
     or_model* m = new or_model;
     m->p = *p;
     int L = p->layers;
-    m->d = make_decomp(p->ii, p->jj, L, false);
+    m->d = make_decomp(p->ii, p->jj, L, p->periodic_j != 0);
     m->beta.assign(p->beta, p->beta + L);
     m->h.assign(p->h, p->h + L);
     m->s1.assign(p->s1, p->s1 + L);
@@ -1598,7 +1733,10 @@ or_model* or_model_create(const or_params* p) {
     m->p.beta = m->p.h = m->p.s1 = m->p.s2 = m->p.ss = m->p.m2z = m->p.z2m = m->p.force_wind = nullptr;
     m->dt = p->dt;
     helm_init(m->hc, m->d, m->ss.data());
-    correction_function_mass(*m);
+    if (m->d.periodic_j)
+        correction_function_momentum(*m);
+    else
+        correction_function_mass(*m);
     for (int lv = 0; lv < 2; ++lv) {
         m->psi[lv].assign(m->nfull(), 0.0);
         m->rel[lv].assign(m->nfull(), 0.0);
@@ -1637,17 +1775,20 @@ int or_model_init(or_model* m, const double* zeta_ic) {
             for (int j = 1; j <= d.jj; ++j)
                 for (int i = 1; i <= d.ii; ++i)
                     z(i + 1, j + 1, l) = src[(size_t)(i - 1) + (size_t)d.ii * ((j - 1) + (size_t)d.jj * (l - 1))];
-        // apply_dirichlet_bc(0, zeta) on sdata.
+        // apply_dirichlet_bc(0, zeta) on sdata (the walls only in a channel),
+        // then update(zeta) (qg3.F90:383-385).
         for (int l = 1; l <= d.layers; ++l) {
-            for (int i = 1; i <= d.ii; ++i) {
-                z(i + 1, 2, l) = 0.0;
-                z(i + 1, d.jj + 1, l) = 0.0;
-            }
+            if (!d.periodic_j)
+                for (int i = 1; i <= d.ii; ++i) {
+                    z(i + 1, 2, l) = 0.0;
+                    z(i + 1, d.jj + 1, l) = 0.0;
+                }
             for (int j = 1; j <= d.jj; ++j) {
                 z(2, j + 1, l) = 0.0;
                 z(d.ii + 1, j + 1, l) = 0.0;
             }
         }
+        update_pdata(*m, m->zeta[lv]);
         int rc = invert_level(*m, lv);
         if (rc) return rc;
     }
@@ -1709,13 +1850,17 @@ int or_model_step_to_dump(or_model* m) {
     if (m->p.adapt_dt) cabaret_adapt_dt(*m);
     cabaret_predictor(*m);
     cabaret_beta(*m);
+    update_pdata(*m, m->zeta[0]);  // qg3.F90:610
     int rc = invert_level(*m, 0);
     if (rc) return rc;
     m->model_time += 0.5 * m->dt;
     accumulate_average(*m, 0);
     cabaret_forcing(*m);
+    update_pdata(*m, m->zeta[0]);  // :786
     cabaret_cell_boundaries(*m);
+    update_flux_j(*m, m->uj, true);  // :795-796 (update(ui) has no halo on one rank)
     cabaret_extrapolator(*m);
+    update_flux_j(*m, m->zeta_fj, true);  // :802-803
     cabaret_flux(*m);
     return 0;
 }
@@ -1725,6 +1870,7 @@ int or_model_step_to_dump(or_model* m) {
 int or_model_finish_step(or_model* m) {
     if (m->p.scheme != 0) return -1;
     cabaret_corrector(*m);
+    update_pdata(*m, m->zeta[0]);  // qg3.F90:945
     m->zeta_old[0] = m->zeta[0];
     m->model_time += 0.5 * m->dt;
     return 0;

@@ -249,7 +249,7 @@ class Config:
             s2=list(d.s2[:L]), ss=ss, m2z=m2z, z2m=z2m, viscosity=d.viscosity, visc_bot=d.visc_bot,
             bc_type=d.bc_type, alpha=d.alpha, force_wind=self.wind, scheme=d.scheme, limiter=d.limiter,
             adapt_dt=d.adapt_dt, target_cfl=d.target_cfl, max_dt=d.max_dt, max_dt_increase=d.max_dt_increase,
-            ra_nu=d.ra_nu, ra_alpha=d.ra_alpha,
+            ra_nu=d.ra_nu, ra_alpha=d.ra_alpha, periodic_j=d.periodic_j,
         )
 
 
