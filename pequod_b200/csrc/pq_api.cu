@@ -169,9 +169,24 @@ int run_step(pq_ctx* c, int par) {
         c->zpar = par;
         return PQ_OK;
     }
+    const int f32 = c->mixed ? 1 : 0;
+    if (c->periodic) {
+        // Channel: predictor + beta in the forward DST, the momentum-corrected
+        // inversion, then the four channel CABARET kernels.
+        CK(launch_dst_forward(c->ls[par], PRO_STEP, f32, c->stream));
+        if (ev) CK(cudaEventRecord(ev[1], c->stream));
+        CK(launch_tridiag(c->ls[par], 1, f32, c->stream));
+        if (ev) CK(cudaEventRecord(ev[2], c->stream));
+        CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
+        if (ev) CK(cudaEventRecord(ev[3], c->stream));
+        CK(launch_cabaret_channel(c->ls[par], f32, c->stream));
+        if (ev) CK(cudaEventRecord(ev[4], c->stream));
+        c->pred_ready = false;
+        c->zpar = par;
+        return PQ_OK;
+    }
     // The predictor + beta update runs in the forward DST unless the previous
     // fused step already produced this step's inversion input.
-    const int f32 = c->mixed ? 1 : 0;
     CK(launch_dst_forward(c->ls[par], (c->fuse && c->pred_ready) ? PRO_MODAL : PRO_STEP, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[1], c->stream));
     CK(launch_tridiag(c->ls[par], 1, f32, c->stream));
@@ -221,9 +236,9 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     *out = nullptr;
     const int ii = d->ii, jj = d->jj, L = d->layers;
     if (ii < 5 || jj < 5 || !is_pow2(ii - 1) || L < 1 || L > PQ_MAX_LAYERS) return PQ_ERR_ARG;
-    // A channel periodic in j is supported by the Helmholtz solver (pq_helm);
-    // the time step of a channel (its momentum correction) is not built.
     if (d->precision != PQ_PREC_FP64 && d->precision != PQ_PREC_MIXED) return PQ_ERR_UNSUPPORTED;
+    // A channel (periodic in j) steps with CABARET; its leapfrog is not built.
+    if (d->periodic_j && d->scheme == PQ_SCHEME_LEAPFROG && !helm_only) return PQ_ERR_UNSUPPORTED;
     if (d->scheme != PQ_SCHEME_CABARET && d->scheme != PQ_SCHEME_LEAPFROG) return PQ_ERR_UNSUPPORTED;
     // The leapfrog scheme runs in FP64 with a fixed dt (the reference's
     // adaptive step is a CABARET routine).
@@ -266,8 +281,11 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     // CABARET formulation by grid size (measured on B200): tiles up to
     // 700 rows, warp sweeps above (pq_tuning.cab_kernel overrides).
     const int cab_kernel = jj <= 700 ? 0 : 1;
-    const int ntiles_cab = cab_kernel == 0 ? cabaret_tile_ctas(ii, jj, L) : cabaret_ctas(ii, jj, L, cab_sh);
-    const int ntiles_cab_max = std::max(cabaret_ctas(ii, jj, L, kMinBand), cabaret_tile_ctas(ii, jj, L));
+    const int ntiles_cab = d->periodic_j ? channel_ctas(ii, jj)
+                           : cab_kernel == 0 ? cabaret_tile_ctas(ii, jj, L)
+                                             : cabaret_ctas(ii, jj, L, cab_sh);
+    const int ntiles_cab_max =
+        std::max({cabaret_ctas(ii, jj, L, kMinBand), cabaret_tile_ctas(ii, jj, L), channel_ctas(ii, jj)});
 
     // Tables.
     std::vector<double2> tw(M), wsplit(M);
@@ -291,7 +309,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
                                   : 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 2 /*res*/ + 2 /*res_beta*/ +
                                         1 /*ui*/ + 1 /*uj*/ + 2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ +
                                         1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ + 1 /*corr*/ + 1 /*spec64*/ +
-                                        2 /*leapfrog psi(2), rel(2)*/;
+                                        2 /*leapfrog psi(2), rel(2)*/ + (d->periodic_j ? 1 /*corr2*/ : 0);
     const size_t fb = align256(c->field_bytes);
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -367,7 +385,26 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     }
     const size_t o_pb = take(pbv.size() * sizeof(double));
     const size_t o_pc = take(pcv.size() * sizeof(double));
-    const size_t npart = std::max((size_t)ntiles_tri, (size_t)jj * (PQ_MAXL + 1));
+    // Channel wall weights (zeta_boundary of a solved mode in spectral space,
+    // qg3p_aux.F90:289-379): sum_j phi(i, j) = 2 sum_k sin(i k pi / N) C_k
+    // for node i, and phi is 0 on the walls, so the mean PV of wall i = 0 is
+    // sum_k wwall[k] C_k (the other wall takes (-1)^(k+1) wwall[k]).
+    std::vector<double> wwall(n, 0.0);
+    if (d->periodic_j) {
+        const long double pi = 3.141592653589793238462643383279502884L;
+        for (int k = 1; k <= n; ++k) {
+            const long double s1 = sinl(pi * k / N), s2 = sinl(2.0L * pi * k / N);
+            long double w = 0.0L;
+            if (d->bc_type == PQ_BC_PARTIAL_SLIP)
+                w = ((long double)d->alpha / ((long double)d->alpha + 3.0L)) * 2.0L * (4.0L * s1 - 0.5L * s2);
+            else if (d->bc_type == PQ_BC_NO_SLIP)
+                w = 2.0L * 2.0L * s1;
+            wwall[k - 1] = (double)(w / (long double)jj);
+        }
+    }
+    const size_t o_ww = take(wwall.size() * sizeof(double));
+    const size_t o_ica = take((size_t)4 * PQ_MAXL * sizeof(double));
+    const size_t npart = std::max((size_t)2 * ntiles_tri, (size_t)jj * (PQ_MAXL + 1));
     const size_t o_part = take(npart * sizeof(double));
     const size_t o_maxu = take(ntiles_cab_max * sizeof(double));
     const size_t o_cnt = take(4 * sizeof(unsigned));
@@ -385,6 +422,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     CK(cudaMemcpyAsync(A + o_wsf, wsplit_f.data(), M * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_wasf, was_f.data(), was_f.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_wm, wmean.data(), wmean.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A + o_ww, wwall.data(), wwall.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_poff, pv.off.data(), pv.off.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_plen, pv.len.data(), pv.len.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(A + o_piv, pv.piv.data(), pv.piv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -425,7 +463,10 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         m.h[a] = d->h[a];
         m.htot += d->h[a];
     }
-    m.mean_scale = 1.0 / ((double)(ii - 1) * (double)(jj - 1));
+    // 1 / (g_ii_int g_jj_int); a channel has jj distinct rows.
+    m.mean_scale = 1.0 / ((double)(ii - 1) * (double)(d->periodic_j ? jj : jj - 1));
+    m.wwall = reinterpret_cast<const double*>(A + o_ww);
+    m.inv_corr_a = reinterpret_cast<const double*>(A + o_ica);
     m.tw = reinterpret_cast<const double2*>(A + o_tw);
     m.wsplit = reinterpret_cast<const double2*>(A + o_ws);
     m.was = reinterpret_cast<const double*>(A + o_was);
@@ -478,6 +519,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         m.spec64 = (double*)fld();
         psi2 = (double*)fld();
         rel2 = fld();
+        if (d->periodic_j) m.corr2 = (const double*)fld();
     }
     m.wind = c->wind.empty() ? nullptr : reinterpret_cast<const double*>(A + o_wind);
     m.partials = reinterpret_cast<double*>(A + o_part);
@@ -508,7 +550,9 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     // res[p] (the previous step's) and writes res[p ^ 1].
     c->hm[0].res = c->hm[1].res_out = m.res;
     c->hm[1].res = c->hm[0].res_out = rs1;
-    c->fuse = !d->adapt_dt;
+    // The fused next-step predictor needs a fixed dt and the closed basin's
+    // fused CABARET kernels; the channel steps through its own kernels.
+    c->fuse = !d->adapt_dt && !d->periodic_j;
     c->leapfrog = d->scheme == PQ_SCHEME_LEAPFROG;
     if (c->leapfrog) {
         // Level descriptors: hm[p] advances level p with the other level q.
@@ -598,6 +642,86 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
         rc = copy_in(c, (void*)m.corr, h.data(), PQ_PTR_HOST);
         if (rc) return rc;
     }
+    if (!helm_only && c->periodic) {
+        // correction_function_momentum (qg3p_aux.F90:233-285): Helmholtz
+        // solutions with zero right-hand side and psi = 1 on wall i = 0 and 0
+        // on wall i = ii - 1 (corr), and the other way round (corr2), through
+        // the laplace_bc lifting (qg3p_laplace_bc.F90:128-150, 227-251); then
+        // per baroclinic mode the inverse of the 2 x 2 matrix of their wall PV
+        // means (zeta_boundary, :289-379).
+        const size_t nn = (size_t)ii * jj;
+        std::vector<double> cf[2];
+        double zb[2][2][PQ_MAXL];  // [function][wall][mode]
+        for (int w = 0; w < 2; ++w) {
+            const double bb = w == 0 ? 1.0 : 0.0, bd = w == 0 ? 0.0 : 1.0;
+            std::vector<double> h(nn * L, 0.0);
+            for (int l = 0; l < L; ++l)
+                for (int j = 0; j < jj; ++j) {
+                    h[(size_t)l * nn + (size_t)ii * j + 1] -= bb;
+                    h[(size_t)l * nn + (size_t)ii * j + ii - 2] -= bd;
+                }
+            rc = copy_in(c, m.helm_io, h.data(), PQ_PTR_HOST);
+            if (rc) return rc;
+            rc = run_helm(c, 0, PRO_PLAIN, EPI_HELM, 0);
+            if (rc) return rc;
+            rc = copy_out(c, h.data(), m.helm_io, PQ_PTR_HOST);
+            if (rc) return rc;
+            CK(cudaStreamSynchronize(c->stream));
+            for (int l = 0; l < L; ++l)
+                for (int j = 0; j < jj; ++j) {
+                    h[(size_t)l * nn + (size_t)ii * j] = bb;
+                    h[(size_t)l * nn + (size_t)ii * j + ii - 1] = bd;
+                }
+            for (int l = 0; l < L; ++l) {
+                const double* p = h.data() + (size_t)l * nn;
+                double sb = 0.0, sd = 0.0;
+                if (d->bc_type == PQ_BC_PARTIAL_SLIP) {
+                    const double cff = d->alpha / (d->alpha + 3.0);
+                    for (int j = 0; j < jj; ++j) {
+                        const double* r = p + (size_t)ii * j;
+                        sb = sb + cff * (-3.5 * r[0] + 4.0 * r[1] - 0.5 * r[2]);
+                    }
+                    for (int j = 0; j < jj; ++j) {
+                        const double* r = p + (size_t)ii * j;
+                        sd = sd + cff * (-3.5 * r[ii - 1] + 4.0 * r[ii - 2] - 0.5 * r[ii - 3]);
+                    }
+                } else if (d->bc_type == PQ_BC_NO_SLIP) {
+                    for (int j = 0; j < jj; ++j) sb = sb + 2.0 * (p[(size_t)ii * j + 1] - p[(size_t)ii * j]);
+                    for (int j = 0; j < jj; ++j)
+                        sd = sd + 2.0 * (p[(size_t)ii * j + ii - 2] - p[(size_t)ii * j + ii - 1]);
+                }
+                for (int j = 0; j < jj; ++j) sb = sb - d->ss[l] * p[(size_t)ii * j];
+                for (int j = 0; j < jj; ++j) sd = sd - d->ss[l] * p[(size_t)ii * j + ii - 1];
+                zb[w][0][l] = sb / (double)jj;
+                zb[w][1][l] = sd / (double)jj;
+            }
+            cf[w] = std::move(h);
+        }
+        rc = copy_in(c, (void*)m.corr, cf[0].data(), PQ_PTR_HOST);
+        if (rc) return rc;
+        rc = copy_in(c, (void*)m.corr2, cf[1].data(), PQ_PTR_HOST);
+        if (rc) return rc;
+        // inverse(z_b(mode, :, :)): rows = walls, columns = functions;
+        // column-major [a11, a21, a12, a22].
+        std::vector<double> ica((size_t)4 * PQ_MAXL, 0.0);
+        for (int l = 1; l < L; ++l) {
+            const double a11 = zb[0][0][l], a21 = zb[0][1][l], a12 = zb[1][0][l], a22 = zb[1][1][l];
+            const double det = a11 * a22 - a12 * a21;
+            if (!(std::fabs(det) > 0.0) || det != det) {
+                // No momentum correction exists (e.g. a baroclinic mode with
+                // ss = 0 and free slip): the context still solves Helmholtz
+                // problems, but refuses the time step.
+                c->channel_singular = true;
+                continue;
+            }
+            ica[4 * l + 0] = a22 / det;
+            ica[4 * l + 1] = -a21 / det;
+            ica[4 * l + 2] = -a12 / det;
+            ica[4 * l + 3] = a11 / det;
+        }
+        CK(cudaMemcpyAsync((void*)m.inv_corr_a, ica.data(), ica.size() * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
+    }
     CK(cudaStreamSynchronize(c->stream));
     return PQ_OK;
 }
@@ -620,7 +744,7 @@ int pq_helm(pq_ctx* c, double* zeta, int ptr_kind) {
 
 int pq_pv_inversion(pq_ctx* c, const double* zeta, double* psi, int ptr_kind) {
     if (!c || !zeta || !psi) return PQ_ERR_ARG;
-    if (c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "the channel (periodic j) time step is not built; pq_helm only");
+    if (c->channel_singular) return fail(c, PQ_ERR_UNSUPPORTED, "singular channel correction matrix");
     CK(cudaSetDevice(c->device));
     int rc = copy_in_state(c, c->hm[c->cur].zeta, zeta, ptr_kind);
     if (rc) return rc;
@@ -636,7 +760,7 @@ int pq_pv_inversion(pq_ctx* c, const double* zeta, double* psi, int ptr_kind) {
 
 int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     if (!c || !zeta_ic) return PQ_ERR_ARG;
-    if (c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "the channel (periodic j) time step is not built; pq_helm only");
+    if (c->channel_singular) return fail(c, PQ_ERR_UNSUPPORTED, "singular channel correction matrix");
     CK(cudaSetDevice(c->device));
     const int ii = c->ii, jj = c->jj, L = c->L;
     const int nlev = c->leapfrog ? 2 : 1;  // init_rand fills both leapfrog levels
@@ -645,10 +769,12 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
         CK(cudaMemcpy(z.data(), zeta_ic, z.size() * sizeof(double), cudaMemcpyDeviceToHost));
     else
         std::memcpy(z.data(), zeta_ic, z.size() * sizeof(double));
-    // apply_dirichlet_bc(0, zeta), qg3.F90:383.
+    // apply_dirichlet_bc(0, zeta), qg3.F90:383 (a channel has walls at
+    // i = 0 and ii - 1 only, qg3p_laplace_bc.F90:227-251).
     for (int l = 0; l < L * nlev; ++l) {
         double* p = z.data() + (size_t)ii * jj * l;
-        for (int i = 0; i < ii; ++i) p[i] = p[i + (size_t)ii * (jj - 1)] = 0.0;
+        if (!c->periodic)
+            for (int i = 0; i < ii; ++i) p[i] = p[i + (size_t)ii * (jj - 1)] = 0.0;
         for (int j = 0; j < jj; ++j) p[(size_t)ii * j] = p[(size_t)ii * j + ii - 1] = 0.0;
     }
     const Member& m = c->hm[0];
@@ -826,8 +952,9 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     }
     for (int p = 0; p < 2; ++p) {
         c->hm[p].cab_sh = t->cab_band;
-        c->hm[p].ntiles_cab = t->cab_kernel ? cabaret_ctas(c->ii, c->jj, c->L, t->cab_band)
-                                            : cabaret_tile_ctas(c->ii, c->jj, c->L);
+        c->hm[p].ntiles_cab = c->periodic   ? channel_ctas(c->ii, c->jj)
+                              : t->cab_kernel ? cabaret_ctas(c->ii, c->jj, c->L, t->cab_band)
+                                              : cabaret_tile_ctas(c->ii, c->jj, c->L);
         c->ls[p].cab_kernel = t->cab_kernel;
         c->ls[p].ctas_cab = c->hm[p].ntiles_cab;
         c->ls[p].dst_group = t->dst_group;
@@ -941,7 +1068,7 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc) {
     return PQ_OK;
 }
 
-int step_launches(const pq_ctx* c) { return c->leapfrog ? (c->psi_av ? 6 : 5) : 4; }
+int step_launches(const pq_ctx* c) { return c->leapfrog ? (c->psi_av ? 6 : 5) : c->periodic ? 7 : 4; }
 
 int read_scalars(pq_ctx* c, Scalars* sc) {
     CK(cudaSetDevice(c->device));
@@ -1045,7 +1172,10 @@ int pq_get_field(pq_ctx* c, int field, double* out) {
     RefShape s;
     if (!ref_shape(field, c->ii, c->jj, &s)) return fail(c, PQ_ERR_ARG, "unknown field");
     CK(cudaSetDevice(c->device));
-    if (field == PQ_F_REL && !c->leapfrog) CK(launch_rel(c->ls[c->zpar], c->mixed ? 1 : 0, c->stream));
+    // The closed-basin step keeps rel in registers: rebuild it.  The channel
+    // and leapfrog steps store it.
+    if (field == PQ_F_REL && !c->leapfrog && !c->periodic)
+        CK(launch_rel(c->ls[c->zpar], c->mixed ? 1 : 0, c->stream));
     if (!field_ptr(c, field)) return fail(c, PQ_ERR_ARG, "field not held by this scheme");
     std::vector<double> dense((size_t)c->ii * c->jj * c->L);
     int rc = (field == PQ_F_PSI || field == PQ_F_PSI2 || field == PQ_F_CORR)

@@ -41,7 +41,8 @@ extern "C" {
 
 int pq_average(pq_ctx* c, int enable, double threshold) {
     if (!c) return PQ_ERR_ARG;
-    if (c->helm_only || c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "no time loop on this context");
+    if (c->helm_only) return fail(c, PQ_ERR_UNSUPPORTED, "no time loop on this context");
+    if (c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "the channel step does not accumulate the time average");
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     if (enable && !c->psi_av) {

@@ -987,6 +987,275 @@ static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+
+// ---------------------------------------------------------------------------
+// The channel (periodic in j) CABARET step: the same sub-steps as the fused
+// closed-basin kernels (qg3.F90:640-807, 940-956), as four node-parallel
+// kernels.  Every row is interior in j; rows, j-faces and corners wrap
+// modulo jj (the reference's halo rows and seam faces, qg3p_base.F90:
+// 1887-1956, 2964-3003, hold exactly the wrapped values); the walls are the
+// columns i = 0 and ii - 1.  One thread per (column, row) with all layers;
+// face a (i-faces) and face b (j-faces) belong to node (a, b).  Arithmetic
+// in FP64, fields stored as T.
+namespace {
+
+struct ChannelIdx {
+    int ii, jj, pitch;
+    long long ls;
+    __device__ __forceinline__ long long at(int i, int j, int l) const {
+        j = j < 0 ? j + jj : (j >= jj ? j - jj : j);
+        return (long long)j * pitch + i + l * ls;
+    }
+};
+
+// rel_from_zeta_and_psi + apply_rel_bc, then update_zeta_bc on the walls.
+// rel is also kept in FP64 (in helm_io, free during a step) for the forcing's
+// Laplacian, whose differences would lose the mixed form's FP32 digits.
+template <typename T>
+__global__ void k_ch_rel(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.y, &local);
+    const Member& Mb = mems[mi];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = local;
+    if (i >= Mb.ii) return;
+    const long long o = (long long)j * Mb.pitch + i;
+    T* z = reinterpret_cast<T*>(Mb.zeta);
+    T* rel = reinterpret_cast<T*>(Mb.rel);
+    double* rel64 = reinterpret_cast<double*>(Mb.helm_io);
+    auto ps = [&](int a, int b, int l) { return Mb.psi[(long long)b * Mb.pitch + a + l * Mb.lstride]; };
+    const bool wall = (i == 0 || i == Mb.ii - 1);
+    for (int l = 0; l < Mb.L; ++l) {
+        const long long ol = o + l * Mb.lstride;
+        const double r = rel_node(Mb, ps, (double)z[ol], i, j, l);
+        rel[ol] = (T)r;
+        rel64[ol] = r;
+        if (wall) z[ol] = (T)zeta_bc_node(Mb, ps, r, i, j, l);
+    }
+}
+
+// cabaret_forcing (qg3p_aux.F90:1065-1164) on the interior columns, and the
+// time-integrated cell-boundary velocities (cabaret_cell_boundaries_
+// time_integrated, :1235-1313) of the faces a = i (i-faces) and b = j
+// (j-faces) of this node.
+template <typename T>
+__global__ void k_ch_force_cell(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.y, &local);
+    const Member& Mb = mems[mi];
+    const int ii = Mb.ii, L = Mb.L, i = blockIdx.x * blockDim.x + threadIdx.x, j = local;
+    if (i >= ii) return;
+    const ChannelIdx X{ii, Mb.jj, Mb.pitch, Mb.lstride};
+    const int cur = Mb.cur, nxt = cur ^ 1;
+    const double dt = Mb.sc->dt, tu = Mb.sc->tweight_u;
+    T* z = reinterpret_cast<T*>(Mb.zeta);
+    const double* rel = reinterpret_cast<const double*>(Mb.helm_io);  // FP64 rel of k_ch_rel
+    const double* psi = Mb.psi;
+    const double nu = Mb.viscosity, vb = Mb.visc_bot;
+    if (i >= 1 && i <= ii - 2) {
+        for (int l = 0; l < L; ++l) {
+            auto rp = [&](int a, int b) { return rel[X.at(a, b, l)]; };
+            const double lap = -4.0 * rp(i, j) + rp(i - 1, j) + rp(i + 1, j) + rp(i, j - 1) + rp(i, j + 1);
+            const double wnd = (l == 0 && Mb.wind) ? Mb.wind[X.at(i, j, 0)] : 0.0;
+            double rv;
+            if (L == 1)
+                rv = dt * (wnd - vb * rp(i, j) + nu * lap);
+            else if (l == 0)
+                rv = dt * (wnd + nu * lap);
+            else if (l < L - 1)
+                rv = dt * nu * lap;
+            else
+                rv = dt * (-vb * rp(i, j) + nu * lap);
+            const long long o = X.at(i, j, l);
+            z[o] = (T)((double)z[o] + rv);
+        }
+    }
+    // psi_edge(a, b): the corner between nodes a-1, a and rows b-1, b.
+    auto pe = [&](int a, int b, int l) {
+        return 0.25 * (psi[X.at(a, b, l)] + psi[X.at(a, b - 1, l)] + psi[X.at(a - 1, b, l)] + psi[X.at(a - 1, b - 1, l)]);
+    };
+    T* ui = reinterpret_cast<T*>(Mb.ui);
+    T* uj = reinterpret_cast<T*>(Mb.uj);
+    const T* uimo = reinterpret_cast<const T*>(Mb.uimo[cur]);
+    const T* ujmo = reinterpret_cast<const T*>(Mb.ujmo[cur]);
+    T* uimn = reinterpret_cast<T*>(Mb.uimo[nxt]);
+    T* ujmn = reinterpret_cast<T*>(Mb.ujmo[nxt]);
+    for (int l = 0; l < L; ++l) {
+        const long long o = X.at(i, j, l);
+        if (i >= 1) {  // i-face a = i, row j
+            const double uim = -pe(i, j + 1, l) + pe(i, j, l);
+            ui[o] = (T)((1.0 + tu) * uim - tu * (double)uimo[o]);
+            uimn[o] = (T)uim;
+        }
+        if (i >= 1 && i <= ii - 2) {  // j-face b = j of column i
+            const double ujm = pe(i + 1, j, l) - pe(i, j, l);
+            uj[o] = (T)((1.0 + tu) * ujm - tu * (double)ujmo[o]);
+            ujmn[o] = (T)ujm;
+        }
+    }
+}
+
+// cabaret_extrapolator (qg3p_aux.F90:1317-1544) for the faces of this node;
+// the j-faces of a channel always take the interior branch.
+template <typename T>
+__global__ void k_ch_extrap(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.y, &local);
+    const Member& Mb = mems[mi];
+    const int ii = Mb.ii, L = Mb.L, i = blockIdx.x * blockDim.x + threadIdx.x, j = local;
+    if (i < 1 || i >= ii) return;
+    const ChannelIdx X{ii, Mb.jj, Mb.pitch, Mb.lstride};
+    const int cur = Mb.cur, nxt = cur ^ 1;
+    const double dt = Mb.sc->dt;
+    const bool lim = Mb.limiter != 0;
+    const T* z = reinterpret_cast<const T*>(Mb.zeta);
+    const T* zo = reinterpret_cast<const T*>(Mb.zeta_old[cur]);
+    const T* ui = reinterpret_cast<const T*>(Mb.ui);
+    const T* uj = reinterpret_cast<const T*>(Mb.uj);
+    const T* fio = reinterpret_cast<const T*>(Mb.zfi[cur]);
+    const T* fjo = reinterpret_cast<const T*>(Mb.zfj[cur]);
+    T* fin = reinterpret_cast<T*>(Mb.zfi[nxt]);
+    T* fjn = reinterpret_cast<T*>(Mb.zfj[nxt]);
+    auto limit = [&](double v, double fi1, double fi2, double psi_n, double d_f) {
+        if (lim) {
+            const double fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
+            const double fmn = fmin(fmin(fi1, fi2), psi_n) - d_f;
+            if (v > fmx) v = fmx;
+            if (v < fmn) v = fmn;
+        }
+        return v;
+    };
+    for (int l = 0; l < L; ++l) {
+        const long long o = X.at(i, j, l);
+        {  // i-face a = i between nodes i-1 and i
+            const double u1 = ui[o], fi1 = fio[o];
+            double fi2, psi_n, psi_o, d_f;
+            if (u1 >= 0.0) {
+                psi_n = z[o - 1];
+                psi_o = zo[o - 1];
+                if (i > 1) {
+                    const double u2 = ui[o - 1];
+                    fi2 = fio[o - 1];
+                    const double v0 = (u1 + u2) / 2.0;
+                    d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi1 - fi2);
+                } else {
+                    fi2 = psi_n;
+                    d_f = -(psi_n - psi_o);
+                }
+            } else {
+                psi_n = z[o];
+                psi_o = zo[o];
+                if (i < ii - 1) {
+                    const double u2 = ui[o + 1];
+                    fi2 = fio[o + 1];
+                    const double v0 = (u1 + u2) / 2.0;
+                    d_f = -(psi_n - psi_o) * 2.0 - dt * v0 * (fi2 - fi1);
+                } else {
+                    fi2 = psi_n;
+                    d_f = -(psi_n - psi_o);
+                }
+            }
+            fin[o] = (T)limit(2.0 * psi_n - fi2, fi1, fi2, psi_n, d_f);
+        }
+        if (i <= ii - 2) {  // j-face b = j between rows j-1 and j of column i
+            const double u1 = uj[o], fi1 = fjo[o];
+            double u2, fi2, psi_n, psi_o, d_f;
+            if (u1 >= 0.0) {
+                const long long om = X.at(i, j - 1, l);
+                u2 = uj[om];
+                fi2 = fjo[om];
+                psi_n = z[om];
+                psi_o = zo[om];
+                d_f = -(psi_n - psi_o) * 2.0 - dt * ((u1 + u2) / 2.0) * (fi1 - fi2);
+            } else {
+                const long long op = X.at(i, j + 1, l);
+                u2 = uj[op];
+                fi2 = fjo[op];
+                psi_n = z[o];
+                psi_o = zo[o];
+                d_f = -(psi_n - psi_o) * 2.0 - dt * ((u1 + u2) / 2.0) * (fi2 - fi1);
+            }
+            fjn[o] = (T)limit(2.0 * psi_n - fi2, fi1, fi2, psi_n, d_f);
+        }
+    }
+}
+
+// cabaret_flux + cabaret_corrector (qg3p_aux.F90:1547-1642), zeta_old =
+// zeta; the largest |u| of this node's faces, and the last CTA's
+// cabaret_cfl / cabaret_adapt_dt / model time (finish_step).
+template <typename T>
+__global__ void __launch_bounds__(128) k_ch_corrector(const Member* __restrict__ mems, const int* __restrict__ prefix,
+                                                       int nmem) {
+    __shared__ double red[4];
+    __shared__ int is_last;
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.y, &local);
+    const Member& Mb = mems[mi];
+    const int ii = Mb.ii, L = Mb.L, i = blockIdx.x * blockDim.x + threadIdx.x, j = local;
+    const ChannelIdx X{ii, Mb.jj, Mb.pitch, Mb.lstride};
+    const int nxt = Mb.cur ^ 1;
+    double umax = 0.0;
+    if (i < ii) {
+        const double hdt = 0.5 * Mb.sc->dt;
+        const T* z = reinterpret_cast<const T*>(Mb.zeta);
+        const T* ui = reinterpret_cast<const T*>(Mb.ui);
+        const T* uj = reinterpret_cast<const T*>(Mb.uj);
+        const T* fin = reinterpret_cast<const T*>(Mb.zfi[nxt]);
+        const T* fjn = reinterpret_cast<const T*>(Mb.zfj[nxt]);
+        T* res = reinterpret_cast<T*>(Mb.res_out);
+        T* zn = reinterpret_cast<T*>(Mb.zeta_old[nxt]);
+        for (int l = 0; l < L; ++l) {
+            const long long o = X.at(i, j, l);
+            if (i >= 1) umax = fmax(umax, fabs((double)ui[o]));
+            if (i >= 1 && i <= ii - 2) umax = fmax(umax, fabs((double)uj[o]));
+            double zz = z[o];
+            if (i >= 1 && i <= ii - 2) {
+                const long long op = X.at(i, j + 1, l);
+                const double fl0 = (double)ui[o] * (double)fin[o], fl1 = (double)ui[o + 1] * (double)fin[o + 1];
+                const double fj0 = (double)uj[o] * (double)fjn[o], fj1 = (double)uj[op] * (double)fjn[op];
+                const double r = -(fl1 - fl0 + fj1 - fj0);
+                res[o] = (T)r;
+                zz = zz + hdt * r;
+            }
+            zn[o] = (T)zz;
+        }
+    }
+    umax = warp_max(umax);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = umax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 4; ++w) t = fmax(t, red[w]);
+        const int cta = blockIdx.x + gridDim.x * local;
+        Mb.maxu_part[cta] = t;
+        __threadfence();
+        const unsigned prev = atomicAdd(&Mb.counters[1], 1u);
+        is_last = (prev == (unsigned)(Mb.ntiles_cab - 1));
+    }
+    __syncthreads();
+    if (is_last) finish_step(Mb, red);
+}
+
+}  // namespace
+
+cudaError_t launch_cabaret_channel(const LaunchSet& ls, int f32, cudaStream_t st) {
+    const dim3 g((ls.maxI + 127) / 128, ls.maxJ * ls.nmem);
+    if (f32) {
+        k_ch_rel<float><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_ch_force_cell<float><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_ch_extrap<float><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_ch_corrector<float><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    } else {
+        k_ch_rel<double><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_ch_force_cell<double><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_ch_extrap<double><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_ch_corrector<double><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    }
+    return cudaGetLastError();
+}
+
+int channel_ctas(int ii, int jj) { return ((ii + 127) / 128) * jj; }
+
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, int f32, cudaStream_t st) {
     if (f32) return predict_next ? launch_cab<true, float>(ls, st) : launch_cab<false, float>(ls, st);
     return predict_next ? launch_cab<true, double>(ls, st) : launch_cab<false, double>(ls, st);
@@ -1009,7 +1278,7 @@ __global__ void k_rel(const Member* __restrict__ mems, const int* __restrict__ p
     for (int i = threadIdx.x; i < ii; i += blockDim.x)
         for (int l = 0; l < L; ++l) {
             const long long o = (long long)j * pitch + i + l * ls;
-            const bool interior = i > 0 && i < ii - 1 && j > 0 && j < jj - 1;
+            const bool interior = i > 0 && i < ii - 1 && (Mb.periodic || (j > 0 && j < jj - 1));
             rel[o] = (T)rel_node(Mb, ps, interior ? (double)zp[o] : 0.0, i, j, l);
         }
 }
@@ -1040,7 +1309,7 @@ __global__ void k_init_finish(const Member* __restrict__ mems, const int* __rest
     for (int i = threadIdx.x; i < ii; i += blockDim.x)
         for (int l = 0; l < L; ++l) {
             const long long o = (long long)j * pitch + i + l * ls;
-            const bool interior = i > 0 && i < ii - 1 && j > 0 && j < jj - 1;
+            const bool interior = i > 0 && i < ii - 1 && (Mb.periodic || (j > 0 && j < jj - 1));
             const double r = rel_node(Mb, ps, (double)zp[o], i, j, l);
             rel[o] = (T)r;
             zo[o] = interior ? zp[o] : (T)zeta_bc_node(Mb, ps, r, i, j, l);
@@ -1073,7 +1342,10 @@ __global__ void __launch_bounds__(256) k_energy(const Member* __restrict__ mems,
     const double* psi = Mb.psi;
     double acc[PQ_MAXL + 1];
     for (int q = 0; q <= L; ++q) acc[q] = 0.0;
-    const double wj = (j == 0 || j == jj - 1) ? 0.5 : 1.0;
+    // A channel has no j boundary: full weights, and the kinetic-energy
+    // corners of row 0 reach back to row jj - 1.
+    const double wj = (!Mb.periodic && (j == 0 || j == jj - 1)) ? 0.5 : 1.0;
+    const long long back = (j == 0) ? (long long)(jj - 1) * pitch : -(long long)pitch;  // row j-1, wrapped
     for (int i = threadIdx.x; i < ii; i += blockDim.x) {
         const double w = wj * ((i == 0 || i == ii - 1) ? 0.5 : 1.0);
         const long long o = (long long)j * pitch + i;
@@ -1082,11 +1354,11 @@ __global__ void __launch_bounds__(256) k_energy(const Member* __restrict__ mems,
             const double d = psi[o + k * ls] - psi[o + (k + 1) * ls];
             acc[L] += w * fac * (d * d);
         }
-        if (i >= 1 && j >= 1) {
+        if (i >= 1 && (j >= 1 || Mb.periodic)) {
             for (int k = 0; k < L; ++k) {
                 const long long lo = k * ls;
-                const double a = psi[o - 1 + lo] + psi[o + lo] - psi[o - 1 - pitch + lo] - psi[o - pitch + lo];
-                const double b = psi[o - pitch + lo] + psi[o + lo] - psi[o - 1 - pitch + lo] - psi[o - 1 + lo];
+                const double a = psi[o - 1 + lo] + psi[o + lo] - psi[o - 1 + back + lo] - psi[o + back + lo];
+                const double b = psi[o + back + lo] + psi[o + lo] - psi[o - 1 + back + lo] - psi[o - 1 + lo];
                 acc[k] += 0.25 * (a * a + b * b);
             }
         }

@@ -107,7 +107,7 @@ void unpack(Ref& a, const Range& r, int l, const std::vector<double>& in) {
 
 bool supported(pq_ctx* c) {
     if (c->helm_only) return !fail(c, PQ_ERR_UNSUPPORTED, "checkpoint of a Helmholtz-only context");
-    if (c->periodic) return !fail(c, PQ_ERR_UNSUPPORTED, "the channel (periodic j) time step is not built");
+    if (c->periodic) return !fail(c, PQ_ERR_UNSUPPORTED, "checkpoints of a channel (periodic j) are not built");
     return true;
 }
 

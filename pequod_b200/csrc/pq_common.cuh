@@ -33,7 +33,8 @@ struct Scalars {
     double tweight_u;
     double max_u;      // max |u| over the faces, from the last fused step
     double cfl;        // max_u * dt
-    double psiC[PQ_MAXL];
+    double psiC[PQ_MAXL];   // mass correction per mode; channel: coefficient of corr (wall i = 0)
+    double psiC2[PQ_MAXL];  // channel: coefficient of corr2 (wall i = ii - 1)
     double ekin[PQ_MAXL];
     double epot;
     double model_time;  // advanced by dt at the end of every fused step
@@ -79,7 +80,7 @@ struct Member {
     const float2* tw_f;     // FP32 copies of tw, wsplit, was (mixed path)
     const float2* wsplit_f;
     const float* was_f;
-    int periodic;           // 1: channel periodic in j (helm only)
+    int periodic;           // 1: channel periodic in j
     const double* pb;       // periodic_coefficients b, c of the channel,
     const double* pc;       //   [(m * jj + j) * n + k-1], j 0-based
     int mixed;              // 1: FP32 storage of the CABARET fields and the
@@ -118,6 +119,12 @@ struct Member {
     void* spec;
     double* spec64;   // barotropic-mode spectral rows of the mixed path (FP64)
     const double* corr;
+    // Channel (momentum correction, correction_function_momentum): the second
+    // correction function, the spectral weights of the two walls' mean PV
+    // (per wavenumber), and per mode the inverse 2 x 2 wall matrix.
+    const double* corr2;
+    const double* wwall;       // [n]: wall i = 0; the other wall has (-1)^(k+1) times it
+    const double* inv_corr_a;  // [L][4], column-major 2 x 2
     const double* wind;
     double* partials;     // [L * ntiles_tri]
     double* maxu_part;    // [ntiles_cab]
@@ -270,7 +277,7 @@ __device__ __forceinline__ double block_sum_l2(const double* p, int n, long long
 template <class PS>
 __device__ __forceinline__ double rel_node(const Member& Mb, PS ps, double zeta, int i, int j, int l) {
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
-    const bool bj = (j == 0 || j == jj - 1), bi = (i == 0 || i == ii - 1);
+    const bool bj = !Mb.periodic && (j == 0 || j == jj - 1), bi = (i == 0 || i == ii - 1);
     if (bj || bi) {
         if (Mb.bc_type == 3) return 0.0;
         int di = 0, dj = 0;

@@ -33,7 +33,8 @@ struct pq_ctx {
     bool initialized = false;
     bool fuse = false;        // fixed dt: the CABARET kernel applies the next predictor
     bool mixed = false;       // PQ_PREC_MIXED
-    bool periodic = false;    // channel periodic in j (pq_helm only)
+    bool periodic = false;    // channel periodic in j
+    bool channel_singular = false;  // channel without a momentum correction (singular wall matrix): pq_helm only
     bool leapfrog = false;    // PQ_SCHEME_LEAPFROG: cur is the level advanced next (lf - 1)
     bool pred_ready = false;  // zeta[cur] / res_beta[cur] already hold the next step's predictor
     int zpar = 0;             // parity whose zeta entered the last inversion

@@ -545,16 +545,23 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
         // row; phi is zero on the boundary (apply_dirichlet_bc(0),
         // qg3p_aux.F90:470).
         __syncthreads();
+        // A channel (modes_to_z_correct_momentum + modes_to_z, qg3p_aux.F90:
+        // 524-575) subtracts psiC_m corr_m + psiC2_m corr2_m from the
+        // baroclinic modes; its psiC_0 is zero.
         const double* psiC = Mb.sc->psiC;
-        double pc[PQ_MAXL];
+        const double* psiC2 = Mb.sc->psiC2;
+        double pc[PQ_MAXL], pc2[PQ_MAXL];
 #pragma unroll
-        for (int m = 0; m < PQ_MAXL; ++m) pc[m] = (m < L) ? psiC[m] : 0.0;
+        for (int m = 0; m < PQ_MAXL; ++m) {
+            pc[m] = (m < L) ? psiC[m] : 0.0;
+            pc2[m] = (m < L && Mb.periodic) ? psiC2[m] : 0.0;
+        }
         double* psi = Mb.psi;
         for (int r = 0; r < R; ++r)
             for (int i = threadIdx.x; i < ii; i += nthr) {
                 const int j = j0 + r;
                 if (j >= jend) break;
-                const bool inner = j >= 1 && j <= jj - 2 && i >= 1 && i <= n;
+                const bool inner = (Mb.periodic || (j >= 1 && j <= jj - 2)) && i >= 1 && i <= n;
                 // corr_m at cr[m * cst] (staged rows, or the field itself)
                 const double* cr = corr_smem ? extra + ((long long)r * (L - 1) - 1) * pitch + i
                                              : Mb.corr + (long long)j * pitch + i;
@@ -566,6 +573,12 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
 #pragma unroll
                 for (int m = 1; m < PQ_MAXL; ++m)
                     if (m < L) ph[m] -= pc[m] * cr[m * cst];
+                if (Mb.periodic) {
+                    const double* c2 = Mb.corr2 + (long long)j * pitch + i;
+#pragma unroll
+                    for (int m = 1; m < PQ_MAXL; ++m)
+                        if (m < L) ph[m] -= pc2[m] * c2[m * ls];
+                }
                 const double b0 = ph[0] - pc[0];
                 const long long o = (long long)j * pitch + i;
 #pragma unroll
@@ -618,6 +631,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                                                           const int* __restrict__ prefix, int nmem, int do_mean) {
     __shared__ Member Mb;
     __shared__ double wpart[TRI_THREADS / 32];
+    __shared__ double wpart2[TRI_THREADS / 32];  // channel: the second wall
     __shared__ double tot[2][TRI_THREADS / 32][2];  // per-warp affine totals (forward, backward)
     __shared__ int is_last;
     extern __shared__ __align__(16) double strip[];
@@ -821,7 +835,10 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                 const int ql = (Mr - 1) / R, tl = (Mr - 1) - ql * R;
                 const double z2 = strip[c * CS];                 // row 2 (1-based) after the solve
                 const double zl = strip[c * CS + ql * RS + tl];  // row jj-1
-                const double z1i = spec[kk], zji = spec[(long long)(jj - 1) * pitch + kk];
+                // rows 1 and jj (0 and jj-1) of this mode's spectral field
+                const double z1i = f32 ? (double)specf[kk] : spec[kk];
+                const double zji = f32 ? (double)specf[(long long)(jj - 1) * pitch + kk]
+                                       : spec[(long long)(jj - 1) * pitch + kk];
                 z1 = (z1i - z2) / __ldg(&pb[0]);
                 zj = ((zji - zl) - z1 * __ldg(&pb[(long long)(jj - 1) * n])) / __ldg(&pc[(long long)(jj - 1) * n]);
             }
@@ -830,8 +847,14 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         }
         __syncthreads();  // every warp has read rows 1 and jj before they are written
         if (active && h == 0 && lane == 0) {
-            spec[kk] = z1 - zj * __ldg(&Mb.pc[(long long)m * jj * n + kk]);
-            spec[(long long)(jj - 1) * pitch + kk] = zj;
+            const double r0 = z1 - zj * __ldg(&Mb.pc[(long long)m * jj * n + kk]);
+            if (f32) {
+                specf[kk] = (float)r0;
+                specf[(long long)(jj - 1) * pitch + kk] = (float)zj;
+            } else {
+                spec[kk] = r0;
+                spec[(long long)(jj - 1) * pitch + kk] = zj;
+            }
         }
         if (active)
             for (int t = 0; t < cnt; ++t) {
@@ -839,9 +862,33 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                 s[t] = (s[t] - z1 * __ldg(&Mb.pb[((long long)m * jj + row) * n + kk])) -
                        zj * __ldg(&Mb.pc[((long long)m * jj + row) * n + kk]);
             }
+        if (do_mean) {
+            // The column sum over every row of the closed solution.
+            lsum = 0.0;
+            for (int t = 0; t < cnt; ++t) lsum += s[t];
+            if (active && h == 0 && lane == 0) lsum += (z1 - zj * __ldg(&Mb.pc[(long long)m * jj * n + kk])) + zj;
+        }
     }
-    const double colsum = (active && do_mean) ? warp_sum(lsum) * __ldg(&Mb.wmean[kk]) : 0.0;
-    if (lane == 0) wpart[warp] = colsum;
+    // Closed basin: the domain mean of the mode (wmean weights).  Channel:
+    // the mean PV of the two walls (zeta_boundary of the solved mode,
+    // qg3p_aux.F90:289-379), linear in the column sums: sum_j phi(i, j) =
+    // 2 sum_k sin(i k pi / N) C_k, so wall i = 0 gets wwall[k] C_k and wall
+    // ii - 1 gets (-1)^(k+1) wwall[k] C_k.
+    double colsum = 0.0, colsum2 = 0.0;
+    if (active && do_mean) {
+        const double cs = warp_sum(lsum);
+        if (Mb.periodic) {
+            const double w = __ldg(&Mb.wwall[kk]);
+            colsum = cs * w;
+            colsum2 = (kk & 1) ? -colsum : colsum;
+        } else {
+            colsum = cs * __ldg(&Mb.wmean[kk]);
+        }
+    }
+    if (lane == 0) {
+        wpart[warp] = colsum;
+        wpart2[warp] = colsum2;
+    }
     pdl_release();
     __syncthreads();
     {
@@ -861,25 +908,45 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     }
     if (!do_mean) return;
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < TRI_THREADS / 32; ++w) t += wpart[w];
+        double t = 0.0, t2 = 0.0;
+        for (int w = 0; w < TRI_THREADS / 32; ++w) {
+            t += wpart[w];
+            t2 += wpart2[w];
+        }
         Mb.partials[local] = t;
+        if (Mb.periodic) Mb.partials[Mb.ntiles_tri + local] = t2;
         __threadfence();
         const unsigned prev = atomicAdd(&Mb.counters[0], 1u);
         is_last = (prev == (unsigned)(Mb.ntiles_tri - 1));
     }
     __syncthreads();
     if (!is_last) return;
-    // Last CTA of this member: psiC_m = (sum of partials) / (g_ii_int g_jj_int),
-    // summed in a fixed order so that the result is independent of CTA timing.
+    // Last CTA of this member, every sum in a fixed order so that the result
+    // is independent of CTA timing.  Closed basin: psiC_m = (sum of partials)
+    // / (g_ii_int g_jj_int).  Channel (modes_to_z_correct_momentum,
+    // qg3p_aux.F90:524-575): the baroclinic modes' coefficients of the two
+    // correction functions, inv_corr_a times the wall PV means; the
+    // barotropic mode is not corrected.
     __threadfence();
     for (int mm = 0; mm < Mb.L; ++mm) {
         const double t = block_sum_l2(Mb.partials + (long long)mm * tiles_per_mode, tiles_per_mode, 1, wpart);
+        double t2 = 0.0;
+        if (Mb.periodic)
+            t2 = block_sum_l2(Mb.partials + Mb.ntiles_tri + (long long)mm * tiles_per_mode, tiles_per_mode, 1,
+                              wpart2);
         if (threadIdx.x == 0) {
-            const double pc = t * Mb.mean_scale;
+            double pc, pc2 = 0.0;
+            if (Mb.periodic) {
+                const double* A = Mb.inv_corr_a + 4 * mm;
+                pc = mm == 0 ? 0.0 : A[0] * t + A[2] * t2;
+                pc2 = mm == 0 ? 0.0 : A[1] * t + A[3] * t2;
+                Mb.sc->psiC2[mm] = pc2;
+            } else {
+                pc = t * Mb.mean_scale;
+            }
             Mb.sc->psiC[mm] = pc;
-            if (pc != pc) atomicOr(Mb.status, (int)ST_NAN_PSIC);
-            else if (fabs(pc) > 1.0e100) atomicOr(Mb.status, (int)ST_LARGE_PSIC);
+            if (pc != pc || pc2 != pc2) atomicOr(Mb.status, (int)ST_NAN_PSIC);
+            else if (fabs(pc) > 1.0e100 || fabs(pc2) > 1.0e100) atomicOr(Mb.status, (int)ST_LARGE_PSIC);
         }
     }
     if (threadIdx.x == 0) Mb.counters[0] = 0u;
@@ -911,7 +978,7 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const int threads = L * R * (M / V);
     size_t bytes = (size_t)L * R * dst_unit_len(ls.maxN) * sizeof(double);
     const size_t cbytes = (size_t)R * (L - 1) * ls.maxPitch * sizeof(double);
-    const int corr_smem = (EPI == EPI_PV && bytes + cbytes <= 200 * 1024) ? 1 : 0;
+    const int corr_smem = (EPI == EPI_PV && !ls.periodic && bytes + cbytes <= 200 * 1024) ? 1 : 0;
     if (corr_smem) bytes += cbytes;
     if (sizeof(S) == 4 && EPI == EPI_SPEC && PRO != PRO_STEP) bytes += (size_t)R * L * ls.maxN * sizeof(float);
     cudaError_t e =

@@ -67,6 +67,10 @@ cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, int f32, cudaStream
 // pq_cabaret.cu
 // predict_next: also apply the next step's predictor + beta (fixed dt only)
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, int f32, cudaStream_t st);
+// The channel (periodic j) CABARET step after the inversion: four
+// node-parallel kernels; channel_ctas is the last kernel's CTA count.
+cudaError_t launch_cabaret_channel(const LaunchSet& ls, int f32, cudaStream_t st);
+int channel_ctas(int ii, int jj);
 int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of the sweep kernel per member (band height sh)
 int cabaret_tile_ctas(int ii, int jj, int L);     // CTAs of the tile kernel per member
 cudaError_t launch_rel(const LaunchSet& ls, int f32, cudaStream_t st);

@@ -324,8 +324,8 @@ long pq_server_launches(const pq_server* s) { return s ? s->launches : 0; }
 
 int pq_server_submit(pq_server* s, const pq_model_desc* d, const double* zeta_ic, int nsteps, long* id) {
     if (!s || !d || !zeta_ic || nsteps < 0 || !id) return PQ_ERR_ARG;
-    if (d->scheme != PQ_SCHEME_CABARET || d->adapt_dt)
-        return sfail(s, PQ_ERR_UNSUPPORTED, "the server runs the CABARET scheme with a fixed dt");
+    if (d->scheme != PQ_SCHEME_CABARET || d->adapt_dt || d->periodic_j)
+        return sfail(s, PQ_ERR_UNSUPPORTED, "the server runs closed-basin CABARET runs with a fixed dt");
     pq_server::Run r;
     r.id = s->next_id++;
     r.desc = *d;

@@ -109,8 +109,11 @@ def test_helm_periodic_matches_oracle(ii, jj, ss):
     for l in range(L):
         assert rel_l2(out[:, :, l], ref[:, :, l]) <= TOL_STEP, (l, rel_l2(out[:, :, l], ref[:, :, l]))
     assert np.array_equal(out[0, :, :], rhs[0, :, :])
-    with pytest.raises(pq.PQError):
-        g.init_perturb(np.zeros((ii, jj, L)))
+    if any(s == 0.0 for s in ss[1:]):
+        # free slip and ss = 0 in a baroclinic mode: no momentum correction,
+        # so no channel time step on this context
+        with pytest.raises(pq.PQError):
+            g.init_perturb(np.zeros((ii, jj, L)))
 
 
 @pytest.mark.parametrize("ss,min_order", [(0.0, 2.0), (0.5, 3.9)])
