@@ -206,8 +206,17 @@ PQ_API int pq_check(pq_ctx* ctx);
  * way a host-side driver that owns its arrays would call the solver: if
  * zeta_in is not NULL it replaces zeta (sdata (ii, jj, L)) before the step;
  * if psi_out is not NULL it receives the step's psi (sdata).  Asynchronous:
- * host buffers should be pinned; pq_check or pq_sync completes the copies. */
+ * host buffers should be pinned; pq_check or pq_sync completes the copies.
+ * With both host buffers given, the copies are pipelined: the input and
+ * output transfers run on the context's own copy streams through device
+ * staging buffers, overlapping the kernels of the neighbouring calls'
+ * steps.  The buffers must stay valid, and zeta_in unchanged, until
+ * pq_sync / pq_check; successive calls may reuse the same buffers (psi_out
+ * then holds the last step's psi).  The first copy of a sequence follows
+ * the work already on pq_stream(ctx); pq_join(ctx) makes work enqueued on
+ * that stream afterwards follow the sequence's copies, without a host wait. */
 PQ_API int pq_step_exchange(pq_ctx* ctx, const double* zeta_in, double* psi_out, int ptr_kind);
+PQ_API int pq_join(pq_ctx* ctx);
 
 /* energy(strat, psi, ekin, epot), qg3p_diagnostics.F90:778-863, on the
  * current psi.  ekin: L doubles. */

@@ -93,6 +93,7 @@ SIGNATURES = {
     "pq_step_async": (C.c_int, [C.c_void_p, C.c_int]),
     "pq_check": (C.c_int, [C.c_void_p]),
     "pq_step_exchange": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    "pq_join": (C.c_int, [C.c_void_p]),
     "pq_energy": (C.c_int, [C.c_void_p, _dp, _dp]),
     "pq_cfl": (C.c_int, [C.c_void_p, _dp]),
     "pq_get_field": (C.c_int, [C.c_void_p, C.c_int, _dp]),
@@ -326,6 +327,10 @@ class Model:
 
     def sync(self) -> None:
         _check(lib().pq_sync(self.ctx), self.ctx)
+
+    def join(self) -> None:
+        """Order the context's stream after the pipelined exchange copies."""
+        _check(lib().pq_join(self.ctx), self.ctx)
 
     def energy(self):
         ekin = np.zeros(self.cfg.layers)

@@ -109,7 +109,16 @@ int copy_out_state(pq_ctx* c, double* dst, const void* src, int kind) {
     return copy_out(c, dst, c->hm[0].helm_io, kind);
 }
 
+int join_exchange(pq_ctx* c) {
+    if (c->x.last >= 0) CK(cudaStreamWaitEvent(c->stream, c->x.done[c->x.last], 0));
+    c->x.last = -1;
+    c->x.sequence = false;
+    return PQ_OK;
+}
+
 int check_status(pq_ctx* c) {
+    int rc = join_exchange(c);
+    if (rc) return rc;
     int st = 0;
     CK(cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -220,6 +229,21 @@ void pq_destroy(pq_ctx* c) {
         if (g) cudaGraphExecDestroy(g);
     if (c->arena) cudaFree(c->arena);
     if (c->psi_av) cudaFree(c->psi_av);
+    if (c->x.in) {
+        cudaStreamSynchronize(c->x.in);
+        cudaStreamSynchronize(c->x.out);
+        for (int s = 0; s < 2; ++s) {
+            cudaFree(c->x.stage_in[s]);
+            cudaFree(c->x.stage_out[s]);
+            cudaEventDestroy(c->x.ready[s]);
+            cudaEventDestroy(c->x.consumed[s]);
+            cudaEventDestroy(c->x.produced[s]);
+            cudaEventDestroy(c->x.done[s]);
+        }
+        cudaEventDestroy(c->x.entry);
+        cudaStreamDestroy(c->x.in);
+        cudaStreamDestroy(c->x.out);
+    }
     if (c->d_members) cudaFree(c->d_members);
     if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -846,6 +870,57 @@ int pq_step_exchange(pq_ctx* c, const double* zeta_in, double* psi_out, int ptr_
     if (!c) return PQ_ERR_ARG;
     if (!c->initialized) return fail(c, PQ_ERR_STATE, "pq_step_exchange before pq_init_perturb");
     CK(cudaSetDevice(c->device));
+    if (ptr_kind == PQ_PTR_HOST && zeta_in && psi_out) {
+        // Pipelined: H2D into staging slot s on the input stream, D2D into
+        // the state and the step on the context's stream, D2D of psi into
+        // the output slot, D2H on the output stream.  A slot is reused two
+        // calls later, after the events that guard it.
+        auto& x = c->x;
+        const size_t bytes = (size_t)c->ii * c->jj * c->L * sizeof(double);
+        if (!x.in) {
+            CK(cudaStreamCreateWithFlags(&x.in, cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithFlags(&x.out, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&x.entry, cudaEventDisableTiming));
+            for (int s = 0; s < 2; ++s) {
+                if (cudaMalloc(&x.stage_in[s], bytes) != cudaSuccess || cudaMalloc(&x.stage_out[s], bytes) != cudaSuccess) {
+                    cudaGetLastError();
+                    return fail(c, PQ_ERR_NOMEM, "cudaMalloc of the exchange staging buffers failed");
+                }
+                CK(cudaEventCreateWithFlags(&x.ready[s], cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&x.consumed[s], cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&x.produced[s], cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&x.done[s], cudaEventDisableTiming));
+            }
+        }
+        const int s = x.slot;
+        x.slot ^= 1;
+        if (!x.sequence) {
+            // The first copy of a sequence follows everything already on the
+            // context's stream.
+            CK(cudaEventRecord(x.entry, c->stream));
+            CK(cudaStreamWaitEvent(x.in, x.entry, 0));
+            x.sequence = true;
+        }
+        CK(cudaStreamWaitEvent(x.in, x.consumed[s], 0));
+        CK(cudaMemcpyAsync(x.stage_in[s], zeta_in, bytes, cudaMemcpyHostToDevice, x.in));
+        CK(cudaEventRecord(x.ready[s], x.in));
+        CK(cudaStreamWaitEvent(c->stream, x.ready[s], 0));
+        int rc = copy_in_state(c, c->hm[c->cur].zeta_old[c->cur], x.stage_in[s], PQ_PTR_DEVICE);
+        if (rc) return rc;
+        CK(cudaEventRecord(x.consumed[s], c->stream));
+        c->pred_ready = false;
+        rc = pq_step_async(c, 1);
+        if (rc) return rc;
+        CK(cudaStreamWaitEvent(c->stream, x.done[s], 0));
+        rc = copy_out(c, x.stage_out[s], c->hm[0].psi, PQ_PTR_DEVICE);
+        if (rc) return rc;
+        CK(cudaEventRecord(x.produced[s], c->stream));
+        CK(cudaStreamWaitEvent(x.out, x.produced[s], 0));
+        CK(cudaMemcpyAsync(psi_out, x.stage_out[s], bytes, cudaMemcpyDeviceToHost, x.out));
+        CK(cudaEventRecord(x.done[s], x.out));
+        x.last = s;
+        return PQ_OK;
+    }
     if (zeta_in) {
         int rc = copy_in_state(c, c->hm[c->cur].zeta_old[c->cur], zeta_in, ptr_kind);
         if (rc) return rc;
@@ -994,8 +1069,16 @@ int pq_get_tuning(pq_ctx* c, pq_tuning* t) {
 
 int pq_sync(pq_ctx* c) {
     if (!c) return PQ_ERR_ARG;
+    int rc = join_exchange(c);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
     return PQ_OK;
+}
+
+int pq_join(pq_ctx* c) {
+    if (!c) return PQ_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    return join_exchange(c);
 }
 
 int pq_kernel_timing(pq_ctx* c, int enable) {

@@ -52,6 +52,19 @@ struct pq_ctx {
     int ii = 0, jj = 0, L = 0, pitch = 0;
     size_t field_bytes = 0;  // bytes of one L-layer field
     double* psi_av = nullptr;  // time average of psi (pq_average), FP64, node-shaped like psi
+    // Pipelined host exchange (pq_step_exchange with host buffers): the
+    // copies run on their own streams through two dense device staging slots
+    // each way, so that a step's input and output transfers overlap the
+    // neighbouring steps' kernels.
+    struct Exchange {
+        cudaStream_t in = nullptr, out = nullptr;
+        double* stage_in[2] = {nullptr, nullptr};
+        double* stage_out[2] = {nullptr, nullptr};
+        cudaEvent_t entry = nullptr, ready[2] = {}, consumed[2] = {}, produced[2] = {}, done[2] = {};
+        int slot = 0;
+        int last = -1;          // slot of the newest output copy, -1: none pending
+        bool sequence = false;  // copies issued since the last join
+    } x;
 };
 
 namespace pq {
@@ -89,6 +102,9 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc);
 int read_scalars(pq_ctx* c, Scalars* sc);
 // Kernel launches of one step (the leapfrog time average adds one).
 int step_launches(const pq_ctx* c);
+// Order the context's stream after the pipelined exchange copies issued so
+// far (no host wait).
+int join_exchange(pq_ctx* c);
 // pq_create's body.  helm_only: allocate only the Helmholtz fields (helm_io,
 // spec) -- the batched solver's members; stream: use this stream instead of
 // creating one (not owned).

@@ -342,3 +342,31 @@ def test_programmatic_dependent_launch_matches_oracle(ii, kernel):
         g.step(n)
         o.step(n)
     compare(g, o, TOL_STEP * 10)
+
+
+def test_pipelined_exchange_matches_oracle():
+    """pq_step_exchange with host buffers overlaps its copies with the
+    neighbouring steps; every step still takes its own input and returns
+    its own psi."""
+    cfg = double_gyre(129, 3)
+    g, o = start(cfg, seed=10)
+    g.step(2)
+    o.step(2)
+    ii, jj, L = cfg.ii, cfg.jj, cfg.layers
+    rng = np.random.default_rng(10)
+    inputs, outs = [], []
+    for k in range(5):
+        z = np.asfortranarray(o.sdata("zeta") * (1.0 + 1e-3 * rng.standard_normal((ii, jj, L))))
+        inputs.append(np.ascontiguousarray(z.ravel(order="F")))
+        outs.append(np.zeros(ii * jj * L))
+    for k in range(5):
+        g.step_exchange(inputs[k].ctypes.data, outs[k].ctypes.data, pq.PTR_HOST)
+    g.sync()
+    for k in range(5):
+        zd = o.get("zeta")
+        zd[1:-1, 1:-1] = inputs[k].reshape((ii, jj, L), order="F")
+        o.set("zeta", zd)
+        o.set("zeta_old", zd)
+        o.step(1)
+        psi = outs[k].reshape((ii, jj, L), order="F")
+        assert rel_l2(psi, o.sdata("psi")) <= TOL_STEP * 10, k
