@@ -220,20 +220,18 @@ def run_ours(a, rank, world, local_rank):
 
     import pequod_b200 as pq
 
+    from pequod_b200 import multirank
+
     dev = local_rank
     torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-
-        dist = dist_mod
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dist = multirank.init(world)
     cfg = make_config(a.size, a.layers, a.dt, precision=0 if a.precision == "fp64" else 1)
     units = cfg.ii * cfg.jj * cfg.layers
     m = pq.Model(cfg, device=dev)
     if getattr(a, "pdl", False):
         m.set_tuning(pdl=1)
-    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=1 + rank, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=multirank.rank_seed(1, rank), amplitude=1e-7 * cfg.t_scale,
+                    sigma=3.0)
     m.init_perturb(ic)
     m.step(max(3, a.warmup))
     stream = torch.cuda.ExternalStream(m.stream, device=dev)
@@ -271,11 +269,7 @@ def run_ours(a, rank, world, local_rank):
     barrier()
     m.check()
     step_ms = [s.elapsed_time(e) for s, e in ev]
-    total_ms = float(sum(step_ms))
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = multirank.max_over_ranks(dist, [float(sum(step_ms))], device=dev)[0]
     value = world * units * K / (total_ms * 1e-3)
 
     # ---- back-to-back steps (CUDA graphs, L2 warm), informational -----------
@@ -310,17 +304,11 @@ def run_ours(a, rank, world, local_rank):
         e2e_e.record(stream)
     stream.synchronize()
     m.check()
-    e2e_ms = float(e2e_s.elapsed_time(e2e_e))
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = multirank.max_over_ranks(dist, [float(e2e_s.elapsed_time(e2e_e))], device=dev)[0]
     e2e = world * units * K / (e2e_ms * 1e-3)
 
     if rank != 0:
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
+        multirank.close(dist)
         return
 
     # ---- roofline of the dominant kernel --------------------------------------
@@ -372,9 +360,7 @@ def run_ours(a, rank, world, local_rank):
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    multirank.close(dist)
 
 
 def run_batched(a, rank, world, local_rank):
@@ -387,13 +373,11 @@ def run_batched(a, rank, world, local_rank):
     import pequod_b200 as pq
     from pequod_b200.workloads import batched_helmholtz, gaussian_random_field
 
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
+    from pequod_b200 import multirank
 
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    shapes, ss = batched_helmholtz(a.batch, seed=2 + rank)
+    torch.cuda.set_device(local_rank)
+    dist = multirank.init(world)
+    shapes, ss = batched_helmholtz(a.batch, seed=multirank.rank_seed(2, rank))
     b = pq.Batch(shapes, ss, device=local_rank)
     # One right-hand side per distinct shape (the timing does not depend on the values).
     rhs_of = {}
@@ -434,10 +418,7 @@ def run_batched(a, rank, world, local_rank):
         rc = pq.lib().pq_batch_helm(b.ctx, ptrs, pq.PTR_HOST)
         assert rc == 0, pq.lib().pq_batch_last_error(b.ctx)
     e2e_s = (time.perf_counter() - t0) / KE
-    if dist:
-        t = torch.tensor([ms, e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(t[0]), float(t[1])
+    ms, e2e_s = multirank.max_over_ranks(dist, [ms, e2e_s], device=f"cuda:{local_rank}")
     if rank == 0:
         peak, peak_kind = peaks()
         per_solve_s = ms / K * 1e-3
@@ -479,9 +460,7 @@ def run_batched(a, rank, world, local_rank):
         }
         print(json.dumps(line), flush=True)
     b.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    multirank.close(dist)
 
 
 def dptr(t):
@@ -503,8 +482,11 @@ def run_serving(a, rank, world, local_rank):
     import pequod_b200 as pq
     from pequod_b200.workloads import double_gyre, initial_condition, serving_requests
 
+    from pequod_b200 import multirank
+
     torch.cuda.set_device(local_rank)
-    reqs = serving_requests(rate=a.rate, window=a.window, seed=3 + rank)
+    dist = multirank.init(world)
+    reqs = serving_requests(rate=a.rate, window=a.window, seed=multirank.rank_seed(3, rank))
     cfgs = {}
     srv = pq.Server(int(a.budget_gb * (1 << 30)), device=local_rank)
     pending = list(reqs)
@@ -531,22 +513,24 @@ def run_serving(a, rank, world, local_rank):
                 ids_done.append((lat, work, t3[2] - t_start))
             if not ids and pending:
                 time.sleep(max(0.0, min(0.01, pending[0][0] - (srv.clock() - t_start))))
-    lat = np.array([d[0] for d in ids_done])
-    work = float(sum(d[1] for d in ids_done))
-    span = max(d[2] for d in ids_done)
+    # Every rank served its own request stream; the statistics cover all.
+    summary = multirank.serving_summary(multirank.gather_lists(dist, ids_done))
+    launches = int(sum(multirank.gather_lists(dist, [srv.launches()])))
     line = {
-        "metric": "serving latency p50/p99 (s)", "value": float(np.percentile(lat, 50)), "unit": "s",
-        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-        "n_gpus": 1, "steps": len(ids_done), "warmup": 0, "higher_is_better": False, "scaling": "weak",
+        "metric": "serving latency p50/p99 (s)", "value": summary["p50_s"], "unit": "s",
+        "p50_s": summary["p50_s"], "p99_s": summary["p99_s"],
+        "n_gpus": world, "steps": summary["runs"], "warmup": 0, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "serving_double_gyre", "rate_per_s": a.rate, "window_s": a.window,
-                   "runs": len(ids_done), "budget_gb": a.budget_gb, "round_steps": a.round_steps},
-        "throughput": {"value": work / span, "unit": "cell-layer-steps/s"},
-        "gpu_launches": srv.launches(), "clocks": clk.summary(),
+                   "runs": summary["runs"], "budget_gb": a.budget_gb, "round_steps": a.round_steps,
+                   "parallelism": f"replicas{world}"},
+        "throughput": {"value": summary["throughput"], "unit": "cell-layer-steps/s"},
+        "gpu_launches": launches, "clocks": clk.summary(),
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     srv.close()
+    multirank.close(dist)
 
 
 ids_done = []
