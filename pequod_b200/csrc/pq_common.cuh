@@ -164,10 +164,12 @@ __device__ __forceinline__ bool cab_average_gate(const Member& Mb) {
 
 // Tridiagonal solve geometry: W warps of row chunks per wavenumber column,
 // 8 / W columns per CTA of 256 threads (chosen so a lane's chunk stays
-// short; measured on B200 against W one step up and down at 129..2049 rows).
+// short, and its column segments 32 bytes wide: measured on B200 against W
+// one step up and down at 129..2049 rows; at 2049 rows W = 4 would read
+// 16-byte segments, half a DRAM sector).
 __host__ __device__ inline int tri_warps(int jj) {
     const int Mr = jj - 2;
-    return Mr > 1024 ? 4 : Mr > 64 ? 2 : 1;
+    return Mr > 64 ? 2 : 1;
 }
 __host__ __device__ inline int tri_ctas(int n, int jj, int L) {
     const int KT = 8 / tri_warps(jj);
