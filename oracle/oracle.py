@@ -79,6 +79,8 @@ def lib():
         L.or_model_average.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.or_model_get_average.restype = C.c_double
         L.or_model_get_average.argtypes = [C.c_void_p, _dp]
+        L.or_model_get_quad.restype = C.c_long
+        L.or_model_get_quad.argtypes = [C.c_void_p, C.c_int, _dp]
         L.or_model_finish_step.argtypes = [C.c_void_p]
         _lib = L
     return _lib
@@ -309,6 +311,20 @@ class Model:
     def average(self, enable: bool = True, threshold: float = 0.0) -> None:
         """Start (clearing) or stop the time average of psi."""
         lib().or_model_average(self.m, int(enable), float(threshold))
+
+    QUAD = ("uu", "vv", "uu_i", "vv_i", "uv", "ur", "vr", "rr", "pr", "uz", "vz", "zz", "zr", "pp", "pz", "ut", "vt",
+            "rt", "tt", "sc_ub", "sc_vb", "sc_bb", "sc_bb_i")
+
+    def get_quad(self, q: int):
+        """Quad accumulator q divided by diagnostic_time, (ii, jj, layers)."""
+        n = lib().or_model_get_quad(self.m, int(q), None)
+        if n < 0:
+            raise KeyError(q)
+        ii, jj = self.cfg["ii"], self.cfg["jj"]
+        out = np.zeros(n)
+        lib().or_model_get_quad(self.m, int(q), _p(out))
+        t = lib().or_model_get_average(self.m, None)
+        return out.reshape((ii, jj, n // (ii * jj)), order="F") * (1.0 / t)
 
     def get_average(self):
         """(psi_av / diagnostic_time as (ii, jj, L), diagnostic_time)."""

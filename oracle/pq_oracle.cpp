@@ -12,6 +12,7 @@
 #include "pq_oracle.h"
 
 #include <cmath>
+#include <limits>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -857,6 +858,11 @@ struct or_model {
     std::vector<double> psi_av;  // (ii, jj, L)
     double diag_time = 0, av_threshold = 0;
     bool av_on = false;
+    // quad eddy covariances (qg3.F90:505-558, 683-721), in output order:
+    // uu vv uu_i vv_i uv ur vr rr pr uz vz zz zr pp pz ut vt rt tt sc_ub
+    // sc_vb sc_bb sc_bb_i; *_i and sc_ub, sc_vb, sc_bb_i have L - 1 layers.
+    bool quad_on = false;
+    std::vector<double> quad[23];
     std::vector<double> p_beta_y;  // (ii+2, L)
     // Scratch arrays the reference keeps as module-level `save` arrays.
     std::vector<double> psi_edge, zeta_fin, zeta_fjn, res_visc;
@@ -1813,6 +1819,8 @@ int or_model_init(or_model* m, const double* zeta_ic) {
     return 0;
 }
 
+static void accumulate_quad(or_model& m, int lv);
+
 // psi_av += dt * psi%sdata and diagnostic_time += dt once start_time +
 // model_time > max_spin (qg3.F90:672-680, 725); av_threshold holds
 // max_spin - start_time.  lv: the time level just inverted (psi BLEAPFROG).
@@ -1823,15 +1831,156 @@ static void accumulate_average(or_model& m, int lv) {
     for (int l = 1; l <= d.layers; ++l)
         for (int j = 1; j <= d.jj; ++j)
             for (int i = 1; i <= d.ii; ++i) av(i, j, l) = av(i, j, l) + m.dt * psi(i + 1, j + 1, l);
+    if (m.quad_on) accumulate_quad(m, lv);
     m.diag_time = m.diag_time + m.dt;
 }
 
-// Start (clearing the sum, qg3.F90:502-503) or stop the time average.
+// Layers of quad accumulator q (EC_INTERFACES: L - 1).
+static int quad_layers(const or_model& m, int q) {
+    return (q == 2 || q == 3 || q == 19 || q == 20 || q == 22) ? m.d.layers - 1 : m.d.layers;
+}
+
+// The quad diagnostics of one step, qg3.F90:683-721: zonal_velocity,
+// meridional_velocity (qg3p_diagnostics.F90:941-1107; rows / columns the
+// reference never writes stay 0 as at their allocation, qg3.F90:508-512),
+// interface_velocity (:1163-1194), thickness (:1197-1227), the dt-weighted
+// products (add_eddy_covariance_*_scale, :1360-1427) and
+// add_scaled_buoyancy_corr (:1430-1537).  The reference zeroes every
+// accumulator but ut, vt, rt and tt (qg3.F90:540-558), which it leaves
+// uninitialised; here all start at 0.
+static void accumulate_quad(or_model& m, int lv) {
+    const Decomp& d = m.d;
+    const int L = d.layers, ii = d.ii, jj = d.jj;
+    V3 psi = m.full(m.psi[lv]), rel = m.full(m.rel[lv]), zeta = m.full(m.zeta[lv]);
+    auto sd = [&](V3& a, int i, int j, int l) -> double& { return a(i + 1, j + 1, l); };
+    std::vector<double> uv(m.nsd(), 0.0), vv(m.nsd(), 0.0), tv(m.nsd(), 0.0);
+    V3 u = m.sdv(uv), v = m.sdv(vv), t = m.sdv(tv);
+    const double nanv = std::numeric_limits<double>::quiet_NaN();
+    for (int l = 1; l <= L; ++l)
+        for (int j = d.f_j_min; j <= d.f_j_max; ++j)
+            for (int i = d.f_i_min; i <= d.f_i_max; ++i) u(i - 1, j - 1, l) = 0.5 * (psi(i + 1, j, l) - psi(i - 1, j, l));
+    for (int l = 1; l <= L; ++l)
+        for (int j = d.f_j_min; j <= d.f_j_max; ++j) {
+            double w1, w2;
+            if (m.p.bc_type == OR_BC_PARTIAL_SLIP) {
+                w1 = sd(rel, 1, j - 1, l) / m.p.alpha;
+                w2 = sd(rel, ii, j - 1, l) / m.p.alpha;
+            } else if (m.p.bc_type == OR_BC_NO_SLIP) {
+                w1 = w2 = 0.0;
+            } else {
+                w1 = w2 = nanv;
+            }
+            if (d.p_b == -1) u(1, j - 1, l) = w1;
+            if (d.p_d == -1) u(ii, j - 1, l) = w2;
+        }
+    for (int l = 1; l <= L; ++l)
+        for (int j = d.f_j_min; j <= d.f_j_max; ++j)
+            for (int i = d.f_i_min; i <= d.f_i_max; ++i) v(i - 1, j - 1, l) = 0.5 * (psi(i, j + 1, l) - psi(i, j - 1, l));
+    for (int l = 1; l <= L; ++l)
+        for (int i = d.f_i_min; i <= d.f_i_max; ++i) {
+            double w1, w2;
+            if (m.p.bc_type == OR_BC_PARTIAL_SLIP) {
+                w1 = sd(rel, i - 1, 1, l) / m.p.alpha;
+                w2 = sd(rel, i - 1, jj, l) / m.p.alpha;
+            } else if (m.p.bc_type == OR_BC_NO_SLIP) {
+                w1 = w2 = 0.0;
+            } else {
+                w1 = w2 = nanv;
+            }
+            if (d.p_c == -1) v(i - 1, 1, l) = w1;
+            if (d.p_a == -1) v(i - 1, jj, l) = w2;
+        }
+    if (L > 1) {
+        for (int j = 1; j <= jj; ++j)
+            for (int i = 1; i <= ii; ++i) {
+                t(i, j, 1) = -m.s2[0] * (sd(psi, i, j, 1) - sd(psi, i, j, 2));
+                t(i, j, L) = -m.s1[L - 1] * (sd(psi, i, j, L) - sd(psi, i, j, L - 1));
+            }
+        for (int l = 2; l <= L - 1; ++l)
+            for (int j = 1; j <= jj; ++j)
+                for (int i = 1; i <= ii; ++i)
+                    t(i, j, l) = -m.s1[l - 1] * (sd(psi, i, j, l) - sd(psi, i, j, l - 1)) -
+                                 m.s2[l - 1] * (sd(psi, i, j, l) - sd(psi, i, j, l + 1));
+    }
+    const double dt = m.dt;
+    auto acc = [&](int q, int i, int j, int l) -> double& {
+        return m.quad[q][(size_t)(i - 1) + (size_t)ii * ((size_t)(j - 1) + (size_t)jj * (size_t)(l - 1))];
+    };
+    for (int l = 1; l <= L; ++l)
+        for (int j = 1; j <= jj; ++j)
+            for (int i = 1; i <= ii; ++i) {
+                const double U = u(i, j, l), Vv = v(i, j, l), R = sd(rel, i, j, l), Z = sd(zeta, i, j, l);
+                const double Pp = sd(psi, i, j, l), T = t(i, j, l);
+                acc(0, i, j, l) += dt * U * U;
+                acc(1, i, j, l) += dt * Vv * Vv;
+                acc(4, i, j, l) += dt * U * Vv;
+                acc(5, i, j, l) += dt * U * R;
+                acc(6, i, j, l) += dt * Vv * R;
+                acc(7, i, j, l) += dt * R * R;
+                acc(8, i, j, l) += dt * Pp * R;
+                acc(9, i, j, l) += dt * U * Z;
+                acc(10, i, j, l) += dt * Vv * Z;
+                acc(11, i, j, l) += dt * Z * Z;
+                acc(12, i, j, l) += dt * Z * R;
+                acc(13, i, j, l) += dt * Pp * Pp;
+                acc(14, i, j, l) += dt * Pp * Z;
+                acc(15, i, j, l) += dt * U * T;
+                acc(16, i, j, l) += dt * Vv * T;
+                acc(17, i, j, l) += dt * T * R;
+                acc(18, i, j, l) += dt * T * T;
+            }
+    for (int l = 1; l <= L - 1; ++l)
+        for (int j = 1; j <= jj; ++j)
+            for (int i = 1; i <= ii; ++i) {
+                const double ui = 0.5 * (u(i, j, l) + u(i, j, l + 1)), vi = 0.5 * (v(i, j, l) + v(i, j, l + 1));
+                acc(2, i, j, l) += dt * ui * ui;
+                acc(3, i, j, l) += dt * vi * vi;
+            }
+    if (L == 1) return;
+    for (int l = 1; l <= L - 1; ++l)
+        for (int j = 1; j <= jj; ++j)
+            for (int i = 1; i <= ii; ++i) {
+                const double dp = sd(psi, i, j, l) - sd(psi, i, j, l + 1);
+                const double sc_b = m.s2[l - 1] * m.h[l - 1] * dp;
+                acc(19, i, j, l) += dt * (0.5 * (u(i, j, l + 1) + u(i, j, l)) * sc_b);
+                acc(20, i, j, l) += dt * (0.5 * (v(i, j, l + 1) + v(i, j, l)) * sc_b);
+                acc(22, i, j, l) += dt * (m.s2[l - 1] * m.h[l - 1] * (dp * dp) / (m.h[l - 1] + m.h[l]));
+            }
+    for (int j = 1; j <= jj; ++j)
+        for (int i = 1; i <= ii; ++i) {
+            const double a = sd(psi, i, j, 2) - sd(psi, i, j, 1);
+            acc(21, i, j, 1) += dt * (0.25 * (m.s2[0] * (a * a)));
+        }
+    for (int l = 2; l <= L - 1; ++l)
+        for (int j = 1; j <= jj; ++j)
+            for (int i = 1; i <= ii; ++i) {
+                const double a = sd(psi, i, j, l - 1) - sd(psi, i, j, l), b = sd(psi, i, j, l + 1) - sd(psi, i, j, l);
+                acc(21, i, j, l) += dt * (0.25 * (m.s1[l - 1] * (a * a) + m.s2[l - 1] * (b * b)));
+            }
+    for (int j = 1; j <= jj; ++j)
+        for (int i = 1; i <= ii; ++i) {
+            const double a = sd(psi, i, j, L - 1) - sd(psi, i, j, L);
+            acc(21, i, j, L) += dt * (0.25 * (m.s1[L - 1] * (a * a)));
+        }
+}
+
+// Start (clearing the sums, qg3.F90:502-503, 540-558) or stop the time
+// average; enable = 2 adds the quad eddy covariances.
 void or_model_average(or_model* m, int enable, double threshold) {
     m->av_on = enable != 0;
+    m->quad_on = enable == 2;
     m->av_threshold = threshold;
     m->diag_time = 0.0;
     m->psi_av.assign(m->nsd(), 0.0);
+    for (int q = 0; q < 23; ++q)
+        m->quad[q].assign(m->quad_on ? (size_t)m->d.ii * m->d.jj * quad_layers(*m, q) : 0, 0.0);
+}
+
+// Quad accumulator q (ii, jj, layers of q), unscaled; returns its length.
+long or_model_get_quad(or_model* m, int q, double* out) {
+    if (q < 0 || q >= 23 || !m->quad_on) return -1;
+    if (out) std::memcpy(out, m->quad[q].data(), m->quad[q].size() * sizeof(double));
+    return (long)m->quad[q].size();
 }
 
 // The summed dt * psi (ii, jj, L) and diagnostic_time.

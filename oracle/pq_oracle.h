@@ -128,6 +128,10 @@ int or_model_finish_step(or_model* m);
  * threshold = max_spin - start_time add dt * psi.  get returns
  * diagnostic_time and copies the sum (ii, jj, L). */
 void or_model_average(or_model* m, int enable, double threshold);
+/* enable = 2 also accumulates the 23 quad eddy covariances (qg3.F90:683-721);
+ * or_model_get_quad copies accumulator q (output order) unscaled and returns
+ * its length, or -1. */
+long or_model_get_quad(or_model* m, int q, double* out);
 double or_model_get_average(or_model* m, double* sum);
 /* Checkpoint pickup (qg3.F90:314-363, :448-497) on fields loaded with
  * or_model_set; dt is the checkpoint's (CABARET; ignored for leapfrog). */

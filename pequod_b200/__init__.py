@@ -104,6 +104,8 @@ SIGNATURES = {
     "pq_average": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "pq_get_average": (C.c_int, [C.c_void_p, _dp, _dp]),
     "pq_write_average": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double]),
+    "pq_get_quad": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "pq_write_quad": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double]),
     "pq_read_checkpoint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, _dp]),
     "pq_stream": (C.c_void_p, [C.c_void_p]),
     "pq_last_launch_count": (C.c_long, [C.c_void_p]),
@@ -383,9 +385,24 @@ class Model:
         _check(lib().pq_read_checkpoint(self.ctx, s_path.encode(), supp, _p(ttd)), self.ctx)
         return float(ttd[0])
 
-    def average(self, enable: bool = True, threshold: float = 0.0) -> None:
-        """Start (clearing) or stop the time average of psi (psi_av)."""
+    QUAD = ("uu", "vv", "uu_i", "vv_i", "uv", "ur", "vr", "rr", "pr", "uz", "vz", "zz", "zr", "pp", "pz", "ut", "vt",
+            "rt", "tt", "sc_ub", "sc_vb", "sc_bb", "sc_bb_i")
+
+    def average(self, enable=True, threshold: float = 0.0) -> None:
+        """Start (clearing) or stop the time average of psi (psi_av);
+        enable = 2 also accumulates the quad eddy covariances."""
         _check(lib().pq_average(self.ctx, int(enable), float(threshold)), self.ctx)
+
+    def get_quad(self, q: int) -> np.ndarray:
+        """Quad accumulator q (QUAD order) / diagnostic_time, (ii, jj, layers)."""
+        L = self.cfg.layers - 1 if self.QUAD[q] in ("uu_i", "vv_i", "sc_ub", "sc_vb", "sc_bb_i") else self.cfg.layers
+        out = np.zeros((self.cfg.ii, self.cfg.jj, L), order="F")
+        _check(lib().pq_get_quad(self.ctx, int(q), _p(out)), self.ctx)
+        return out
+
+    def write_quad(self, path: str, t_scale: float = 1.0, start_time_day: float = 0.0) -> None:
+        """The reference's qg<L>_<ii>_quad_av.d file of the current sums."""
+        _check(lib().pq_write_quad(self.ctx, path.encode(), t_scale, start_time_day), self.ctx)
 
     def get_average(self):
         """(psi_av / diagnostic_time as sdata (ii, jj, L), diagnostic_time)."""

@@ -202,6 +202,7 @@ int run_step(pq_ctx* c, int par) {
     if (ev) CK(cudaEventRecord(ev[2], c->stream));
     CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[3], c->stream));
+    if (c->quad) CK(launch_quad(c->ls[par], f32, c->stream));
     CK(launch_cabaret_fused(c->ls[par], c->fuse ? 1 : 0, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[4], c->stream));
     c->pred_ready = c->fuse;
@@ -229,6 +230,7 @@ void pq_destroy(pq_ctx* c) {
         if (g) cudaGraphExecDestroy(g);
     if (c->arena) cudaFree(c->arena);
     if (c->psi_av) cudaFree(c->psi_av);
+    if (c->quad) cudaFree(c->quad);
     if (c->x.in) {
         cudaStreamSynchronize(c->x.in);
         cudaStreamSynchronize(c->x.out);
@@ -821,8 +823,9 @@ int pq_init_perturb(pq_ctx* c, const double* zeta_ic, int ptr_kind) {
     sc.tweight_u_last = sc.tweight_u;
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
-    // diagnostic_time = 0, psi_av = 0 (qg3.F90:502-503)
+    // diagnostic_time = 0, psi_av = 0, the quad sums 0 (qg3.F90:502-503, 540-558)
     if (c->psi_av) CK(cudaMemsetAsync(c->psi_av, 0, c->field_bytes, c->stream));
+    if (c->quad) CK(cudaMemsetAsync(c->quad, 0, 23 * c->field_bytes, c->stream));
     // zeta was cleared together with the other fields; upload it again.
     rc = copy_in_state(c, m.zeta, z.data(), PQ_PTR_HOST);
     if (rc) return rc;
@@ -1144,6 +1147,7 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc) {
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
     if (c->psi_av) CK(cudaMemsetAsync(c->psi_av, 0, c->field_bytes, c->stream));
+    if (c->quad) CK(cudaMemsetAsync(c->quad, 0, 23 * c->field_bytes, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->cur = 0;
     c->zpar = 0;
@@ -1151,7 +1155,9 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc) {
     return PQ_OK;
 }
 
-int step_launches(const pq_ctx* c) { return c->leapfrog ? (c->psi_av ? 6 : 5) : c->periodic ? 7 : 4; }
+int step_launches(const pq_ctx* c) {
+    return c->leapfrog ? (c->psi_av ? 6 : 5) : c->periodic ? 7 : (c->quad ? 5 : 4);
+}
 
 int read_scalars(pq_ctx* c, Scalars* sc) {
     CK(cudaSetDevice(c->device));

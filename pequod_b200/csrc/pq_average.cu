@@ -7,6 +7,7 @@
 // (the layout of psi) added to inside the fused CABARET kernel (the leapfrog
 // scheme: one small kernel per sub-step), so a step costs one extra read and
 // write of the sum and no launch; the host only starts, reads and writes it.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -40,11 +41,25 @@ bool put_record(FILE* f, const double* p, size_t n) {
 extern "C" {
 
 int pq_average(pq_ctx* c, int enable, double threshold) {
-    if (!c) return PQ_ERR_ARG;
+    if (!c || enable < 0 || enable > 2) return PQ_ERR_ARG;
     if (c->helm_only) return fail(c, PQ_ERR_UNSUPPORTED, "no time loop on this context");
     if (c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "the channel step does not accumulate the time average");
+    if (enable == 2 && c->leapfrog)
+        return fail(c, PQ_ERR_UNSUPPORTED, "the quad covariances are accumulated by the CABARET step only");
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
+    if (enable == 2 && !c->quad) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, 23 * c->field_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, PQ_ERR_NOMEM, "cudaMalloc of the quad accumulators failed");
+        }
+        c->quad = static_cast<double*>(p);
+    } else if (enable != 2 && c->quad) {
+        CK(cudaFree(c->quad));
+        c->quad = nullptr;
+    }
+    if (c->quad) CK(cudaMemsetAsync(c->quad, 0, 23 * c->field_bytes, c->stream));
     if (enable && !c->psi_av) {
         void* p = nullptr;
         if (cudaMalloc(&p, c->field_bytes) != cudaSuccess) {
@@ -60,6 +75,8 @@ int pq_average(pq_ctx* c, int enable, double threshold) {
     for (int p = 0; p < 2; ++p) {
         c->hm[p].psi_av = c->psi_av;
         c->hm[p].av_threshold = threshold;
+        c->hm[p].quad = c->quad;
+        c->hm[p].quad_stride = (long long)(c->field_bytes / sizeof(double));
     }
     int rc = upload_members(c);
     if (rc) return rc;
@@ -68,7 +85,8 @@ int pq_average(pq_ctx* c, int enable, double threshold) {
     sc.diag_time = 0.0;
     CK(cudaMemcpyAsync(c->d_sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    // The leapfrog step gains or loses a kernel: capture its graphs again.
+    // The leapfrog step (average) or the CABARET step (quad) gains or loses
+    // a kernel: capture the graphs again.
     drop_graphs(c);
     return PQ_OK;
 }
@@ -87,6 +105,56 @@ int pq_get_average(pq_ctx* c, double* psi_av, double* diagnostic_time) {
     const double cff = 1.0 / sc.diag_time;  // qg3.F90:891
     const size_t n = (size_t)c->ii * c->jj * c->L;
     for (size_t k = 0; k < n; ++k) psi_av[k] = psi_av[k] * cff;
+    return PQ_OK;
+}
+
+// Layers of quad accumulator q: the interface ones (uu_i, vv_i, sc_ub,
+// sc_vb, sc_bb_i) have L - 1.
+static int quad_layers(const pq_ctx* c, int q) {
+    return (q == 2 || q == 3 || q == 19 || q == 20 || q == 22) ? c->L - 1 : c->L;
+}
+
+int pq_get_quad(pq_ctx* c, int q, double* out) {
+    if (!c || q < 0 || q >= 23 || !out) return PQ_ERR_ARG;
+    if (!c->quad) return fail(c, PQ_ERR_STATE, "the quad covariances are not on (pq_average mode 2)");
+    Scalars sc;
+    int rc = read_scalars(c, &sc);
+    if (rc) return rc;
+    if (!(sc.diag_time > 0.0)) return fail(c, PQ_ERR_STATE, "no step has entered the time average yet");
+    const int nl = quad_layers(c, q);
+    if (nl <= 0) return PQ_OK;
+    const size_t w = (size_t)c->ii * sizeof(double);
+    CK(cudaMemcpy2DAsync(out, w, c->quad + (size_t)q * (c->field_bytes / sizeof(double)),
+                         (size_t)c->pitch * sizeof(double), w, (size_t)c->jj * nl, cudaMemcpyDeviceToHost,
+                         c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double cff = 1.0 / sc.diag_time;  // qg3.F90:891
+    const size_t n = (size_t)c->ii * c->jj * nl;
+    for (size_t k = 0; k < n; ++k) out[k] = out[k] * cff;
+    return PQ_OK;
+}
+
+int pq_write_quad(pq_ctx* c, const char* path, double t_scale, double start_time_day) {
+    if (!c || !path) return PQ_ERR_ARG;
+    if (!c->quad) return fail(c, PQ_ERR_STATE, "the quad covariances are not on (pq_average mode 2)");
+    double sc4[4];
+    int rc = pq_get_scalars(c, sc4);
+    if (rc) return rc;
+    const double model_time_day = (sc4[3] - 0.5 * sc4[0]) * t_scale / 86400.0;
+    const double total_time_day = start_time_day + model_time_day;
+    std::vector<std::vector<double>> f(23);
+    for (int q = 0; q < 23; ++q) {
+        f[q].assign((size_t)c->ii * c->jj * std::max(quad_layers(c, q), 0), 0.0);
+        if ((rc = pq_get_quad(c, q, f[q].data()))) return rc;
+    }
+    // qg3.F90:903-929: the two times, then each accumulator's whole data
+    // array times 1 / diagnostic_time as one record.
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(c, PQ_ERR_ARG, std::string("Failed to open output file ") + path);
+    bool ok = put_record(fp, &model_time_day, 1) && put_record(fp, &total_time_day, 1);
+    for (int q = 0; q < 23 && ok; ++q) ok = put_record(fp, f[q].data(), f[q].size());
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(c, PQ_ERR_ARG, std::string("write failed: ") + path);
     return PQ_OK;
 }
 

@@ -1256,6 +1256,116 @@ cudaError_t launch_cabaret_channel(const LaunchSet& ls, int f32, cudaStream_t st
 
 int channel_ctas(int ii, int jj) { return ((ii + 127) / 128) * jj; }
 
+
+// ---------------------------------------------------------------------------
+// The quad eddy covariances of a step (qg3.F90:683-721), at the point of the
+// reference's diagnostics: psi of the inversion, rel (rel_from_zeta_and_psi
+// with its boundary condition) and zeta with its boundary PV.  The zonal and
+// meridional velocities (qg3p_diagnostics.F90:941-1107) are 0 on the nodes
+// the reference never writes, rel / alpha, 0 or NaN on the walls by the
+// velocity boundary condition; interface velocities (:1163-1194), thickness
+// (:1197-1227), the dt-weighted products (:1360-1427) and the scaled
+// buoyancy correlations (:1430-1537).  One thread per node, all layers.
+// Launched before the step's CABARET kernel, so the model-time gate is the
+// one the fused kernel uses for psi_av.
+template <typename T>
+__global__ void k_quad(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
+    int local;
+    const int mi = find_member(prefix, nmem, blockIdx.y, &local);
+    const Member& Mb = mems[mi];
+    if (Mb.quad == nullptr || !cab_average_gate(Mb)) return;
+    const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
+    const long long ls = Mb.lstride, qs = Mb.quad_stride;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = local;
+    if (i >= ii) return;
+    const double dt = Mb.sc->dt;
+    const T* zp = reinterpret_cast<const T*>(Mb.zeta);
+    auto ps = [&](int a, int b, int l) { return Mb.psi[(long long)b * pitch + a + l * ls]; };
+    const long long o = (long long)j * pitch + i;
+    const bool in_i = i > 0 && i < ii - 1, in_j = j > 0 && j < jj - 1;
+    const int bc = Mb.bc_type;  // u, v on a wall from rel: rel / alpha, 0, or NaN
+    double P[PQ_MAXL], R[PQ_MAXL], Z[PQ_MAXL], U[PQ_MAXL], V[PQ_MAXL], Tn[PQ_MAXL];
+#pragma unroll
+    for (int l = 0; l < PQ_MAXL; ++l) {
+        if (l >= L) break;
+        P[l] = ps(i, j, l);
+        const double r = rel_node(Mb, ps, (in_i && in_j) ? (double)zp[o + l * ls] : 0.0, i, j, l);
+        R[l] = r;
+        Z[l] = (in_i && in_j) ? (double)zp[o + l * ls] : zeta_bc_node(Mb, ps, r, i, j, l);
+        auto wall = [&]() { return bc == 1 ? r / Mb.alpha : bc == 2 ? 0.0 : __longlong_as_double(0x7ff8000000000000LL); };
+        U[l] = (in_i && in_j) ? 0.5 * (ps(i + 1, j, l) - ps(i - 1, j, l)) : (in_j ? wall() : 0.0);
+        V[l] = (in_i && in_j) ? 0.5 * (ps(i, j + 1, l) - ps(i, j - 1, l)) : (in_i ? wall() : 0.0);
+    }
+#pragma unroll
+    for (int l = 0; l < PQ_MAXL; ++l) {
+        if (l >= L) break;
+        if (L == 1)
+            Tn[l] = 0.0;
+        else if (l == 0)
+            Tn[l] = -Mb.s2[0] * (P[0] - P[1]);
+        else if (l == L - 1)
+            Tn[l] = -Mb.s1[l] * (P[l] - P[l - 1]);
+        else
+            Tn[l] = -Mb.s1[l] * (P[l] - P[l - 1]) - Mb.s2[l] * (P[l] - P[l + 1]);
+    }
+    double* q = Mb.quad + o;
+    auto add = [&](int f, int l, double v) { q[f * qs + l * ls] += v; };
+#pragma unroll
+    for (int l = 0; l < PQ_MAXL; ++l) {
+        if (l >= L) break;
+        add(0, l, dt * U[l] * U[l]);
+        add(1, l, dt * V[l] * V[l]);
+        add(4, l, dt * U[l] * V[l]);
+        add(5, l, dt * U[l] * R[l]);
+        add(6, l, dt * V[l] * R[l]);
+        add(7, l, dt * R[l] * R[l]);
+        add(8, l, dt * P[l] * R[l]);
+        add(9, l, dt * U[l] * Z[l]);
+        add(10, l, dt * V[l] * Z[l]);
+        add(11, l, dt * Z[l] * Z[l]);
+        add(12, l, dt * Z[l] * R[l]);
+        add(13, l, dt * P[l] * P[l]);
+        add(14, l, dt * P[l] * Z[l]);
+        add(15, l, dt * U[l] * Tn[l]);
+        add(16, l, dt * V[l] * Tn[l]);
+        add(17, l, dt * Tn[l] * R[l]);
+        add(18, l, dt * Tn[l] * Tn[l]);
+        if (l < L - 1) {
+            const double ui = 0.5 * (U[l] + U[l + 1]), vi = 0.5 * (V[l] + V[l + 1]);
+            add(2, l, dt * ui * ui);
+            add(3, l, dt * vi * vi);
+            const double dp = P[l] - P[l + 1];
+            const double scb = Mb.s2[l] * Mb.h[l] * dp;
+            add(19, l, dt * (0.5 * (U[l + 1] + U[l]) * scb));
+            add(20, l, dt * (0.5 * (V[l + 1] + V[l]) * scb));
+            add(22, l, dt * (Mb.s2[l] * Mb.h[l] * (dp * dp) / (Mb.h[l] + Mb.h[l + 1])));
+        }
+        if (L > 1) {
+            double sbb;
+            if (l == 0) {
+                const double a = P[1] - P[0];
+                sbb = 0.25 * (Mb.s2[0] * (a * a));
+            } else if (l == L - 1) {
+                const double a = P[l - 1] - P[l];
+                sbb = 0.25 * (Mb.s1[l] * (a * a));
+            } else {
+                const double a = P[l - 1] - P[l], b = P[l + 1] - P[l];
+                sbb = 0.25 * (Mb.s1[l] * (a * a) + Mb.s2[l] * (b * b));
+            }
+            add(21, l, dt * sbb);
+        }
+    }
+}
+
+cudaError_t launch_quad(const LaunchSet& ls, int f32, cudaStream_t st) {
+    const dim3 g((ls.maxI + 127) / 128, ls.maxJ * ls.nmem);
+    if (f32)
+        k_quad<float><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    else
+        k_quad<double><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, int f32, cudaStream_t st) {
     if (f32) return predict_next ? launch_cab<true, float>(ls, st) : launch_cab<false, float>(ls, st);
     return predict_next ? launch_cab<true, double>(ls, st) : launch_cab<false, double>(ls, st);

@@ -143,6 +143,11 @@ struct Member {
     // and dt to the scalars' diag_time.
     double* psi_av;
     double av_threshold;
+    // The quad eddy covariances (qg3.F90:683-721) when on: 23 accumulator
+    // fields node-shaped like psi, quad_stride doubles apart, in the
+    // reference's output order.
+    double* quad;
+    long long quad_stride;
 };
 
 // Programmatic dependent launch: the step kernels are launched so that the

@@ -52,6 +52,7 @@ struct pq_ctx {
     int ii = 0, jj = 0, L = 0, pitch = 0;
     size_t field_bytes = 0;  // bytes of one L-layer field
     double* psi_av = nullptr;  // time average of psi (pq_average), FP64, node-shaped like psi
+    double* quad = nullptr;    // the 23 quad eddy-covariance accumulators (pq_average mode 2)
     // Pipelined host exchange (pq_step_exchange with host buffers): the
     // copies run on their own streams through two dense device staging slots
     // each way, so that a step's input and output transfers overlap the

@@ -209,3 +209,78 @@ def test_oracle_time_average(scheme):
     got, t = o.get_average()
     assert t == dtime and dtime > 0 and dtime < 7 * dt
     np.testing.assert_allclose(got, want / dtime, rtol=1e-14, atol=0)
+
+
+def numpy_quad_terms(psi, rel, zeta, cfg):
+    """qg3.F90:683-721 in numpy on sdata (ii, jj, L): the 23 products."""
+    oc = cfg.oracle_cfg()
+    ii, jj, L = psi.shape
+    bc, alpha = oc["bc_type"], oc["alpha"]
+    s1, s2, h = np.array(oc["s1"]), np.array(oc["s2"]), np.array(oc["h"])
+    u = np.zeros_like(psi)
+    v = np.zeros_like(psi)
+    u[1:-1, 1:-1] = 0.5 * (psi[2:, 1:-1] - psi[:-2, 1:-1])
+    v[1:-1, 1:-1] = 0.5 * (psi[1:-1, 2:] - psi[1:-1, :-2])
+    wall = {pq.BC_PARTIAL_SLIP: None, pq.BC_NO_SLIP: 0.0, pq.BC_FREE_SLIP: np.nan}[bc]
+    if wall is None:
+        u[0, 1:-1], u[-1, 1:-1] = rel[0, 1:-1] / alpha, rel[-1, 1:-1] / alpha
+        v[1:-1, 0], v[1:-1, -1] = rel[1:-1, 0] / alpha, rel[1:-1, -1] / alpha
+    else:
+        u[0, 1:-1] = u[-1, 1:-1] = wall
+        v[1:-1, 0] = v[1:-1, -1] = wall
+    t = np.zeros_like(psi)
+    if L > 1:
+        t[:, :, 0] = -s2[0] * (psi[:, :, 0] - psi[:, :, 1])
+        t[:, :, -1] = -s1[L - 1] * (psi[:, :, -1] - psi[:, :, -2])
+        for l in range(1, L - 1):
+            t[:, :, l] = -s1[l] * (psi[:, :, l] - psi[:, :, l - 1]) - s2[l] * (psi[:, :, l] - psi[:, :, l + 1])
+    ui = 0.5 * (u[:, :, :-1] + u[:, :, 1:])
+    vi = 0.5 * (v[:, :, :-1] + v[:, :, 1:])
+    dp = psi[:, :, :-1] - psi[:, :, 1:]
+    scb = s2[:-1] * h[:-1] * dp
+    sc_bb = np.zeros_like(psi)
+    sc_bb[:, :, 0] = 0.25 * (s2[0] * (psi[:, :, 1] - psi[:, :, 0]) ** 2)
+    for l in range(1, L - 1):
+        sc_bb[:, :, l] = 0.25 * (s1[l] * (psi[:, :, l - 1] - psi[:, :, l]) ** 2 + s2[l] * (psi[:, :, l + 1] - psi[:, :, l]) ** 2)
+    sc_bb[:, :, -1] = 0.25 * (s1[L - 1] * (psi[:, :, -2] - psi[:, :, -1]) ** 2)
+    return [u * u, v * v, ui * ui, vi * vi, u * v, u * rel, v * rel, rel * rel, psi * rel, u * zeta, v * zeta,
+            zeta * zeta, zeta * rel, psi * psi, psi * zeta, u * t, v * t, t * rel, t * t,
+            0.5 * (u[:, :, 1:] + u[:, :, :-1]) * scb, 0.5 * (v[:, :, 1:] + v[:, :, :-1]) * scb, sc_bb,
+            s2[:-1] * h[:-1] * dp ** 2 / (h[:-1] + h[1:])]
+
+
+@pytest.mark.parametrize("partial_slip", [True, False])
+def test_oracle_quad_diagnostics(partial_slip):
+    """The quad eddy covariances (qg3.F90:683-721, qg3p_diagnostics.F90:941-1537)
+    of the oracle against a numpy statement, over steps with and without the
+    threshold passed."""
+    cfg = double_gyre(17, 3, partial_slip=partial_slip)
+    o = run_oracle(cfg, 1, seed=7)
+    dt = cfg.oracle_cfg()["dt"]
+    thr = o.scalars()["model_time"] + 1.2 * dt
+    o.average(2, thr)
+    acc = None
+    dtime = 0.0
+    for k in range(5):
+        o.step_to_dump()
+        t = o.scalars()["model_time"]
+        if t > thr:
+            # zeta at the diagnostics (before the forcing the dump point
+            # includes): rel minus the stratification coupling, the inverse
+            # of rel_from_zeta_and_psi / update_zeta_bc
+            psi, rel = o.sdata("psi"), o.sdata("rel")
+            oc = cfg.oracle_cfg()
+            s1, s2 = np.array(oc["s1"]), np.array(oc["s2"])
+            zeta = rel.copy()
+            zeta[:, :, 0] -= s2[0] * (psi[:, :, 0] - psi[:, :, 1])
+            zeta[:, :, 1] -= s1[1] * (psi[:, :, 1] - psi[:, :, 0]) + s2[1] * (psi[:, :, 1] - psi[:, :, 2])
+            zeta[:, :, 2] -= s1[2] * (psi[:, :, 2] - psi[:, :, 1])
+            terms = numpy_quad_terms(psi, rel, zeta, cfg)
+            acc = [dt * x for x in terms] if acc is None else [a + dt * x for a, x in zip(acc, terms)]
+            dtime += dt
+        o.finish_step()
+    for q, want in enumerate(acc):
+        got = o.get_quad(q)
+        assert got.shape == want.shape, (q, got.shape, want.shape)
+        np.testing.assert_allclose(got, want / dtime, rtol=1e-9, atol=1e-12 * np.abs(want).max() / dtime,
+                                   err_msg=O.Model.QUAD[q])

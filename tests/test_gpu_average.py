@@ -106,3 +106,58 @@ def test_leapfrog_average_matches_oracle():
     a_o, t_o = o.get_average()
     assert abs(t_g - t_o) <= 1e-12 * t_o
     assert rel_l2(a_g, a_o) <= 1e-12
+
+
+@pytest.mark.parametrize("kernel,partial_slip,prec", [(0, True, pq.PREC_FP64), (1, False, pq.PREC_FP64),
+                                                      (0, True, pq.PREC_MIXED)])
+def test_quad_covariances_match_oracle(kernel, partial_slip, prec):
+    """The 23 quad eddy covariances (qg3.F90:683-721) on the device against
+    the oracle, with the model-time threshold passed mid-run."""
+    cfg = double_gyre(129, 3, precision=prec, partial_slip=partial_slip)
+    g, o = start(cfg, seed=44)
+    g.set_tuning(cab_kernel=kernel, cab_band=16, dst_group=0)
+    g.step(1)
+    o.step(1)
+    thr = o.scalars()["model_time"] + 1.7 * cfg.desc.dt
+    g.average(2, thr)
+    o.average(2, thr)
+    for n in (1, 2, 3):
+        g.step(n)
+        o.step(n)
+    assert g.last_launch_count() == 3 * 5    # the covariances add one kernel per step
+    tol = 1e-11 if prec == pq.PREC_FP64 else 1e-5
+    worst = {}
+    for q, name in enumerate(g.QUAD):
+        a, b = g.get_quad(q), o.get_quad(q)
+        assert a.shape == b.shape, name
+        worst[name] = rel_l2(a, b)
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, worst
+    a_g, t_g = g.get_average()
+    a_o, t_o = o.get_average()
+    assert abs(t_g - t_o) <= 1e-12 * t_o
+
+
+def test_quad_free_slip_walls_and_file(tmp_path):
+    """Free slip leaves the wall velocities NaN (the reference's nan()), so
+    the velocity products are NaN on those nodes on both sides; the
+    _quad_av file holds the two times and 23 whole-array records."""
+    cfg = double_gyre(65, 2, partial_slip=True, alpha=1.0e300)
+    assert cfg.desc.bc_type == pq.BC_FREE_SLIP
+    g, o = start(cfg, seed=45)
+    g.average(2, 0.0)
+    o.average(2, 0.0)
+    g.step(3)
+    o.step(3)
+    for q in range(23):
+        a, b = g.get_quad(q), o.get_quad(q)
+        np.testing.assert_array_equal(np.isnan(a), np.isnan(b), err_msg=g.QUAD[q])
+        m = ~np.isnan(b)
+        assert rel_l2(a[m], b[m]) <= 1e-11, g.QUAD[q]
+    assert np.isnan(g.get_quad(0)).any() and not np.isnan(g.get_quad(13)).any()
+    path = str(tmp_path / "qg2_65_quad_av.d")
+    g.write_quad(path, t_scale=cfg.t_scale)
+    recs = O._records(path)
+    assert len(recs) == 2 + 23
+    assert [r.size for r in recs[2:]] == [65 * 65 * (1 if n in ("uu_i", "vv_i", "sc_ub", "sc_vb", "sc_bb_i") else 2)
+                                          for n in g.QUAD]
