@@ -430,12 +430,17 @@ def _write_records(path, recs):
             f.write(n.tobytes() + r.tobytes() + n.tobytes())
 
 
-def _face_ranges(ii, jj):
-    # 0-based slices of the FLUX_II / FLUX_JJ reference-layout arrays.
-    return (slice(2, ii + 1), slice(2, jj)), (slice(2, ii), slice(2, jj + 1))
+def _face_ranges(ii, jj, periodic_j=False):
+    # 0-based slices of the saved FLUX_II / FLUX_JJ faces (qg3.F90:864-875):
+    # rows fa_j_min+1 .. fa_j_max-1 and faces fa_j_min+1 .. fa_j_max, where a
+    # channel (its own j neighbour) has fa_j_min = 1, fa_j_max = jj + 2 and a
+    # closed basin fa_j_min = 2, fa_j_max = jj + 1 (qg3p_base.F90:893-918).
+    lo = 1 if periodic_j else 2
+    hi = jj + 1 if periodic_j else jj
+    return (slice(2, ii + 1), slice(lo, hi)), (slice(2, ii), slice(lo, hi + 1))
 
 
-def read_checkpoint(s_path, supp_path, ii, jj, L, leapfrog=False):
+def read_checkpoint(s_path, supp_path, ii, jj, L, leapfrog=False, periodic_j=False):
     """Parse a checkpoint into reference-layout arrays and the three times."""
     rs = _records(s_path)
     out = {"model_time_day": float(rs[0][0]), "total_time_day": float(rs[1][0])}
@@ -457,7 +462,7 @@ def read_checkpoint(s_path, supp_path, ii, jj, L, leapfrog=False):
     if rp[0][0] != out["model_time_day"] or rp[1][0] != out["total_time_day"]:
         raise ValueError("Input times do not match in CABARET checkpoint data")
     out["dt"] = float(rp[2][0])
-    (fi_i, fi_j), (fj_i, fj_j) = _face_ranges(ii, jj)
+    (fi_i, fi_j), (fj_i, fj_j) = _face_ranges(ii, jj, periodic_j)
     k = 3
     for name, shape, (si, sj) in (("ui", (ii + 3, jj + 2), (fi_i, fi_j)), ("uj", (ii + 2, jj + 3), (fj_i, fj_j)),
                                   ("zeta_fi", (ii + 3, jj + 2), (fi_i, fi_j)),
@@ -476,7 +481,8 @@ def read_checkpoint(s_path, supp_path, ii, jj, L, leapfrog=False):
     return out
 
 
-def write_checkpoint(s_path, supp_path, fields, model_time_day, total_time_day, dt=None, leapfrog=False):
+def write_checkpoint(s_path, supp_path, fields, model_time_day, total_time_day, dt=None, leapfrog=False,
+                     periodic_j=False):
     """Write reference-layout arrays as a checkpoint (the reference's writer)."""
     L = fields["psi"].shape[2]
     recs = [[model_time_day], [total_time_day]]
@@ -490,7 +496,7 @@ def write_checkpoint(s_path, supp_path, fields, model_time_day, total_time_day, 
     if leapfrog or supp_path is None:
         return
     ii, jj = fields["psi"].shape[0] - 2, fields["psi"].shape[1] - 2
-    (fi_i, fi_j), (fj_i, fj_j) = _face_ranges(ii, jj)
+    (fi_i, fi_j), (fj_i, fj_j) = _face_ranges(ii, jj, periodic_j)
     recs = [[model_time_day], [total_time_day], [dt]]
     for name, (si, sj) in (("ui", (fi_i, fi_j)), ("uj", (fj_i, fj_j)), ("zeta_fi", (fi_i, fi_j)),
                            ("zeta_fj", (fj_i, fj_j))):

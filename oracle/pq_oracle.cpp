@@ -2060,9 +2060,14 @@ int or_model_step(or_model* m, int nsteps) {
 int or_model_pickup(or_model* m, double dt) {
     if (m->p.scheme == 0) {
         m->dt = dt;
+        // qg3.F90:324-329: halos of psi and of the face PV (a channel's
+        // only; update(zeta_fi) has no neighbour in i on one rank).
+        update_pdata(*m, m->psi[0]);
+        update_flux_j(*m, m->zeta_fj, false);
         cabaret_cell_boundaries_velocity(*m);
         cabaret_flux(*m);
         cabaret_corrector(*m);
+        update_pdata(*m, m->zeta[0]);  // :339
         m->zeta_old[0] = m->zeta[0];
         m->model_time = m->dt / 2.0;
         m->tweight_a = 0.5;

@@ -188,6 +188,7 @@ int run_step(pq_ctx* c, int par) {
         if (ev) CK(cudaEventRecord(ev[2], c->stream));
         CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
         if (ev) CK(cudaEventRecord(ev[3], c->stream));
+        if (c->quad) CK(launch_quad(c->ls[par], f32, c->stream));
         CK(launch_cabaret_channel(c->ls[par], f32, c->stream));
         if (ev) CK(cudaEventRecord(ev[4], c->stream));
         c->pred_ready = false;
@@ -1156,7 +1157,7 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc) {
 }
 
 int step_launches(const pq_ctx* c) {
-    return c->leapfrog ? (c->psi_av ? 6 : 5) : c->periodic ? 7 : (c->quad ? 5 : 4);
+    return c->leapfrog ? (c->psi_av ? 6 : 5) : (c->periodic ? 7 : 4) + (c->quad ? 1 : 0);
 }
 
 int read_scalars(pq_ctx* c, Scalars* sc) {

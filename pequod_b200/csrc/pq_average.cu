@@ -4,9 +4,10 @@
 // whose model time exceeds max_spin, with diagnostic_time the summed dt
 // (qg3.F90:93, 502-503, 672-680, 725), and writes psi_av / diagnostic_time
 // to qg<L>_<ii>_s_av.d (:886-899).  Here the sum is a node-shaped FP64 field
-// (the layout of psi) added to inside the fused CABARET kernel (the leapfrog
-// scheme: one small kernel per sub-step), so a step costs one extra read and
-// write of the sum and no launch; the host only starts, reads and writes it.
+// (the layout of psi) added to inside the fused CABARET kernel (the channel:
+// inside its rel kernel; the leapfrog scheme: one small kernel per sub-step),
+// so a step costs one extra read and write of the sum and no launch; the
+// host only starts, reads and writes it.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -43,7 +44,6 @@ extern "C" {
 int pq_average(pq_ctx* c, int enable, double threshold) {
     if (!c || enable < 0 || enable > 2) return PQ_ERR_ARG;
     if (c->helm_only) return fail(c, PQ_ERR_UNSUPPORTED, "no time loop on this context");
-    if (c->periodic) return fail(c, PQ_ERR_UNSUPPORTED, "the channel step does not accumulate the time average");
     if (enable == 2 && c->leapfrog)
         return fail(c, PQ_ERR_UNSUPPORTED, "the quad covariances are accumulated by the CABARET step only");
     CK(cudaSetDevice(c->device));

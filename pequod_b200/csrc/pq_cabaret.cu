@@ -1024,12 +1024,16 @@ __global__ void k_ch_rel(const Member* __restrict__ mems, const int* __restrict_
     double* rel64 = reinterpret_cast<double*>(Mb.helm_io);
     auto ps = [&](int a, int b, int l) { return Mb.psi[(long long)b * Mb.pitch + a + l * Mb.lstride]; };
     const bool wall = (i == 0 || i == Mb.ii - 1);
+    // psi_av += dt * psi once model time passes the threshold (qg3.F90:672-680).
+    double* av = cab_average_gate(Mb) ? Mb.psi_av : nullptr;
+    const double dt = Mb.sc->dt;
     for (int l = 0; l < Mb.L; ++l) {
         const long long ol = o + l * Mb.lstride;
         const double r = rel_node(Mb, ps, (double)z[ol], i, j, l);
         rel[ol] = (T)r;
         rel64[ol] = r;
         if (wall) z[ol] = (T)zeta_bc_node(Mb, ps, r, i, j, l);
+        if (av) av[ol] = av[ol] + dt * Mb.psi[ol];
     }
 }
 
@@ -1282,7 +1286,11 @@ __global__ void k_quad(const Member* __restrict__ mems, const int* __restrict__ 
     const T* zp = reinterpret_cast<const T*>(Mb.zeta);
     auto ps = [&](int a, int b, int l) { return Mb.psi[(long long)b * pitch + a + l * ls]; };
     const long long o = (long long)j * pitch + i;
-    const bool in_i = i > 0 && i < ii - 1, in_j = j > 0 && j < jj - 1;
+    // A channel (periodic j) has no j walls: every row is interior and its
+    // j neighbours wrap.
+    const bool per = Mb.periodic != 0;
+    const bool in_i = i > 0 && i < ii - 1, in_j = per || (j > 0 && j < jj - 1);
+    const int jm = (per && j == 0) ? jj - 1 : j - 1, jp = (per && j == jj - 1) ? 0 : j + 1;
     const int bc = Mb.bc_type;  // u, v on a wall from rel: rel / alpha, 0, or NaN
     double P[PQ_MAXL], R[PQ_MAXL], Z[PQ_MAXL], U[PQ_MAXL], V[PQ_MAXL], Tn[PQ_MAXL];
 #pragma unroll
@@ -1294,7 +1302,7 @@ __global__ void k_quad(const Member* __restrict__ mems, const int* __restrict__ 
         Z[l] = (in_i && in_j) ? (double)zp[o + l * ls] : zeta_bc_node(Mb, ps, r, i, j, l);
         auto wall = [&]() { return bc == 1 ? r / Mb.alpha : bc == 2 ? 0.0 : __longlong_as_double(0x7ff8000000000000LL); };
         U[l] = (in_i && in_j) ? 0.5 * (ps(i + 1, j, l) - ps(i - 1, j, l)) : (in_j ? wall() : 0.0);
-        V[l] = (in_i && in_j) ? 0.5 * (ps(i, j + 1, l) - ps(i, j - 1, l)) : (in_i ? wall() : 0.0);
+        V[l] = (in_i && in_j) ? 0.5 * (ps(i, jp, l) - ps(i, jm, l)) : (in_i ? wall() : 0.0);
     }
 #pragma unroll
     for (int l = 0; l < PQ_MAXL; ++l) {

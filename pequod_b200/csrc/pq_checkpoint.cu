@@ -82,16 +82,26 @@ struct Ref {
     }
 };
 
-// The saved face ranges of one process without neighbours: FLUX_II faces
-// i in [3, ii+1], rows j in [3, jj]; FLUX_JJ columns i in [3, ii], faces
-// j in [3, jj+1] (fa_i_min = 2, fa_i_max = ii+1, fa_j_min = 2, fa_j_max = jj+1).
 struct Range {
     int i0, i1, j0, j1;
     size_t count() const { return (size_t)(i1 - i0 + 1) * (j1 - j0 + 1); }
 };
 
-Range fi_range(int ii, int jj) { return {3, ii + 1, 3, jj}; }
-Range fj_range(int ii, int jj) { return {3, ii, 3, jj + 1}; }
+// The owned interior rows f_j_min..f_j_max of one process
+// (qg3p_base.F90:893-912): a closed basin has no j neighbour, rows 3..jj;
+// a channel is its own j neighbour, rows 2..jj+1 (every row, the halo rows
+// 1 and jj+2 copies of rows jj+1 and 2).  fa_j_min = lo - 1, fa_j_max =
+// hi + 1; in i there is never a neighbour (f_i 3..ii, fa_i 2..ii+1).
+struct Rows {
+    int lo, hi;
+};
+Rows rows_of(const pq_ctx* c) { return c->periodic ? Rows{2, c->jj + 1} : Rows{3, c->jj}; }
+
+// The saved face ranges: FLUX_II faces i in [fa_i_min+1, fa_i_max], rows
+// [fa_j_min+1, fa_j_max-1]; FLUX_JJ columns [fa_i_min+1, fa_i_max-1], faces
+// [fa_j_min+1, fa_j_max] (qg3.F90:864-875).
+Range fi_range(int ii, Rows r) { return {3, ii + 1, r.lo, r.hi}; }
+Range fj_range(int ii, Rows r) { return {3, ii, r.lo, r.hi + 1}; }
 
 void pack(Ref& a, const Range& r, int l, std::vector<double>& out) {
     out.clear();
@@ -107,7 +117,6 @@ void unpack(Ref& a, const Range& r, int l, const std::vector<double>& in) {
 
 bool supported(pq_ctx* c) {
     if (c->helm_only) return !fail(c, PQ_ERR_UNSUPPORTED, "checkpoint of a Helmholtz-only context");
-    if (c->periodic) return !fail(c, PQ_ERR_UNSUPPORTED, "checkpoints of a channel (periodic j) are not built");
     return true;
 }
 
@@ -176,8 +185,9 @@ int pq_write_checkpoint(pq_ctx* c, const char* s_path, const char* supp_path, do
         if ((rc = get_ref(c, PQ_F_RES, res))) return rc;
         if ((rc = copy_out_state(c, res_prev.v.data(), c->hm[c->cur].res_out, PQ_PTR_HOST))) return rc;
         CK(cudaStreamSynchronize(c->stream));
+        const Rows rw = rows_of(c);
         for (int l = 1; l <= L; ++l)
-            for (int j = 3; j <= jj; ++j)
+            for (int j = rw.lo; j <= rw.hi; ++j)
                 for (int i = 3; i <= ii; ++i) zeta(i, j, l) = zeta(i, j, l) - 0.5 * dt * res(i - 1, j - 1, l);
     }
     {
@@ -204,12 +214,21 @@ int pq_write_checkpoint(pq_ctx* c, const char* s_path, const char* supp_path, do
     if ((rc = get_ref(c, PQ_F_UI, ui)) || (rc = get_ref(c, PQ_F_UJ, uj)) || (rc = get_ref(c, PQ_F_ZETA_FI, zfi)) ||
         (rc = get_ref(c, PQ_F_ZETA_FJ, zfj)) || (rc = get_ref(c, PQ_F_RES_BETA, rb)))
         return rc;
+    if (c->periodic) {
+        // The device keeps j faces 2..jj+1; face jj+2 is face 2 of the next
+        // period (update(uj, level_1), qg3.F90:795-803).
+        for (int l = 1; l <= L; ++l)
+            for (int i = 2; i <= ii + 1; ++i) {
+                uj(i, jj + 2, l) = uj(i, 2, l);
+                zfj(i, jj + 2, l) = zfj(i, 2, l);
+            }
+    }
     File out;
     out.f = std::fopen(supp_path, "wb");
     if (!out.f) return fail(c, PQ_ERR_ARG, std::string("Failed to open output file ") + supp_path);
     bool ok = put_record(out.f, &model_time_day, 1) && put_record(out.f, &total_time_day, 1) &&
               put_record(out.f, &dt, 1);
-    const Range ri = fi_range(ii, jj), rj = fj_range(ii, jj), rs{1, ii, 1, jj};
+    const Range ri = fi_range(ii, rows_of(c)), rj = fj_range(ii, rows_of(c)), rs{1, ii, 1, jj};
     std::vector<double> rec;
     const std::pair<Ref*, Range> order[] = {{&ui, ri},  {&uj, rj},       {&zfi, ri},
                                             {&zfj, rj}, {&res_prev, rs}, {&rb, rs}};
@@ -280,7 +299,7 @@ int pq_read_checkpoint(pq_ctx* c, const char* s_path, const char* supp_path, dou
         if (ok && (fne(mts, mtd) || fne(tts, ttd)))
             return fail(c, PQ_ERR_ARG, "Input times do not match in CABARET checkpoint data");
         ok = ok && get_record(in.f, &dt, 1);
-        const Range ri = fi_range(ii, jj), rj = fj_range(ii, jj), rs{1, ii, 1, jj};
+        const Range ri = fi_range(ii, rows_of(c)), rj = fj_range(ii, rows_of(c)), rs{1, ii, 1, jj};
         const std::pair<Ref*, Range> order[] = {{&ui, ri}, {&uj, rj}, {&zfi, ri}, {&zfj, rj}, {&res, rs}, {&rb, rs}};
         std::vector<double> rec;
         for (const auto& fr : order)
@@ -296,21 +315,28 @@ int pq_read_checkpoint(pq_ctx* c, const char* s_path, const char* supp_path, dou
     // uimo / ujmo (cabaret_cell_boundaries_velocity, qg3p_aux.F90:1168-1231),
     // flux = u * zeta_f (cabaret_flux, :1547-1594), corrector half step
     // (cabaret_corrector, :1597-1642).
+    // A channel first fills psi's halo rows (update(psi), qg3.F90:324).
+    const Rows rw = rows_of(c);
     Ref pe(ii + 2, jj + 2, L), uimo(ii + 3, jj + 2, L), ujmo(ii + 2, jj + 3, L);
     Ref fli(ii + 3, jj + 2, L), flj(ii + 2, jj + 3, L);
     for (int l = 1; l <= L; ++l) {
-        for (int j = 3; j <= jj + 1; ++j)
+        if (c->periodic)
+            for (int i = 2; i <= ii + 1; ++i) {
+                psi(i, 1, l) = psi(i, jj + 1, l);
+                psi(i, jj + 2, l) = psi(i, 2, l);
+            }
+        for (int j = rw.lo; j <= rw.hi + 1; ++j)
             for (int i = 3; i <= ii + 1; ++i)
                 pe(i, j, l) = 0.25 * (psi(i, j, l) + psi(i, j - 1, l) + psi(i - 1, j, l) + psi(i - 1, j - 1, l));
-        for (int j = 3; j <= jj; ++j)
+        for (int j = rw.lo; j <= rw.hi; ++j)
             for (int i = 3; i <= ii + 1; ++i) uimo(i, j, l) = -pe(i, j + 1, l) + pe(i, j, l);
-        for (int j = 3; j <= jj + 1; ++j)
+        for (int j = rw.lo; j <= rw.hi + 1; ++j)
             for (int i = 3; i <= ii; ++i) ujmo(i, j, l) = pe(i + 1, j, l) - pe(i, j, l);
-        for (int j = 3; j <= jj; ++j)
+        for (int j = rw.lo; j <= rw.hi; ++j)
             for (int i = 2; i <= ii + 2; ++i) fli(i, j, l) = ui(i, j, l) * zfi(i, j, l);
-        for (int j = 2; j <= jj + 2; ++j)
+        for (int j = rw.lo; j <= rw.hi + 1; ++j)
             for (int i = 3; i <= ii; ++i) flj(i, j, l) = uj(i, j, l) * zfj(i, j, l);
-        for (int j = 3; j <= jj; ++j)
+        for (int j = rw.lo; j <= rw.hi; ++j)
             for (int i = 3; i <= ii; ++i) {
                 const double r = -(fli(i + 1, j, l) - fli(i, j, l) + flj(i, j + 1, l) - flj(i, j, l));
                 res(i - 1, j - 1, l) = r;
@@ -322,9 +348,9 @@ int pq_read_checkpoint(pq_ctx* c, const char* s_path, const char* supp_path, dou
     // applies at the end of the step before; apply it here instead.
     double mu = 0.0;
     for (int l = 1; l <= L; ++l) {
-        for (int j = 3; j <= jj; ++j)
+        for (int j = rw.lo; j <= rw.hi; ++j)
             for (int i = 3; i <= ii + 1; ++i) mu = std::fmax(mu, std::fabs(ui(i, j, l)));
-        for (int j = 3; j <= jj + 1; ++j)
+        for (int j = rw.lo; j <= rw.hi + 1; ++j)
             for (int i = 3; i <= ii; ++i) mu = std::fmax(mu, std::fabs(uj(i, j, l)));
     }
     Scalars sc;

@@ -17,6 +17,16 @@ def double_gyre(ii, layers=2, dt=1800.0, **kw):
     return pq.Config.from_physical(p)
 
 
+def channel(ii, jj, layers=3, dt=1800.0, **kw):
+    """A channel (periodic in j) of the double-gyre physics."""
+    H = {1: (1.0e5,), 2: (1.0e5, 3.0e5), 3: (3.0e4, 7.0e4, 3.0e5)}[layers]
+    gp = {1: (), 2: (1.5,), 3: (1.5, 0.75)}[layers]
+    p = pq.double_gyre_physical(ii, jj=jj, layers=layers, dt=dt, dx=3.84e8 / (ii - 1), H=H, gprime=gp, **kw)
+    cfg = pq.Config.from_physical(p)
+    cfg.desc.periodic_j = 1
+    return cfg
+
+
 def run_oracle(cfg, steps, seed):
     ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     if cfg.oracle_cfg().get("scheme", 0) == 1:
@@ -141,6 +151,38 @@ def test_cabaret_pickup_matches_numpy(tmp_path, adapt):
     assert p.scalars()["dt"] == o.scalars()["dt"]
 
 
+@pytest.mark.parametrize("adapt", [0, 1])
+def test_channel_pickup_resumes_bit_for_bit(tmp_path, adapt):
+    """A channel's checkpoint (faces fa_j_min+1 .. fa_j_max with fa_j_min = 1,
+    fa_j_max = jj + 2, qg3.F90:864-875) and its pickup with the periodic halo
+    updates (qg3.F90:324-339): the resumed oracle is the uninterrupted one."""
+    s, supp = str(tmp_path / "ch_s.d"), str(tmp_path / "ch_s_supp.d")
+    kw = dict(adapt_dt=1, target_cfl=0.1, max_dt=86400.0) if adapt else {}
+    cfg = channel(17, 20, 3, **kw)
+    ii, jj = 17, 20
+    o = run_oracle(cfg, 4, seed=8)
+    o.step_to_dump()
+    fields = o.dump_fields()
+    O.write_checkpoint(s, supp, fields, 0.1, 0.1, dt=o.scalars()["dt"], periodic_j=True)
+    recs = O._records(supp)
+    assert [r.size for r in recs[3:3 + 4 * 3:3]] == [(ii - 1) * jj, (ii - 2) * (jj + 1), (ii - 1) * jj, (ii - 2) * (jj + 1)]
+    ck = O.read_checkpoint(s, supp, ii, jj, 3, periodic_j=True)
+    for n in ("ui", "zeta_fi"):
+        np.testing.assert_array_equal(ck[n][2:ii + 1, 1:jj + 1], fields[n][2:ii + 1, 1:jj + 1])
+    for n in ("uj", "zeta_fj"):
+        np.testing.assert_array_equal(ck[n][2:ii, 1:jj + 2], fields[n][2:ii, 1:jj + 2])
+    p = O.Model(cfg.oracle_cfg())
+    p.pickup(ck)
+    o.finish_step()
+    for n in ("psi", "zeta", "zeta_old", "uimo", "ujmo", "zeta_fj", "res", "res_beta"):
+        np.testing.assert_array_equal(p.get(n), o.get(n), err_msg=n)
+    p.step(3)
+    o.step(3)
+    for n in ("psi", "zeta", "ui", "uj", "uimo", "ujmo", "zeta_fi", "zeta_fj", "res", "res_beta"):
+        np.testing.assert_array_equal(p.get(n), o.get(n), err_msg=n)
+    assert p.scalars()["dt"] == o.scalars()["dt"]
+
+
 @pytest.mark.parametrize("bc", [pq.BC_PARTIAL_SLIP, pq.BC_NO_SLIP, pq.BC_FREE_SLIP])
 def test_leapfrog_pickup_rel_from_psi(tmp_path, bc):
     """rel_from_psi (qg3p_aux.F90:579-603) + apply_rel_bc on both levels."""
@@ -182,17 +224,18 @@ def test_leapfrog_pickup_rel_from_psi(tmp_path, bc):
     assert p.scalars()["model_time"] == 0.0
 
 
-@pytest.mark.parametrize("scheme", [pq.SCHEME_CABARET, pq.SCHEME_LEAPFROG])
-def test_oracle_time_average(scheme):
+@pytest.mark.parametrize("scheme,periodic", [(pq.SCHEME_CABARET, False), (pq.SCHEME_LEAPFROG, False),
+                                             (pq.SCHEME_CABARET, True)])
+def test_oracle_time_average(scheme, periodic):
     """psi_av (qg3.F90:672-680, 725): the sum of dt * psi over the steps whose
     model time passed the threshold, restated step by step in numpy."""
-    cfg = double_gyre(17, 2, scheme=scheme)
+    cfg = channel(17, 20, 2) if periodic else double_gyre(17, 2, scheme=scheme)
     o = run_oracle(cfg, 0, seed=5)
     dt = cfg.oracle_cfg()["dt"]
     t0 = o.scalars()["model_time"]
     thr = t0 + 3.2 * dt          # the first steps are not averaged
     o.average(True, thr)
-    want = np.zeros((17, 17, 2), order="F")
+    want = np.zeros((cfg.ii, cfg.jj, 2), order="F")
     dtime = 0.0
     for k in range(7):
         if scheme == pq.SCHEME_CABARET:
@@ -211,23 +254,32 @@ def test_oracle_time_average(scheme):
     np.testing.assert_allclose(got, want / dtime, rtol=1e-14, atol=0)
 
 
-def numpy_quad_terms(psi, rel, zeta, cfg):
-    """qg3.F90:683-721 in numpy on sdata (ii, jj, L): the 23 products."""
+def numpy_quad_terms(psi, rel, zeta, cfg, periodic_j=False):
+    """qg3.F90:683-721 in numpy on sdata (ii, jj, L): the 23 products.  A
+    channel has no j walls: u is central on every row, v wraps in j."""
     oc = cfg.oracle_cfg()
     ii, jj, L = psi.shape
     bc, alpha = oc["bc_type"], oc["alpha"]
     s1, s2, h = np.array(oc["s1"]), np.array(oc["s2"]), np.array(oc["h"])
     u = np.zeros_like(psi)
     v = np.zeros_like(psi)
-    u[1:-1, 1:-1] = 0.5 * (psi[2:, 1:-1] - psi[:-2, 1:-1])
-    v[1:-1, 1:-1] = 0.5 * (psi[1:-1, 2:] - psi[1:-1, :-2])
     wall = {pq.BC_PARTIAL_SLIP: None, pq.BC_NO_SLIP: 0.0, pq.BC_FREE_SLIP: np.nan}[bc]
-    if wall is None:
-        u[0, 1:-1], u[-1, 1:-1] = rel[0, 1:-1] / alpha, rel[-1, 1:-1] / alpha
-        v[1:-1, 0], v[1:-1, -1] = rel[1:-1, 0] / alpha, rel[1:-1, -1] / alpha
+    if periodic_j:
+        u[1:-1, :] = 0.5 * (psi[2:, :] - psi[:-2, :])
+        v[1:-1, :] = 0.5 * (np.roll(psi, -1, axis=1) - np.roll(psi, 1, axis=1))[1:-1, :]
+        if wall is None:
+            u[0, :], u[-1, :] = rel[0, :] / alpha, rel[-1, :] / alpha
+        else:
+            u[0, :] = u[-1, :] = wall
     else:
-        u[0, 1:-1] = u[-1, 1:-1] = wall
-        v[1:-1, 0] = v[1:-1, -1] = wall
+        u[1:-1, 1:-1] = 0.5 * (psi[2:, 1:-1] - psi[:-2, 1:-1])
+        v[1:-1, 1:-1] = 0.5 * (psi[1:-1, 2:] - psi[1:-1, :-2])
+        if wall is None:
+            u[0, 1:-1], u[-1, 1:-1] = rel[0, 1:-1] / alpha, rel[-1, 1:-1] / alpha
+            v[1:-1, 0], v[1:-1, -1] = rel[1:-1, 0] / alpha, rel[1:-1, -1] / alpha
+        else:
+            u[0, 1:-1] = u[-1, 1:-1] = wall
+            v[1:-1, 0] = v[1:-1, -1] = wall
     t = np.zeros_like(psi)
     if L > 1:
         t[:, :, 0] = -s2[0] * (psi[:, :, 0] - psi[:, :, 1])
@@ -249,12 +301,12 @@ def numpy_quad_terms(psi, rel, zeta, cfg):
             s2[:-1] * h[:-1] * dp ** 2 / (h[:-1] + h[1:])]
 
 
-@pytest.mark.parametrize("partial_slip", [True, False])
-def test_oracle_quad_diagnostics(partial_slip):
+@pytest.mark.parametrize("partial_slip,periodic", [(True, False), (False, False), (True, True)])
+def test_oracle_quad_diagnostics(partial_slip, periodic):
     """The quad eddy covariances (qg3.F90:683-721, qg3p_diagnostics.F90:941-1537)
     of the oracle against a numpy statement, over steps with and without the
-    threshold passed."""
-    cfg = double_gyre(17, 3, partial_slip=partial_slip)
+    threshold passed; in a closed basin and in a channel."""
+    cfg = channel(17, 20, 3, partial_slip=partial_slip) if periodic else double_gyre(17, 3, partial_slip=partial_slip)
     o = run_oracle(cfg, 1, seed=7)
     dt = cfg.oracle_cfg()["dt"]
     thr = o.scalars()["model_time"] + 1.2 * dt
@@ -275,7 +327,7 @@ def test_oracle_quad_diagnostics(partial_slip):
             zeta[:, :, 0] -= s2[0] * (psi[:, :, 0] - psi[:, :, 1])
             zeta[:, :, 1] -= s1[1] * (psi[:, :, 1] - psi[:, :, 0]) + s2[1] * (psi[:, :, 1] - psi[:, :, 2])
             zeta[:, :, 2] -= s1[2] * (psi[:, :, 2] - psi[:, :, 1])
-            terms = numpy_quad_terms(psi, rel, zeta, cfg)
+            terms = numpy_quad_terms(psi, rel, zeta, cfg, periodic)
             acc = [dt * x for x in terms] if acc is None else [a + dt * x for a, x in zip(acc, terms)]
             dtime += dt
         o.finish_step()

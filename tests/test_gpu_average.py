@@ -161,3 +161,38 @@ def test_quad_free_slip_walls_and_file(tmp_path):
     assert len(recs) == 2 + 23
     assert [r.size for r in recs[2:]] == [65 * 65 * (1 if n in ("uu_i", "vv_i", "sc_ub", "sc_vb", "sc_bb_i") else 2)
                                           for n in g.QUAD]
+
+
+def channel(ii, jj, layers=3, dt=1800.0, **kw):
+    H = {2: (1.0e5, 3.0e5), 3: (3.0e4, 7.0e4, 3.0e5)}[layers]
+    gp = {2: (1.5,), 3: (1.5, 0.75)}[layers]
+    p = pq.double_gyre_physical(ii, jj=jj, layers=layers, dt=dt, dx=3.84e8 / (ii - 1), H=H, gprime=gp, **kw)
+    cfg = pq.Config.from_physical(p)
+    cfg.desc.periodic_j = 1
+    return cfg
+
+
+@pytest.mark.parametrize("partial_slip,prec", [(True, pq.PREC_FP64), (False, pq.PREC_FP64),
+                                               (True, pq.PREC_MIXED)])
+def test_channel_average_and_quad_match_oracle(partial_slip, prec):
+    """A channel's psi_av (accumulated in its rel kernel) and quad
+    covariances (v central across the periodic rows, no j walls)."""
+    cfg = channel(129, 96, 3, precision=prec, partial_slip=partial_slip)
+    g, o = start(cfg, seed=46)
+    g.step(1)
+    o.step(1)
+    thr = o.scalars()["model_time"] + 1.7 * cfg.desc.dt
+    g.average(2, thr)
+    o.average(2, thr)
+    for n in (1, 2, 3):
+        g.step(n)
+        o.step(n)
+    assert g.last_launch_count() == 3 * 8    # seven channel kernels and the covariances
+    tol = 1e-11 if prec == pq.PREC_FP64 else 1e-5
+    a_g, t_g = g.get_average()
+    a_o, t_o = o.get_average()
+    assert t_o > 0 and abs(t_g - t_o) <= 1e-12 * t_o
+    assert rel_l2(a_g, a_o) <= (1e-12 if prec == pq.PREC_FP64 else 1e-6), rel_l2(a_g, a_o)
+    worst = {name: rel_l2(g.get_quad(q), o.get_quad(q)) for q, name in enumerate(g.QUAD)}
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, worst

@@ -211,3 +211,95 @@ def test_checkpoint_errors(tmp_path):
     # The context is still usable after the refusals.
     g2.read_checkpoint(s, supp)
     g2.step(1)
+
+
+def channel(ii, jj, layers=3, dt=1800.0, **kw):
+    H = {1: (1.0e5,), 2: (1.0e5, 3.0e5), 3: (3.0e4, 7.0e4, 3.0e5)}[layers]
+    gp = {1: (), 2: (1.5,), 3: (1.5, 0.75)}[layers]
+    p = pq.double_gyre_physical(ii, jj=jj, layers=layers, dt=dt, dx=3.84e8 / (ii - 1), H=H, gprime=gp, **kw)
+    cfg = pq.Config.from_physical(p)
+    cfg.desc.periodic_j = 1
+    return cfg
+
+
+def channel_saved(name, a, ii, jj):
+    """The part of a channel's reference-layout array that its checkpoint
+    holds: rows 2..jj+1 and faces 2..jj+2 (fa_j_min = 1, fa_j_max = jj+2)."""
+    if name in ("psi", "zeta"):
+        return a[1:-1, 1:-1]
+    if name in ("ui", "zeta_fi"):
+        return a[2:ii + 1, 1:jj + 1]
+    if name in ("uj", "zeta_fj"):
+        return a[2:ii, 1:jj + 2]
+    return a
+
+
+def channel_owned(name, a, ii, jj):
+    """The part of a channel's reference-layout array the device stores (the
+    halo rows are copies of it)."""
+    if name in ("ui", "uimo", "zeta_fi", "uj", "ujmo", "zeta_fj"):
+        return a[1:ii + 1, 1:jj + 1]
+    if name in ("res", "res_beta"):
+        return a
+    return a[1:-1, 1:-1]
+
+
+def compare_channel(g, o, names, tol):
+    ii, jj = g.cfg.ii, g.cfg.jj
+    worst = {n: rel_l2(channel_owned(n, g.get(n), ii, jj), channel_owned(n, o.get(n), ii, jj)) for n in names}
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, worst
+
+
+@pytest.mark.parametrize("ii,jj,layers", [(65, 64, 3), (33, 40, 1)])
+def test_channel_dump_matches_oracle_state(tmp_path, ii, jj, layers):
+    """The channel's _s / _s_supp files: face jj+2 of the j faces is face 2
+    of the next period, written from the device's face 2."""
+    cfg = channel(ii, jj, layers)
+    g, o = start(cfg, seed=35)
+    g.step(7)
+    o.step(6)
+    o.step_to_dump()
+    s, supp = str(tmp_path / "ch_s.d"), str(tmp_path / "ch_s_supp.d")
+    g.write_checkpoint(s, supp, t_scale=cfg.t_scale, start_time_day=1.0)
+    ck = O.read_checkpoint(s, supp, ii, jj, layers, periodic_j=True)
+    so = o.scalars()
+    want_day = so["model_time"] * cfg.t_scale / 86400.0
+    assert abs(ck["model_time_day"] - want_day) <= 1e-14 * want_day
+    assert ck["dt"] == so["dt"]
+    for n in CAB:
+        a = channel_saved(n, ck[n], ii, jj)
+        b = channel_saved(n, o.get(n), ii, jj)
+        assert rel_l2(a, b) <= TOL, (n, rel_l2(a, b))
+
+
+@pytest.mark.parametrize("adapt", [0, 1])
+def test_channel_pickup_matches_oracle(tmp_path, adapt):
+    kw = dict(adapt_dt=1, target_cfl=0.1, max_dt=86400.0) if adapt else {}
+    cfg = channel(129, 96, 3, **kw)
+    g, o = start(cfg, seed=36)
+    g.step(9)
+    o.step(8)
+    o.step_to_dump()
+    s, supp = str(tmp_path / "ch3_s.d"), str(tmp_path / "ch3_s_supp.d")
+    g.write_checkpoint(s, supp, t_scale=cfg.t_scale, start_time_day=2.0)
+    ck = O.read_checkpoint(s, supp, 129, 96, 3, periodic_j=True)
+    g2 = pq.Model(cfg)
+    total = g2.read_checkpoint(s, supp)
+    assert total == ck["total_time_day"]
+    o2 = O.Model(cfg.oracle_cfg())
+    o2.pickup(ck)
+    compare_channel(g2, o2, AFTER, 1e-15)
+    assert g2.scalars()["model_time"] == o2.scalars()["model_time"]
+    o.finish_step()
+    compare_channel(g2, o, AFTER, TOL)
+    compare_channel(g, o, AFTER, TOL)
+    for n in (1, 2, 5):
+        for m in (g, g2, o, o2):
+            m.step(n)
+        compare_channel(g2, o2, AFTER, TOL * 10)
+        compare_channel(g2, o, AFTER, TOL * 10)
+        assert max(rel_l2(g2.get(f), g.get(f)) for f in ("psi", "zeta")) <= TOL
+    sg, so = g2.scalars(), o2.scalars()
+    for k in ("dt", "tweight_a", "tweight_u", "model_time"):
+        assert abs(sg[k] - so[k]) <= 1e-12 * abs(so[k]), (k, sg[k], so[k])
