@@ -258,8 +258,10 @@ PQ_API int pq_get_scalars(pq_ctx* ctx, double* out4);
  * model_time = 0 and skips the forward-Euler start.  The file times must
  * agree (PQ_ERR_ARG "Input times do not match", as the reference aborts);
  * total_time_day receives the checkpoint's total time (the new run's
- * start_time_day) and may be NULL.  Not for periodic-channel contexts
- * (PQ_ERR_UNSUPPORTED). */
+ * start_time_day) and may be NULL.  A channel (periodic_j) saves rows
+ * 2..jj+1 and j faces 2..jj+2 (it is its own j neighbour: fa_j_min = 1,
+ * fa_j_max = jj + 2, qg3p_base.F90:893-918) and its pickup fills psi's
+ * periodic halo rows first (qg3.F90:324-339). */
 PQ_API int pq_write_checkpoint(pq_ctx* ctx, const char* s_path, const char* supp_path, double t_scale,
                                double start_time_day);
 PQ_API int pq_read_checkpoint(pq_ctx* ctx, const char* s_path, const char* supp_path, double* total_time_day);
@@ -289,7 +291,8 @@ PQ_API int pq_average(pq_ctx* ctx, int enable, double threshold);
  * PQ_QUAD_NAMES) times 1 / diagnostic_time as (ii, jj, layers of q);
  * pq_write_quad writes the qg<L>_<ii>_quad_av.d file (qg3.F90:903-929).
  * The reference leaves ut, vt, rt and tt uninitialised; here all start at 0.
- * CABARET, closed basin. */
+ * CABARET, closed basin or channel (no j walls: v is central across the
+ * periodic seam). */
 #define PQ_QUAD_NAMES "uu vv uu_i vv_i uv ur vr rr pr uz vz zz zr pp pz ut vt rt tt sc_ub sc_vb sc_bb sc_bb_i"
 PQ_API int pq_get_quad(pq_ctx* ctx, int q, double* out);
 PQ_API int pq_write_quad(pq_ctx* ctx, const char* path, double t_scale, double start_time_day);
