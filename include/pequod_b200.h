@@ -283,7 +283,8 @@ PQ_API int pq_read_checkpoint(pq_ctx* ctx, const char* s_path, const char* supp_
  * the averaged sdata, in the checkpoint's record format. */
 PQ_API int pq_average(pq_ctx* ctx, int enable, double threshold);
 /* enable = 2 also accumulates the 23 quad eddy covariances (qg3.F90:683-721,
- * the reference's `quad` option) in one extra kernel per CABARET step:
+ * the reference's `quad` option) in one extra kernel per CABARET step or
+ * leapfrog sub-step (on the level just inverted):
  * products of the zonal / meridional velocities (0 where the reference
  * never writes them, rel / alpha, 0 or NaN on the walls by the velocity
  * boundary condition), interface velocities, thickness, rel, zeta and psi,
@@ -291,8 +292,8 @@ PQ_API int pq_average(pq_ctx* ctx, int enable, double threshold);
  * PQ_QUAD_NAMES) times 1 / diagnostic_time as (ii, jj, layers of q);
  * pq_write_quad writes the qg<L>_<ii>_quad_av.d file (qg3.F90:903-929).
  * The reference leaves ut, vt, rt and tt uninitialised; here all start at 0.
- * CABARET, closed basin or channel (no j walls: v is central across the
- * periodic seam). */
+ * Closed basin or channel (no j walls: v is central across the periodic
+ * seam). */
 #define PQ_QUAD_NAMES "uu vv uu_i vv_i uv ur vr rr pr uz vz zz zr pp pz ut vt rt tt sc_ub sc_vb sc_bb sc_bb_i"
 PQ_API int pq_get_quad(pq_ctx* ctx, int q, double* out);
 PQ_API int pq_write_quad(pq_ctx* ctx, const char* path, double t_scale, double start_time_day);

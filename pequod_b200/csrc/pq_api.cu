@@ -174,6 +174,7 @@ int run_step(pq_ctx* c, int par) {
         if (ev) CK(cudaEventRecord(ev[3], c->stream));
         CK(launch_lf_rel_bc(c->ls[par], 0, 1, c->stream));
         if (ev) CK(cudaEventRecord(ev[4], c->stream));
+        if (c->quad) CK(launch_quad(c->ls[par], 0, 1, c->stream));
         if (c->psi_av) CK(launch_lf_average(c->ls[par], c->stream));
         c->zpar = par;
         return PQ_OK;
@@ -188,7 +189,7 @@ int run_step(pq_ctx* c, int par) {
         if (ev) CK(cudaEventRecord(ev[2], c->stream));
         CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
         if (ev) CK(cudaEventRecord(ev[3], c->stream));
-        if (c->quad) CK(launch_quad(c->ls[par], f32, c->stream));
+        if (c->quad) CK(launch_quad(c->ls[par], f32, 0, c->stream));
         CK(launch_cabaret_channel(c->ls[par], f32, c->stream));
         if (ev) CK(cudaEventRecord(ev[4], c->stream));
         c->pred_ready = false;
@@ -203,7 +204,7 @@ int run_step(pq_ctx* c, int par) {
     if (ev) CK(cudaEventRecord(ev[2], c->stream));
     CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[3], c->stream));
-    if (c->quad) CK(launch_quad(c->ls[par], f32, c->stream));
+    if (c->quad) CK(launch_quad(c->ls[par], f32, 0, c->stream));
     CK(launch_cabaret_fused(c->ls[par], c->fuse ? 1 : 0, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[4], c->stream));
     c->pred_ready = c->fuse;
@@ -1157,7 +1158,7 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc) {
 }
 
 int step_launches(const pq_ctx* c) {
-    return c->leapfrog ? (c->psi_av ? 6 : 5) : (c->periodic ? 7 : 4) + (c->quad ? 1 : 0);
+    return (c->leapfrog ? (c->psi_av ? 6 : 5) : c->periodic ? 7 : 4) + (c->quad ? 1 : 0);
 }
 
 int read_scalars(pq_ctx* c, Scalars* sc) {

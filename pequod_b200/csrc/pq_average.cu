@@ -44,8 +44,6 @@ extern "C" {
 int pq_average(pq_ctx* c, int enable, double threshold) {
     if (!c || enable < 0 || enable > 2) return PQ_ERR_ARG;
     if (c->helm_only) return fail(c, PQ_ERR_UNSUPPORTED, "no time loop on this context");
-    if (enable == 2 && c->leapfrog)
-        return fail(c, PQ_ERR_UNSUPPORTED, "the quad covariances are accumulated by the CABARET step only");
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     if (enable == 2 && !c->quad) {
@@ -140,7 +138,7 @@ int pq_write_quad(pq_ctx* c, const char* path, double t_scale, double start_time
     double sc4[4];
     int rc = pq_get_scalars(c, sc4);
     if (rc) return rc;
-    const double model_time_day = (sc4[3] - 0.5 * sc4[0]) * t_scale / 86400.0;
+    const double model_time_day = (c->leapfrog ? sc4[3] : sc4[3] - 0.5 * sc4[0]) * t_scale / 86400.0;
     const double total_time_day = start_time_day + model_time_day;
     std::vector<std::vector<double>> f(23);
     for (int q = 0; q < 23; ++q) {

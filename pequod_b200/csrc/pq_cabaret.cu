@@ -1271,13 +1271,17 @@ int channel_ctas(int ii, int jj) { return ((ii + 127) / 128) * jj; }
 // (:1197-1227), the dt-weighted products (:1360-1427) and the scaled
 // buoyancy correlations (:1430-1537).  One thread per node, all layers.
 // Launched before the step's CABARET kernel, so the model-time gate is the
-// one the fused kernel uses for psi_av.
+// one the fused kernel uses for psi_av.  lf: a leapfrog sub-step, launched
+// after its rel kernel on the level just inverted (psi, rel, zeta
+// BLEAPFROG); its gate is the model time already advanced by the sub-step,
+// as k_lf_average's.
 template <typename T>
-__global__ void k_quad(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem) {
+__global__ void k_quad(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem, int lf) {
     int local;
     const int mi = find_member(prefix, nmem, blockIdx.y, &local);
     const Member& Mb = mems[mi];
-    if (Mb.quad == nullptr || !cab_average_gate(Mb)) return;
+    if (Mb.quad == nullptr) return;
+    if (lf ? !(Mb.psi_av != nullptr && Mb.sc->model_time > Mb.av_threshold) : !cab_average_gate(Mb)) return;
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride, qs = Mb.quad_stride;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = local;
@@ -1365,12 +1369,12 @@ __global__ void k_quad(const Member* __restrict__ mems, const int* __restrict__ 
     }
 }
 
-cudaError_t launch_quad(const LaunchSet& ls, int f32, cudaStream_t st) {
+cudaError_t launch_quad(const LaunchSet& ls, int f32, int lf, cudaStream_t st) {
     const dim3 g((ls.maxI + 127) / 128, ls.maxJ * ls.nmem);
     if (f32)
-        k_quad<float><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_quad<float><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem, lf);
     else
-        k_quad<double><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem);
+        k_quad<double><<<g, 128, 0, st>>>(ls.members, ls.prefix_rows_all, ls.nmem, lf);
     return cudaGetLastError();
 }
 

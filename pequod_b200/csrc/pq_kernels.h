@@ -72,7 +72,7 @@ cudaError_t launch_cabaret_fused(const LaunchSet& ls, int predict_next, int f32,
 cudaError_t launch_cabaret_channel(const LaunchSet& ls, int f32, cudaStream_t st);
 int channel_ctas(int ii, int jj);
 // The quad eddy covariances of the step (before its CABARET kernel).
-cudaError_t launch_quad(const LaunchSet& ls, int f32, cudaStream_t st);
+cudaError_t launch_quad(const LaunchSet& ls, int f32, int lf, cudaStream_t st);
 int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of the sweep kernel per member (band height sh)
 int cabaret_tile_ctas(int ii, int jj, int L);     // CTAs of the tile kernel per member
 cudaError_t launch_rel(const LaunchSet& ls, int f32, cudaStream_t st);

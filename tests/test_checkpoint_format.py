@@ -336,3 +336,28 @@ def test_oracle_quad_diagnostics(partial_slip, periodic):
         assert got.shape == want.shape, (q, got.shape, want.shape)
         np.testing.assert_allclose(got, want / dtime, rtol=1e-9, atol=1e-12 * np.abs(want).max() / dtime,
                                    err_msg=O.Model.QUAD[q])
+
+
+def test_oracle_quad_diagnostics_leapfrog():
+    """The leapfrog sub-step accumulates the covariances of the level it just
+    inverted (psi, rel, zeta BLEAPFROG, qg3.F90:683-721), gated on the model
+    time after its increment."""
+    cfg = double_gyre(17, 3, scheme=pq.SCHEME_LEAPFROG)
+    o = run_oracle(cfg, 2, seed=9)
+    dt = cfg.oracle_cfg()["dt"]
+    thr = o.scalars()["model_time"] + 1.5 * dt
+    o.average(2, thr)
+    acc = None
+    dtime = 0.0
+    for k in range(5):
+        o.step(1)
+        t = o.scalars()["model_time"]
+        suf = "" if k % 2 == 0 else "2"      # sub-steps alternate levels 1, 2
+        if t > thr:
+            terms = numpy_quad_terms(o.sdata("psi" + suf), o.sdata("rel" + suf), o.sdata("zeta" + suf), cfg)
+            acc = [dt * x for x in terms] if acc is None else [a + dt * x for a, x in zip(acc, terms)]
+            dtime += dt
+    assert 0 < dtime < 5 * dt
+    for q, want in enumerate(acc):
+        np.testing.assert_allclose(o.get_quad(q), want / dtime, rtol=1e-9, atol=1e-12 * np.abs(want).max() / dtime,
+                                   err_msg=O.Model.QUAD[q])

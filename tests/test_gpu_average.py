@@ -196,3 +196,30 @@ def test_channel_average_and_quad_match_oracle(partial_slip, prec):
     worst = {name: rel_l2(g.get_quad(q), o.get_quad(q)) for q, name in enumerate(g.QUAD)}
     bad = {k: v for k, v in worst.items() if not v <= tol}
     assert not bad, worst
+
+
+def test_leapfrog_quad_matches_oracle(tmp_path):
+    """The leapfrog sub-step's covariances: one kernel after its rel kernel
+    on the level just inverted."""
+    cfg = double_gyre(129, 3, scheme=pq.SCHEME_LEAPFROG)
+    g, o = start(cfg, seed=47)
+    g.step(2)
+    o.step(2)
+    thr = o.scalars()["model_time"] + 1.5 * cfg.desc.dt
+    g.average(2, thr)
+    o.average(2, thr)
+    for n in (1, 2, 3):
+        g.step(n)
+        o.step(n)
+    assert g.last_launch_count() == 3 * 7    # average + covariances per sub-step
+    worst = {name: rel_l2(g.get_quad(q), o.get_quad(q)) for q, name in enumerate(g.QUAD)}
+    bad = {k: v for k, v in worst.items() if not v <= 1e-11}
+    assert not bad, worst
+    a_g, t_g = g.get_average()
+    a_o, t_o = o.get_average()
+    assert abs(t_g - t_o) <= 1e-12 * t_o and rel_l2(a_g, a_o) <= 1e-12
+    path = str(tmp_path / "qg3_129_quad_av.d")
+    g.write_quad(path, t_scale=cfg.t_scale)
+    recs = O._records(path)
+    want_day = o.scalars()["model_time"] * cfg.t_scale / 86400.0
+    assert abs(recs[0][0] - want_day) <= 1e-13 * want_day
