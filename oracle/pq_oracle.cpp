@@ -1723,7 +1723,6 @@ void or_energy(int ii, int jj, int layers, int periodic_j, const double* h, cons
 
 or_model* or_model_create(const or_params* p) {
     if (!p || p->ii < 5 || p->jj < 5 || p->layers < 1) return nullptr;
-    if (p->periodic_j && p->scheme != 0) return nullptr;  // the leapfrog channel is not restated
     or_model* m = new or_model;
     m->p = *p;
     int L = p->layers;
@@ -1811,6 +1810,7 @@ int or_model_init(or_model* m, const double* zeta_ic) {
         m->model_time = 0.0;
         m->lf_count = 0;
         zeta_forward_euler(*m);
+        update_pdata(*m, m->zeta[1]);  // qg3.F90:475
         int rc = invert_level(*m, 1);
         if (rc) return rc;
         m->zeta_old[1] = m->zeta[1];
@@ -2038,6 +2038,7 @@ int or_model_step(or_model* m, int nsteps) {
             int lf = (m->lf_count % 2 == 0) ? 1 : 2;
             m->lf_count += 1;
             zeta_centred(*m, lf);
+            update_pdata(*m, m->zeta[lf - 1]);  // qg3.F90:625
             raw_filter(*m, lf);
             int rc = invert_level(*m, lf - 1);
             if (rc) return rc;
@@ -2074,7 +2075,11 @@ int or_model_pickup(or_model* m, double dt) {
         m->tweight_u = 0.5;
     } else {
         for (int lv = 0; lv < 2; ++lv) {
+            // qg3.F90:355-361: halos of psi and zeta, rel from psi, halo of rel.
+            update_pdata(*m, m->psi[lv]);
+            update_pdata(*m, m->zeta[lv]);
             rel_from_psi(*m, m->psi[lv], m->rel[lv]);
+            update_pdata(*m, m->rel[lv]);
             m->zeta_old[lv] = m->zeta[lv];
         }
         m->model_time = 0.0;

@@ -265,8 +265,6 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     const int ii = d->ii, jj = d->jj, L = d->layers;
     if (ii < 5 || jj < 5 || !is_pow2(ii - 1) || L < 1 || L > PQ_MAX_LAYERS) return PQ_ERR_ARG;
     if (d->precision != PQ_PREC_FP64 && d->precision != PQ_PREC_MIXED) return PQ_ERR_UNSUPPORTED;
-    // A channel (periodic in j) steps with CABARET; its leapfrog is not built.
-    if (d->periodic_j && d->scheme == PQ_SCHEME_LEAPFROG && !helm_only) return PQ_ERR_UNSUPPORTED;
     if (d->scheme != PQ_SCHEME_CABARET && d->scheme != PQ_SCHEME_LEAPFROG) return PQ_ERR_UNSUPPORTED;
     // The leapfrog scheme runs in FP64 with a fixed dt (the reference's
     // adaptive step is a CABARET routine).

@@ -121,12 +121,21 @@ bool supported(pq_ctx* c) {
 }
 
 // rel_from_psi (qg3p_aux.F90:579-603) with apply_rel_bc (:779-915) for one
-// process without neighbours: the five-point Laplacian on interior nodes,
-// then the i boundaries and the j boundaries (which own the corners).
+// process: the five-point Laplacian on the interior nodes f_i x f_j, then the
+// i boundaries and the j boundaries (which own the corners).  A channel is
+// its own j neighbour: psi's halo rows are filled first (update(psi),
+// qg3.F90:355), every row is interior and there are no j boundaries.
 void rel_from_psi(const pq_model_desc& d, Ref& psi, Ref& rel) {
     const int ii = d.ii, jj = d.jj, L = d.layers;
+    const bool per = d.periodic_j != 0;
+    if (per)
+        for (int l = 1; l <= L; ++l)
+            for (int i = 2; i <= ii + 1; ++i) {
+                psi(i, 1, l) = psi(i, jj + 1, l);
+                psi(i, jj + 2, l) = psi(i, 2, l);
+            }
     for (int l = 1; l <= L; ++l)
-        for (int j = 3; j <= jj; ++j)
+        for (int j = per ? 2 : 3; j <= (per ? jj + 1 : jj); ++j)
             for (int i = 3; i <= ii; ++i)
                 rel(i, j, l) = -4.0 * psi(i, j, l) + psi(i - 1, j, l) + psi(i, j + 1, l) + psi(i + 1, j, l) +
                                psi(i, j - 1, l);
@@ -145,10 +154,11 @@ void rel_from_psi(const pq_model_desc& d, Ref& psi, Ref& rel) {
             rel(2, j, l) = bc(2, j, 1, 0, l);
             rel(ii + 1, j, l) = bc(ii + 1, j, -1, 0, l);
         }
-        for (int i = 2; i <= ii + 1; ++i) {
-            rel(i, 2, l) = bc(i, 2, 0, 1, l);
-            rel(i, jj + 1, l) = bc(i, jj + 1, 0, -1, l);
-        }
+        if (!per)
+            for (int i = 2; i <= ii + 1; ++i) {
+                rel(i, 2, l) = bc(i, 2, 0, 1, l);
+                rel(i, jj + 1, l) = bc(i, jj + 1, 0, -1, l);
+            }
     }
 }
 

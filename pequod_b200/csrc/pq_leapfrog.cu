@@ -25,13 +25,19 @@ namespace pq {
 __device__ __forceinline__ double lf_increment(const Member& Mb, const double* __restrict__ psi,
                                                const double* __restrict__ rel, const double* __restrict__ relp,
                                                int i, int j, int l) {
-    const int L = Mb.L, pitch = Mb.pitch, ii = Mb.ii;
+    const int L = Mb.L, pitch = Mb.pitch, ii = Mb.ii, jj = Mb.jj;
     const long long ls = Mb.lstride;
     const long long o = (long long)j * pitch + i + l * ls;
+    // Row neighbours.  Only a channel (periodic in j) steps rows 0 and jj-1,
+    // whose neighbours wrap (the reference's halo rows hold those rows).
+    const int jm = (j == 0) ? jj - 1 : j - 1, jp = (j == jj - 1) ? 0 : j + 1;
+    auto at = [&](int di, int dj) {
+        return (long long)(dj == 0 ? j : (dj > 0 ? jp : jm)) * pitch + i + di + l * ls;
+    };
     // beta * y with y measured from the basin centre (p_beta_y, qg3.F90:303-307)
     const double by = Mb.beta[l];
     auto q = [&](int di, int dj) {
-        const long long p = o + (long long)dj * pitch + di;
+        const long long p = at(di, dj);
         double v = by * (0.5 * (double)(ii - 3) - (double)(i + di)) + rel[p];
         if (L > 1) {
             if (l == 0)
@@ -43,10 +49,10 @@ __device__ __forceinline__ double lf_increment(const Member& Mb, const double* _
         }
         return v;
     };
-    auto ps = [&](int di, int dj) { return psi[o + (long long)dj * pitch + di]; };
+    auto ps = [&](int di, int dj) { return psi[at(di, dj)]; };
     const double jac = 0.25 * ((q(0, 1) * (ps(-1, 1) - ps(1, 1))) - (q(0, -1) * (ps(-1, -1) - ps(1, -1))) -
                                (q(-1, 0) * (ps(-1, 1) - ps(-1, -1))) + (q(1, 0) * (ps(1, 1) - ps(1, -1))));
-    const double lap = -4.0 * relp[o] + relp[o - 1] + relp[o + 1] + relp[o - pitch] + relp[o + pitch];
+    const double lap = -4.0 * relp[o] + relp[o - 1] + relp[o + 1] + relp[at(0, -1)] + relp[at(0, 1)];
     const double nu = Mb.viscosity, vb = Mb.visc_bot;
     const double w = (l == 0 && Mb.wind) ? Mb.wind[(long long)j * pitch + i] : 0.0;
     if (L == 1) return jac + w + nu * (lap - vb * relp[o]);  // friction inside the bracket for one layer
@@ -77,7 +83,7 @@ __global__ void k_lf_step(const Member* __restrict__ mems, const int* __restrict
     // RA_DOUBLE_FILTER weights, qg3p_aux.F90:48-64
     const double w21 = 0.5 * ra_nu * ra_alpha, w22 = 1.0 - 2.0 * w21;
     const double w11 = -0.5 * ra_nu * (1.0 - ra_alpha), w12 = -2.0 * w11, w13 = 1.0 + w11;
-    const bool interior = i > 0 && i < ii - 1 && j > 0 && j < jj - 1;
+    const bool interior = i > 0 && i < ii - 1 && (Mb.periodic || (j > 0 && j < jj - 1));
     for (int l = 0; l < L; ++l) {
         const long long o = (long long)j * pitch + i + l * ls;
         double lphi = zl[o];
@@ -101,7 +107,7 @@ __global__ void k_lf_forward_euler(const Member* __restrict__ mems, const int* _
     const long long ls = Mb.lstride;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = local;
-    if (i < 1 || i >= ii - 1 || j < 1 || j >= jj - 1) return;
+    if (i < 1 || i >= ii - 1 || (!Mb.periodic && (j < 1 || j >= jj - 1))) return;
     const double* z1 = reinterpret_cast<const double*>(Mb.zeta);
     double* z2 = reinterpret_cast<double*>(Mb.zeta_next);
     const double* rel = reinterpret_cast<const double*>(Mb.rel);
@@ -131,7 +137,7 @@ __global__ void k_lf_rel_bc(const Member* __restrict__ mems, const int* __restri
     double* zo = reinterpret_cast<double*>(Mb.zeta_old[0]);
     const double* psi = Mb.psi;
     auto ps = [&](int a, int b, int l) { return psi[(long long)b * pitch + a + l * ls]; };
-    const bool interior = i > 0 && i < ii - 1 && j > 0 && j < jj - 1;
+    const bool interior = i > 0 && i < ii - 1 && (Mb.periodic || (j > 0 && j < jj - 1));
     for (int l = 0; l < L; ++l) {
         const long long o = (long long)j * pitch + i + l * ls;
         const double r = rel_node(Mb, ps, z[o], i, j, l);

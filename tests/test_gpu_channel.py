@@ -128,8 +128,58 @@ def test_channel_mixed_precision():
     assert rel_l2(owned("psi", g.get("psi"), ii, jj), owned("psi", o.get("psi"), ii, jj)) <= 1e-6
 
 
-def test_channel_leapfrog_is_refused():
+def start_lf(cfg, seed):
+    ic = [pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed + k, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+          for k in (0, 1000)]
+    ic = np.asfortranarray(np.stack(ic, axis=3))
+    g = pq.Model(cfg)
+    g.init_perturb(ic)
+    o = O.Model(cfg.oracle_cfg())
+    o.init(ic)
+    return g, o
+
+
+LF = ["psi", "zeta", "rel", "zeta_old", "psi2", "zeta2", "rel2", "zeta_old2"]
+
+
+@pytest.mark.parametrize("ii,jj,layers", [(65, 64, 3), (33, 40, 1)])
+def test_channel_leapfrog_matches_oracle(ii, jj, layers):
+    """The leapfrog channel: centred step and filter with rows wrapped, the
+    momentum-corrected inversion, rel and the wall PV of each level."""
+    g, o = start_lf(channel(ii, jj, layers, scheme=pq.SCHEME_LEAPFROG), seed=57)
+    compare(g, o, TOL_STEP, LF)
+    for n in (1, 2, 3):
+        g.step(n)
+        o.step(n)
+        compare(g, o, TOL_STEP * 10, LF)
+    g.step(40)
+    o.step(40)
+    compare(g, o, TOL_100, LF)
+    assert abs(g.scalars()["model_time"] - o.scalars()["model_time"]) <= 1e-12 * o.scalars()["model_time"]
+
+
+def test_channel_leapfrog_pickup_and_average(tmp_path):
+    """A leapfrog channel checkpoint (both levels) picks up with rel from psi
+    over the periodic rows; the time average and covariances follow."""
     cfg = channel(65, 64, 3, scheme=pq.SCHEME_LEAPFROG)
-    with pytest.raises(pq.PQError) as e:
-        pq.Model(cfg)
-    assert e.value.code == pq.PQ_ERR_UNSUPPORTED
+    g, o = start_lf(cfg, seed=58)
+    g.step(4)
+    o.step(4)
+    s = str(tmp_path / "lfc_s.d")
+    g.write_checkpoint(s, None, t_scale=cfg.t_scale)
+    ck = O.read_checkpoint(s, None, 65, 64, 3, leapfrog=True)
+    g2 = pq.Model(cfg)
+    g2.read_checkpoint(s)
+    o2 = O.Model(cfg.oracle_cfg())
+    o2.pickup(ck)
+    compare(g2, o2, 1e-13, LF)
+    g2.average(2, 0.0)
+    o2.average(2, 0.0)
+    g2.step(5)
+    o2.step(5)
+    compare(g2, o2, TOL_STEP * 10, LF)
+    a_g, t_g = g2.get_average()
+    a_o, t_o = o2.get_average()
+    assert abs(t_g - t_o) <= 1e-12 * t_o and rel_l2(a_g, a_o) <= 1e-12
+    worst = {n: rel_l2(g2.get_quad(q), o2.get_quad(q)) for q, n in enumerate(g2.QUAD)}
+    assert max(worst.values()) <= 1e-11, worst
