@@ -27,6 +27,8 @@
 // and transformed by a radix-4/2 Stockham FFT in shared memory, the real-FFT
 // split gives C_q = R_q + i I_q, and X_2q = -I_q, X_2q+1 = R_0/2 + sum_{p<=q} R_p
 // (the odd outputs are a prefix sum, done as a block scan).
+#include <type_traits>
+
 #include "pq_common.cuh"
 #include "pq_kernels.h"
 
@@ -387,6 +389,45 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
             __syncthreads();
             // Node k of the L layer rows -> node k of the L mode rows (in
             // place for FP64: a node's values are read before they are written).
+            // z_to_modes with an exact layer count up to five: loops unrolled to
+            // L, z2m in registers (as the back-projection below).
+            auto exact = [&](auto lc) {
+                constexpr int LC = decltype(lc)::value;
+                double zm[LC][LC];
+#pragma unroll
+                for (int m = 0; m < LC; ++m)
+#pragma unroll
+                    for (int l = 0; l < LC; ++l) zm[m][l] = Mb.z2m[m * PQ_MAXL + l];
+                for (int r = 0; r < R; ++r)
+                    for (int k = threadIdx.x; k < N; k += nthr) {
+                        double z[LC];
+#pragma unroll
+                        for (int l = 0; l < LC; ++l)
+                            z[l] = MX ? (double)reinterpret_cast<const float*>(extra)[(size_t)(r * LC + l) * N + k]
+                                      : ubuf(l, r)[k];
+#pragma unroll
+                        for (int m = 0; m < LC; ++m) {
+                            // z_to_modes, qg3p_diagnostics.F90:545-549
+                            double sacc = 0.0;
+#pragma unroll
+                            for (int l = 0; l < LC; ++l) sacc += zm[m][l] * z[l];
+                            put(m, r, k, cff * sacc);
+                        }
+                    }
+            };
+            bool done = false;
+            if constexpr (PRO == PRO_MODAL) {
+                done = true;
+                switch (L) {
+                    case 1: exact(std::integral_constant<int, 1>{}); break;
+                    case 2: exact(std::integral_constant<int, 2>{}); break;
+                    case 3: exact(std::integral_constant<int, 3>{}); break;
+                    case 4: exact(std::integral_constant<int, 4>{}); break;
+                    case 5: exact(std::integral_constant<int, 5>{}); break;
+                    default: done = false;
+                }
+            }
+            if (!done)
             for (int r = 0; r < R; ++r)
                 for (int k = threadIdx.x; k < N; k += nthr) {
                     double z[PQ_MAXL];
@@ -557,6 +598,57 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
             pc2[m] = (m < L && Mb.periodic) ? psiC2[m] : 0.0;
         }
         double* psi = Mb.psi;
+        // Exact layer counts up to five (every configuration here) run with
+        // the loops unrolled to L and m2z in registers: the loops below,
+        // unrolled to PQ_MAXL under predicates, issue several times the
+        // instructions and shared-memory loads (measured 0.6-0.8 us per node
+        // row pass at 513 x 513 x 3 against ~0.1 us for L = 3).
+        auto exact = [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            double mz[LC][LC];
+#pragma unroll
+            for (int l = 0; l < LC; ++l)
+#pragma unroll
+                for (int m = 1; m < LC; ++m) mz[l][m] = Mb.m2z[l * PQ_MAXL + m];
+            const double* c2b = Mb.corr2;
+            for (int r = 0; r < R; ++r) {
+                const int j = j0 + r;
+                if (j >= jend) break;
+                const double* crs = extra + ((long long)r * (LC - 1) - 1) * pitch;  // staged corr rows
+                const double* crg = Mb.corr + (long long)j * pitch;
+                for (int i = threadIdx.x; i < ii; i += nthr) {
+                    const bool inner = (Mb.periodic || (j >= 1 && j <= jj - 2)) && i >= 1 && i <= n;
+                    double ph[LC];
+#pragma unroll
+                    for (int m = 0; m < LC; ++m) ph[m] = inner ? get(m, r, xpad(i)) : 0.0;
+#pragma unroll
+                    for (int m = 1; m < LC; ++m)
+                        ph[m] -= pc[m] * (corr_smem ? crs[m * (long long)pitch + i] : crg[m * ls + i]);
+                    if (Mb.periodic) {
+                        const double* c2 = c2b + (long long)j * pitch + i;
+#pragma unroll
+                        for (int m = 1; m < LC; ++m) ph[m] -= pc2[m] * c2[m * ls];
+                    }
+                    const double b0 = ph[0] - pc[0];
+                    const long long o = (long long)j * pitch + i;
+#pragma unroll
+                    for (int l = 0; l < LC; ++l) {
+                        double dot = 0.0;
+#pragma unroll
+                        for (int m = 1; m < LC; ++m) dot += mz[l][m] * ph[m];
+                        psi[o + l * ls] = b0 + dot;
+                    }
+                }
+            }
+        };
+        switch (L) {
+            case 1: exact(std::integral_constant<int, 1>{}); return;
+            case 2: exact(std::integral_constant<int, 2>{}); return;
+            case 3: exact(std::integral_constant<int, 3>{}); return;
+            case 4: exact(std::integral_constant<int, 4>{}); return;
+            case 5: exact(std::integral_constant<int, 5>{}); return;
+            default: break;
+        }
         for (int r = 0; r < R; ++r)
             for (int i = threadIdx.x; i < ii; i += nthr) {
                 const int j = j0 + r;
