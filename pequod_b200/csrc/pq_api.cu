@@ -609,6 +609,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     for (int p = 0; p < 2; ++p) {
         LaunchSet& s = c->ls[p];
         s.members = c->d_members + p;
+        s.one = &c->hm[p];  // the same descriptor, passed by value to the step kernels
         s.nmem = 1;
         s.maxL = L;
         s.maxN = N;

@@ -17,13 +17,6 @@
 
 namespace pq {
 
-__device__ __forceinline__ void load_member_c(Member& dst, const Member* src) {
-    const int n = sizeof(Member) / 4;
-    const int* s = reinterpret_cast<const int*>(src);
-    int* d = reinterpret_cast<int*>(&dst);
-    for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
-}
-
 // Sweep decomposition: a warp owns one layer of a strip of 32 columns
 // (CAB_SW = 28 output columns plus 2 halo lanes on each side) and marches down
 // a band of Mb.cab_sh output rows (a tuning parameter).  Every per-lane quantity lives in registers as
@@ -446,15 +439,15 @@ __device__ void finish_step(const Member& Mb, double* red) {
 // 2049 x 2049 x 5; four CTAs spill heavily and are slower.
 template <bool PRED, typename T>
 __global__ void __launch_bounds__(CAB_WARPS * 32, 3) k_cabaret_fused(const Member* __restrict__ mems,
-                                                                    const int* __restrict__ prefix, int nmem) {
+                                                                    const int* __restrict__ prefix, int nmem,
+                                                                    const __grid_constant__ Member one, int use_one) {
     __shared__ Member Mb;
     __shared__ double red[CAB_WARPS];
     __shared__ int is_last;
     extern __shared__ __align__(16) double cab_ring[];  // [CAB_WARPS][CAB_RING]
     pdl_wait();
     int local;
-    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
-    load_member_c(Mb, mems + mi);
+    cta_member(Mb, one, use_one, mems, prefix, nmem, blockIdx.x, &local);
     __syncthreads();
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
     const int SH = Mb.cab_sh;
@@ -919,15 +912,15 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
 // (measured -8 % at 513 x 513 x 3); one for short FP64 grids.
 template <bool PRED, typename T, int MINB>
 __global__ void __launch_bounds__(CT_THREADS, MINB) k_cabaret_tile(const Member* __restrict__ mems,
-                                                              const int* __restrict__ prefix, int nmem) {
+                                                              const int* __restrict__ prefix, int nmem,
+                                                              const __grid_constant__ Member one, int use_one) {
     __shared__ Member Mb;
     __shared__ double red[CT_THREADS / 32];
     __shared__ int is_last;
     extern __shared__ __align__(16) char tsm[];
     pdl_wait();
     int local;
-    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
-    load_member_c(Mb, mems + mi);
+    cta_member(Mb, one, use_one, mems, prefix, nmem, blockIdx.x, &local);
     __syncthreads();
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
     const int tx = (ii + CT_X - 1) / CT_X;
@@ -975,14 +968,15 @@ static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb);
         if (e != cudaSuccess) return e;
         return launch_step_kernel(ls.pdl, kern, dim3(ls.ctas_cab), dim3(CT_THREADS), tb, st, ls.members,
-                                  ls.prefix_cab, ls.nmem);
+                                  ls.prefix_cab, ls.nmem, member_arg(ls), member_arg_used(ls));
     }
     const size_t bytes = (size_t)CAB_WARPS * CAB_RING * sizeof(double);
     cudaError_t e =
         cudaFuncSetAttribute(k_cabaret_fused<PRED, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     cudaError_t le = launch_step_kernel(ls.pdl, k_cabaret_fused<PRED, T>, dim3(ls.ctas_cab), dim3(CAB_WARPS * 32),
-                                        bytes, st, ls.members, ls.prefix_cab, ls.nmem);
+                                        bytes, st, ls.members, ls.prefix_cab, ls.nmem, member_arg(ls),
+                                        member_arg_used(ls));
     if (le != cudaSuccess) return le;
     return cudaGetLastError();
 }

@@ -181,6 +181,30 @@ __host__ __device__ inline int tri_ctas(int n, int jj, int L) {
     return L * ((n + KT - 1) / KT);
 }
 
+// The descriptor of this CTA's member into shared memory dst (every thread
+// takes part; the caller synchronises).  A context's own launches (use_one)
+// carry their single member by value in the kernel's parameters, so the copy
+// needs no global-memory round trip before the CTA's first real load (about
+// 1-2 us per kernel at the step's sizes); grouped launches (batches, the
+// server) read it from the device array through the CTA prefix sums.
+__device__ __forceinline__ int find_member(const int* __restrict__ prefix, int nmem, int cta, int* local);
+__device__ __forceinline__ void cta_member(Member& dst, const Member& one, int use_one,
+                                           const Member* __restrict__ mems, const int* __restrict__ prefix,
+                                           int nmem, int cta, int* local) {
+    const Member* src;
+    if (use_one) {
+        *local = cta;
+        src = &one;
+    } else {
+        src = mems + find_member(prefix, nmem, cta, local);
+    }
+    static_assert(sizeof(Member) % 8 == 0, "Member copies in 8-byte words");
+    const int n = sizeof(Member) / 8;
+    const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
+}
+
 // Map a flat CTA index to (member, local CTA) given prefix sums.
 __device__ __forceinline__ int find_member(const int* __restrict__ prefix, int nmem, int cta, int* local) {
     int lo = 0, hi = nmem - 1;

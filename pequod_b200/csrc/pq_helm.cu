@@ -39,13 +39,6 @@ enum { EPI_SPEC = 0, EPI_HELM = 1, EPI_PV = 2 };
 
 constexpr int TRI_THREADS = 256;
 
-__device__ __forceinline__ void load_member(Member& dst, const Member* src) {
-    const int n = sizeof(Member) / 4;
-    const int* s = reinterpret_cast<const int*>(src);
-    int* d = reinterpret_cast<int*>(&dst);
-    for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
-}
-
 // ---------------------------------------------------------------------------
 // Row DSTs: one group of P lanes per (row, mode) unit.
 //
@@ -335,14 +328,14 @@ __device__ __forceinline__ void cp4z(void* dst, const void* src, bool ok) {
 // end to end (spec64), as are the projection, the back-projection and psi.
 template <typename S, int V, int PRO, int EPI>
 __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
-                                             int nmem, int row_offset, int c, int corr_smem) {
+                                             int nmem, int row_offset, int c, int corr_smem,
+                                             const __grid_constant__ Member one, int use_one) {
     constexpr bool MX = sizeof(S) == 4;
     __shared__ Member Mb;
     extern __shared__ __align__(16) double sm[];
     pdl_wait();
     int local;
-    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
-    load_member(Mb, mems + mi);
+    cta_member(Mb, one, use_one, mems, prefix, nmem, blockIdx.x, &local);
     __syncthreads();
     const int L = Mb.L, N = Mb.N, M = Mb.M, logM = Mb.logM, n = Mb.n, ii = Mb.ii, jj = Mb.jj, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
@@ -720,7 +713,8 @@ struct PivotRow {
 // the last CTA of a member finishes psiC.
 template <typename S, bool GS>
 __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restrict__ mems,
-                                                          const int* __restrict__ prefix, int nmem, int do_mean) {
+                                                          const int* __restrict__ prefix, int nmem, int do_mean,
+                                                          const __grid_constant__ Member one, int use_one) {
     __shared__ Member Mb;
     __shared__ double wpart[TRI_THREADS / 32];
     __shared__ double wpart2[TRI_THREADS / 32];  // channel: the second wall
@@ -729,8 +723,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     extern __shared__ __align__(16) double strip[];
     pdl_wait();
     int local;
-    const int mi = find_member(prefix, nmem, blockIdx.x, &local);
-    load_member(Mb, mems + mi);
+    cta_member(Mb, one, use_one, mems, prefix, nmem, blockIdx.x, &local);
     __syncthreads();
     const int n = Mb.n, jj = Mb.jj, pitch = Mb.pitch;
     const int W = tri_warps(jj), KT = 8 / W, NQ = 32 * W;
@@ -1079,7 +1072,7 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const int dir = (EPI == EPI_SPEC) ? 0 : 1;
     return launch_step_kernel(ls.pdl, k_dst<S, V, PRO, EPI>, dim3(ls.ctas_dst[dir]), dim3(threads), bytes, st,
                               ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0,
-                              ls.dst_group, corr_smem);
+                              ls.dst_group, corr_smem, member_arg(ls), member_arg_used(ls));
 }
 
 template <typename S, int PRO, int EPI>
@@ -1114,7 +1107,8 @@ static cudaError_t launch_tri(const LaunchSet& ls, int do_mean, size_t bytes, cu
     cudaError_t e = cudaFuncSetAttribute(k_tridiag<S, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     cudaError_t le = launch_step_kernel(ls.pdl, k_tridiag<S, GS>, dim3(ls.ctas_tri), dim3(TRI_THREADS), bytes, st,
-                                        ls.members, ls.prefix_tri, ls.nmem, do_mean);
+                                        ls.members, ls.prefix_tri, ls.nmem, do_mean, member_arg(ls),
+                                        member_arg_used(ls));
     if (le != cudaSuccess) return le;
     return cudaGetLastError();
 }

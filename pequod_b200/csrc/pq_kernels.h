@@ -12,6 +12,8 @@ namespace pq {
 struct LaunchSet {
     const Member* members;  // device
     int nmem;
+    const Member* one = nullptr;  // host copy of a context's single member (passed by value to the
+                                  // step kernels), null for grouped launches
     int maxL, maxN, maxJ, maxI, maxPitch;
     const int* prefix_rows_interior;  // jj - 2 CTAs per member
     int ctas_rows_interior;
@@ -30,6 +32,13 @@ struct LaunchSet {
     int sm_count;                     // SMs of the device (persistent grids)
     int pdl;                          // launch the step kernels with programmatic dependent launch
 };
+
+// The by-value member argument of a launch and whether the kernel uses it.
+inline const Member& member_arg(const LaunchSet& ls) {
+    static const Member none{};
+    return ls.one ? *ls.one : none;
+}
+inline int member_arg_used(const LaunchSet& ls) { return (ls.one != nullptr && ls.nmem == 1) ? 1 : 0; }
 
 // Launch `kernel` on `st`, with programmatic stream serialisation when pdl
 // is set: the kernel may be scheduled before its predecessor in the stream

@@ -220,6 +220,7 @@ int round_steps(pq_server* s, int max_steps) {
         g.ptri = prefix(l0.ctas_tri);
         g.pcab = prefix(l0.ctas_cab);
         g.ls = l0;
+        g.ls.one = nullptr;  // the group's descriptors come from the device array
         const int n = (int)ids.size();
         g.ls.nmem = n;
         g.ls.ctas_dst[0] = n * l0.ctas_dst[0];
