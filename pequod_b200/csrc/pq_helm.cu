@@ -1113,12 +1113,38 @@ static cudaError_t launch_tri(const LaunchSet& ls, int do_mean, size_t bytes, cu
     return cudaGetLastError();
 }
 
+// Resident CTAs per SM of k_tridiag<S, GS> with `bytes` of shared memory
+// (cached for the last size asked).
+template <typename S, bool GS>
+static int tri_resident(size_t bytes) {
+    static size_t cached_bytes = 0;
+    static int cached = 0;
+    if (cached_bytes != bytes) {
+        int n = 0;
+        if (cudaFuncSetAttribute(k_tridiag<S, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tridiag<S, GS>, TRI_THREADS, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        cached_bytes = bytes;
+        cached = n;
+    }
+    return cached;
+}
+
 cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, int f32, cudaStream_t st) {
     const size_t bytes = tri_smem_bytes(ls.maxJ);
-    // Pivots staged beside the strip when both fit; the FP32 form (whose
-    // strip is loaded synchronously) only while two CTAs still fit an SM.
-    const bool gs = 2 * bytes <= (f32 ? 100 : 160) * 1024;
-    if (f32) return gs ? launch_tri<float, true>(ls, do_mean, 2 * bytes, st) : launch_tri<float, false>(ls, do_mean, bytes, st);
+    // Pivots staged beside the strip when both fit (the FP32 form, whose
+    // strip is loaded synchronously, only while two CTAs still fit an SM) and
+    // the staging costs no resident CTA per SM: measured on B200, staging that
+    // lowers occupancy is slower (1025 x 1025 x 3: -2 % FP64, -4 % mixed per
+    // step; 2049 x 2049 x 5 FP64: -4 %).
+    if (f32) {
+        const bool gs = 2 * bytes <= 100 * 1024 && tri_resident<float, true>(2 * bytes) >= tri_resident<float, false>(bytes);
+        return gs ? launch_tri<float, true>(ls, do_mean, 2 * bytes, st) : launch_tri<float, false>(ls, do_mean, bytes, st);
+    }
+    const bool gs = 2 * bytes <= 160 * 1024 && tri_resident<double, true>(2 * bytes) >= tri_resident<double, false>(bytes);
     return gs ? launch_tri<double, true>(ls, do_mean, 2 * bytes, st) : launch_tri<double, false>(ls, do_mean, bytes, st);
 }
 
