@@ -453,6 +453,71 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
             S* __restrict__ rb = reinterpret_cast<S*>(Mb.res_beta);
             const S* __restrict__ ui = reinterpret_cast<const S*>(Mb.ui);
             S* __restrict__ zp = reinterpret_cast<S*>(Mb.zeta);
+            // Exact layer counts up to five: loops unrolled to L, beta and
+            // z2m in registers (as the modal prologue); the same arithmetic.
+            auto exact = [&](auto lc) {
+                constexpr int LC = decltype(lc)::value;
+                double zm[LC][LC], bt[LC];
+#pragma unroll
+                for (int m = 0; m < LC; ++m) {
+                    bt[m] = Mb.beta[m];
+#pragma unroll
+                    for (int l = 0; l < LC; ++l) zm[m][l] = Mb.z2m[m * PQ_MAXL + l];
+                }
+                for (int r = 0; r < R; ++r) {
+                    const int j = j0 + r;
+                    const bool ok = j < jend;
+                    for (int k = 1 + threadIdx.x; k <= n; k += nthr) {
+                        const long long o = (long long)j * pitch + k;
+                        double a0[LC], a1[LC], a2[LC], a3[LC], a4[LC];
+#pragma unroll
+                        for (int l = 0; l < LC; ++l) {
+                            if (ok) {
+                                const long long ol = o + l * ls;
+                                a0[l] = zo[ol];
+                                a1[l] = rs[ol];
+                                a2[l] = ui[ol];
+                                a3[l] = ui[ol + 1];
+                                a4[l] = rbo[ol];
+                            }
+                        }
+                        double z[LC];
+#pragma unroll
+                        for (int l = 0; l < LC; ++l) {
+                            double zz = 0.0;
+                            if (ok) {
+                                const long long ol = o + l * ls;
+                                // cabaret_predictor, qg3p_aux.F90:1012-1018
+                                zz = a0[l] + 0.5 * dt * a1[l];
+                                // cabaret_beta, qg3p_aux.F90:1051-1059
+                                const double rbn = dt * (0.5 * (a3[l] + a2[l]) * bt[l]);
+                                zz = zz + (1.0 + ta) * rbn - ta * a4[l];
+                                rb[ol] = (S)rbn;
+                                zp[ol] = (S)zz;
+                                if (MX) zz = (double)(S)zz;  // the stored (FP32) value
+                            }
+                            z[l] = zz;
+                        }
+#pragma unroll
+                        for (int m = 0; m < LC; ++m) {
+                            double sacc = 0.0;
+#pragma unroll
+                            for (int l = 0; l < LC; ++l) sacc += zm[m][l] * z[l];
+                            put(m, r, k, cff * sacc);
+                        }
+                    }
+                }
+            };
+            bool done = true;
+            switch (L) {
+                case 1: exact(std::integral_constant<int, 1>{}); break;
+                case 2: exact(std::integral_constant<int, 2>{}); break;
+                case 3: exact(std::integral_constant<int, 3>{}); break;
+                case 4: exact(std::integral_constant<int, 4>{}); break;
+                case 5: exact(std::integral_constant<int, 5>{}); break;
+                default: done = false;
+            }
+            if (!done)
             for (int r = 0; r < R; ++r) {
                 const int j = j0 + r;
                 const bool ok = j < jend;
