@@ -328,10 +328,12 @@ __device__ __forceinline__ void cp4z(void* dst, const void* src, bool ok) {
 // end to end (spec64), as are the projection, the back-projection and psi.
 template <typename S, int V, int PRO, int EPI>
 __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
-                                             int nmem, int row_offset, int c, int corr_smem,
+                                             int nmem, int row_offset, int c, int corr_smem, int psic_here,
                                              const __grid_constant__ Member one, int use_one) {
     constexpr bool MX = sizeof(S) == 4;
     __shared__ Member Mb;
+    __shared__ double psic_s[PQ_MAXL];                   // closed basin: psiC of the inverse
+    __shared__ double psic_red[dst_max_threads(V) / 32 * PQ_MAXL];
     extern __shared__ __align__(16) double sm[];
     pdl_wait();
     int local;
@@ -583,6 +585,44 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
                 for (int k = 1 + lane; k <= n; k += 32) cp4z(d + k, g + k, ok);
             }
         }
+        if (EPI == EPI_PV && psic_here) {
+            // psiC_m = (sum of the tridiagonal CTAs' partial means of mode m)
+            // / (g_ii_int g_jj_int) (modes_to_z_correct_mass,
+            // qg3p_aux.F90:482-521), summed in the same fixed order by every
+            // CTA while its rows load (one pass for all modes); the member's
+            // first CTA publishes it and flags a NaN (the reference aborts,
+            // :504-510) or a value above 1e100 (it warns, :511-517).
+            const int KT = 8 / tri_warps(jj), tpm = (n + KT - 1) / KT;
+            double acc[PQ_MAXL];
+#pragma unroll
+            for (int mm = 0; mm < PQ_MAXL; ++mm) acc[mm] = 0.0;
+            for (int q = threadIdx.x; q < tpm; q += nthr)
+#pragma unroll
+                for (int mm = 0; mm < PQ_MAXL; ++mm)
+                    if (mm < L) acc[mm] += __ldcg(Mb.partials + (long long)mm * tpm + q);
+#pragma unroll
+            for (int mm = 0; mm < PQ_MAXL; ++mm) {
+                if (mm < L) {
+                    const double w = warp_sum(acc[mm]);
+                    if (lane == 0) psic_red[warp * PQ_MAXL + mm] = w;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < L) {
+                const int mm = threadIdx.x;
+                double t = 0.0;
+                for (int w = 0; w < nwarp; ++w) t += psic_red[w * PQ_MAXL + mm];
+                const double pc = t * Mb.mean_scale;
+                psic_s[mm] = pc;
+                if (local == 0) {
+                    Mb.sc->psiC[mm] = pc;
+                    if (pc != pc)
+                        atomicOr(Mb.status, (int)ST_NAN_PSIC);
+                    else if (fabs(pc) > 1.0e100)
+                        atomicOr(Mb.status, (int)ST_LARGE_PSIC);
+                }
+            }
+        }
         if (EPI == EPI_PV && corr_smem) {
             const double* corr = Mb.corr;
             const int cw = pitch >> 1;
@@ -652,7 +692,7 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
         double pc[PQ_MAXL], pc2[PQ_MAXL];
 #pragma unroll
         for (int m = 0; m < PQ_MAXL; ++m) {
-            pc[m] = (m < L) ? psiC[m] : 0.0;
+            pc[m] = (m < L) ? (psic_here ? psic_s[m] : psiC[m]) : 0.0;
             pc2[m] = (m < L && Mb.periodic) ? psiC2[m] : 0.0;
         }
         double* psi = Mb.psi;
@@ -1065,6 +1105,12 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
         }
         Mb.partials[local] = t;
         if (Mb.periodic) Mb.partials[Mb.ntiles_tri + local] = t2;
+    }
+    // do_mean 2 (closed basin, an inverse DST of one wave): its CTAs sum the
+    // partials themselves (psiC_m, while their rows load), so no CTA here
+    // waits on a counter.
+    if (!Mb.periodic && do_mean == 2) return;
+    if (threadIdx.x == 0) {
         __threadfence();
         const unsigned prev = atomicAdd(&Mb.counters[0], 1u);
         is_last = (prev == (unsigned)(Mb.ntiles_tri - 1));
@@ -1121,6 +1167,15 @@ int dst_lanes_batched(int M) {
 int dst_max_threads_host(int V) { return dst_max_threads(V); }
 int dst_rows_per_cta_host(int P, int c) { return dst_rows_per_cta(P, c); }
 
+// Whether the inverse DST sums the closed basin's psiC itself: when its grid
+// is one wave (at most four CTAs per SM; measured: +1 % per step at 513^2 x 3,
+// +2.4 % at 129^2, but -1.2 % at 1025^2, whose inverse runs in several waves),
+// so that the tridiagonal kernel's CTAs skip the last-CTA counter.  The
+// tridiagonal launch and the inverse launch decide from the same LaunchSet.
+static int psic_in_inverse(const LaunchSet& ls) {
+    return (!ls.periodic && ls.ctas_dst[1] <= 4 * ls.sm_count) ? 1 : 0;
+}
+
 template <typename S, int V, int PRO, int EPI>
 static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const int M = ls.maxN / 2, L = ls.maxL;
@@ -1137,7 +1192,8 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const int dir = (EPI == EPI_SPEC) ? 0 : 1;
     return launch_step_kernel(ls.pdl, k_dst<S, V, PRO, EPI>, dim3(ls.ctas_dst[dir]), dim3(threads), bytes, st,
                               ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0,
-                              ls.dst_group, corr_smem, member_arg(ls), member_arg_used(ls));
+                              ls.dst_group, corr_smem, (EPI == EPI_PV) ? psic_in_inverse(ls) : 0, member_arg(ls),
+                              member_arg_used(ls));
 }
 
 template <typename S, int PRO, int EPI>
@@ -1198,8 +1254,9 @@ static int tri_resident(size_t bytes) {
     return cached;
 }
 
-cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean, int f32, cudaStream_t st) {
+cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean_in, int f32, cudaStream_t st) {
     const size_t bytes = tri_smem_bytes(ls.maxJ);
+    const int do_mean = (do_mean_in && psic_in_inverse(ls)) ? 2 : do_mean_in;
     // Pivots staged beside the strip when both fit (the FP32 form, whose
     // strip is loaded synchronously, only while two CTAs still fit an SM) and
     // the staging costs no resident CTA per SM: measured on B200, staging that
