@@ -93,10 +93,10 @@ extern "C" {
 typedef struct pq_model_desc {
     int ii, jj, layers;   /* nodes including the boundary; ii - 1 = 2^p, p >= 2 */
     int periodic_j;       /* 0: closed basin; 1: zonal channel periodic in j, walls at
-                             i = 1 and ii (CABARET only): the momentum-corrected
-                             inversion (qg3p_aux.F90:233-379, 524-575) and periodic
-                             stencils; checkpoints and the time average are closed-
-                             basin only */
+                             i = 1 and ii: the momentum-corrected inversion
+                             (qg3p_aux.F90:233-379, 524-575) and periodic stencils,
+                             CABARET or leapfrog, with checkpoints, the time
+                             average and the quad covariances */
     int scheme;           /* PQ_SCHEME_* */
     int limiter;          /* CABARET_LIMITER (1 = on) */
     int bc_type;          /* PQ_BC_* */
