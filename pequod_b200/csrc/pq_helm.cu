@@ -1235,11 +1235,12 @@ static cudaError_t launch_tri(const LaunchSet& ls, int do_mean, size_t bytes, cu
 }
 
 // Resident CTAs per SM of k_tridiag<S, GS> with `bytes` of shared memory
-// (cached for the last size asked).
+// (cached per host thread for the last size asked: contexts may be driven
+// from several threads).
 template <typename S, bool GS>
 static int tri_resident(size_t bytes) {
-    static size_t cached_bytes = 0;
-    static int cached = 0;
+    thread_local size_t cached_bytes = 0;
+    thread_local int cached = 0;
     if (cached_bytes != bytes) {
         int n = 0;
         if (cudaFuncSetAttribute(k_tridiag<S, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
