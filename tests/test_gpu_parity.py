@@ -370,3 +370,19 @@ def test_pipelined_exchange_matches_oracle():
         o.step(1)
         psi = outs[k].reshape((ii, jj, L), order="F")
         assert rel_l2(psi, o.sdata("psi")) <= TOL_STEP * 10, k
+
+
+@pytest.mark.parametrize("tuning", [{}, {"dst_group": 2, "dst_lanes": 32, "dst_lanes_inv": 32}])
+def test_1025_steps_match_oracle(tuning):
+    """1025 x 1025 x 3: the warp-sweep CABARET kernel, the unstaged
+    tridiagonal kernel, and both places the mass correction psiC is summed:
+    the tridiagonal kernel's last CTA when the inverse DST's grid is several
+    waves (default geometry, 1025 CTAs) and the inverse DST's own CTAs when it
+    is one wave (two rows per CTA, 513 CTAs)."""
+    cfg = double_gyre(1025, 3)
+    g, o = start(cfg, seed=9)
+    if tuning:
+        g.set_tuning(**tuning)
+    g.step(2)
+    o.step(2)
+    compare(g, o, TOL_STEP * 10)
