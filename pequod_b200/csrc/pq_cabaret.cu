@@ -962,9 +962,15 @@ template <bool PRED, typename T>
 static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
     if (ls.cab_kernel == 0) {
         const size_t tb = TileSmem<T>::bytes();
-        // FP32 fits three CTAs per SM at any size; FP64 only on many-wave grids.
-        auto kern = (sizeof(T) == 4 || ls.ctas_cab > 4 * ls.sm_count) ? k_cabaret_tile<PRED, T, 3>
-                                                                       : k_cabaret_tile<PRED, T, 1>;
+        // CTAs per SM the registers must allow (measured on B200): FP64 three
+        // on grids of many waves, else one; FP32 four on grids of more than two
+        // CTAs per SM (40 KB of shared memory each: +2.9 % per step at
+        // 513^2 x 3, +5.1 % at 257^2; -4.8 % on 129^2's 135 CTAs), else three.
+        void (*kern)(const Member*, const int*, int, Member, int);
+        if constexpr (sizeof(T) == 4)
+            kern = ls.ctas_cab > 2 * ls.sm_count ? k_cabaret_tile<PRED, T, 4> : k_cabaret_tile<PRED, T, 3>;
+        else
+            kern = ls.ctas_cab > 4 * ls.sm_count ? k_cabaret_tile<PRED, T, 3> : k_cabaret_tile<PRED, T, 1>;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb);
         if (e != cudaSuccess) return e;
         return launch_step_kernel(ls.pdl, kern, dim3(ls.ctas_cab), dim3(CT_THREADS), tb, st, ls.members,
