@@ -402,7 +402,10 @@ PQ_API int pq_batch_launch_count(const pq_batch* b);
  * the device bytes of the admitted and pooled contexts stay within
  * hbm_budget_bytes.  Each pq_server_poll retires finished runs, admits
  * queued ones (initialisation + first step) and advances every active run
- * by up to max_steps steps with one launch per kernel per shape group.  A
+ * with one launch per kernel per shape group and step: the group with the
+ * most work per step by up to max_steps steps, cheaper groups
+ * proportionally more (up to 64 max_steps), each group up to its nearest
+ * member's end, so that small runs keep their own pace.  A
  * run's result is bit-identical to running it alone (pq_init_perturb +
  * pq_step).  Contexts of finished runs are pooled by configuration and
  * reused. */

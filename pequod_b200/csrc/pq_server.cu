@@ -181,15 +181,37 @@ int admit(pq_server* s) {
     return PQ_OK;
 }
 
-// K steps of every active run, one launch per kernel per shape group.
+// One scheduling round, one launch per kernel per shape group and step.
+// The group with the most work per step (cell-layers over its members, with
+// a floor for the latency-bound small grids) advances up to max_steps steps;
+// cheaper groups advance proportionally more (up to 64 max_steps), so that
+// every group's share of the round takes about the same time on its own
+// stream and a small run does not wait for the big grids' pace -- each group
+// stops at its nearest member's end.
 int round_steps(pq_server* s, int max_steps) {
-    int K = max_steps;
-    for (long id : s->active) K = std::min(K, s->runs[id].nsteps - s->runs[id].done);
-    if (K <= 0 || s->active.empty()) return PQ_OK;
+    if (s->active.empty()) return PQ_OK;
     std::map<std::vector<int>, std::vector<long>> groups;
     for (long id : s->active) {
         const pq_model_desc& d = s->runs[id].desc;
         groups[{d.ii, d.jj, d.layers, d.precision}].push_back(id);
+    }
+    std::vector<int> Kg;
+    {
+        std::vector<double> work;
+        double wmax = 0.0;
+        for (auto& kv : groups) {
+            const pq_model_desc& d = s->runs[kv.second[0]].desc;
+            const double w = std::max((double)d.ii * d.jj * d.layers * kv.second.size(), 5.0e5);
+            work.push_back(w);
+            wmax = std::max(wmax, w);
+        }
+        size_t q = 0;
+        for (auto& kv : groups) {
+            int rem = max_steps * 64;
+            for (long id : kv.second) rem = std::min(rem, s->runs[id].nsteps - s->runs[id].done);
+            const double k = (double)max_steps * wmax / work[q++];
+            Kg.push_back(std::max(0, std::min(rem, (int)std::min(k, (double)max_steps * 64))));
+        }
     }
     // Host staging: for each group two descriptor arrays (the members at
     // their current parity and at the next), then its prefix arrays.
@@ -248,6 +270,7 @@ int round_steps(pq_server* s, int max_steps) {
     for (int q = 0; q < S; ++q) SK(cudaStreamWaitEvent(s->side[q], s->ev[0], 0));
     for (size_t q = 0; q < gs.size(); ++q) {
         G& g = gs[q];
+        const int K = Kg[q];
         cudaStream_t st = s->side[q % S];
         g.ls.prefix_dst[0] = s->d_pref + g.pfwd;
         g.ls.prefix_dst[1] = s->d_pref + g.pinv;
@@ -269,13 +292,18 @@ int round_steps(pq_server* s, int max_steps) {
     }
     SK(cudaEventRecord(s->round_done, s->stream));
     s->round_pending = true;
-    for (long id : s->active) {
-        pq_server::Run& r = s->runs[id];
-        pq_ctx* c = r.c;
-        c->zpar = c->cur ^ ((K - 1) & 1);
-        c->cur ^= (K & 1);
-        c->pred_ready = true;
-        r.done += K;
+    size_t q = 0;
+    for (auto& kv : groups) {
+        const int K = Kg[q++];
+        if (K <= 0) continue;
+        for (long id : kv.second) {
+            pq_server::Run& r = s->runs[id];
+            pq_ctx* c = r.c;
+            c->zpar = c->cur ^ ((K - 1) & 1);
+            c->cur ^= (K & 1);
+            c->pred_ready = true;
+            r.done += K;
+        }
     }
     return PQ_OK;
 }
