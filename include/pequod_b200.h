@@ -343,7 +343,7 @@ PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int 
  *              layer, 1 warp sweeps down bands of cab_band rows (default:
  *              tiles up to jj = 700, sweeps above)
  *   cab_band   output rows per warp of the sweep formulation, 4..128
- *              (default: 8, 32, 40 or 56 for up to 300, 700, 1500 rows
+ *              (default: 8, 32, 35 or 56 for up to 300, 700, 1500 rows
  *              and above)
  *   dst_group  row groups per DST CTA: a CTA holds dst_group * layers
  *              warps (0: automatic, 1); layers * dst_group <= 8

@@ -303,9 +303,9 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     const int ntiles_tri = tri_ctas(n, jj, L);
     // Default CABARET band height by grid size (measured on B200: shorter
     // bands give small grids enough warps, taller ones cut halo rows on big
-    // ones; swept 32..128 at 1025 x 1025 x 3 (best 40) and 2049 x 2049 x 5
+    // ones; swept 32..128 at 1025 x 1025 x 3 (best 35) and 2049 x 2049 x 5
     // (best 56)).
-    const int cab_sh = jj <= 300 ? 8 : jj <= 700 ? 32 : jj <= 1500 ? 40 : 56;
+    const int cab_sh = jj <= 300 ? 8 : jj <= 700 ? 32 : jj <= 1500 ? 35 : 56;
     // CABARET formulation by grid size (measured on B200): tiles up to
     // 700 rows, warp sweeps above (pq_tuning.cab_kernel overrides).
     const int cab_kernel = jj <= 700 ? 0 : 1;
