@@ -517,12 +517,23 @@ struct TileSmem {
 __host__ __device__ constexpr int ct_rows(int h) { return (h + 7) / 8; }
 
 template <bool PRED, bool EDGE, typename T>
-__device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int j0, char* smem) {
+// FP64: the CTA's CFL partial and its count towards the last-CTA step finish
+// are issued right after the face velocities (stage 3), so that the
+// counter's round trip overlaps the extrapolation and the corrector (+1 % per
+// step at 513^2 x 3, +2.6 % at 257^2); every scalar the later stages need is
+// read before (the last CTA may advance them once every CTA has counted).
+// FP32 (64-80 registers, where the extra live values cost more: -5 % at 513^2)
+// counts at the end.  *is_last is set by thread 0 at the end.
+__device__ __forceinline__ void cab_tile(const Member& Mb, int l, int i0, int j0, char* smem, double* red,
+                                         int* is_last, int local) {
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
     const int cur = Mb.cur, nxt = cur ^ 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const T dt = (T)Mb.sc->dt, tu = (T)Mb.sc->tweight_u, ta = (T)Mb.sc->tweight_a;
+    constexpr bool EARLY = sizeof(T) == 8;
+    const bool avg_early = EARLY && cab_average_gate(Mb);
+    const double dt64_early = EARLY ? Mb.sc->dt : 0.0;
     const T hdt = (T)0.5 * dt;
     const double s1 = Mb.s1[l], s2 = Mb.s2[l];
     const int bc = Mb.bc_type;
@@ -820,7 +831,23 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
         }
         sUj[q] = u;
     }
-    __syncthreads();
+    unsigned prev = 0u;
+    auto count = [&]() {
+        umax = warp_max(umax);
+        if (lane == 0) red[warp] = umax;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = 0.0;
+            for (int w = 0; w < CT_THREADS / 32; ++w) m = fmax(m, red[w]);
+            Mb.maxu_part[local] = m;
+            __threadfence();
+            prev = atomicAdd(&Mb.counters[1], 1u);
+        }
+    };
+    if constexpr (EARLY)
+        count();
+    else
+        __syncthreads();
 
     // ---- stage 4: extrapolated face values (cabaret_extrapolator) and fluxes
     T* fin_g = reinterpret_cast<T*>(Mb.zfi[nxt]);
@@ -876,8 +903,8 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
     T* zn_g = reinterpret_cast<T*>(Mb.zeta_old[nxt]);
     T* rbn_g = reinterpret_cast<T*>(Mb.res_beta_other);
     T* zpn_g = reinterpret_cast<T*>(Mb.zeta_next);
-    const bool avg = cab_average_gate(Mb);
-    const double dt64 = Mb.sc->dt;
+    const bool avg = EARLY ? avg_early : cab_average_gate(Mb);
+    const double dt64 = EARLY ? dt64_early : Mb.sc->dt;
 #pragma unroll
     for (int k = 0; k < NU; ++k) {
         const int r = 2 + warp + 8 * k;
@@ -903,7 +930,8 @@ __device__ __forceinline__ double cab_tile(const Member& Mb, int l, int i0, int 
         }
         zn_g[o] = z;
     }
-    return umax;
+    if constexpr (!EARLY) count();
+    if (threadIdx.x == 0) *is_last = (prev == (unsigned)(Mb.ntiles_cab - 1));
 }
 
 // MINB: CTAs per SM the register allocation must allow.  Three (80
@@ -930,21 +958,11 @@ __global__ void __launch_bounds__(CT_THREADS, MINB) k_cabaret_tile(const Member*
     // Interior tiles: footprint [i0-2, i0+CT_X+1] x [j0-2, j0+CT_Y+1] inside
     // the interior nodes.
     const bool inner = i0 - 2 >= 1 && i0 + CT_X + 1 <= ii - 2 && j0 - 2 >= 1 && j0 + CT_Y + 1 <= jj - 2;
-    double umax = inner ? cab_tile<PRED, false, T>(Mb, l, i0, j0, tsm) : cab_tile<PRED, true, T>(Mb, l, i0, j0, tsm);
+    if (inner)
+        cab_tile<PRED, false, T>(Mb, l, i0, j0, tsm, red, &is_last, local);
+    else
+        cab_tile<PRED, true, T>(Mb, l, i0, j0, tsm, red, &is_last, local);
     pdl_release();
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    umax = warp_max(umax);
-    if (lane == 0) red[warp] = umax;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < CT_THREADS / 32; ++w) t = fmax(t, red[w]);
-        Mb.maxu_part[local] = t;
-        __threadfence();
-        const unsigned prev = atomicAdd(&Mb.counters[1], 1u);
-        is_last = (prev == (unsigned)(Mb.ntiles_cab - 1));
-    }
     __syncthreads();
     if (is_last) finish_step(Mb, red);
 }
