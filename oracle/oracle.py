@@ -82,6 +82,8 @@ def lib():
         L.or_model_get_quad.restype = C.c_long
         L.or_model_get_quad.argtypes = [C.c_void_p, C.c_int, _dp]
         L.or_model_finish_step.argtypes = [C.c_void_p]
+        L.or_setup_double_gyre.argtypes = [C.c_void_p, C.c_void_p, _dp]
+        L.or_make_ic.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.c_double, C.c_double, _dp]
         _lib = L
     return _lib
 
@@ -213,6 +215,97 @@ def determinant(a):
     return lib().or_determinant(a.shape[0], _p(a))
 
 
+
+class _Physical(C.Structure):
+    _fields_ = [
+        ("ii", C.c_int), ("jj", C.c_int), ("layers", C.c_int),
+        ("basinscale", C.c_double), ("dt", C.c_double), ("f0", C.c_double), ("beta", C.c_double),
+        ("H", C.c_double * 8), ("gprime", C.c_double * 8), ("tau", C.c_double),
+        ("wind_asym", C.c_double), ("wind_tilt", C.c_double), ("wind_shift", C.c_double),
+        ("visc", C.c_double), ("visc_bot", C.c_double), ("alpha", C.c_double), ("partial_slip", C.c_int),
+        ("max_dt", C.c_double), ("u_scale", C.c_double),
+    ]
+
+
+class _Setup(C.Structure):
+    _fields_ = [
+        ("l_scale", C.c_double), ("t_scale", C.c_double), ("dt", C.c_double), ("max_dt", C.c_double),
+        ("alpha", C.c_double), ("viscosity", C.c_double), ("visc_bot", C.c_double), ("bc_type", C.c_int),
+        ("beta", C.c_double * 8), ("h", C.c_double * 8), ("s1", C.c_double * 8), ("s2", C.c_double * 8),
+        ("ss", C.c_double * 8), ("m2z", C.c_double * 64), ("z2m", C.c_double * 64),
+    ]
+
+
+PHYSICAL_KEYS = ("ii", "jj", "layers", "basinscale", "dt", "f0", "beta", "H", "gprime", "tau", "wind_asym",
+                 "wind_tilt", "wind_shift", "visc", "visc_bot", "alpha", "partial_slip", "max_dt", "u_scale")
+
+
+def setup_double_gyre(phys) -> dict:
+    """The double-gyre driver's set-up (qg3.F90:150-307) computed by the
+    oracle from physical (cgs) parameters alone: a dict with the keys of
+    PHYSICAL_KEYS (H and gprime sequences) or any object with those
+    attributes.  Returns the oracle's model parameters, the wind forcing and
+    t_scale."""
+    get = (lambda k: phys[k]) if isinstance(phys, dict) else (lambda k: getattr(phys, k))
+    p = _Physical()
+    for k in PHYSICAL_KEYS:
+        v = get(k)
+        if k in ("H", "gprime"):
+            for n, x in enumerate(list(v)[:8]):
+                getattr(p, k)[n] = float(x)
+        else:
+            setattr(p, k, v)
+    L = p.layers
+    st = _Setup()
+    wind = np.zeros((p.ii, p.jj), order="F")
+    rc = lib().or_setup_double_gyre(C.addressof(p), C.addressof(st), _p(wind))
+    if rc:
+        raise RuntimeError(f"or_setup_double_gyre rc={rc}")
+    m2z = np.array(st.m2z[: L * L]).reshape((L, L), order="F")
+    z2m = np.array(st.z2m[: L * L]).reshape((L, L), order="F")
+    return dict(ii=p.ii, jj=p.jj, layers=L, dt=st.dt, max_dt=st.max_dt, alpha=st.alpha, viscosity=st.viscosity,
+                visc_bot=st.visc_bot, bc_type=st.bc_type, beta=list(st.beta[:L]), h=list(st.h[:L]),
+                s1=list(st.s1[:L]), s2=list(st.s2[:L]), ss=np.array(st.ss[:L]), m2z=m2z, z2m=z2m,
+                force_wind=wind, t_scale=st.t_scale, l_scale=st.l_scale,
+                ra_nu=0.02, ra_alpha=0.5)  # qg3p_params.F90:31-36
+
+
+def cfg_from(cfg) -> dict:
+    """The oracle's configuration for a model description.
+
+    A description built from physical parameters (it carries them as
+    `physical`) is set up again here, by the oracle's own restatement of the
+    driver; only the run's switches (scheme, limiter, channel, adaptive step)
+    are taken from the description.  A hand-written description (no
+    `physical`, e.g. a Helmholtz test problem) is taken as it stands."""
+    d = cfg.desc
+    L = d.layers
+    out = dict(ii=d.ii, jj=d.jj, layers=L, periodic_j=d.periodic_j, scheme=d.scheme, limiter=d.limiter,
+               adapt_dt=d.adapt_dt, target_cfl=d.target_cfl, max_dt_increase=d.max_dt_increase)
+    phys = getattr(cfg, "physical", None)
+    if phys is not None:
+        st = setup_double_gyre(phys)
+        st.pop("t_scale")
+        st.pop("l_scale")
+        out.update(st)
+        return out
+    m2z = np.array(d.m2z[: L * L]).reshape((L, L), order="F")
+    z2m = np.array(d.z2m[: L * L]).reshape((L, L), order="F")
+    out.update(dt=d.dt, beta=list(d.beta[:L]), h=list(d.h[:L]), s1=list(d.s1[:L]), s2=list(d.s2[:L]),
+               ss=np.array(d.ss[:L]), m2z=m2z, z2m=z2m, viscosity=d.viscosity, visc_bot=d.visc_bot,
+               bc_type=d.bc_type, alpha=d.alpha, force_wind=getattr(cfg, "wind", None), max_dt=d.max_dt,
+               ra_nu=d.ra_nu, ra_alpha=d.ra_alpha)
+    return out
+
+
+def make_ic(ii, jj, layers, seed=0, amplitude=1.0, sigma=3.0) -> np.ndarray:
+    """The seeded synthetic initial PV, (ii, jj, layers), Fortran order."""
+    out = np.zeros((ii, jj, layers), order="F")
+    rc = lib().or_make_ic(ii, jj, layers, seed, amplitude, sigma, _p(out))
+    if rc:
+        raise RuntimeError(f"or_make_ic rc={rc}")
+    return out
+
 class _Params(C.Structure):
     _fields_ = [
         ("ii", C.c_int), ("jj", C.c_int), ("layers", C.c_int),
@@ -229,8 +322,8 @@ class _Params(C.Structure):
 class Model:
     """The serial qg3 time loop (qg3.F90:590-967) on reference-layout state.
 
-    ``cfg`` is the non-dimensional configuration dictionary produced by
-    pequod_b200.setup (keys: ii, jj, layers, dt, beta, h, s1, s2, ss, m2z,
+    ``cfg`` is the non-dimensional configuration dictionary of cfg_from /
+    setup_double_gyre (keys: ii, jj, layers, dt, beta, h, s1, s2, ss, m2z,
     z2m, viscosity, visc_bot, bc_type, alpha, force_wind, scheme, ...).
     """
 

@@ -12,6 +12,7 @@
 #include "pq_oracle.h"
 
 #include <cmath>
+#include <cstdint>
 #include <limits>
 #include <cstdlib>
 #include <cstring>
@@ -2164,6 +2165,130 @@ int or_pv_inversion(or_model* m, const double* zeta_data, double* psi_data) {
     int rc = pv_inversion(*m, z, p);
     std::memcpy(psi_data, p.data(), p.size() * sizeof(double));
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Double-gyre driver set-up, restated from the reference's qg3 program for
+// the configuration the tests and the CPU baseline run: the
+// non-dimensionalisation (qg3.F90:152-168), the STRAT_INPUT stratification
+// file (qg3p_io.F90:56-102: line k holds h(k), s1(k-1), s2(k)) with
+// s2(k) = f0^2 / (g'_k H_k), s1(k+1) = f0^2 / (g'_k H_(k+1)), the
+// stratification object (qg3p_diagnostics.F90:210-236, 342-422), tau / h(1)
+// (qg3.F90:235), the boundary condition (:239-248), the wind curl (:253-271)
+// and beta (:163).  Computed here from the physical parameters alone, so the
+// checker does not share the product's set-up code.
+int or_setup_double_gyre(const or_physical* p, or_setup* out, double* wind) {
+    if (!p || !out || p->layers < 1 || p->layers > 8 || p->ii < 5 || p->jj < 5) return -1;
+    std::memset(out, 0, sizeof(*out));
+    const int L = p->layers;
+    const double u_scale = p->u_scale > 0.0 ? p->u_scale : 1.0;
+    const int g_ii_int = p->ii - 1;
+    const double l_scale = p->basinscale / (double)g_ii_int;  // qg3.F90:152
+    const double t_scale = l_scale / u_scale;                 // :153
+    out->l_scale = l_scale;
+    out->t_scale = t_scale;
+    out->dt = p->dt / t_scale;                                // :155
+    out->max_dt = p->max_dt > 0.0 ? p->max_dt / t_scale : 1.0e300;  // :159
+    out->alpha = l_scale / p->alpha;                          // :161
+    const double beta = p->beta * l_scale * l_scale / u_scale;  // :162
+    out->viscosity = p->visc / (l_scale * u_scale);           // :166
+    out->visc_bot = p->visc_bot * l_scale / u_scale;          // :167
+    double tau = p->tau / (u_scale * u_scale * (double)g_ii_int);  // :164
+    // Stratification file values (cgs): s1_in(k) = strat%s1(k+1),
+    // s2_in(k) = strat%s2(k), k = 1..L-1.
+    double s1_in[8] = {0}, s2_in[8] = {0};
+    for (int k = 0; k < L - 1; ++k) {
+        s2_in[k] = p->f0 * p->f0 / (p->gprime[k] * p->H[k]);
+        s1_in[k] = p->f0 * p->f0 / (p->gprime[k] * p->H[k + 1]);
+    }
+    int rc = or_strat_from_parameters(L, p->H, s1_in, s2_in, l_scale, out->h, out->s1, out->s2, out->ss,
+                                      out->m2z, out->z2m);
+    if (rc) return rc;
+    for (int k = 0; k < L; ++k) out->beta[k] = beta;
+    tau = tau / out->h[0];  // qg3.F90:235
+    if (p->partial_slip) {  // :239-248
+        if (p->alpha >= 1.0e100) {
+            out->bc_type = OR_BC_FREE_SLIP;
+            out->alpha = 0.0;
+        } else {
+            out->bc_type = OR_BC_PARTIAL_SLIP;
+        }
+    } else {
+        out->bc_type = OR_BC_NO_SLIP;
+    }
+    if (wind) {  // :253-271 (one rank: ii_0 = jj_0 = 0)
+        const double pi = 3.14159265358979323846;
+        const double a_wind = -1.0 * p->wind_asym, b_wind = 1.0 / p->wind_asym;
+        for (int j = 1; j <= p->jj; ++j)
+            for (int i = 1; i <= p->ii; ++i) {
+                const double x = (double)(j - 1) / (double)(p->jj - 1) - 0.5;
+                const double y = -(double)(i - 1) / (double)(p->ii - 1) + 0.5;
+                const double y_mid = p->wind_shift + p->wind_tilt * x;
+                double f;
+                if (y < y_mid)
+                    f = a_wind * std::sin(pi * (0.5 + y) / (0.5 + y_mid));
+                else
+                    f = b_wind * std::sin(pi * (y - y_mid) / (0.5 - y_mid));
+                wind[(size_t)(i - 1) + (size_t)p->ii * (j - 1)] = tau * 2.0 * pi * f;
+            }
+    }
+    return 0;
+}
+
+// The seeded synthetic initial PV of the benchmark workloads (the reference's
+// own random_number IC is gfortran-specific, so the runs take this one as
+// input): splitmix64 uniforms, Box-Muller normals in pairs, a separable
+// Gaussian smoothing of standard deviation sigma cells truncated at 3 sigma
+// and renormalised, times amplitude.  out: (ii, jj, L) sdata.
+static uint64_t or_splitmix64(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+int or_make_ic(int ii, int jj, int L, unsigned long long seed, double amplitude, double sigma, double* out) {
+    if (ii < 1 || jj < 1 || L < 1 || !out) return -1;
+    const double pi = 3.14159265358979323846;
+    const size_t plane = (size_t)ii * jj, total = plane * L;
+    uint64_t s = seed * 0x2545F4914F6CDD1Dull + 0x1234567ull;
+    std::vector<double> g(total);
+    for (size_t k = 0; k < total; k += 2) {
+        const double u1 = ((or_splitmix64(s) >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+        const double u2 = ((or_splitmix64(s) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        const double r = std::sqrt(-2.0 * std::log(u1));
+        g[k] = r * std::cos(2.0 * pi * u2);
+        if (k + 1 < total) g[k + 1] = r * std::sin(2.0 * pi * u2);
+    }
+    const int R = sigma > 0.0 ? (int)std::ceil(3.0 * sigma) : 0;
+    std::vector<double> w(2 * R + 1, 1.0);
+    if (R > 0) {
+        double sum = 0.0;
+        for (int q = -R; q <= R; ++q) sum += (w[q + R] = std::exp(-0.5 * (q * q) / (sigma * sigma)));
+        for (double& v : w) v /= sum;
+    }
+    std::vector<double> row(plane);
+    for (int l = 0; l < L; ++l) {
+        double* f = g.data() + plane * l;
+        if (R > 0) {
+            for (int j = 0; j < jj; ++j)  // along i
+                for (int i = 0; i < ii; ++i) {
+                    double a = 0.0;
+                    for (int q = -R; q <= R; ++q)
+                        if (i + q >= 0 && i + q < ii) a += w[q + R] * f[(size_t)(i + q) + (size_t)ii * j];
+                    row[(size_t)i + (size_t)ii * j] = a;
+                }
+            for (int j = 0; j < jj; ++j)  // along j
+                for (int i = 0; i < ii; ++i) {
+                    double a = 0.0;
+                    for (int q = -R; q <= R; ++q)
+                        if (j + q >= 0 && j + q < jj) a += w[q + R] * row[(size_t)i + (size_t)ii * (j + q)];
+                    f[(size_t)i + (size_t)ii * j] = a;
+                }
+        }
+        for (size_t k = 0; k < plane; ++k) out[plane * l + k] = amplitude * f[k];
+    }
+    return 0;
 }
 
 }  // extern "C"

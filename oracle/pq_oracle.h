@@ -79,6 +79,38 @@ double or_mean(int ii, int jj, int periodic_j, const double* psi);
 void or_energy(int ii, int jj, int layers, int periodic_j, const double* h,
                const double* s2, const double* psi, double* ekin, double* epot);
 
+/* ---- double-gyre driver set-up (qg3.F90:150-307) ------------------------ */
+typedef struct {
+    int ii, jj, layers;
+    double basinscale;        /* cm */
+    double dt;                /* s */
+    double f0, beta;          /* s^-1, cm^-1 s^-1 */
+    double H[8];              /* cm */
+    double gprime[8];         /* cm s^-2, interfaces 1..L-1 */
+    double tau;               /* cm^2 s^-2 */
+    double wind_asym, wind_tilt, wind_shift;
+    double visc, visc_bot;    /* cm^2 s^-1, s^-1 */
+    double alpha;             /* cm; >= 1e100: free slip */
+    int partial_slip;
+    double max_dt;            /* s */
+    double u_scale;           /* cm s^-1 */
+} or_physical;
+
+typedef struct {
+    double l_scale, t_scale;
+    double dt, max_dt, alpha, viscosity, visc_bot;
+    int bc_type;
+    double beta[8], h[8], s1[8], s2[8], ss[8];
+    double m2z[64], z2m[64];  /* L x L column-major, leading dimension L */
+} or_setup;
+
+/* Non-dimensional model parameters and the layer-1 wind forcing (ii, jj)
+ * of the double gyre, from the physical parameters alone. */
+int or_setup_double_gyre(const or_physical* p, or_setup* out, double* wind);
+/* Seeded synthetic initial PV, (ii, jj, L) sdata. */
+int or_make_ic(int ii, int jj, int layers, unsigned long long seed, double amplitude, double sigma,
+               double* out);
+
 /* ---- full model, one rank, closed basin or channel --------------------- */
 typedef struct {
     int ii, jj, layers;

@@ -209,10 +209,11 @@ def double_gyre_physical(ii, jj=None, layers=3, dt=1800.0, dx=30.0e5, H=(3.0e4, 
 class Config:
     """A non-dimensional model description plus its wind-forcing buffer."""
 
-    def __init__(self, desc: ModelDesc, wind: np.ndarray | None, t_scale: float):
+    def __init__(self, desc: ModelDesc, wind: np.ndarray | None, t_scale: float, physical: Physical | None = None):
         self.desc = desc
         self.wind = wind
         self.t_scale = t_scale
+        self.physical = physical  # the cgs description it was set up from, if any
         if wind is not None:
             self.desc.force_wind = _p(self.wind)
 
@@ -222,7 +223,7 @@ class Config:
         wind = np.zeros((p.ii, p.jj), order="F")
         ts = np.zeros(1)
         _check(lib().pq_setup_double_gyre(C.byref(p), C.byref(d), _p(wind), _p(ts)))
-        return cls(d, wind, float(ts[0]))
+        return cls(d, wind, float(ts[0]), p)
 
     @property
     def ii(self):
@@ -241,19 +242,6 @@ class Config:
         m2z = np.array(self.desc.m2z[: L * L]).reshape((L, L), order="F")
         z2m = np.array(self.desc.z2m[: L * L]).reshape((L, L), order="F")
         return np.array(self.desc.ss[:L]), m2z, z2m
-
-    def oracle_cfg(self) -> dict:
-        """The same configuration as a dictionary for the CPU oracle."""
-        L = self.layers
-        ss, m2z, z2m = self.modal()
-        d = self.desc
-        return dict(
-            ii=d.ii, jj=d.jj, layers=L, dt=d.dt, beta=list(d.beta[:L]), h=list(d.h[:L]), s1=list(d.s1[:L]),
-            s2=list(d.s2[:L]), ss=ss, m2z=m2z, z2m=z2m, viscosity=d.viscosity, visc_bot=d.visc_bot,
-            bc_type=d.bc_type, alpha=d.alpha, force_wind=self.wind, scheme=d.scheme, limiter=d.limiter,
-            adapt_dt=d.adapt_dt, target_cfl=d.target_cfl, max_dt=d.max_dt, max_dt_increase=d.max_dt_increase,
-            ra_nu=d.ra_nu, ra_alpha=d.ra_alpha, periodic_j=d.periodic_j,
-        )
 
 
 def make_ic(ii, jj, layers, seed=0, amplitude=1.0, sigma=3.0) -> np.ndarray:

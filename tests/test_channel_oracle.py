@@ -21,7 +21,7 @@ def channel(ii, jj, layers=3, dt=1800.0, **kw):
 
 def wall_pv_means(cfg, psi_modal, ss):
     """zeta_boundary in numpy: mean wall PV of each modal field (ii, jj, L)."""
-    oc = cfg.oracle_cfg()
+    oc = O.cfg_from(cfg)
     bc, alpha = oc["bc_type"], oc["alpha"]
     jj = psi_modal.shape[1]
     zb = np.zeros(psi_modal.shape[2])
@@ -42,7 +42,7 @@ def wall_pv_means(cfg, psi_modal, ss):
 
 def start(cfg, seed):
     ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     return o, ic
 
@@ -68,9 +68,9 @@ def test_channel_is_periodic_in_j():
     channel has no seam (up to the order of the wall sums)."""
     cfg = channel(33, 32, 3)
     ic = pq.make_ic(33, 32, 3, seed=12, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
-    a = O.Model(cfg.oracle_cfg())
+    a = O.Model(O.cfg_from(cfg))
     a.init(ic)
-    b = O.Model(cfg.oracle_cfg())
+    b = O.Model(O.cfg_from(cfg))
     b.init(np.asfortranarray(np.roll(ic, 5, axis=1)))
     a.step(6)
     b.step(6)
@@ -107,9 +107,9 @@ def test_leapfrog_channel_is_periodic_with_consistent_halos():
     ic1 = pq.make_ic(33, 32, 3, seed=14, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     ic2 = pq.make_ic(33, 32, 3, seed=15, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     ic = np.asfortranarray(np.stack([ic1, ic2], axis=3))
-    a = O.Model(cfg.oracle_cfg())
+    a = O.Model(O.cfg_from(cfg))
     a.init(ic)
-    b = O.Model(cfg.oracle_cfg())
+    b = O.Model(O.cfg_from(cfg))
     b.init(np.asfortranarray(np.roll(ic, 5, axis=1)))
     a.step(7)
     b.step(7)

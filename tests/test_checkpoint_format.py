@@ -29,10 +29,10 @@ def channel(ii, jj, layers=3, dt=1800.0, **kw):
 
 def run_oracle(cfg, steps, seed):
     ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
-    if cfg.oracle_cfg().get("scheme", 0) == 1:
+    if O.cfg_from(cfg).get("scheme", 0) == 1:
         ic2 = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed + 1000, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
         ic = np.asfortranarray(np.stack([ic, ic2], axis=3))
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     o.step(steps)
     return o
@@ -122,7 +122,7 @@ def test_cabaret_pickup_matches_numpy(tmp_path, adapt):
     dt = o.scalars()["dt"]
     O.write_checkpoint(s, supp, fields, 0.1, 0.1, dt=dt)
     ck = O.read_checkpoint(s, supp, 17, 17, 3)
-    p = O.Model(cfg.oracle_cfg())
+    p = O.Model(O.cfg_from(cfg))
     p.pickup(ck)
     want = numpy_cabaret_pickup(ck, dt)
     ii = jj = 17
@@ -171,7 +171,7 @@ def test_channel_pickup_resumes_bit_for_bit(tmp_path, adapt):
         np.testing.assert_array_equal(ck[n][2:ii + 1, 1:jj + 1], fields[n][2:ii + 1, 1:jj + 1])
     for n in ("uj", "zeta_fj"):
         np.testing.assert_array_equal(ck[n][2:ii, 1:jj + 2], fields[n][2:ii, 1:jj + 2])
-    p = O.Model(cfg.oracle_cfg())
+    p = O.Model(O.cfg_from(cfg))
     p.pickup(ck)
     o.finish_step()
     for n in ("psi", "zeta", "zeta_old", "uimo", "ujmo", "zeta_fj", "res", "res_beta"):
@@ -188,7 +188,7 @@ def test_leapfrog_pickup_rel_from_psi(tmp_path, bc):
     """rel_from_psi (qg3p_aux.F90:579-603) + apply_rel_bc on both levels."""
     s = str(tmp_path / "lf_s.d")
     cfg = double_gyre(17, 2, scheme=pq.SCHEME_LEAPFROG, partial_slip=int(bc == pq.BC_PARTIAL_SLIP))
-    oc = cfg.oracle_cfg()
+    oc = O.cfg_from(cfg)
     oc["bc_type"] = bc
     ic = pq.make_ic(17, 17, 2, seed=4, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     o = O.Model(oc)
@@ -231,7 +231,7 @@ def test_oracle_time_average(scheme, periodic):
     model time passed the threshold, restated step by step in numpy."""
     cfg = channel(17, 20, 2) if periodic else double_gyre(17, 2, scheme=scheme)
     o = run_oracle(cfg, 0, seed=5)
-    dt = cfg.oracle_cfg()["dt"]
+    dt = O.cfg_from(cfg)["dt"]
     t0 = o.scalars()["model_time"]
     thr = t0 + 3.2 * dt          # the first steps are not averaged
     o.average(True, thr)
@@ -257,7 +257,7 @@ def test_oracle_time_average(scheme, periodic):
 def numpy_quad_terms(psi, rel, zeta, cfg, periodic_j=False):
     """qg3.F90:683-721 in numpy on sdata (ii, jj, L): the 23 products.  A
     channel has no j walls: u is central on every row, v wraps in j."""
-    oc = cfg.oracle_cfg()
+    oc = O.cfg_from(cfg)
     ii, jj, L = psi.shape
     bc, alpha = oc["bc_type"], oc["alpha"]
     s1, s2, h = np.array(oc["s1"]), np.array(oc["s2"]), np.array(oc["h"])
@@ -308,7 +308,7 @@ def test_oracle_quad_diagnostics(partial_slip, periodic):
     threshold passed; in a closed basin and in a channel."""
     cfg = channel(17, 20, 3, partial_slip=partial_slip) if periodic else double_gyre(17, 3, partial_slip=partial_slip)
     o = run_oracle(cfg, 1, seed=7)
-    dt = cfg.oracle_cfg()["dt"]
+    dt = O.cfg_from(cfg)["dt"]
     thr = o.scalars()["model_time"] + 1.2 * dt
     o.average(2, thr)
     acc = None
@@ -321,7 +321,7 @@ def test_oracle_quad_diagnostics(partial_slip, periodic):
             # includes): rel minus the stratification coupling, the inverse
             # of rel_from_zeta_and_psi / update_zeta_bc
             psi, rel = o.sdata("psi"), o.sdata("rel")
-            oc = cfg.oracle_cfg()
+            oc = O.cfg_from(cfg)
             s1, s2 = np.array(oc["s1"]), np.array(oc["s2"])
             zeta = rel.copy()
             zeta[:, :, 0] -= s2[0] * (psi[:, :, 0] - psi[:, :, 1])
@@ -344,7 +344,7 @@ def test_oracle_quad_diagnostics_leapfrog():
     time after its increment."""
     cfg = double_gyre(17, 3, scheme=pq.SCHEME_LEAPFROG)
     o = run_oracle(cfg, 2, seed=9)
-    dt = cfg.oracle_cfg()["dt"]
+    dt = O.cfg_from(cfg)["dt"]
     thr = o.scalars()["model_time"] + 1.5 * dt
     o.average(2, thr)
     acc = None

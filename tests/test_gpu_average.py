@@ -32,7 +32,7 @@ def start(cfg, seed):
         ic = np.asfortranarray(np.stack([ic, ic2], axis=3))
     g = pq.Model(cfg)
     g.init_perturb(ic)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     return g, o
 

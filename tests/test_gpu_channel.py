@@ -36,7 +36,7 @@ def start(cfg, seed):
     ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     g = pq.Model(cfg)
     g.init_perturb(ic)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     return g, o
 
@@ -76,7 +76,7 @@ def test_channel_pv_inversion_matches_oracle(partial_slip):
     zeta = np.asfortranarray(rng.standard_normal((129, 128, 3)))
     g = pq.Model(cfg)
     psi = g.pv_inversion(zeta)
-    om = O.Model(cfg.oracle_cfg())
+    om = O.Model(O.cfg_from(cfg))
     zd = np.zeros((131, 130, 3), order="F")
     zd[1:-1, 1:-1, :] = zeta
     ref = om.pv_inversion(zd)[1:-1, 1:-1, :]
@@ -134,7 +134,7 @@ def start_lf(cfg, seed):
     ic = np.asfortranarray(np.stack(ic, axis=3))
     g = pq.Model(cfg)
     g.init_perturb(ic)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     return g, o
 
@@ -170,7 +170,7 @@ def test_channel_leapfrog_pickup_and_average(tmp_path):
     ck = O.read_checkpoint(s, None, 65, 64, 3, leapfrog=True)
     g2 = pq.Model(cfg)
     g2.read_checkpoint(s)
-    o2 = O.Model(cfg.oracle_cfg())
+    o2 = O.Model(O.cfg_from(cfg))
     o2.pickup(ck)
     compare(g2, o2, 1e-13, LF)
     g2.average(2, 0.0)

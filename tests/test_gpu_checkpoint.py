@@ -40,7 +40,7 @@ def start(cfg, seed):
         ic = np.asfortranarray(np.stack([ic, ic2], axis=3))
     g = pq.Model(cfg)
     g.init_perturb(ic)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     return g, o
 
@@ -97,7 +97,7 @@ def test_cabaret_pickup_matches_oracle(tmp_path, adapt):
     g2 = pq.Model(cfg)
     total = g2.read_checkpoint(s, supp)
     assert total == ck["total_time_day"]
-    o2 = O.Model(cfg.oracle_cfg())
+    o2 = O.Model(O.cfg_from(cfg))
     o2.pickup(ck)
     # Both pick up from the same file: the set-up arithmetic is the same.
     compare(g2, o2, AFTER, 1e-15)
@@ -127,7 +127,7 @@ def test_pickup_into_a_context_that_has_run(tmp_path):
     g.write_checkpoint(s, supp)
     g.step(3)   # move on, then go back to the dump
     g.read_checkpoint(s, supp)
-    o2 = O.Model(cfg.oracle_cfg())
+    o2 = O.Model(O.cfg_from(cfg))
     o2.pickup(O.read_checkpoint(s, supp, 65, 65, 3))
     g.step(4)
     o2.step(4)
@@ -150,7 +150,7 @@ def test_leapfrog_checkpoint_round_trip(tmp_path):
         assert rel_l2(ck[n][1:-1, 1:-1], o.get(n)[1:-1, 1:-1]) <= TOL, n
     g2 = pq.Model(cfg)
     g2.read_checkpoint(s)
-    o2 = O.Model(cfg.oracle_cfg())
+    o2 = O.Model(O.cfg_from(cfg))
     o2.pickup(ck)
     levels = ["psi", "zeta", "rel", "zeta_old", "psi2", "zeta2", "rel2", "zeta_old2"]
     compare(g2, o2, levels, 1e-15)
@@ -173,7 +173,7 @@ def test_mixed_precision_pickup(tmp_path):
     ck = O.read_checkpoint(s, supp, 129, 129, 3)
     g2 = pq.Model(cfg)
     g2.read_checkpoint(s, supp)
-    o2 = O.Model(cfg.oracle_cfg())
+    o2 = O.Model(O.cfg_from(cfg))
     o2.pickup(ck)
     g2.step(10)
     o2.step(10)
@@ -287,7 +287,7 @@ def test_channel_pickup_matches_oracle(tmp_path, adapt):
     g2 = pq.Model(cfg)
     total = g2.read_checkpoint(s, supp)
     assert total == ck["total_time_day"]
-    o2 = O.Model(cfg.oracle_cfg())
+    o2 = O.Model(O.cfg_from(cfg))
     o2.pickup(ck)
     compare_channel(g2, o2, AFTER, 1e-15)
     assert g2.scalars()["model_time"] == o2.scalars()["model_time"]

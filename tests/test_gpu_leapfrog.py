@@ -37,7 +37,7 @@ def start(cfg, seed):
     ic = np.asfortranarray(ic)
     g = pq.Model(cfg)
     g.init_perturb(ic)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     return g, o
 

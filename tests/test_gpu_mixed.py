@@ -46,7 +46,7 @@ def test_mixed_pv_inversion(ii, layers):
     zeta = np.asfortranarray(rng.standard_normal((ii, ii, layers)))
     g = pq.Model(cfg)
     psi = g.pv_inversion(zeta)
-    om = O.Model(cfg.oracle_cfg())
+    om = O.Model(O.cfg_from(cfg))
     zd = np.zeros((ii + 2, ii + 2, layers), order="F")
     zd[1:-1, 1:-1, :] = zeta
     ref = om.pv_inversion(zd)[1:-1, 1:-1, :]
@@ -56,7 +56,7 @@ def test_mixed_pv_inversion(ii, layers):
 def test_mixed_hundred_steps_vs_oracle():
     cfg = double_gyre(129, 3)
     g, ic = start(cfg, seed=11)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     g.step(100)
     o.step(100)
@@ -87,7 +87,7 @@ def test_mixed_adaptive_dt():
     """The non-fused step (predictor in the forward DST) in FP32 storage."""
     cfg = double_gyre(65, 3, adapt_dt=1, target_cfl=0.1, max_dt=86400.0)
     g, ic = start(cfg, seed=12)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     g.step(20)
     o.step(20)

@@ -166,7 +166,7 @@ def test_pv_inversion_matches_oracle(ii, layers):
     zeta = np.asfortranarray(rng.standard_normal((ii, ii, layers)))
     g = pq.Model(cfg)
     psi = g.pv_inversion(zeta)
-    om = O.Model(cfg.oracle_cfg())
+    om = O.Model(O.cfg_from(cfg))
     zd = np.zeros((ii + 2, ii + 2, layers), order="F")
     zd[1:-1, 1:-1, :] = zeta
     ref = om.pv_inversion(zd)[1:-1, 1:-1, :]
@@ -177,7 +177,7 @@ def start(cfg, seed=1):
     ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     g = pq.Model(cfg)
     g.init_perturb(ic)
-    o = O.Model(cfg.oracle_cfg())
+    o = O.Model(O.cfg_from(cfg))
     o.init(ic)
     return g, o
 
