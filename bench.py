@@ -451,7 +451,13 @@ def run_batched(a, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dist = multirank.init(world)
-    shapes, ss = batched_helmholtz(a.batch, seed=multirank.rank_seed(2, rank))
+    # One batch for the whole job; each rank solves its share of the members
+    # (balanced by ii * jj * L, no exchange while solving).
+    all_shapes, all_ss = batched_helmholtz(a.batch, seed=2)
+    total_units = sum(i * j * l for i, j, l in all_shapes)
+    mine = multirank.partition([i * j * l for i, j, l in all_shapes], world)[rank]
+    shapes = [all_shapes[k] for k in mine]
+    ss = [all_ss[k] for k in mine]
     b = pq.Batch(shapes, ss, device=local_rank)
     # One right-hand side per distinct shape (the timing does not depend on the values).
     rhs_of = {}
@@ -515,19 +521,20 @@ def run_batched(a, rank, world, local_rank):
             cpu = {"value": done_units / secs, "unit": "cell-layer-solves/s", "cores": 1, "kind": "port",
                    "sample": f"{nsolve} smallest members solved by the oracle's helm in {secs:.1f} s"}
         line = {
-            "metric": "cell-layer-solves/s", "value": world * units * K / (ms * 1e-3), "unit": "cell-layer-solves/s",
+            "metric": "cell-layer-solves/s", "value": total_units * K / (ms * 1e-3), "unit": "cell-layer-solves/s",
             "n_gpus": world, "steps": K, "warmup": a.warmup, "ms_per_step": ms / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"batched_helmholtz_{len(shapes)}", "solves_per_step": len(shapes),
-                       "cell_layers_per_step": units, "sizes": "ii, jj in {65..1025}, L in 1..5",
-                       "l2": f"inputs {8 * units / 1e9:.1f} GB >> L2", "parallelism": f"replicas{world}",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"batched_helmholtz_{len(all_shapes)}", "solves_per_step": len(all_shapes),
+                       "cell_layers_per_step": total_units, "sizes": "ii, jj in {65..1025}, L in 1..5",
+                       "l2": f"inputs {8 * units / 1e9:.1f} GB per rank >> L2",
+                       "parallelism": f"members sharded over {world} rank(s), balanced by ii*jj*L",
                        "launches_per_solve": b.launch_count()},
-            "solves_per_s": world * len(shapes) * K / (ms * 1e-3),
+            "solves_per_s": len(all_shapes) * K / (ms * 1e-3),
             "roofline": {"bound": "hbm", "kernel": "whole batch solve", "achieved": alg / per_solve_s / 1e9,
                          "peak": peak, "unit": "GB/s", "frac": alg / per_solve_s / 1e9 / peak,
                          "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_launch": alg},
             "cpu_baseline": cpu,
-            "e2e": {"value": world * units / e2e_s, "unit": "cell-layer-solves/s",
+            "e2e": {"value": total_units / e2e_s, "unit": "cell-layer-solves/s",
                     "h2d_bytes_per_step": 8 * units, "d2h_bytes_per_step": 8 * units},
             "gpu_launches": b.launch_count() * K,
             "clocks": clk.summary(),
@@ -546,68 +553,107 @@ def dptr(t):
     return ctypes.cast(ctypes.c_void_p(t.data_ptr()), pq._dp)
 
 
-def run_serving(a, rank, world, local_rank):
-    """Serving: Poisson arrivals at 200 runs/s over a window; double gyres of
-    129..1025 squared, 2-5 layers, 100-5000 steps; 150 GB HBM budget.  Reports
-    latency percentiles (arrival to result) and the aggregate throughput."""
-    import numpy as np
-    import torch
-
+def serve(reqs, precision, a, local_rank):
+    """Serve one request stream (arrival_s, ii, L, nsteps, seed) on this GPU:
+    submit each request when its arrival time has passed, poll the server
+    until every run is done.  Returns, per finished run, (latency from
+    arrival to result, cell-layer-steps, finish time, mean time per step
+    while active), the failed-run count and the kernel launches."""
     import pequod_b200 as pq
-    from pequod_b200.workloads import double_gyre, initial_condition, serving_requests
+    from pequod_b200.workloads import double_gyre, initial_condition
 
-    from pequod_b200 import multirank
-
-    torch.cuda.set_device(local_rank)
-    dist = multirank.init(world)
-    reqs = serving_requests(rate=a.rate, window=a.window, seed=multirank.rank_seed(3, rank))
     cfgs = {}
     srv = pq.Server(int(a.budget_gb * (1 << 30)), device=local_rank)
     pending = list(reqs)
     ids = {}
+    done, failed = [], 0
     t_start = srv.clock()
-    with ClockSampler(local_rank) as clk:
-        while pending or ids:
-            now = srv.clock() - t_start
-            while pending and pending[0][0] <= now:
-                t_arr, ii, L, n, seed = pending.pop(0)
-                key = (ii, L)
-                if key not in cfgs:
-                    cfgs[key] = double_gyre(ii, L, 1800.0)
-                cfg = cfgs[key]
-                rid = srv.submit(cfg, initial_condition(cfg, seed), n)
-                ids[rid] = (t_arr, ii * ii * L * n)
-            if ids:
-                srv.poll(a.round_steps)
-            done = [rid for rid in ids if srv.status(rid) == 2]
-            for rid in done:
-                t_arr, work = ids.pop(rid)
+    while pending or ids:
+        now = srv.clock() - t_start
+        while pending and pending[0][0] <= now:
+            t_arr, ii, L, n, seed = pending.pop(0)
+            key = (ii, L)
+            if key not in cfgs:
+                cfgs[key] = double_gyre(ii, L, 1800.0, precision)
+            cfg = cfgs[key]
+            rid = srv.submit(cfg, initial_condition(cfg, seed), n)
+            ids[rid] = (t_arr, ii * ii * L * n, n)
+        if ids:
+            srv.poll(a.round_steps)
+        for rid in [rid for rid in ids if srv.status(rid) in (2, 3)]:
+            t_arr, work, n = ids.pop(rid)
+            try:
                 _, t3 = srv.collect(rid)
-                lat = t3[2] - t_start - t_arr
-                ids_done.append((lat, work, t3[2] - t_start))
-            if not ids and pending:
-                time.sleep(max(0.0, min(0.01, pending[0][0] - (srv.clock() - t_start))))
-    # Every rank served its own request stream; the statistics cover all.
-    summary = multirank.serving_summary(multirank.gather_lists(dist, ids_done))
-    launches = int(sum(multirank.gather_lists(dist, [srv.launches()])))
+            except pq.PQError:
+                failed += 1
+                continue
+            done.append((t3[2] - t_start - t_arr, work, t3[2] - t_start, (t3[2] - t3[1]) / max(1, n - 1)))
+        if not ids and pending:
+            time.sleep(max(0.0, min(0.01, pending[0][0] - (srv.clock() - t_start))))
+    launches = srv.launches()
+    srv.close()
+    return done, failed, launches
+
+
+def run_serving(a, rank, world, local_rank):
+    """Serving: one stream of Poisson arrivals at 200 runs/s over a window;
+    double gyres of 129..1025 squared, 2-5 layers, 100-5000 steps; 150 GB
+    HBM budget.  Multi-GPU: the requests are partitioned across the ranks
+    (whole runs, balanced by ii^2 * L * steps).  Reports the per-request
+    latency (arrival to result) and per-step latency (a run's active time
+    over its steps) percentiles and the aggregate throughput, for the
+    mixed-precision form with the FP64 form beside it."""
+    import numpy as np
+    import torch
+
+    from pequod_b200.workloads import serving_requests
+    from pequod_b200 import multirank
+    import pequod_b200 as pq
+
+    torch.cuda.set_device(local_rank)
+    dist = multirank.init(world)
+    reqs = serving_requests(rate=a.rate, window=a.window, seed=3)
+    mine = multirank.partition([ii * ii * L * n for _, ii, L, n, _ in reqs], world)[rank]
+    my_reqs = [reqs[k] for k in mine]
+    forms = ({"mixed": pq.PREC_MIXED, "fp64": pq.PREC_FP64} if a.precision == "both"
+             else {a.precision: pq.PREC_FP64 if a.precision == "fp64" else pq.PREC_MIXED})
+    out = {}
+    with ClockSampler(local_rank) as clk:
+        for name, prec in forms.items():
+            done, failed, launches = serve(my_reqs, prec, a, local_rank)
+            all_done = multirank.gather_lists(dist, done)
+            summary = multirank.serving_summary(all_done)
+            steps_lat = np.array([d[3] for d in all_done])
+            summary["step_p50_ms"] = float(np.percentile(steps_lat, 50) * 1e3)
+            summary["step_p99_ms"] = float(np.percentile(steps_lat, 99) * 1e3)
+            summary["failed"] = int(sum(multirank.gather_lists(dist, [failed])))
+            summary["launches"] = int(sum(multirank.gather_lists(dist, [launches])))
+            out[name] = summary
+    head_name = "mixed" if "mixed" in out else next(iter(out))
+    head = out[head_name]
     line = {
-        "metric": "serving latency p50/p99 (s)", "value": summary["p50_s"], "unit": "s",
-        "p50_s": summary["p50_s"], "p99_s": summary["p99_s"],
-        "n_gpus": world, "steps": summary["runs"], "warmup": 0, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": "serving latency p50/p99 (s)", "value": head["p50_s"], "unit": "s",
+        "p50_s": head["p50_s"], "p99_s": head["p99_s"],
+        "step_latency_ms": {"p50": head["step_p50_ms"], "p99": head["step_p99_ms"]},
+        "n_gpus": world, "steps": head["runs"], "warmup": 0, "higher_is_better": False, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32/f64" if head_name == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": "serving_double_gyre", "rate_per_s": a.rate, "window_s": a.window,
-                   "runs": summary["runs"], "budget_gb": a.budget_gb, "round_steps": a.round_steps,
-                   "parallelism": f"replicas{world}"},
-        "throughput": {"value": summary["throughput"], "unit": "cell-layer-steps/s"},
-        "gpu_launches": launches, "clocks": clk.summary(),
+                   "runs": len(reqs), "budget_gb": a.budget_gb, "round_steps": a.round_steps,
+                   "precision": head_name,
+                   "parallelism": f"requests sharded over {world} rank(s), balanced by ii^2*L*steps"},
+        "throughput": {"value": head["throughput"], "unit": "cell-layer-steps/s"},
+        "failed_runs": head["failed"],
+        "gpu_launches": head["launches"], "clocks": clk.summary(),
     }
+    if len(out) == 2:
+        f = out["fp64"]
+        line["fp64"] = {"p50_s": f["p50_s"], "p99_s": f["p99_s"],
+                        "step_latency_ms": {"p50": f["step_p50_ms"], "p99": f["step_p99_ms"]},
+                        "throughput": f["throughput"], "failed_runs": f["failed"], "gpu_launches": f["launches"]}
+        line["mixed_over_fp64_throughput"] = head["throughput"] / f["throughput"]
     if rank == 0:
         print(json.dumps(line), flush=True)
-    srv.close()
     multirank.close(dist)
-
-
-ids_done = []
 
 
 def main():

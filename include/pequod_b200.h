@@ -7,7 +7,7 @@
  * and the advection routines are qg_aux's public list (qg3p_aux.F90:33-43),
  * called positionally from qg3.F90:598-807,952.  Every entry point below is
  * the C side of a bind(C) interface that replaces one of those Fortran
- * routines; INTEGRATION.md shows the Fortran interface module.
+ * routines.
  *
  * Conventions
  *  - Arrays are Fortran column-major, i (first index) fastest, REAL(8).
@@ -181,6 +181,31 @@ PQ_API int pq_helm(pq_ctx* ctx, double* zeta, int ptr_kind);
  * where the reference aborts on a NaN psiC. */
 PQ_API int pq_pv_inversion(pq_ctx* ctx, const double* zeta_sdata, double* psi_sdata, int ptr_kind);
 
+/* ---- Dirichlet boundary conditions (qg_laplace_bc) -----------------------
+ * The public routines of qg3p_laplace_bc.F90:14-36 on the context's grid,
+ * as device kernels.  field / rhs: (ii, jj, layers) column-major, layers
+ * 1..L of the context (1 for the reference's *_layer variants).  bc: nbc
+ * values, nbc = 1 (one value for every layer, *_layers_single) or
+ * nbc = layers (one per layer, *_layers_multiple).  Closed basin: bc is
+ * the value on all four walls and bc_d must be NULL.  Channel (periodic_j):
+ * bc is the wall i = 1 (bc_b) and bc_d the wall i = ii (NULL: the same as
+ * bc), the *_periodic_* variants.  Host arrays are copied in and out and
+ * the call returns when done; device arrays are updated in place,
+ * asynchronously on pq_stream(ctx).  Results equal the reference's to the
+ * bit (each node subtracts or takes its values in the reference's order).
+ *
+ * add_laplace_bc_rhs (:55-190): rhs(i, j) -= bc on the nodes next to each
+ * wall (i = 2, ii-1 and, closed basin, j = 2, jj-1; a corner of that ring
+ * twice). */
+PQ_API int pq_add_laplace_bc_rhs(pq_ctx* ctx, double* rhs, int layers, const double* bc, const double* bc_d,
+                                 int nbc, int ptr_kind);
+/* apply_dirichlet_bc (:193-374): the boundary nodes take the wall values. */
+PQ_API int pq_apply_dirichlet_bc(pq_ctx* ctx, double* field, int layers, const double* bc, const double* bc_d,
+                                 int nbc, int ptr_kind);
+/* laplace_bc_rhs (:42-51): rhs (ii, jj) = 0, then add_laplace_bc_rhs with
+ * one value. */
+PQ_API int pq_laplace_bc_rhs(pq_ctx* ctx, double bc, double* rhs, int ptr_kind);
+
 /* ---- model state and time stepping -------------------------------------- */
 
 /* START_PERTURB initialisation, qg3.F90:365-404 and :450-459: zeta sdata
@@ -318,24 +343,32 @@ PQ_API int pq_kernel_times(pq_ctx* ctx, double* ms4, long* launches4);
  * No counterpart in the reference: its energy() (qg3p_diagnostics.F90:778-
  * 863) runs on host arrays.  pq_energy_noalloc computes the same ekin / epot
  * as pq_energy on a psi array the caller already owns on the device, without
- * a context and without allocating anything: for a host driver that is
- * capturing a CUDA graph (where cudaMalloc is not allowed) or whose device
- * memory is fully reserved by an HBM budget.
- *   psi    device, (ld, jj, layers) column-major, node values (sdata)
- *   h, s2  host, layers entries (strat%h, strat%s2)
- *   out    device, layers + 1 doubles: ekin(1:layers), then epot
- *   stream cudaStream_t to order the work on (NULL: legacy default stream)
+ * a context and without allocating anything.  It is for host drivers that
+ * cannot let a library allocate device memory: one whose device memory is
+ * reserved up front (an HBM budget, or a caching allocator that owns the
+ * whole device), where a cudaMalloc would fail or break the budget, and one
+ * that keeps its streams pipelined and cannot afford the device-wide
+ * synchronisation that cudaMalloc / cudaFree may cause.
+ *   psi        device, (ld, jj, layers) column-major, node values (sdata)
+ *   periodic_j 0: closed basin; 1: channel periodic in j (full row weights,
+ *              the kinetic-energy cells of row 1 wrap to row jj, and the
+ *              area (ii - 1) jj), as pq_energy does for a channel context
+ *   h, s2      host, layers entries (strat%h, strat%s2)
+ *   out        device, layers + 1 doubles: ekin(1:layers), then epot
+ *   stream     cudaStream_t to order the work on (NULL: legacy default stream)
  * Limits: jj <= PQ_NOALLOC_MAX_JJ, layers <= PQ_MAX_LAYERS; larger sizes
  * return PQ_ERR_ARG.  The reduction's scratch (row partials and a counter,
  * about 300 KB) is a fixed array inside the library that every GPU which
- * loads it keeps until exit; all calls share it, so calls whose device work
- * overlaps race and must be serialised by the caller.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress); make
- * that first call before starting any stream capture.  Asynchronous: `out`
- * is valid once the stream has reached the call. */
+ * loads it keeps until exit; all calls share it and it keeps the last
+ * call's contents (each call clears the counter it needs at zero), so calls
+ * whose device work overlaps race and must be serialised by the caller.
+ * The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before starting any stream capture.  Asynchronous: `out` is valid once
+ * the stream has reached the call. */
 #define PQ_NOALLOC_MAX_JJ 4097
-PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int ld, const double* h,
-                             const double* s2, double* out, void* stream);
+PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int ld, int periodic_j,
+                             const double* h, const double* s2, double* out, void* stream);
 
 /* Tile parameters of the step kernels (defaults per grid size are set by
  * pq_create; results do not depend on them).
@@ -417,10 +450,18 @@ PQ_API const char* pq_server_last_error(const pq_server* s);
  * exceeds the budget. */
 PQ_API int pq_server_submit(pq_server* s, const pq_model_desc* desc, const double* zeta_ic, int nsteps, long* id);
 PQ_API int pq_server_poll(pq_server* s, int max_steps, int* active, int* queued);
-/* 0 queued, 1 running, 2 finished, -1 unknown id. */
+/* 0 queued, 1 running, 2 finished, 3 failed, -1 unknown id.  A run fails
+ * alone -- the others carry on -- when its device status reports a NaN
+ * psiC or energy (where the reference aborts the program,
+ * qg3p_aux.F90:504-510, qg3p_diagnostics.F90:858-861; checked after every
+ * round) or when its admission fails (an invalid description, a failed
+ * allocation); its context is destroyed. */
 PQ_API int pq_server_status(pq_server* s, long id);
 /* psi (ii, jj, L) of a finished run and t3 = {submitted, started, finished}
- * in seconds of pq_server_clock; releases the run (PQ_ERR_NOTFOUND after). */
+ * in seconds of pq_server_clock; releases the run (PQ_ERR_NOTFOUND after).
+ * For a failed run: t3 (finished = when it failed), no psi, and the run's
+ * error code (PQ_ERR_NAN, PQ_ERR_ARG, PQ_ERR_NOMEM, ...) with
+ * pq_server_last_error giving its message. */
 PQ_API int pq_server_collect(pq_server* s, long id, double* psi, double* t3);
 PQ_API size_t pq_server_device_bytes(const pq_server* s);
 PQ_API double pq_server_clock(const pq_server* s);

@@ -27,6 +27,7 @@ SCHEME_CABARET, SCHEME_LEAPFROG = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 BC_PARTIAL_SLIP, BC_NO_SLIP, BC_FREE_SLIP = 1, 2, 3
 MAX_LAYERS = 8
+NOALLOC_MAX_JJ = 4097  # PQ_NOALLOC_MAX_JJ: largest jj pq_energy_noalloc accepts
 
 FIELDS = {
     "psi": 0, "zeta": 1, "rel": 2, "zeta_old": 3, "ui": 4, "uj": 5, "uimo": 6, "ujmo": 7,
@@ -88,6 +89,9 @@ SIGNATURES = {
     "pq_device_bytes": (C.c_size_t, [C.c_void_p]),
     "pq_helm": (C.c_int, [C.c_void_p, _dp, C.c_int]),
     "pq_pv_inversion": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    "pq_add_laplace_bc_rhs": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, _dp, C.c_int, C.c_int]),
+    "pq_apply_dirichlet_bc": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, _dp, C.c_int, C.c_int]),
+    "pq_laplace_bc_rhs": (C.c_int, [C.c_void_p, C.c_double, _dp, C.c_int]),
     "pq_init_perturb": (C.c_int, [C.c_void_p, _dp, C.c_int]),
     "pq_step": (C.c_int, [C.c_void_p, C.c_int]),
     "pq_step_async": (C.c_int, [C.c_void_p, C.c_int]),
@@ -113,8 +117,8 @@ SIGNATURES = {
     "pq_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "pq_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "pq_kernel_times": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_long)]),
-    "pq_energy_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_void_p,
-                                    C.c_void_p]),
+    "pq_energy_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp,
+                                    C.c_void_p, C.c_void_p]),
     "pq_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), _dp, C.c_int]),
     "pq_batch_destroy": (None, [C.c_void_p]),
@@ -290,6 +294,46 @@ class Model:
         psi = np.zeros(self.shape, order="F")
         _check(lib().pq_pv_inversion(self.ctx, _p(z), _p(psi), PTR_HOST), self.ctx)
         return psi
+
+    def _bc_field(self, a):
+        a = np.array(a, dtype=np.float64, order="F")
+        layers = 1 if a.ndim == 2 else a.shape[2]
+        if a.shape[:2] != (self.cfg.ii, self.cfg.jj):
+            raise ValueError("field must be (ii, jj) or (ii, jj, layers)")
+        return a, layers
+
+    @staticmethod
+    def _bc_values(bc, bc_d, layers):
+        b = np.ascontiguousarray(np.atleast_1d(np.asarray(bc, dtype=np.float64)))
+        d = None if bc_d is None else np.ascontiguousarray(np.atleast_1d(np.asarray(bc_d, dtype=np.float64)))
+        if d is not None and d.size != b.size:
+            raise ValueError("bc and bc_d must have the same length")
+        return b, d
+
+    def add_laplace_bc_rhs(self, rhs: np.ndarray, bc, bc_d=None) -> np.ndarray:
+        """add_laplace_bc_rhs (qg3p_laplace_bc.F90:55-190) on the device: a
+        copy of rhs ((ii, jj) or (ii, jj, layers)) with the Dirichlet values
+        lifted in; bc a number or one value per layer, bc_d the channel's
+        wall i = ii."""
+        a, layers = self._bc_field(rhs)
+        b, d = self._bc_values(bc, bc_d, layers)
+        _check(lib().pq_add_laplace_bc_rhs(self.ctx, _p(a), layers, _p(b), None if d is None else _p(d), b.size,
+                                           PTR_HOST), self.ctx)
+        return a
+
+    def apply_dirichlet_bc(self, field: np.ndarray, bc, bc_d=None) -> np.ndarray:
+        """apply_dirichlet_bc (qg3p_laplace_bc.F90:193-374) on the device."""
+        a, layers = self._bc_field(field)
+        b, d = self._bc_values(bc, bc_d, layers)
+        _check(lib().pq_apply_dirichlet_bc(self.ctx, _p(a), layers, _p(b), None if d is None else _p(d), b.size,
+                                           PTR_HOST), self.ctx)
+        return a
+
+    def laplace_bc_rhs(self, bc: float) -> np.ndarray:
+        """laplace_bc_rhs (qg3p_laplace_bc.F90:42-51): (ii, jj)."""
+        out = np.zeros((self.cfg.ii, self.cfg.jj), order="F")
+        _check(lib().pq_laplace_bc_rhs(self.ctx, float(bc), _p(out), PTR_HOST), self.ctx)
+        return out
 
     def init_perturb(self, zeta_ic: np.ndarray) -> None:
         """zeta_ic: (ii, jj, L), or (ii, jj, L, 2) -- both time levels -- for the leapfrog scheme."""
@@ -541,11 +585,17 @@ class Server:
         return int(lib().pq_server_status(self.ctx, rid))
 
     def collect(self, rid: int):
-        """(psi, (t_submit, t_start, t_done)) of a finished run."""
+        """(psi, (t_submit, t_start, t_done)) of a finished run; releases it.
+        A failed run (status 3) raises PQError with the run's own error code
+        and message (and is released too)."""
         psi = np.zeros(self.shapes[rid], order="F")
         t3 = np.zeros(3)
-        self._chk(lib().pq_server_collect(self.ctx, rid, _p(psi), _p(t3)))
-        del self.shapes[rid]
+        rc = lib().pq_server_collect(self.ctx, rid, _p(psi), _p(t3))
+        msg = lib().pq_server_last_error(self.ctx).decode() if rc != PQ_OK else ""
+        if self.status(rid) == -1:  # released (finished or failed)
+            self.shapes.pop(rid, None)
+        if rc != PQ_OK:
+            raise PQError(rc, msg)
         return psi, tuple(t3)
 
     def run_until_done(self, max_steps: int = 32):

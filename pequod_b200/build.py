@@ -38,6 +38,9 @@ def headers():
                   glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
+OBJ_DIR = os.path.join(PKG, "_build")
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
@@ -45,16 +48,40 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(f) <= t for f in sources() + headers() + [__file__])
 
 
+def _flags():
+    return [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
+            "-Xptxas", "-warn-spills", "-I", os.path.join(ROOT, "include"), "-I", SRC]
+
+
+def _compile(src, verbose):
+    obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+    newest = max(os.path.getmtime(f) for f in [src, __file__] + headers())
+    if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
+        return obj
+    cmd = [nvcc(), *_flags(), "-c", "-o", obj + ".tmp", src]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(obj + ".tmp", obj)
+    return obj
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel (only those older than
+    their inputs), then link the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
+
     if not force and up_to_date():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    if force:
+        for f in glob.glob(os.path.join(OBJ_DIR, "*.o")):
+            os.remove(f)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(lambda src: _compile(src, verbose), sources()))
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "--shared",
-           "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
-           "-Xptxas", "-warn-spills",
-           "-I", os.path.join(ROOT, "include"), "-I", SRC,
-           "-o", tmp, *sources(), "-lcuda"]
+    cmd = [nvcc(), *ARCH, "--shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lcuda"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

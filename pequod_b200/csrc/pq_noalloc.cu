@@ -2,10 +2,12 @@
 //
 // pq_energy (pq_api.cu) reduces per-row partial sums through scratch memory
 // that the context allocated.  Some callers have no context and may not
-// allocate: a host driver that is capturing a CUDA graph (cudaMalloc is not
-// allowed while a capture is in progress), or one whose device memory is
-// fully reserved up front by an HBM budget and that hands this library only
-// the arrays it already owns.  For them this file provides the same
+// allocate: a host driver whose device memory is reserved up front (by an
+// HBM budget, or by a caching allocator that owns the whole device) and
+// that hands this library only the arrays it already owns, so that a
+// cudaMalloc would fail or break the budget; or a driver that keeps its
+// streams pipelined and cannot afford the device-wide synchronisation a
+// cudaMalloc / cudaFree may cause.  For them this file provides the same
 // reduction with its scratch in a fixed, file-scope device array.
 //
 // The array (below) holds PQ_NOALLOC_MAX_JJ rows of PQ_MAX_LAYERS + 1 partial
@@ -36,14 +38,16 @@ static __device__ __align__(256) NoAllocScratch g_scratch;
 struct EnergyArgs {
     const double* psi;
     double* out;
-    int ii, jj, L, ld;
+    int ii, jj, L, ld, periodic;
     double fac[PQ_MAX_LAYERS];   // 0.5 s2_k h_k / H, k = 1..L-1
     double hfrac[PQ_MAX_LAYERS]; // h_k / H
-    double cff;                  // 1 / ((ii-1)(jj-1))
+    double cff;                  // 1 / (g_ii_int g_jj_int): (ii-1)(jj-1), channel (ii-1) jj
 };
 
 // Same reduction as k_energy (pq_cabaret.cu): one CTA per row of nodes, the
-// last CTA adds the row partials in row order.
+// last CTA adds the row partials in row order.  A channel (periodic in j)
+// has no j boundary: full row weights, and the kinetic-energy corners of
+// row 0 reach back to row jj - 1.
 __global__ void __launch_bounds__(256) k_energy_noalloc(EnergyArgs a, NoAllocScratch* s) {
     __shared__ double red[8][kCols];
     __shared__ int is_last;
@@ -51,7 +55,8 @@ __global__ void __launch_bounds__(256) k_energy_noalloc(EnergyArgs a, NoAllocScr
     const long long ls = (long long)a.ld * jj;
     double acc[kCols];
     for (int q = 0; q <= L; ++q) acc[q] = 0.0;
-    const double wj = (j == 0 || j == jj - 1) ? 0.5 : 1.0;
+    const double wj = (!a.periodic && (j == 0 || j == jj - 1)) ? 0.5 : 1.0;
+    const long long back = (j == 0) ? (long long)(jj - 1) * a.ld : -(long long)a.ld;  // row j-1, wrapped
     for (int i = threadIdx.x; i < ii; i += blockDim.x) {
         const double w = wj * ((i == 0 || i == ii - 1) ? 0.5 : 1.0);
         const long long o = (long long)j * a.ld + i;
@@ -59,11 +64,11 @@ __global__ void __launch_bounds__(256) k_energy_noalloc(EnergyArgs a, NoAllocScr
             const double d = a.psi[o + k * ls] - a.psi[o + (k + 1) * ls];
             acc[L] += w * a.fac[k] * (d * d);
         }
-        if (i >= 1 && j >= 1) {
+        if (i >= 1 && (j >= 1 || a.periodic)) {
             for (int k = 0; k < L; ++k) {
                 const double* p = a.psi + k * ls;
-                const double x = p[o - 1] + p[o] - p[o - 1 - a.ld] - p[o - a.ld];
-                const double y = p[o - a.ld] + p[o] - p[o - 1 - a.ld] - p[o - 1];
+                const double x = p[o - 1] + p[o] - p[o - 1 + back] - p[o + back];
+                const double y = p[o + back] + p[o] - p[o - 1 + back] - p[o - 1];
                 acc[k] += 0.25 * (x * x + y * y);
             }
         }
@@ -117,10 +122,10 @@ cudaError_t scratch_address(int dev, NoAllocScratch** out) {
 
 }  // namespace
 
-extern "C" PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int ld, const double* h,
-                                        const double* s2, double* out, void* stream) {
+extern "C" PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int ld, int periodic_j,
+                                        const double* h, const double* s2, double* out, void* stream) {
     if (!psi || !out || !h || (layers > 1 && !s2)) return PQ_ERR_ARG;
-    if (ii < 2 || jj < 2 || ld < ii || layers < 1) return PQ_ERR_ARG;
+    if (ii < 2 || jj < 2 || ld < ii || layers < 1 || (periodic_j != 0 && periodic_j != 1)) return PQ_ERR_ARG;
     if (jj > PQ_NOALLOC_MAX_JJ || layers > PQ_MAX_LAYERS) return PQ_ERR_ARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return PQ_ERR_CUDA;
@@ -133,6 +138,7 @@ extern "C" PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int l
     a.jj = jj;
     a.L = layers;
     a.ld = ld;
+    a.periodic = periodic_j;
     double htot = 0.0;
     for (int k = 0; k < layers; ++k) htot += h[k];
     for (int k = 0; k < PQ_MAX_LAYERS; ++k) a.fac[k] = a.hfrac[k] = 0.0;
@@ -140,7 +146,7 @@ extern "C" PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int l
         a.hfrac[k] = h[k] / htot;
         if (k + 1 < layers) a.fac[k] = 0.5 * s2[k] * h[k] / htot;
     }
-    a.cff = 1.0 / ((double)(ii - 1) * (double)(jj - 1));
+    a.cff = 1.0 / ((double)(ii - 1) * (double)(periodic_j ? jj : jj - 1));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // The completion counter must start at zero on every call.
     if (cudaMemsetAsync(&s->counter, 0, sizeof(unsigned int), st) != cudaSuccess) return PQ_ERR_CUDA;

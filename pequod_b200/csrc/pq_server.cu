@@ -15,6 +15,15 @@
 // in steady state); idle pooled contexts are freed when the budget needs
 // the room.  A run's result does not depend on what it was batched with:
 // the kernels compute every member independently.
+//
+// Faults stay with the run that raised them.  The reference aborts the
+// whole program on a NaN psiC or energy (qg3p_aux.F90:504-510,
+// qg3p_diagnostics.F90:858-861); here the device status word of every
+// active run is read back after each round, and a run whose word reports a
+// NaN -- or whose admission fails (an invalid description, a failed
+// allocation, a NaN already in its initial inversion) -- is marked failed
+// with that error and evicted: its context is destroyed (not pooled) and
+// the other runs carry on untouched.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -42,7 +51,9 @@ struct pq_server {
         pq_model_desc desc{};
         std::vector<double> wind, ic, psi;
         int nsteps = 0, done = 0;
-        int state = 0;  // 0 queued, 1 running, 2 finished
+        int state = 0;  // 0 queued, 1 running, 2 finished, 3 failed
+        int error = 0;  // PQ_ERR_* of a failed run
+        std::string msg;
         pq_ctx* c = nullptr;
         size_t bytes = 0;
         double t_submit = 0, t_start = 0, t_done = 0;
@@ -61,6 +72,10 @@ struct pq_server {
     int sm_count = 0;
     long launches = 0;
     std::string err;
+    // Status words of the active runs, copied after each round (pinned).
+    int* h_status = nullptr;
+    size_t status_cap = 0;
+    std::vector<long> status_ids;
 };
 
 namespace {
@@ -115,6 +130,42 @@ void evict(pq_server* s, size_t need) {
     }
 }
 
+// Mark a run failed with `code` and drop its context (destroyed, not
+// pooled: its state is not trusted).  The caller removes it from the active
+// list or the queue.
+void fail_run(pq_server* s, pq_server::Run& r, int code, const std::string& msg) {
+    r.state = 3;
+    r.error = code;
+    r.msg = "run " + std::to_string(r.id) + ": " + msg;
+    r.t_done = now(s);
+    r.ic.clear();
+    r.ic.shrink_to_fit();
+    if (r.c) {
+        s->held -= std::min(s->held, r.c->arena_bytes);
+        pq_destroy(r.c);
+        r.c = nullptr;
+    }
+}
+
+// Evict the active runs whose device status reported a NaN in the round
+// just completed (the status words were copied at its end).
+void evict_faulted(pq_server* s) {
+    std::vector<long> bad;
+    for (size_t k = 0; k < s->status_ids.size(); ++k)
+        if (s->h_status[k] & (ST_NAN_PSIC | ST_NAN_ENERGY)) bad.push_back(s->status_ids[k]);
+    s->status_ids.clear();
+    if (bad.empty()) return;
+    std::vector<long> keep;
+    for (long id : s->active)
+        if (std::find(bad.begin(), bad.end(), id) == bad.end()) keep.push_back(id);
+    for (long id : bad) {
+        pq_server::Run& r = s->runs[id];
+        fail_run(s, r, PQ_ERR_NAN, "NaN psiC or energy after " + std::to_string(r.done) +
+                                       " steps (the reference aborts here)");
+    }
+    s->active.swap(keep);
+}
+
 int retire(pq_server* s) {
     std::vector<long> keep;
     for (long id : s->active) {
@@ -127,7 +178,12 @@ int retire(pq_server* s) {
         pq_ctx* c = r.c;
         int rc = copy_out(c, r.psi.data(), c->hm[0].psi, PQ_PTR_HOST);
         if (!rc) rc = check_status(c);  // synchronises the stream, reports NaNs
-        if (rc) return sfail(s, rc, "run " + std::to_string(id) + ": " + c->err);
+        if (rc == PQ_ERR_CUDA) return sfail(s, rc, "run " + std::to_string(id) + ": " + c->err);
+        if (rc) {
+            r.psi.clear();
+            fail_run(s, r, rc, c->err);
+            continue;
+        }
         r.t_done = now(s);
         r.state = 2;
         release_ctx(s, r);
@@ -153,9 +209,14 @@ int admit(pq_server* s) {
             d.force_wind = r.wind.empty() ? nullptr : r.wind.data();
             const int rc = create_ctx(&c, &d, s->device, false, s->stream);
             if (rc) {
-                const std::string msg = c ? c->err : std::string();
+                // This run alone fails (an invalid description or a failed
+                // allocation); the queue moves on.
+                const std::string msg = c ? c->err : std::string("context creation failed");
                 if (c) pq_destroy(c);
-                return sfail(s, rc, "admitting run " + std::to_string(r.id) + ": " + msg);
+                cudaGetLastError();
+                fail_run(s, r, rc, "admission: " + msg);
+                s->queue.pop_front();
+                continue;
             }
             s->held += c->arena_bytes;
             s->known_bytes[r.key] = c->arena_bytes;
@@ -170,7 +231,12 @@ int admit(pq_server* s) {
             r.done = 1;
             s->launches += 4;
         }
-        if (rc) return sfail(s, rc, "initialising run " + std::to_string(r.id) + ": " + c->err);
+        if (rc == PQ_ERR_CUDA) return sfail(s, rc, "initialising run " + std::to_string(r.id) + ": " + c->err);
+        if (rc) {
+            fail_run(s, r, rc, "initialisation: " + c->err);
+            s->queue.pop_front();
+            continue;
+        }
         r.state = 1;
         r.t_start = now(s);
         r.ic.clear();
@@ -290,6 +356,17 @@ int round_steps(pq_server* s, int max_steps) {
         SK(cudaEventRecord(s->ev[1 + q], s->side[q]));
         SK(cudaStreamWaitEvent(s->stream, s->ev[1 + q], 0));
     }
+    // Every active run's status word, read at the next poll.
+    if (s->active.size() > s->status_cap) {
+        if (s->h_status) cudaFreeHost(s->h_status);
+        s->h_status = nullptr;
+        s->status_cap = s->active.size() * 2;
+        SK(cudaMallocHost(&s->h_status, s->status_cap * sizeof(int)));
+    }
+    s->status_ids = s->active;
+    for (size_t k = 0; k < s->active.size(); ++k)
+        SK(cudaMemcpyAsync(s->h_status + k, s->runs[s->active[k]].c->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                           s->stream));
     SK(cudaEventRecord(s->round_done, s->stream));
     s->round_pending = true;
     size_t q = 0;
@@ -339,6 +416,7 @@ void pq_server_destroy(pq_server* s) {
     for (auto& kv : s->pool) pq_destroy(kv.second);
     if (s->d_desc) cudaFree(s->d_desc);
     if (s->d_pref) cudaFree(s->d_pref);
+    if (s->h_status) cudaFreeHost(s->h_status);
     for (auto& st : s->side) cudaStreamDestroy(st);
     for (auto& e : s->ev) cudaEventDestroy(e);
     if (s->round_done) cudaEventDestroy(s->round_done);
@@ -378,6 +456,7 @@ int pq_server_poll(pq_server* s, int max_steps, int* active, int* queued) {
     if (s->round_pending) {
         SK(cudaEventSynchronize(s->round_done));
         s->round_pending = false;
+        evict_faulted(s);
     }
     int rc = retire(s);
     if (!rc) rc = admit(s);
@@ -397,13 +476,20 @@ int pq_server_collect(pq_server* s, long id, double* psi, double* t3) {
     if (!s) return PQ_ERR_ARG;
     auto it = s->runs.find(id);
     if (it == s->runs.end()) return sfail(s, PQ_ERR_NOTFOUND, "unknown run id");
-    if (it->second.state != 2) return sfail(s, PQ_ERR_STATE, "run not finished");
-    if (psi) std::memcpy(psi, it->second.psi.data(), it->second.psi.size() * sizeof(double));
+    if (it->second.state != 2 && it->second.state != 3) return sfail(s, PQ_ERR_STATE, "run not finished");
     if (t3) {
         t3[0] = it->second.t_submit;
         t3[1] = it->second.t_start;
         t3[2] = it->second.t_done;
     }
+    if (it->second.state == 3) {
+        // A failed run: its error code and message, no psi.
+        const int code = it->second.error;
+        s->err = it->second.msg;
+        s->runs.erase(it);
+        return code;
+    }
+    if (psi) std::memcpy(psi, it->second.psi.data(), it->second.psi.size() * sizeof(double));
     s->runs.erase(it);
     return PQ_OK;
 }

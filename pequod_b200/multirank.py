@@ -1,11 +1,14 @@
 """One process per GPU: the host-side plumbing of multi-GPU runs.
 
-A single domain does not shard without an exchange step, so the multi-GPU
-runs are independent replicas (one run, batch or request stream per rank,
-each with its own seed) and the only collectives are the measurement's:
-the slowest rank's time and the serving statistics over all ranks.  The
-process group is NCCL on GPUs; the same functions run on gloo (CPU) in the
-tests.
+Ensembles shard: the members of one batched-Helmholtz workload and the
+requests of one serving stream are independent, so they are partitioned
+across the ranks as whole members, balanced by their work (ii * jj * L, and
+times the step count for a serving request), with no exchange while they
+run; only the measurement's collectives follow (the slowest rank's time,
+the serving statistics over all ranks).  A single domain does not shard
+without an exchange step, so single runs are independent replicas (one per
+rank, each with its own seed).  The process group is NCCL on GPUs; the same
+functions run on gloo (CPU) in the tests.
 """
 from __future__ import annotations
 
@@ -35,6 +38,27 @@ def init(world: int, backend: str = "nccl", timeout_s: float = 300.0):
 def rank_seed(base: int, rank: int) -> int:
     """Each replica draws its own workload."""
     return base + rank
+
+
+def partition(weights, world: int):
+    """Split items of the given work weights over `world` ranks: the longest
+    processing time first rule (heaviest item to the least-loaded rank, ties
+    to the lower index), deterministic.  Returns, per rank, the sorted item
+    indices; the heaviest rank carries at most the mean load plus the
+    heaviest item."""
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    order = sorted(range(len(weights)), key=lambda k: (-float(weights[k]), k))
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += float(weights[k])
+    return [sorted(p) for p in parts]
+
+
+def shard(items, weights, rank: int, world: int):
+    """This rank's share of `items` (in their original order)."""
+    return [items[k] for k in partition(weights, world)[rank]]
 
 
 def max_over_ranks(dist, values, device=None):

@@ -146,3 +146,11 @@ def test_make_ic_matches_oracle_generator():
         a = pq.make_ic(*shape, seed=seed, amplitude=2.5, sigma=sig)
         b = O.make_ic(*shape, seed=seed, amplitude=2.5, sigma=sig)
         assert np.array_equal(a, b)
+
+
+def test_python_constants_match_the_header():
+    hdr = open(os.path.join(ROOT, "include", "pequod_b200.h")).read()
+    defs = dict(re.findall(r"#define\s+(PQ_\w+)\s+(-?\d+)", hdr))
+    assert int(defs["PQ_NOALLOC_MAX_JJ"]) == pq.NOALLOC_MAX_JJ
+    assert int(defs["PQ_MAX_LAYERS"]) == pq.MAX_LAYERS
+    assert int(defs["PQ_PREC_MIXED"]) == pq.PREC_MIXED

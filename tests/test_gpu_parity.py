@@ -142,13 +142,90 @@ def test_helm_periodic_convergence_gpu(ss, min_order):
     assert min(orders) >= min_order, orders
 
 
+EPS = np.finfo(np.float64).eps
+
+
+def fne(a, b):
+    """test_tools' fne: differ by more than 10 ulp."""
+    a = np.atleast_1d(np.asarray(a, dtype=np.float64))
+    b = np.atleast_1d(np.asarray(b, dtype=np.float64))
+    return bool(np.any(np.abs(a - b) > 10.0 * np.maximum(np.spacing(np.abs(a)), EPS)))
+
+
 def test_laplace_bc_gpu():
-    """test_laplace_bc.F90:21-31: Dirichlet BC = 1 with zero RHS gives psi == 1."""
+    """test_laplace_bc.F90:21-44 entirely on the device: laplace_bc_rhs,
+    helm and apply_dirichlet_bc give psi == 1 to 10 ulp for BC = 1; and the
+    lifting is linear (add_laplace_bc_rhs on a RHS of ones minus the BC = 0
+    solution is 1)."""
     ii = jj = 9
     m = pq.Model(helm_cfg(ii, jj, [0.0]))
-    rhs = O.add_laplace_bc_rhs(np.zeros((ii, jj), order="F"), 1.0)
-    out = O.apply_dirichlet_bc(m.helm(rhs[:, :, None]), 1.0)
-    assert np.abs(out - 1.0).max() <= 1e-14
+    phi = m.laplace_bc_rhs(1.0)
+    phi = m.apply_dirichlet_bc(m.helm(phi[:, :, None]), 1.0)
+    assert not (fne(phi.min(), 1.0) or fne(phi.max(), 1.0)), (phi.min(), phi.max())
+    phi0 = m.apply_dirichlet_bc(m.helm(np.ones((ii, jj, 1), order="F")), 0.0)
+    phi1 = m.add_laplace_bc_rhs(np.ones((ii, jj), order="F"), 1.0)
+    phi1 = m.apply_dirichlet_bc(m.helm(phi1[:, :, None]), 1.0)
+    d = phi1 - phi0
+    assert not (fne(d.min(), 1.0) or fne(d.max(), 1.0)), (d.min(), d.max())
+
+
+def test_laplace_bc_periodic_gpu():
+    """test_laplace_bc.F90:50-80 on the device: in the channel, the wall
+    values (1, 0) and (0, 1) give psi linear in i, exactly."""
+    ii = jj = 9
+    m = pq.Model(helm_cfg(ii, jj, [0.0], periodic=True))
+    i = np.arange(1, ii + 1)[:, None]
+    for bc_b, bc_d in ((1.0, 0.0), (0.0, 1.0)):
+        phi = m.add_laplace_bc_rhs(np.zeros((ii, jj), order="F"), bc_b, bc_d)
+        phi = m.apply_dirichlet_bc(m.helm(phi[:, :, None]), bc_b, bc_d)
+        exact = (ii - i) / (ii - 1) if bc_b == 1.0 else (i - 1) / (ii - 1)
+        assert not fne(np.abs(phi[:, :, 0] - exact).max(), 0.0)
+
+
+@pytest.mark.parametrize("ii,jj,periodic", [(33, 20, False), (65, 65, False), (17, 40, True), (129, 64, True)])
+def test_laplace_bc_matches_oracle_bitwise(ii, jj, periodic):
+    """Every variant (one layer; all layers with one value; one value per
+    layer; the channel's two walls) equals the oracle's restatement of
+    qg3p_laplace_bc.F90 to the bit, with host and device arrays."""
+    import torch
+
+    L = 3
+    m = pq.Model(helm_cfg(ii, jj, [0.0, 1.0, 2.0], periodic=periodic))
+    rng = np.random.default_rng(ii + jj)
+    f = np.asfortranarray(rng.standard_normal((ii, jj, L)))
+    bcs = np.array([0.3, -1.7, 2.9])
+    bds = np.array([1.1, 0.25, -0.6]) if periodic else None
+    # one layer, one value
+    out = m.add_laplace_bc_rhs(f[:, :, 1], 0.7, 0.2 if periodic else None)
+    ref = O.add_laplace_bc_rhs(f[:, :, 1], 0.7, 0.2 if periodic else None, periodic_j=periodic)
+    assert np.array_equal(out, ref)
+    out = m.apply_dirichlet_bc(f[:, :, 1], 0.7, 0.2 if periodic else None)
+    ref = O.apply_dirichlet_bc(f[:, :, 1], 0.7, 0.2 if periodic else None, periodic_j=periodic)
+    assert np.array_equal(out, ref)
+    # all layers, one value per layer
+    out_a = m.add_laplace_bc_rhs(f, bcs, bds)
+    out_d = m.apply_dirichlet_bc(f, bcs, bds)
+    for l in range(L):
+        bd = None if bds is None else bds[l]
+        assert np.array_equal(out_a[:, :, l], O.add_laplace_bc_rhs(f[:, :, l], bcs[l], bd, periodic_j=periodic))
+        assert np.array_equal(out_d[:, :, l], O.apply_dirichlet_bc(f[:, :, l], bcs[l], bd, periodic_j=periodic))
+    # device arrays, asynchronous on the context's stream
+    dev = torch.from_numpy(np.ascontiguousarray(f.ravel(order="F"))).cuda()
+    torch.cuda.synchronize()
+    b = np.ascontiguousarray(bcs)
+    d = None if bds is None else np.ascontiguousarray(bds)
+    rc = pq.lib().pq_add_laplace_bc_rhs(m.ctx, pq.C.cast(dev.data_ptr(), pq._dp), L, pq._p(b),
+                                        None if d is None else pq._p(d), L, pq.PTR_DEVICE)
+    assert rc == 0
+    m.sync()
+    got = dev.cpu().numpy().reshape((ii, jj, L), order="F")
+    assert np.array_equal(got, out_a)
+    # argument checks
+    with pytest.raises(pq.PQError):
+        m.add_laplace_bc_rhs(np.zeros((ii, jj, 4)), 1.0)  # more layers than the context
+    if not periodic:
+        with pytest.raises(pq.PQError):
+            m.apply_dirichlet_bc(f, 1.0, 2.0)  # a second wall value in a closed basin
 
 
 def double_gyre(ii, layers=3, dt=1800.0, **kw):

@@ -73,3 +73,45 @@ def test_server_budget_staging_and_pool():
         srv.submit(cfg_of(513, 5), np.zeros((513, 513, 5)), 1)
     assert e.value.code == pq.PQ_ERR_BUDGET
     srv.close()
+
+
+def test_server_isolates_faulted_runs():
+    """Faults injected from the host stay with their run: a NaN in one
+    run's initial PV (fails at admission, where the initial inversion's psiC
+    is NaN), a run whose huge initial PV overflows to NaN a few steps in
+    (fails mid-run, evicted after the round that raised it), and an invalid
+    grid (ii - 1 not a power of two: admission fails).  Each reports its own
+    error; every other run, batched with them in the same shape groups,
+    finishes bit-identical to its run alone."""
+    srv = pq.Server(8 << 30)
+    cfg = cfg_of(65, 3)
+    good = []
+    for seed, n in ((21, 9), (22, 14), (23, 6)):
+        good.append((srv.submit(cfg, ic_of(cfg, seed), n), seed, n))
+    nan_ic = ic_of(cfg, 24)
+    nan_ic[30, 31, 1] = np.nan
+    r_nan = srv.submit(cfg, nan_ic, 10)
+    r_blow = srv.submit(cfg, ic_of(cfg, 25) * 1e200, 40)
+    bad = cfg_of(65, 3)
+    bad.desc.ii = 60
+    r_bad = srv.submit(bad, np.zeros((60, 65, 3)), 5)
+    mixed = cfg_of(129, 3, pq.PREC_MIXED)
+    good_mixed = (srv.submit(mixed, ic_of(mixed, 26), 7), 26, 7)
+    srv.run_until_done(max_steps=2)
+    for rid, code in ((r_nan, pq.PQ_ERR_NAN), (r_blow, pq.PQ_ERR_NAN), (r_bad, pq.PQ_ERR_ARG)):
+        assert srv.status(rid) == 3, rid
+        with pytest.raises(pq.PQError) as e:
+            srv.collect(rid)
+        assert e.value.code == code, (rid, e.value)
+        assert srv.status(rid) == -1
+    for rid, seed, n in good:
+        assert srv.status(rid) == 2
+        psi, _ = srv.collect(rid)
+        assert np.array_equal(psi, alone(cfg, ic_of(cfg, seed), n))
+    rid, seed, n = good_mixed
+    psi, _ = srv.collect(rid)
+    assert np.array_equal(psi, alone(mixed, ic_of(mixed, seed), n))
+    # The failed runs' contexts were destroyed, not pooled: only the good
+    # configurations' contexts are held.
+    assert srv.device_bytes() <= 4 * pq.Model(cfg).device_bytes() + 2 * pq.Model(mixed).device_bytes()
+    srv.close()

@@ -1,7 +1,9 @@
-"""The multi-GPU plumbing on gloo, world size 2, on the CPU: each replica
-draws its own workload, the measurement takes the slowest rank, and the
-serving statistics cover every rank's requests (pequod_b200.multirank, as
-bench.py uses it under torchrun)."""
+"""The multi-GPU plumbing on gloo, world size 2, on the CPU: one ensemble
+workload (a batch of Helmholtz problems, a serving request stream) is
+partitioned across the ranks as whole members balanced by their work,
+single-run replicas draw their own workload, the measurement takes the
+slowest rank, and the serving statistics cover every rank's requests
+(pequod_b200.multirank, as bench.py uses it under torchrun)."""
 import json
 import os
 import socket
@@ -30,8 +32,17 @@ def _worker(rank, world, port, out_dir):
     done = [(0.1 * (k + 1) + rank, 1000.0 * (k + 1), 1.0 + k + rank) for k in range(3 + rank)]
     gathered = multirank.gather_lists(dist, done)
     summary = multirank.serving_summary(gathered)
+    # One shared serving stream and one shared batch, each rank its share.
+    stream = serving_requests(rate=200.0, window=0.25, seed=3)
+    my_reqs = multirank.shard(stream, [ii * ii * L * n for _, ii, L, n, _ in stream], rank, w)
+    batch = [(ii, jj, L) for ii in (65, 129, 257, 513, 1025) for jj in (65, 257, 1025) for L in (1, 3, 5)]
+    my_batch = multirank.shard(batch, [i * j * l for i, j, l in batch], rank, w)
+    all_reqs = multirank.gather_lists(dist, my_reqs)
+    all_batch = multirank.gather_lists(dist, my_batch)
     with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
-        json.dump({"slow": slow, "reqs": reqs, "gathered": gathered, "summary": summary}, f)
+        json.dump({"slow": slow, "reqs": reqs, "gathered": gathered, "summary": summary, "stream": stream,
+                   "my_reqs": my_reqs, "batch": batch, "my_batch": my_batch, "all_reqs": all_reqs,
+                   "all_batch": all_batch}, f)
     multirank.close(dist)
 
 
@@ -50,12 +61,42 @@ def test_two_ranks_on_gloo(tmp_path):
     for r in res:
         assert np.allclose(np.array(r["gathered"]), np.array(expect))
         assert r["summary"] == res[0]["summary"]
+    # The shared workloads: every member on exactly one rank, and the union
+    # of the ranks' shares is the single-rank workload; loads balanced to
+    # within the heaviest member.
+    for key, mine, allk, wt in (("stream", "my_reqs", "all_reqs", lambda q: q[1] * q[1] * q[2] * q[3]),
+                                ("batch", "my_batch", "all_batch", lambda q: q[0] * q[1] * q[2])):
+        whole = [tuple(x) for x in res[0][key]]
+        assert [tuple(x) for x in res[1][key]] == whole
+        shares = [[tuple(x) for x in r[mine]] for r in res]
+        assert not set(shares[0]) & set(shares[1])
+        assert sorted(shares[0] + shares[1]) == sorted(whole)
+        assert sorted(tuple(x) for x in res[0][allk]) == sorted(whole)
+        loads = [sum(wt(q) for q in sh) for sh in shares]
+        assert max(loads) <= sum(loads) / world + max(wt(q) for q in whole)
+        assert min(loads) > 0
     lat = np.array([e[0] for e in expect])
     s = res[0]["summary"]
     assert s["runs"] == 7
     assert abs(s["p50_s"] - np.percentile(lat, 50)) < 1e-12
     assert abs(s["p99_s"] - np.percentile(lat, 99)) < 1e-12
     assert abs(s["throughput"] - sum(e[1] for e in expect) / max(e[2] for e in expect)) < 1e-9
+
+
+def test_partition_is_balanced_and_deterministic():
+    from pequod_b200 import multirank
+
+    rng = np.random.default_rng(7)
+    w = list(rng.integers(1, 1000, 200))
+    for world in (1, 2, 3, 8):
+        parts = multirank.partition(w, world)
+        assert parts == multirank.partition(w, world)
+        assert sorted(k for p in parts for k in p) == list(range(len(w)))
+        loads = [sum(w[k] for k in p) for p in parts]
+        assert max(loads) <= sum(w) / world + max(w)
+        if world == 8:  # many light items: close to even
+            assert max(loads) / (sum(w) / world) < 1.05
+    assert multirank.partition([5.0], 4) == [[0], [], [], []]
 
 
 def test_single_rank_needs_no_process_group():
