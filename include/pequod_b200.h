@@ -399,8 +399,25 @@ typedef struct pq_tuning {
                            waits for the predecessor's results before reading
                            anything); 0 (default): one after another, which
                            measured 0-5 % faster on B200 */
-    int reserved[2];
+    int dst_algo;       /* row DSTs of the mixed form's baroclinic modes:
+                           PQ_DST_BUTTERFLY (FP32 FFT in registers, the default)
+                           or PQ_DST_TENSOR (dense DST-matrix products on the
+                           tensor cores, three-term BF16 split with FP32
+                           accumulation; ii >= 65); 0 keeps the current one.
+                           The FP64 form and the barotropic mode always use
+                           the FP64 butterfly. */
+    int reserved[1];
 } pq_tuning;
+#define PQ_DST_BUTTERFLY 1
+#define PQ_DST_TENSOR 2
+/* The autotuner: times the step's inversion with each row-DST algorithm
+ * this context supports (the butterfly, and for the mixed form the tensor-
+ * core DST) on its own stream, selects the faster, and returns it in
+ * *choice (PQ_DST_*).  The decision is cached per (ii, jj, L, channel) for
+ * the process, so later contexts of the same shape take it without timing.
+ * The model state is left as it was (psi and the scalars are restored).
+ * Call it between steps, not while a stream capture is in progress. */
+PQ_API int pq_autotune(pq_ctx* ctx, int* choice);
 PQ_API int pq_set_tuning(pq_ctx* ctx, const pq_tuning* t);
 PQ_API int pq_get_tuning(pq_ctx* ctx, pq_tuning* t);
 

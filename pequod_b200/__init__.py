@@ -26,6 +26,7 @@ PTR_HOST, PTR_DEVICE = 0, 1
 SCHEME_CABARET, SCHEME_LEAPFROG = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 BC_PARTIAL_SLIP, BC_NO_SLIP, BC_FREE_SLIP = 1, 2, 3
+DST_BUTTERFLY, DST_TENSOR = 1, 2
 MAX_LAYERS = 8
 NOALLOC_MAX_JJ = 4097  # PQ_NOALLOC_MAX_JJ: largest jj pq_energy_noalloc accepts
 
@@ -62,7 +63,7 @@ class ModelDesc(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("cab_band", C.c_int), ("dst_group", C.c_int), ("cab_kernel", C.c_int), ("dst_lanes", C.c_int),
-                ("dst_lanes_inv", C.c_int), ("pdl", C.c_int), ("reserved", C.c_int * 2)]
+                ("dst_lanes_inv", C.c_int), ("pdl", C.c_int), ("dst_algo", C.c_int), ("reserved", C.c_int * 1)]
 
 
 class Physical(C.Structure):
@@ -116,6 +117,7 @@ SIGNATURES = {
     "pq_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "pq_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "pq_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    "pq_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "pq_kernel_times": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_long)]),
     "pq_energy_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp,
                                     C.c_void_p, C.c_void_p]),
@@ -464,7 +466,15 @@ class Model:
         t = Tuning()
         _check(lib().pq_get_tuning(self.ctx, C.byref(t)), self.ctx)
         return {"cab_band": t.cab_band, "dst_group": t.dst_group, "cab_kernel": t.cab_kernel, "dst_lanes": t.dst_lanes,
-                "dst_lanes_inv": t.dst_lanes_inv, "pdl": t.pdl}
+                "dst_lanes_inv": t.dst_lanes_inv, "pdl": t.pdl, "dst_algo": t.dst_algo}
+
+    def autotune(self) -> int:
+        """Time the inversion with each row-DST algorithm this context
+        supports, select the faster (cached per shape for the process) and
+        return it (DST_BUTTERFLY or DST_TENSOR)."""
+        ch = C.c_int()
+        _check(lib().pq_autotune(self.ctx, C.byref(ch)), self.ctx)
+        return ch.value
 
     def kernel_timing(self, enable: bool) -> None:
         _check(lib().pq_kernel_timing(self.ctx, int(enable)), self.ctx)

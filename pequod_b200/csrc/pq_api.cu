@@ -1,6 +1,8 @@
 // pq_api.cu -- the C ABI: contexts, device state, tables and the time loop.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -10,6 +12,7 @@
 #include "pq_common.cuh"
 #include "pq_kernels.h"
 #include "pq_ctx.h"
+#include "pq_dst_mma.h"
 
 using namespace pq;
 
@@ -133,7 +136,91 @@ int upload_members(pq_ctx* c) {
 }
 
 // The three Helmholtz kernels.
+namespace {
+
+// Arguments of the tensor-core DST over the baroclinic rows: forward (dir 0)
+// from the node rows in gbuf to the spectral rows, inverse (dir 1) back.
+DstMmaArgs mma_args(const pq_ctx* c, int dir) {
+    const Member& m = c->hm[0];
+    DstMmaArgs a;
+    a.x = static_cast<const float*>(dir == 0 ? m.gbuf : m.spec);
+    a.y = static_cast<float*>(dir == 0 ? m.spec : m.gbuf);
+    a.ls = m.lstride;
+    a.pitch = m.pitch;
+    a.N = m.N;
+    a.Kp = std::max(64, m.N / 2);
+    a.nj = c->periodic ? c->jj : c->jj - 2;
+    a.jlo = c->periodic ? 0 : 1;
+    a.rows = (c->L - 1) * a.nj;
+    a.status = c->d_status;
+    return a;
+}
+
+}  // namespace
+
+int set_dst_algo(pq_ctx* c, int algo) {
+    if (algo != PQ_DST_BUTTERFLY && algo != PQ_DST_TENSOR) return fail(c, PQ_ERR_ARG, "dst_algo is 1 or 2");
+    if (algo == PQ_DST_TENSOR) {
+        if (!c->mixed || c->leapfrog || c->helm_only)
+            return fail(c, PQ_ERR_UNSUPPORTED, "the tensor-core DST serves the mixed-precision CABARET form");
+        if (!dst_mma_supported(c->hm[0].N)) return fail(c, PQ_ERR_UNSUPPORTED, "the tensor-core DST needs ii >= 65");
+        if (!c->mma_mem) {
+            const size_t gbytes = align256((size_t)c->L * c->hm[0].lstride * sizeof(float));
+            const size_t tbytes = dst_mma_table_bytes(c->hm[0].N);
+            void* mem = nullptr;
+            if (cudaMalloc(&mem, gbytes + tbytes) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(c, PQ_ERR_NOMEM, "allocation of the tensor-core DST buffers failed");
+            }
+            c->mma_mem = mem;
+            c->mma_bytes = gbytes + tbytes;
+            std::vector<unsigned short> table;
+            dst_mma_table(c->hm[0].N, table);
+            void* tab = static_cast<char*>(mem) + gbytes;
+            CK(cudaMemsetAsync(mem, 0, gbytes, c->stream));
+            CK(cudaMemcpyAsync(tab, table.data(), tbytes, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            if (dst_mma_tensor_map(&c->mma_map, tab, c->hm[0].N) != 0)
+                return fail(c, PQ_ERR_CUDA, "cuTensorMapEncodeTiled failed for the DST table");
+            for (int p = 0; p < 2; ++p) c->hm[p].gbuf = mem;
+            int rc = upload_members(c);
+            if (rc) return rc;
+        }
+    }
+    if (algo != c->dst_algo) {
+        c->dst_algo = algo;
+        // captured step graphs hold the old kernel sequence
+        for (auto& g : c->graph1)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        if (c->graph2) {
+            cudaGraphExecDestroy(c->graph2);
+            c->graph2 = nullptr;
+        }
+    }
+    return PQ_OK;
+}
+
+int run_inversion(pq_ctx* c, int par, int prologue, cudaEvent_t* ev) {
+    const int f32 = c->mixed ? 1 : 0;
+    const bool tc = f32 && c->dst_algo == PQ_DST_TENSOR && c->mma_mem;
+    LaunchSet ls = c->ls[par];
+    ls.gemm_bc = tc ? 1 : 0;
+    CK(launch_dst_forward(ls, prologue, f32, c->stream));
+    if (tc) CK(launch_dst_mma(mma_args(c, 0), c->mma_map, c->stream));
+    if (ev) CK(cudaEventRecord(ev[1], c->stream));
+    CK(launch_tridiag(ls, 1, f32, c->stream));
+    if (ev) CK(cudaEventRecord(ev[2], c->stream));
+    if (tc) CK(launch_dst_mma(mma_args(c, 1), c->mma_map, c->stream));
+    CK(launch_dst_inverse(ls, EPI_PV, f32, c->stream));
+    if (ev) CK(cudaEventRecord(ev[3], c->stream));
+    return PQ_OK;
+}
+
 int run_helm(pq_ctx* c, int par, int prologue, int epilogue, int mean) {
+    if (epilogue == EPI_PV && mean && c->mixed) return run_inversion(c, par, prologue, nullptr);
     // The stand-alone helm entry (PRO_PLAIN / EPI_HELM) is always FP64, and
     // runs the row DSTs with the batched solver's geometry, so that a batch
     // member and the same problem through pq_helm agree bit for bit.
@@ -183,12 +270,8 @@ int run_step(pq_ctx* c, int par) {
     if (c->periodic) {
         // Channel: predictor + beta in the forward DST, the momentum-corrected
         // inversion, then the four channel CABARET kernels.
-        CK(launch_dst_forward(c->ls[par], PRO_STEP, f32, c->stream));
-        if (ev) CK(cudaEventRecord(ev[1], c->stream));
-        CK(launch_tridiag(c->ls[par], 1, f32, c->stream));
-        if (ev) CK(cudaEventRecord(ev[2], c->stream));
-        CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
-        if (ev) CK(cudaEventRecord(ev[3], c->stream));
+        int rc = run_inversion(c, par, PRO_STEP, ev);
+        if (rc) return rc;
         if (c->quad) CK(launch_quad(c->ls[par], f32, 0, c->stream));
         CK(launch_cabaret_channel(c->ls[par], f32, c->stream));
         if (ev) CK(cudaEventRecord(ev[4], c->stream));
@@ -198,12 +281,8 @@ int run_step(pq_ctx* c, int par) {
     }
     // The predictor + beta update runs in the forward DST unless the previous
     // fused step already produced this step's inversion input.
-    CK(launch_dst_forward(c->ls[par], (c->fuse && c->pred_ready) ? PRO_MODAL : PRO_STEP, f32, c->stream));
-    if (ev) CK(cudaEventRecord(ev[1], c->stream));
-    CK(launch_tridiag(c->ls[par], 1, f32, c->stream));
-    if (ev) CK(cudaEventRecord(ev[2], c->stream));
-    CK(launch_dst_inverse(c->ls[par], EPI_PV, f32, c->stream));
-    if (ev) CK(cudaEventRecord(ev[3], c->stream));
+    int rc = run_inversion(c, par, (c->fuse && c->pred_ready) ? PRO_MODAL : PRO_STEP, ev);
+    if (rc) return rc;
     if (c->quad) CK(launch_quad(c->ls[par], f32, 0, c->stream));
     CK(launch_cabaret_fused(c->ls[par], c->fuse ? 1 : 0, f32, c->stream));
     if (ev) CK(cudaEventRecord(ev[4], c->stream));
@@ -231,6 +310,7 @@ void pq_destroy(pq_ctx* c) {
     for (auto& g : c->graph1)
         if (g) cudaGraphExecDestroy(g);
     if (c->arena) cudaFree(c->arena);
+    if (c->mma_mem) cudaFree(c->mma_mem);
     if (c->psi_av) cudaFree(c->psi_av);
     if (c->quad) cudaFree(c->quad);
     if (c->x.in) {
@@ -1020,6 +1100,11 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     if (t->dst_group < 0 || c->L * t->dst_group > 8) return fail(c, PQ_ERR_ARG, "dst_group out of range");
     if (t->cab_kernel < 0 || t->cab_kernel > 1) return fail(c, PQ_ERR_ARG, "cab_kernel out of range");
     if (t->pdl < 0 || t->pdl > 1) return fail(c, PQ_ERR_ARG, "pdl is 0 or 1");
+    if (t->dst_algo < 0 || t->dst_algo > PQ_DST_TENSOR) return fail(c, PQ_ERR_ARG, "dst_algo is 0, 1 or 2");
+    if (t->dst_algo) {
+        const int rc = set_dst_algo(c, t->dst_algo);
+        if (rc) return rc;
+    }
     const int M = c->hm[0].M;
     int P[2];
     for (int dir = 0; dir < 2; ++dir) {
@@ -1061,6 +1146,79 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     return PQ_OK;
 }
 
+int pq_autotune(pq_ctx* c, int* choice) {
+    if (!c) return PQ_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    // The decision per shape, for the process.
+    static std::mutex mu;
+    static std::map<std::vector<int>, int> cache;
+    const std::vector<int> key = {c->ii, c->jj, c->L, c->periodic ? 1 : 0, c->mixed ? 1 : 0};
+    int best = PQ_DST_BUTTERFLY;
+    const bool candidates = c->mixed && !c->leapfrog && !c->helm_only && c->L > 1 && dst_mma_supported(c->hm[0].N);
+    if (candidates) {
+        bool known = false;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            auto it = cache.find(key);
+            if (it != cache.end()) {
+                best = it->second;
+                known = true;
+            }
+        }
+        if (!known) {
+            // Time the inversion (forward DST, tridiagonal, inverse DST) of
+            // the current zeta with each algorithm; psi and the scalars it
+            // overwrites are saved and restored, nothing else changes.
+            const int prev = c->dst_algo;
+            int rc = set_dst_algo(c, PQ_DST_TENSOR);
+            if (rc) return rc;
+            void* save = nullptr;
+            if (cudaMalloc(&save, c->field_bytes + sizeof(Scalars)) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(c, PQ_ERR_NOMEM, "autotune: scratch allocation failed");
+            }
+            char* sv = static_cast<char*>(save);
+            CK(cudaMemcpyAsync(sv, c->hm[0].psi, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+            CK(cudaMemcpyAsync(sv + c->field_bytes, c->d_sc, sizeof(Scalars), cudaMemcpyDeviceToDevice, c->stream));
+            cudaEvent_t e0, e1;
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            float ms[3] = {0.f, 0.f, 0.f};
+            const int algos[2] = {PQ_DST_BUTTERFLY, PQ_DST_TENSOR};
+            for (int round = 0; round < 2 && !rc; ++round)  // two rounds: the second is kept
+                for (int a = 0; a < 2 && !rc; ++a) {
+                    rc = set_dst_algo(c, algos[a]);
+                    for (int w = 0; w < 3 && !rc; ++w) rc = run_inversion(c, c->zpar, PRO_MODAL, nullptr);
+                    if (rc) break;
+                    CK(cudaEventRecord(e0, c->stream));
+                    for (int k = 0; k < 10 && !rc; ++k) rc = run_inversion(c, c->zpar, PRO_MODAL, nullptr);
+                    CK(cudaEventRecord(e1, c->stream));
+                    CK(cudaEventSynchronize(e1));
+                    CK(cudaEventElapsedTime(&ms[algos[a]], e0, e1));
+                }
+            CK(cudaMemcpyAsync(c->hm[0].psi, sv, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+            CK(cudaMemcpyAsync(c->d_sc, sv + c->field_bytes, sizeof(Scalars), cudaMemcpyDeviceToDevice, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            cudaFree(save);
+            if (rc) {
+                set_dst_algo(c, prev);
+                return rc;
+            }
+            rc = check_status(c);
+            if (rc) return rc;
+            best = ms[PQ_DST_TENSOR] < ms[PQ_DST_BUTTERFLY] ? PQ_DST_TENSOR : PQ_DST_BUTTERFLY;
+            std::lock_guard<std::mutex> lk(mu);
+            cache[key] = best;
+        }
+    }
+    const int rc = set_dst_algo(c, best);
+    if (rc) return rc;
+    if (choice) *choice = best;
+    return PQ_OK;
+}
+
 int pq_get_tuning(pq_ctx* c, pq_tuning* t) {
     if (!c || !t) return PQ_ERR_ARG;
     std::memset(t, 0, sizeof(*t));
@@ -1070,6 +1228,7 @@ int pq_get_tuning(pq_ctx* c, pq_tuning* t) {
     t->dst_lanes = c->ls[0].dst_lanes[0];
     t->dst_lanes_inv = c->ls[0].dst_lanes[1];
     t->pdl = c->ls[0].pdl;
+    t->dst_algo = c->dst_algo;
     return PQ_OK;
 }
 
@@ -1159,7 +1318,8 @@ int reset_prognostic(pq_ctx* c, const Scalars& sc) {
 }
 
 int step_launches(const pq_ctx* c) {
-    return (c->leapfrog ? (c->psi_av ? 6 : 5) : c->periodic ? 7 : 4) + (c->quad ? 1 : 0);
+    const int tc = (c->mixed && c->dst_algo == PQ_DST_TENSOR && c->mma_mem && c->L > 1) ? 2 : 0;
+    return (c->leapfrog ? (c->psi_av ? 6 : 5) : c->periodic ? 7 : 4) + (c->quad ? 1 : 0) + tc;
 }
 
 int read_scalars(pq_ctx* c, Scalars* sc) {

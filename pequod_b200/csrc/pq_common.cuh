@@ -51,6 +51,7 @@ enum StatusBits : int {
     ST_LARGE_PSIC = 2,    // |psiC| > 1e100: the reference warns (:511-517)
     ST_NAN_ENERGY = 4,    // NaN energy: the reference aborts (qg3p_diagnostics.F90:858-861)
     ST_SMALL_DT = 8,      // dt < 1e-6 after adaptation: the reference warns (qg3p_aux.F90:982-986)
+    ST_MMA_TIMEOUT = 16,  // a bounded wait of the tensor-core DST ran out (its output is not valid)
 };
 
 // Per-member device descriptor.  Lives in device global memory (an array of
@@ -118,6 +119,8 @@ struct Member {
     void* flux_j;
     void* spec;
     double* spec64;   // barotropic-mode spectral rows of the mixed path (FP64)
+    void* gbuf;       // mixed path with the tensor-core DST: baroclinic node rows (FP32),
+                      // the DST's input (forward) and output (inverse)
     const double* corr;
     // Channel (momentum correction, correction_function_momentum): the second
     // correction function, the spectral weights of the two walls' mean PV

@@ -2,6 +2,7 @@
 // shared by the single-model API, the batched solver and the server.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -51,6 +52,13 @@ struct pq_ctx {
     // host copies of layout facts
     int ii = 0, jj = 0, L = 0, pitch = 0;
     size_t field_bytes = 0;  // bytes of one L-layer field
+    // Row-DST algorithm of the mixed form's baroclinic modes (pq_tuning.dst_algo):
+    // PQ_DST_BUTTERFLY, or PQ_DST_TENSOR with its node-row buffer (gbuf) and
+    // the split DST matrices in mma_mem and their TMA descriptor.
+    int dst_algo = PQ_DST_BUTTERFLY;
+    void* mma_mem = nullptr;
+    size_t mma_bytes = 0;
+    CUtensorMap mma_map;
     double* psi_av = nullptr;  // time average of psi (pq_average), FP64, node-shaped like psi
     double* quad = nullptr;    // the 23 quad eddy-covariance accumulators (pq_average mode 2)
     // Pipelined host exchange (pq_step_exchange with host buffers): the
@@ -96,6 +104,12 @@ int copy_out_state(pq_ctx* c, double* dst, const void* src, int kind);
 int check_status(pq_ctx* c);
 int upload_members(pq_ctx* c);
 int run_helm(pq_ctx* c, int par, int prologue, int epilogue, int mean);
+// The inversion of a step (forward DST with `prologue`, tridiagonal,
+// inverse DST with the back-projection), through the tensor-core DST when
+// the context selected it; ev (or null): events after each of the three.
+int run_inversion(pq_ctx* c, int par, int prologue, cudaEvent_t* ev);
+// Select the row-DST algorithm (allocating the tensor-core DST's buffers).
+int set_dst_algo(pq_ctx* c, int algo);
 int run_step(pq_ctx* c, int par);
 // Checkpoint pickup support: clear the prognostic fields and install the
 // scalars (reset_prognostic); copy the device scalars to the host.

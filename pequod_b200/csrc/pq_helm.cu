@@ -329,7 +329,7 @@ __device__ __forceinline__ void cp4z(void* dst, const void* src, bool ok) {
 template <typename S, int V, int PRO, int EPI>
 __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
                                              int nmem, int row_offset, int c, int corr_smem, int psic_here,
-                                             const __grid_constant__ Member one, int use_one) {
+                                             const __grid_constant__ Member one, int use_one, int gemm_bc) {
     constexpr bool MX = sizeof(S) == 4;
     __shared__ Member Mb;
     __shared__ double psic_s[PQ_MAXL];                   // closed basin: psiC of the inverse
@@ -579,6 +579,12 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
                                   (long long)(ok ? j : 1) * pitch - 1;
                 double* d = ubuf(m, r);
                 for (int k = 1 + lane; k <= n; k += 32) cp8z(d + k, g + k, ok);
+            } else if (gemm_bc) {
+                // Rows the tensor-core DST already took back to node values:
+                // straight to the positions the back-projection reads.
+                const float* g = reinterpret_cast<const float*>(Mb.gbuf) + m * ls + (long long)(ok ? j : 1) * pitch - 1;
+                float* d = reinterpret_cast<float*>(ubuf(m, r));
+                for (int k = 1 + lane; k <= n; k += 32) cp4z(d + xpad(k), g + k, ok);
             } else {
                 const float* g = reinterpret_cast<const float*>(Mb.spec) + m * ls + (long long)(ok ? j : 1) * pitch - 1;
                 float* d = reinterpret_cast<float*>(ubuf(m, r));
@@ -646,9 +652,11 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
     double* buf = ubuf(um, ur);
     const bool interior = (Mb.periodic || (ju >= 1 && ju <= jj - 2)) && ju < jend;
     __shared__ double utot[8][2];  // cross-warp scan totals of units wider than a warp
+    // With gemm_bc the baroclinic rows (a whole warp's or unit's mode) are
+    // transformed by the tensor-core DST instead (pq_dst_mma.cu).
     if (fp64_mode(um))
         dst_unit<V, double>(buf, p, P, u, utot[u & 7], N, M, logM, Mb.tw, Mb.wsplit, Mb.was);
-    else
+    else if (!gemm_bc)
         dst_unit<V, float>(reinterpret_cast<float*>(buf), p, P, u, reinterpret_cast<float*>(utot[u & 7]), N, M, logM,
                            Mb.tw_f, Mb.wsplit_f, Mb.was_f);
     pdl_release();
@@ -659,6 +667,11 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
                 double* spec = (MX ? Mb.spec64 : reinterpret_cast<double*>(Mb.spec)) + um * ls +
                                (long long)ju * pitch - 1;
                 for (int k = 1 + p; k <= n; k += P) spec[k] = buf[xpad(k)];
+            } else if (gemm_bc) {
+                // node values of the projected row, for the tensor-core DST
+                float* g = reinterpret_cast<float*>(Mb.gbuf) + um * ls + (long long)ju * pitch - 1;
+                const float* fb = reinterpret_cast<const float*>(buf);
+                for (int k = 1 + p; k <= n; k += P) g[k] = fb[k];
             } else {
                 float* spec = reinterpret_cast<float*>(Mb.spec) + um * ls + (long long)ju * pitch - 1;
                 const float* fb = reinterpret_cast<const float*>(buf);
@@ -1193,7 +1206,7 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     return launch_step_kernel(ls.pdl, k_dst<S, V, PRO, EPI>, dim3(ls.ctas_dst[dir]), dim3(threads), bytes, st,
                               ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0,
                               ls.dst_group, corr_smem, (EPI == EPI_PV) ? psic_in_inverse(ls) : 0, member_arg(ls),
-                              member_arg_used(ls));
+                              member_arg_used(ls), (sizeof(S) == 4 && EPI != EPI_HELM) ? ls.gemm_bc : 0);
 }
 
 template <typename S, int PRO, int EPI>

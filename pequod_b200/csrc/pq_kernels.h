@@ -31,6 +31,8 @@ struct LaunchSet {
     int periodic;                     // channel periodic in j: every row is transformed
     int sm_count;                     // SMs of the device (persistent grids)
     int pdl;                          // launch the step kernels with programmatic dependent launch
+    int gemm_bc = 0;                  // mixed form: the row DSTs leave the baroclinic modes to the
+                                      // tensor-core DST (node rows in Member::gbuf)
 };
 
 // The by-value member argument of a launch and whether the kernel uses it.

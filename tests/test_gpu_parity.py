@@ -362,7 +362,7 @@ def test_tile_parameters_do_not_change_results(kernel, band, group, lanes):
     g.set_tuning(cab_kernel=kernel, cab_band=band, dst_group=group, dst_lanes=lanes, dst_lanes_inv=lanes)
     assert g.get_tuning() == {"cab_band": band, "dst_group": group, "cab_kernel": kernel,
                               "dst_lanes": lanes if lanes else 32, "dst_lanes_inv": lanes if lanes else 32,
-                              "pdl": 0}
+                              "pdl": 0, "dst_algo": 1}
     g.step(3)
     o.step(3)
     compare(g, o, TOL_STEP * 10)
