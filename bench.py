@@ -352,6 +352,43 @@ def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False):
             "launches_per_step": m_launches}
 
 
+def measure_ensemble(cfg, n, K, warmup, dev, dist, rank, world, seed):
+    """n runs of cfg stepped together (pq_ensemble: one launch per kernel
+    over all members, CUDA graphs): device time of K steps of every member,
+    L2 flushed before each step."""
+    import torch
+
+    import pequod_b200 as pq
+    from pequod_b200 import multirank
+
+    ens = pq.Ensemble(cfg, n, device=dev)
+    algo = ens.autotune()
+    for k in range(n):
+        ens.init(k, pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed + 1000 * k, amplitude=1e-7 * cfg.t_scale,
+                               sigma=3.0))
+    ens.step(max(3, warmup))
+    stream = torch.cuda.ExternalStream(ens.stream, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.zero_()
+            ev[k][0].record(stream)
+            ens.step_async(1)
+            ev[k][1].record(stream)
+    stream.synchronize()
+    ens.sync()
+    ms = multirank.max_over_ranks(dist, [float(sum(a.elapsed_time(b) for a, b in ev))], device=dev)[0]
+    units = n * cfg.ii * cfg.jj * cfg.layers
+    launches = ens.members[0].last_launch_count()
+    ens.close()
+    return {"members": n, "value": world * units * K / (ms * 1e-3), "ms_per_step": ms / K,
+            "dst_algo": "tensor" if algo == pq.DST_TENSOR else "butterfly"}
+
+
 def roofline_of(res, layers, mixed):
     peak, peak_kind = peaks()
     kt = res["kt"]
@@ -391,6 +428,13 @@ def run_ours(a, rank, world, local_rank):
     for name, prec in forms.items():
         cfg = make_config(a.size, a.layers, a.dt, precision=prec)
         res[name] = measure_single(cfg, K, a.warmup, dev, dist, rank, world, seed, pdl=a.pdl)
+    batched = {}
+    if a.ensemble > 0:
+        # The batched form: an ensemble of runs of the same configuration
+        # stepped together, each precision (every rank takes part).
+        for name, prec in forms.items():
+            cfg = make_config(a.size, a.layers, a.dt, precision=prec)
+            batched[name] = measure_ensemble(cfg, a.ensemble, K, a.warmup, dev, dist, rank, world, seed)
     if rank != 0:
         multirank.close(dist)
         return
@@ -431,6 +475,10 @@ def run_ours(a, rank, world, local_rank):
                          "note": "CUDA-graph replay, L2 not flushed"},
         "clocks": head["clocks"],
     }
+    if batched:
+        line["batched"] = batched
+        if "mixed" in batched and "fp64" in res:
+            line["batched_mixed_over_fp64_single"] = line["batched"]["mixed"]["value"] / res["fp64"]["value"]
     if "mixed" in res and "fp64" in res:
         f64 = res["fp64"]
         p64, pmx = f64["psi"], res["mixed"]["psi"]
@@ -679,6 +727,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="double-gyre", choices=["double-gyre", "batched-helm", "serving"])
+    ap.add_argument("--ensemble", type=int, default=8,
+                    help="double-gyre: members of the batched form (0: single runs only)")
     ap.add_argument("--batch", type=int, default=512, help="batched-helm: solves per batch")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     ap.add_argument("--window", type=float, default=0.25, help="serving: seconds of arrivals")

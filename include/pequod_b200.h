@@ -484,6 +484,34 @@ PQ_API size_t pq_server_device_bytes(const pq_server* s);
 PQ_API double pq_server_clock(const pq_server* s);
 PQ_API long pq_server_launches(const pq_server* s);
 
+/* ---- ensembles: many runs of one configuration stepped together ---------
+ * n members share a configuration (CABARET, fixed dt, closed basin) and a
+ * stream.  Each member is initialised (START_PERTURB, qg3.F90:365-404) from
+ * its own initial PV; then every step (the timestep_loop body,
+ * qg3.F90:590-957) is one launch per kernel over all members, replayed as
+ * CUDA graphs, so that many small or medium runs fill the GPU.  A member's
+ * results are the same as the run alone.  pq_ensemble_member gives a
+ * member's context for pq_get_field / pq_energy / pq_write_checkpoint (call
+ * pq_ensemble_sync first); do not step a member on its own.  The row-DST
+ * algorithm (pq_ensemble_autotune / pq_ensemble_set_dst_algo, as pq_autotune
+ * and pq_tuning.dst_algo) is chosen before the first step. */
+typedef struct pq_ensemble pq_ensemble;
+PQ_API int pq_ensemble_create(pq_ensemble** out, int n, const pq_model_desc* desc, int device);
+PQ_API void pq_ensemble_destroy(pq_ensemble* e);
+PQ_API const char* pq_ensemble_last_error(const pq_ensemble* e);
+PQ_API int pq_ensemble_size(const pq_ensemble* e);
+PQ_API pq_ctx* pq_ensemble_member(pq_ensemble* e, int k);
+PQ_API void* pq_ensemble_stream(pq_ensemble* e);
+PQ_API int pq_ensemble_init(pq_ensemble* e, int k, const double* zeta_ic, int ptr_kind);
+PQ_API int pq_ensemble_autotune(pq_ensemble* e, int* choice);
+PQ_API int pq_ensemble_set_dst_algo(pq_ensemble* e, int algo);
+/* nsteps steps of every member, enqueued on pq_ensemble_stream; _sync
+ * waits and reports a NaN psiC or energy of any member (PQ_ERR_NAN, the
+ * member named in the message). */
+PQ_API int pq_ensemble_step_async(pq_ensemble* e, int nsteps);
+PQ_API int pq_ensemble_sync(pq_ensemble* e);
+PQ_API int pq_ensemble_step(pq_ensemble* e, int nsteps);
+
 /* Number of kernel launches the last pq_step enqueued. */
 PQ_API long pq_last_launch_count(const pq_ctx* ctx);
 

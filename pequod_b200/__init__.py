@@ -133,6 +133,18 @@ SIGNATURES = {
     "pq_batch_sync": (C.c_int, [C.c_void_p]),
     "pq_batch_helm": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.c_int]),
     "pq_batch_launch_count": (C.c_int, [C.c_void_p]),
+    "pq_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(ModelDesc), C.c_int]),
+    "pq_ensemble_destroy": (None, [C.c_void_p]),
+    "pq_ensemble_last_error": (C.c_char_p, [C.c_void_p]),
+    "pq_ensemble_size": (C.c_int, [C.c_void_p]),
+    "pq_ensemble_member": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "pq_ensemble_stream": (C.c_void_p, [C.c_void_p]),
+    "pq_ensemble_init": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
+    "pq_ensemble_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "pq_ensemble_set_dst_algo": (C.c_int, [C.c_void_p, C.c_int]),
+    "pq_ensemble_step_async": (C.c_int, [C.c_void_p, C.c_int]),
+    "pq_ensemble_sync": (C.c_int, [C.c_void_p]),
+    "pq_ensemble_step": (C.c_int, [C.c_void_p, C.c_int]),
     "pq_server_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t, C.c_int]),
     "pq_server_destroy": (None, [C.c_void_p]),
     "pq_server_last_error": (C.c_char_p, [C.c_void_p]),
@@ -552,6 +564,80 @@ class Batch:
     def close(self):
         if self.ctx:
             lib().pq_batch_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Member(Model):
+    """A view of one ensemble member's context (owned by the ensemble)."""
+
+    def __init__(self, cfg, ctx):  # noqa: D107 - no context of its own
+        self.cfg = cfg
+        self.ctx = ctx
+
+    def close(self):
+        self.ctx = None
+
+
+class Ensemble:
+    """n runs of one configuration stepped together (pq_ensemble_*): one
+    launch per kernel over all members, replayed as CUDA graphs."""
+
+    def __init__(self, cfg: Config, n: int, device: int = 0):
+        self.cfg = cfg
+        self.ctx = C.c_void_p()
+        rc = lib().pq_ensemble_create(C.byref(self.ctx), int(n), C.byref(cfg.desc), device)
+        if rc != PQ_OK:
+            msg = lib().pq_ensemble_last_error(self.ctx).decode() if self.ctx else ""
+            if self.ctx:
+                lib().pq_ensemble_destroy(self.ctx)
+                self.ctx = None
+            raise PQError(rc, msg)
+        self.members = [_Member(cfg, C.c_void_p(lib().pq_ensemble_member(self.ctx, k))) for k in range(n)]
+
+    def _chk(self, rc):
+        if rc != PQ_OK:
+            raise PQError(rc, lib().pq_ensemble_last_error(self.ctx).decode())
+
+    def __len__(self):
+        return len(self.members)
+
+    def init(self, k: int, zeta_ic) -> None:
+        z = np.asfortranarray(zeta_ic, dtype=np.float64).reshape((self.cfg.ii, self.cfg.jj, self.cfg.layers),
+                                                                  order="F")
+        self._chk(lib().pq_ensemble_init(self.ctx, int(k), _p(z), PTR_HOST))
+
+    def autotune(self) -> int:
+        ch = C.c_int()
+        self._chk(lib().pq_ensemble_autotune(self.ctx, C.byref(ch)))
+        return ch.value
+
+    def set_dst_algo(self, algo: int) -> None:
+        self._chk(lib().pq_ensemble_set_dst_algo(self.ctx, int(algo)))
+
+    def step_async(self, n: int = 1) -> None:
+        self._chk(lib().pq_ensemble_step_async(self.ctx, int(n)))
+
+    def sync(self) -> None:
+        self._chk(lib().pq_ensemble_sync(self.ctx))
+
+    def step(self, n: int = 1) -> None:
+        self._chk(lib().pq_ensemble_step(self.ctx, int(n)))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().pq_ensemble_stream(self.ctx) or 0)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            for m in self.members:
+                m.ctx = None
+            lib().pq_ensemble_destroy(self.ctx)
             self.ctx = None
 
     def __del__(self):
