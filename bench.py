@@ -249,12 +249,12 @@ def run_reference(a, rank, world):
 
 def bench_config(a, world):
     return {"workload": workload_name(a.size, a.layers, a.dt), "ii": a.size, "jj": a.size, "layers": a.layers,
-            "dt_s": a.dt, "precision": a.precision,
+            "dt_s": a.dt, "precision": a.precision, "energy_every": a.diag_every,
             "l2": "flushed before every timed step (256 MiB memset)",
             "parallelism": f"replicas{world}"}
 
 
-def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False):
+def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False, diag_every=0):
     """One run of cfg on this rank: device-timed steps (value), back-to-back
     graph replay, per-kernel event times and the e2e exchange through the C
     ABI.  Returns a dict of the measurements (max over ranks)."""
@@ -295,14 +295,19 @@ def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False):
     kt = m.kernel_times()
     m.step(2)  # back to graph launches (one-step graphs of each parity)
 
-    # timed region: K steps (one-step graphs), L2 flushed before each
+    # timed region: K steps (one-step graphs), L2 flushed before each; with
+    # diag_every, the energy diagnostics (pq_energy, which waits for the
+    # step) after every diag_every-th step, inside that step's events
     barrier()
+    energies = []
     with ClockSampler(dev) as clk:
         with torch.cuda.stream(stream):
             for k in range(K):
                 flush.zero_()
                 ev[k][0].record(stream)
                 m.step_async(1)
+                if diag_every and (k + 1) % diag_every == 0:
+                    energies.append(m.energy())
                 ev[k][1].record(stream)
         stream.synchronize()
     barrier()
@@ -349,7 +354,7 @@ def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False):
             "ms_per_step": total_ms / K, "b2b_ms": b2b_ms, "e2e_ms": e2e_ms,
             "e2e": world * units * K / (e2e_ms * 1e-3), "kt": kt, "clocks": clk.summary(), "psi": psi,
             "dst_algo": "tensor" if algo == pq.DST_TENSOR else "butterfly",
-            "launches_per_step": m_launches}
+            "launches_per_step": m_launches, "diagnostics": len(energies)}
 
 
 def measure_ensemble(cfg, n, K, warmup, dev, dist, rank, world, seed):
@@ -427,7 +432,8 @@ def run_ours(a, rank, world, local_rank):
     res = {}
     for name, prec in forms.items():
         cfg = make_config(a.size, a.layers, a.dt, precision=prec)
-        res[name] = measure_single(cfg, K, a.warmup, dev, dist, rank, world, seed, pdl=a.pdl)
+        res[name] = measure_single(cfg, K, a.warmup, dev, dist, rank, world, seed, pdl=a.pdl,
+                                   diag_every=a.diag_every)
     batched = {}
     if a.ensemble > 0:
         # The batched form: an ensemble of runs of the same configuration
@@ -727,6 +733,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="double-gyre", choices=["double-gyre", "batched-helm", "serving"])
+    ap.add_argument("--diag-every", type=int, default=0,
+                    help="double-gyre: energy diagnostics every D timed steps (0: none)")
     ap.add_argument("--ensemble", type=int, default=8,
                     help="double-gyre: members of the batched form (0: single runs only)")
     ap.add_argument("--batch", type=int, default=512, help="batched-helm: solves per batch")

@@ -145,3 +145,20 @@ def test_mixed_1025_hundred_steps_vs_oracle():
     o.step(100)
     e = rel_l2(g.get("psi"), o.get("psi"))
     assert e <= TOL_MIXED, e
+
+
+def test_2049x5_energy_every_ten_steps():
+    """The large eddy-resolving run's diagnostics cadence: 30 steps at
+    2049 x 2049 x 5, dt = 300 s, the energies (qg3.F90:744, energy of
+    qg3p_diagnostics.F90:778-863) and the CFL number taken every 10 steps
+    between graph-launched steps, each within 1e-12 of the oracle's."""
+    cfg = double_gyre(2049, 5, 300.0)
+    g, o = start(cfg, seed=17)
+    for k in range(3):
+        g.step(10)
+        o.step(10)
+        ek, ep = energy_errors(g, o)
+        assert ek <= TOL_STEP and ep <= TOL_STEP, ((k + 1) * 10, ek, ep)
+        assert abs(g.cfl() - o.cfl()) <= TOL_STEP * o.cfl()
+    e = errors(g, o, ["psi", "zeta"])
+    assert max(e.values()) <= TOL_STEP, e
