@@ -221,6 +221,15 @@ PQ_API int pq_init_perturb(pq_ctx* ctx, const double* zeta_ic, int ptr_kind);
  * captured CUDA graphs on the context's stream. */
 PQ_API int pq_step(pq_ctx* ctx, int nsteps);
 
+/* One CABARET step with the time step and time weights the caller gives, as
+ * the reference's loop passes dt, tweight_a and tweight_u to every cabaret_*
+ * routine (qg3.F90:598-807, qg3p_aux.F90:993-1642): a host driver that
+ * chooses dt itself.  The values must satisfy cabaret_adapt_dt's checks
+ * (dt > 0, tweight_a >= 0, 0 <= tweight_u <= 1, qg3p_aux.F90:982-988); the
+ * step recomputes the predictor with this dt.  With adapt_dt set, the
+ * device still adapts dt at the end of the step (pq_get_scalars). */
+PQ_API int pq_cabaret_step(pq_ctx* ctx, double dt, double tweight_a, double tweight_u);
+
 /* pq_step without the final wait: enqueues the steps on the context's stream
  * and returns.  pq_check waits for the stream and reports a NaN psiC or
  * energy (PQ_ERR_NAN) raised by the device since initialisation. */

@@ -96,6 +96,7 @@ SIGNATURES = {
     "pq_init_perturb": (C.c_int, [C.c_void_p, _dp, C.c_int]),
     "pq_step": (C.c_int, [C.c_void_p, C.c_int]),
     "pq_step_async": (C.c_int, [C.c_void_p, C.c_int]),
+    "pq_cabaret_step": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     "pq_check": (C.c_int, [C.c_void_p]),
     "pq_step_exchange": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
     "pq_join": (C.c_int, [C.c_void_p]),
@@ -358,6 +359,10 @@ class Model:
     def step(self, n: int = 1) -> None:
         _check(lib().pq_step(self.ctx, n), self.ctx)
 
+    def cabaret_step(self, dt: float, tweight_a: float = 0.5, tweight_u: float = 0.5) -> None:
+        """One CABARET step with the caller's dt and time weights."""
+        _check(lib().pq_cabaret_step(self.ctx, float(dt), float(tweight_a), float(tweight_u)), self.ctx)
+
     def step_async(self, n: int = 1) -> None:
         _check(lib().pq_step_async(self.ctx, n), self.ctx)
 
@@ -619,6 +624,10 @@ class Ensemble:
 
     def set_dst_algo(self, algo: int) -> None:
         self._chk(lib().pq_ensemble_set_dst_algo(self.ctx, int(algo)))
+
+    def cabaret_step(self, dt: float, tweight_a: float = 0.5, tweight_u: float = 0.5) -> None:
+        """One CABARET step with the caller's dt and time weights."""
+        _check(lib().pq_cabaret_step(self.ctx, float(dt), float(tweight_a), float(tweight_u)), self.ctx)
 
     def step_async(self, n: int = 1) -> None:
         self._chk(lib().pq_ensemble_step_async(self.ctx, int(n)))

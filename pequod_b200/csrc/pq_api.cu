@@ -1,5 +1,6 @@
 // pq_api.cu -- the C ABI: contexts, device state, tables and the time loop.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -945,6 +946,25 @@ int pq_step(pq_ctx* c, int nsteps) {
     int rc = pq_step_async(c, nsteps);
     if (rc) return rc;
     return check_status(c);
+}
+
+int pq_cabaret_step(pq_ctx* c, double dt, double tweight_a, double tweight_u) {
+    if (!c) return PQ_ERR_ARG;
+    if (!c->initialized) return fail(c, PQ_ERR_STATE, "pq_cabaret_step before pq_init_perturb");
+    if (c->leapfrog) return fail(c, PQ_ERR_UNSUPPORTED, "pq_cabaret_step is the CABARET scheme's step");
+    // cabaret_adapt_dt's own checks, qg3p_aux.F90:982-988
+    if (!(dt > 0.0) || !(tweight_a >= 0.0) || !(tweight_u >= 0.0 && tweight_u <= 1.0))
+        return fail(c, PQ_ERR_ARG, "dt > 0, tweight_a >= 0 and 0 <= tweight_u <= 1 required");
+    CK(cudaSetDevice(c->device));
+    static_assert(offsetof(Scalars, tweight_a) == offsetof(Scalars, dt) + sizeof(double) &&
+                      offsetof(Scalars, tweight_u) == offsetof(Scalars, dt) + 2 * sizeof(double),
+                  "dt and the time weights are adjacent");
+    const double v[3] = {dt, tweight_a, tweight_u};
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->d_sc) + offsetof(Scalars, dt), v, sizeof(v),
+                       cudaMemcpyHostToDevice, c->stream));
+    // The predictor fused into the previous step used that step's dt.
+    c->pred_ready = false;
+    return pq_step(c, 1);
 }
 
 int pq_check(pq_ctx* c) {

@@ -463,3 +463,29 @@ def test_1025_steps_match_oracle(tuning):
     g.step(2)
     o.step(2)
     compare(g, o, TOL_STEP * 10)
+
+
+def test_cabaret_step_with_callers_dt():
+    """pq_cabaret_step: the time step and weights come from the caller, as
+    the reference passes them to every cabaret_* routine.  The oracle adapts
+    dt itself (cabaret_adapt_dt); a fixed-dt device context stepped with the
+    oracle's dt and weights of every step follows its trajectory."""
+    cfg_a = double_gyre(65, 3, adapt_dt=1, target_cfl=0.1, max_dt=86400.0)
+    cfg_f = double_gyre(65, 3)
+    ic = pq.make_ic(65, 65, 3, seed=21, amplitude=1e-7 * cfg_a.t_scale, sigma=3.0)
+    o = O.Model(O.cfg_from(cfg_a))
+    o.init(ic)
+    g = pq.Model(cfg_f)
+    g.init_perturb(ic)
+    for k in range(15):
+        o.step(1)
+        s = o.scalars()
+        g.cabaret_step(s["dt"], s["tweight_a"], s["tweight_u"])
+        sg = g.scalars()
+        assert sg["dt"] == s["dt"] and sg["tweight_a"] == s["tweight_a"]
+    compare(g, o, 1e-10)
+    assert abs(g.scalars()["model_time"] - o.scalars()["model_time"]) <= 1e-12 * o.scalars()["model_time"]
+    with pytest.raises(pq.PQError):
+        g.cabaret_step(-1.0)
+    with pytest.raises(pq.PQError):
+        g.cabaret_step(1.0, 0.5, 1.5)
