@@ -442,6 +442,17 @@ PQ_API int pq_get_tuning(pq_ctx* ctx, pq_tuning* t);
 typedef struct pq_batch pq_batch;
 PQ_API int pq_batch_create(pq_batch** out, int n, const int* ii, const int* jj, const int* layers,
                            const double* ss, int device);
+/* The same with a precision: PQ_PREC_FP64 (pq_batch_create), or
+ * PQ_PREC_MIXED -- every member's first layer (the barotropic, ss = 0
+ * problem of a stratified model) keeps the FP64 transforms, the other
+ * layers are transformed in FP32, the tridiagonal solves stay FP64 -- with
+ * dst_algo PQ_DST_BUTTERFLY (FP32 FFT), PQ_DST_TENSOR (tensor-core DST,
+ * three-term BF16 split, where ii >= 65 and L >= 2) or 0 (per DST class
+ * (ii, L), whichever is faster when timed at creation). */
+PQ_API int pq_batch_create_ex(pq_batch** out, int n, const int* ii, const int* jj, const int* layers,
+                              const double* ss, int precision, int dst_algo, int device);
+/* The row-DST algorithm member k's FP32 layers use (PQ_DST_*). */
+PQ_API int pq_batch_member_dst_algo(const pq_batch* b, int k);
 PQ_API void pq_batch_destroy(pq_batch* b);
 PQ_API const char* pq_batch_last_error(const pq_batch* b);
 PQ_API size_t pq_batch_device_bytes(const pq_batch* b);
@@ -452,7 +463,8 @@ PQ_API int pq_batch_solve_async(pq_batch* b); /* all members, on pq_batch_stream
 PQ_API int pq_batch_sync(pq_batch* b);
 /* set_rhs + solve + get for every member (zeta[k] in/out), then sync. */
 PQ_API int pq_batch_helm(pq_batch* b, double* const* zeta, int ptr_kind);
-/* Kernel launches one solve makes (3 phases x classes). */
+/* Kernel launches one solve makes (3 phases x classes, plus two per member
+ * whose layers take the tensor-core DST). */
 PQ_API int pq_batch_launch_count(const pq_batch* b);
 
 /* ---- serving: many model runs, continuously batched --------------------- */

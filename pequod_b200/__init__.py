@@ -124,6 +124,9 @@ SIGNATURES = {
                                     C.c_void_p, C.c_void_p]),
     "pq_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), _dp, C.c_int]),
+    "pq_batch_create_ex": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), _dp, C.c_int, C.c_int, C.c_int]),
+    "pq_batch_member_dst_algo": (C.c_int, [C.c_void_p, C.c_int]),
     "pq_batch_destroy": (None, [C.c_void_p]),
     "pq_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "pq_batch_device_bytes": (C.c_size_t, [C.c_void_p]),
@@ -507,7 +510,7 @@ class Batch:
     """Batched Helmholtz solves (pq_batch_*): member k is an (ii, jj, L) helm
     problem with per-layer constants ss[k] (a sequence of length L)."""
 
-    def __init__(self, shapes, ss, device: int = 0):
+    def __init__(self, shapes, ss, device: int = 0, precision: int = PREC_FP64, dst_algo: int = DST_BUTTERFLY):
         n = len(shapes)
         self.shapes = [tuple(int(v) for v in s) for s in shapes]
         ii = (C.c_int * n)(*[s[0] for s in self.shapes])
@@ -517,7 +520,8 @@ class Batch:
         if flat.size != sum(s[2] for s in self.shapes):
             raise ValueError("ss lengths must match the layer counts")
         self.ctx = C.c_void_p()
-        rc = lib().pq_batch_create(C.byref(self.ctx), n, ii, jj, ll, _p(flat), device)
+        rc = lib().pq_batch_create_ex(C.byref(self.ctx), n, ii, jj, ll, _p(flat), int(precision), int(dst_algo),
+                                      device)
         if rc != PQ_OK:
             msg = lib().pq_batch_last_error(self.ctx).decode() if self.ctx else ""
             if self.ctx:
@@ -565,6 +569,10 @@ class Batch:
 
     def launch_count(self):
         return int(lib().pq_batch_launch_count(self.ctx))
+
+    def member_dst_algo(self, k: int) -> int:
+        """DST_BUTTERFLY or DST_TENSOR: the row-DST algorithm of member k's FP32 layers."""
+        return int(lib().pq_batch_member_dst_algo(self.ctx, int(k)))
 
     def close(self):
         if self.ctx:

@@ -162,8 +162,8 @@ DstMmaArgs mma_args(const pq_ctx* c, int dir) {
 int set_dst_algo(pq_ctx* c, int algo) {
     if (algo != PQ_DST_BUTTERFLY && algo != PQ_DST_TENSOR) return fail(c, PQ_ERR_ARG, "dst_algo is 1 or 2");
     if (algo == PQ_DST_TENSOR) {
-        if (!c->mixed || c->leapfrog || c->helm_only)
-            return fail(c, PQ_ERR_UNSUPPORTED, "the tensor-core DST serves the mixed-precision CABARET form");
+        if (!c->mixed || c->leapfrog)
+            return fail(c, PQ_ERR_UNSUPPORTED, "the tensor-core DST serves the mixed-precision form");
         if (!dst_mma_supported(c->hm[0].N)) return fail(c, PQ_ERR_UNSUPPORTED, "the tensor-core DST needs ii >= 65");
         if (!c->mma_mem) {
             const size_t gbytes = align256((size_t)c->L * c->hm[0].lstride * sizeof(float));
@@ -414,7 +414,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     PivotTables pv = build_pivots(ii, jj, L, d->ss);
 
     // Arena layout.
-    const int nfields = helm_only ? 2 /*helm_io, spec*/
+    const int nfields = helm_only ? 2 /*helm_io, spec*/ + (d->precision == PQ_PREC_MIXED ? 1 /*spec64*/ : 0)
                                   : 2 /*zeta_old*/ + 2 /*zeta*/ + 1 /*psi*/ + 2 /*res*/ + 2 /*res_beta*/ +
                                         1 /*ui*/ + 1 /*uj*/ + 2 /*uimo*/ + 2 /*ujmo*/ + 2 /*zfi*/ + 2 /*zfj*/ +
                                         1 /*rel*/ + 1 /*helm_io*/ + 1 /*spec*/ + 1 /*corr*/ + 1 /*spec64*/ +
@@ -601,6 +601,7 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     if (helm_only) {
         m.helm_io = fld();
         m.spec = fld();
+        if (d->precision == PQ_PREC_MIXED) m.spec64 = (double*)fld();
     } else {
         m.zeta_old[0] = fld();
         m.zeta_old[1] = fld();

@@ -368,16 +368,18 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
     if (EPI == EPI_SPEC) {
         const double cff = 0.5 / (double)(ii - 1);
         if (PRO != PRO_STEP) {
-            const S* src = reinterpret_cast<const S*>(PRO == PRO_PLAIN ? Mb.helm_io : Mb.zeta);
+            // The stand-alone helm input (helm_io) is FP64 in either form.
+            using ST = std::conditional_t<PRO == PRO_PLAIN, double, S>;
+            const ST* src = reinterpret_cast<const ST*>(PRO == PRO_PLAIN ? Mb.helm_io : Mb.zeta);
             // Layer l of row j0 + r: FP64 into unit (l, r) (projected in place
             // below), FP32 into the staging rows; one warp per row.
-            constexpr int PER16 = 16 / sizeof(S);
+            constexpr int PER16 = 16 / sizeof(ST);
             for (int rl = warp; rl < R * L; rl += nwarp) {
                 const int r = rl / L, l = rl - r * L;
                 const int j = j0 + r;
                 const bool ok = j < jend;
-                const S* g = src + l * ls + (long long)(ok ? j : 1) * pitch;
-                S* d = MX ? reinterpret_cast<S*>(extra) + (size_t)rl * N : reinterpret_cast<S*>(ubuf(l, r));
+                const ST* g = src + l * ls + (long long)(ok ? j : 1) * pitch;
+                ST* d = MX ? reinterpret_cast<ST*>(extra) + (size_t)rl * N : reinterpret_cast<ST*>(ubuf(l, r));
                 for (int q = lane; q < N / PER16; q += 32) cp16(d + PER16 * q, g + PER16 * q, ok);
             }
             cp_commit_wait_all();
@@ -398,7 +400,7 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
                         double z[LC];
 #pragma unroll
                         for (int l = 0; l < LC; ++l)
-                            z[l] = MX ? (double)reinterpret_cast<const float*>(extra)[(size_t)(r * LC + l) * N + k]
+                            z[l] = MX ? (double)reinterpret_cast<const ST*>(extra)[(size_t)(r * LC + l) * N + k]
                                       : ubuf(l, r)[k];
 #pragma unroll
                         for (int m = 0; m < LC; ++m) {
@@ -429,7 +431,7 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
 #pragma unroll
                     for (int l = 0; l < PQ_MAXL; ++l)
                         if (l < L)
-                            z[l] = MX ? (double)reinterpret_cast<const float*>(extra)[(size_t)(r * L + l) * N + k]
+                            z[l] = MX ? (double)reinterpret_cast<const ST*>(extra)[(size_t)(r * L + l) * N + k]
                                       : ubuf(l, r)[k];
                     if constexpr (PRO == PRO_PLAIN) {
 #pragma unroll
@@ -679,17 +681,19 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
             }
         }
     } else if (EPI == EPI_HELM) {
-        // helm's in-place output (FP64 only): interior entries of interior
-        // rows, row i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1)
-        // (:1055-1057).
-        if (!MX) {
-            double* io = reinterpret_cast<double*>(Mb.helm_io) + um * ls + (long long)ju * pitch;
-            if (interior) {
+        // helm's in-place output: interior entries of interior rows, row
+        // i = ii zeroed (:758-761); ge_local zeroes psi(2:ii-1, 1)
+        // (:1055-1057).  helm_io is FP64 in either form (the mixed form's
+        // FP32 units are widened).
+        double* io = reinterpret_cast<double*>(Mb.helm_io) + um * ls + (long long)ju * pitch;
+        if (interior) {
+            if (fp64_mode(um))
                 for (int k = 1 + p; k <= n; k += P) io[k] = buf[xpad(k)];
-                if (p == 0) io[ii - 1] = 0.0;
-            } else if (ju == 0 && !Mb.periodic) {
-                for (int k = 1 + p; k <= n; k += P) io[k] = 0.0;
-            }
+            else
+                for (int k = 1 + p; k <= n; k += P) io[k] = (double)reinterpret_cast<const float*>(buf)[xpad(k)];
+            if (p == 0) io[ii - 1] = 0.0;
+        } else if (ju == 0 && !Mb.periodic) {
+            for (int k = 1 + p; k <= n; k += P) io[k] = 0.0;
         }
     } else {
         // psi_l = phi_1 - psiC_1 + sum_{m>=2} m2z(l,m) (phi_m - psiC_m corr_m)
@@ -1198,7 +1202,8 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     const size_t cbytes = (size_t)R * (L - 1) * ls.maxPitch * sizeof(double);
     const int corr_smem = (EPI == EPI_PV && !ls.periodic && bytes + cbytes <= 200 * 1024) ? 1 : 0;
     if (corr_smem) bytes += cbytes;
-    if (sizeof(S) == 4 && EPI == EPI_SPEC && PRO != PRO_STEP) bytes += (size_t)R * L * ls.maxN * sizeof(float);
+    if (sizeof(S) == 4 && EPI == EPI_SPEC && PRO != PRO_STEP)
+        bytes += (size_t)R * L * ls.maxN * (PRO == PRO_PLAIN ? sizeof(double) : sizeof(float));
     cudaError_t e =
         cudaFuncSetAttribute(k_dst<S, V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
@@ -1206,7 +1211,7 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     return launch_step_kernel(ls.pdl, k_dst<S, V, PRO, EPI>, dim3(ls.ctas_dst[dir]), dim3(threads), bytes, st,
                               ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0,
                               ls.dst_group, corr_smem, (EPI == EPI_PV) ? psic_in_inverse(ls) : 0, member_arg(ls),
-                              member_arg_used(ls), (sizeof(S) == 4 && EPI != EPI_HELM) ? ls.gemm_bc : 0);
+                              member_arg_used(ls), sizeof(S) == 4 ? ls.gemm_bc : 0);
 }
 
 template <typename S, int PRO, int EPI>
@@ -1223,7 +1228,8 @@ static cudaError_t launch_dst(const LaunchSet& ls, cudaStream_t st) {
 
 cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, int f32, cudaStream_t st) {
     switch (prologue) {
-        case PRO_PLAIN: return launch_dst<double, PRO_PLAIN, EPI_SPEC>(ls, st);
+        case PRO_PLAIN:
+            return f32 ? launch_dst<float, PRO_PLAIN, EPI_SPEC>(ls, st) : launch_dst<double, PRO_PLAIN, EPI_SPEC>(ls, st);
         case PRO_MODAL:
             return f32 ? launch_dst<float, PRO_MODAL, EPI_SPEC>(ls, st) : launch_dst<double, PRO_MODAL, EPI_SPEC>(ls, st);
         default:
@@ -1232,7 +1238,8 @@ cudaError_t launch_dst_forward(const LaunchSet& ls, int prologue, int f32, cudaS
 }
 
 cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, int f32, cudaStream_t st) {
-    if (epilogue == EPI_HELM) return launch_dst<double, PRO_PLAIN, EPI_HELM>(ls, st);
+    if (epilogue == EPI_HELM)
+        return f32 ? launch_dst<float, PRO_PLAIN, EPI_HELM>(ls, st) : launch_dst<double, PRO_PLAIN, EPI_HELM>(ls, st);
     return f32 ? launch_dst<float, PRO_PLAIN, EPI_PV>(ls, st) : launch_dst<double, PRO_PLAIN, EPI_PV>(ls, st);
 }
 

@@ -68,3 +68,31 @@ def test_batch_device_resident_resolve():
     for a, c in zip(first, second):
         assert np.array_equal(a, c)
     b.close()
+
+
+@pytest.mark.parametrize("algo", [pq.DST_BUTTERFLY, pq.DST_TENSOR, 0])
+def test_batch_mixed_precision_variants(algo):
+    """The mixed batch: each member's first layer (here ss = 0, the
+    barotropic problem) stays FP64 and matches the oracle to 1e-12; the
+    other layers are transformed in FP32 -- FP32 butterfly, tensor-core DST
+    (three-term BF16 split) or whichever the autotuner timed faster per
+    class -- and match the FP64 oracle to FP32 accuracy."""
+    shapes = [(65, 65, 3), (129, 257, 2), (257, 129, 4), (513, 513, 3), (33, 65, 2), (129, 129, 1),
+              (1025, 129, 2)]
+    rng = np.random.default_rng(8)
+    ss = [np.concatenate([[0.0], rng.uniform(0.3, 20.0, s[2] - 1)]) for s in shapes]
+    rhs = [np.asfortranarray(rng.standard_normal(s)) for s in shapes]
+    b = pq.Batch(shapes, ss, precision=pq.PREC_MIXED, dst_algo=algo)
+    out = b.helm(rhs)
+    for k, (ii, jj, L) in enumerate(shapes):
+        ref = O.Helm(ii, jj, L, list(ss[k]))(rhs[k])
+        assert rel_l2(out[k][:, :, 0], ref[:, :, 0]) <= 1e-12, (k, "fp64 layer")
+        for l in range(1, L):
+            e = rel_l2(out[k][:, :, l], ref[:, :, l])
+            assert e <= 2e-6, (k, l, e)
+        used = b.member_dst_algo(k)
+        if algo == pq.DST_TENSOR and L > 1 and ii >= 65:
+            assert used == pq.DST_TENSOR
+        elif algo == pq.DST_BUTTERFLY or L == 1 or ii < 65:
+            assert used == pq.DST_BUTTERFLY
+    b.close()
