@@ -561,6 +561,41 @@ def run_batched(a, rank, world, local_rank):
         assert rc == 0, pq.lib().pq_batch_last_error(b.ctx)
     e2e_s = (time.perf_counter() - t0) / KE
     ms, e2e_s = multirank.max_over_ranks(dist, [ms, e2e_s], device=f"cuda:{local_rank}")
+    # The mixed-precision variants of the same batch (first layer FP64, the
+    # others FP32): FP32 butterfly, tensor-core DST, and the per-class
+    # autotuner's choice; accuracy against this FP64 solve (which equals the
+    # oracle's helm to 1e-12, tests/test_gpu_batch.py).
+    ref = [b.get(k) for k in range(len(shapes))]
+    variants = {}
+    for vname, algo in (("fp32_butterfly", pq.DST_BUTTERFLY), ("bf16x3_tensor", pq.DST_TENSOR),
+                        ("mixed_autotuned", 0)):
+        bv = pq.Batch(shapes, ss, device=local_rank, precision=pq.PREC_MIXED, dst_algo=algo)
+        for k, sh in enumerate(shapes):
+            pq.lib().pq_batch_set_rhs(bv.ctx, k, dptr(rhs_of[sh]), pq.PTR_HOST)
+        for _ in range(a.warmup):
+            bv.solve_async()
+        bv.sync()
+        evv = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        sv = torch.cuda.ExternalStream(bv.stream, device=local_rank)
+        for k in range(K):
+            evv[k][0].record(sv)
+            bv.solve_async()
+            evv[k][1].record(sv)
+        bv.sync()
+        msv = float(sum(x.elapsed_time(y) for x, y in evv))
+        worst = 0.0
+        for k in range(len(shapes)):
+            o = bv.get(k)
+            for l in range(1, shapes[k][2]):
+                den = np.linalg.norm(ref[k][:, :, l])
+                if den > 0:
+                    worst = max(worst, float(np.linalg.norm(o[:, :, l] - ref[k][:, :, l]) / den))
+        ntensor = sum(1 for k in range(len(shapes)) if bv.member_dst_algo(k) == pq.DST_TENSOR)
+        msv = multirank.max_over_ranks(dist, [msv], device=f"cuda:{local_rank}")[0]
+        variants[vname] = {"value": total_units * K / (msv * 1e-3), "ms_per_step": msv / K,
+                           "max_rel_l2_fp32_layers_vs_fp64": worst, "members_on_tensor_dst": ntensor,
+                           "launches_per_solve": bv.launch_count()}
+        bv.close()
     if rank == 0:
         peak, peak_kind = peaks()
         per_solve_s = ms / K * 1e-3
@@ -600,6 +635,7 @@ def run_batched(a, rank, world, local_rank):
                     "h2d_bytes_per_step": 8 * units, "d2h_bytes_per_step": 8 * units},
             "gpu_launches": b.launch_count() * K,
             "clocks": clk.summary(),
+            "mixed_variants": variants,
         }
         print(json.dumps(line), flush=True)
     b.close()
