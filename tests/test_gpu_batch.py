@@ -89,7 +89,7 @@ def test_batch_mixed_precision_variants(algo):
         assert rel_l2(out[k][:, :, 0], ref[:, :, 0]) <= 1e-12, (k, "fp64 layer")
         for l in range(1, L):
             e = rel_l2(out[k][:, :, l], ref[:, :, l])
-            assert e <= 2e-6, (k, l, e)
+            assert e <= 1e-5, (k, l, e)
         used = b.member_dst_algo(k)
         if algo == pq.DST_TENSOR and L > 1 and ii >= 65:
             assert used == pq.DST_TENSOR
