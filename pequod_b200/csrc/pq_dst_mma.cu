@@ -24,17 +24,19 @@
 // Kernel.  A CTA computes a 128-row by NT-column tile of one parity's
 // product: rows are (mode, j) pairs of the baroclinic spectral rows, columns
 // are output wavenumbers.  Per 64-wide K block:
-//   warps 0-3   load the FP32 rows (x_m and its mirror x_{N-m}), fold,
-//               split, and write the three A terms into shared memory in the
-//               128-byte-swizzled K-major layout the MMA reads;
-//   warp 4      one thread loads the three B-term tiles (the split DST
+//   warps 0-7   load the FP32 rows (x_m and its mirror x_{N-m}; eight rows
+//               per warp in flight at once), fold, split, and write the
+//               three A terms into shared memory in the 128-byte-swizzled
+//               K-major layout the MMA reads;
+//   warp 8      one thread loads the three B-term tiles (the split DST
 //               matrix, a constant table) with TMA (cp.async.bulk.tensor);
-//   warp 5      one thread issues 4 K-steps x 6 tcgen05.mma (M 128, N NT,
+//   warp 9      one thread issues 4 K-steps x 6 tcgen05.mma (M 128, N NT,
 //               K 16, BF16 x BF16 -> FP32 in tensor memory) and commits to
 //               the stage's "empty" barrier.
-// Two stages of shared memory alternate.  After the last K block the four
-// loader warps read the accumulator out of tensor memory (tcgen05.ld),
-// stage it through shared memory and write the output rows.
+// Two stages of shared memory alternate.  After the last K block the eight
+// loader warps read the accumulator out of tensor memory (tcgen05.ld, each
+// warp its lane quarter and half the columns), stage it through shared
+// memory and write the output rows.
 //
 // Every wait is bounded: a wait that runs out sets ST_MMA_TIMEOUT in the
 // member's status word, the CTA stops issuing work, waits (bounded) for the
@@ -57,7 +59,9 @@ namespace {
 constexpr int BM = 128;        // rows per CTA (the MMA's M)
 constexpr int BK = 64;         // K elements per stage (one 128-byte swizzle row of BF16)
 constexpr int STAGES = 2;
-constexpr int NTHREADS = 192;  // 4 loader / epilogue warps, a TMA warp, an MMA warp
+constexpr int LOADERS = 8;      // loader / epilogue warps
+constexpr int NTHREADS = 32 * (LOADERS + 2);  // + a TMA warp and an MMA warp
+constexpr int RB = 8;          // rows a loader warp has in flight at once
 constexpr unsigned kSpinLimit = 1u << 22;
 
 __host__ __device__ constexpr int a_tile_bytes() { return BM * BK * 2; }           // 16 KB per term
@@ -190,15 +194,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     auto empty = [&](int s) { return smem_u32(&bars[2 * STAGES + s]); };
     const unsigned done_bar = smem_u32(&bars[3 * STAGES]);
 
+    __shared__ long long rowoff[BM];  // element offset of each tile row in x / y (-1: past the last row)
     if (threadIdx.x == 0) {
         abort_s = 0;
         for (int s = 0; s < STAGES; ++s) {
-            mbar_init(full_a(s), 128);
+            mbar_init(full_a(s), 32 * LOADERS);
             mbar_init(full_b(s), 1);
             mbar_init(empty(s), 1);
         }
         mbar_init(done_bar, 1);
         fence_mbar_init();
+    }
+    if (threadIdx.x < BM) {
+        const int row = mt * BM + threadIdx.x;
+        rowoff[threadIdx.x] =
+            row < a.rows ? (long long)(1 + row / a.nj) * a.ls + (long long)(a.jlo + row % a.nj) * a.pitch : -1;
     }
     if (warp == 0) {
         // Tensor memory: NT (>= 32, a power of two) FP32 columns x 128 lanes.
@@ -214,53 +224,52 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     const unsigned tmem = tmem_base_s;
     bool ok = true;
 
-    if (warp < 4) {
-        // ---- loader: fold, split, swizzled stores of the three A terms ----
-        const int c0 = 2 * lane;  // this lane's two columns of the K block
+    if (warp < LOADERS) {
+        // ---- loaders: fold, split, swizzled stores of the three A terms ----
+        // Warp w owns tile rows 16w .. 16w + 15, RB at a time with every load
+        // of the batch in flight together; lane l owns K-block columns l and
+        // l + 32 (coalesced reads of x_m and of the mirrored x_{N-m}).
+        constexpr int ROWS = BM / LOADERS;
         for (int kb = 0; kb < nkb && ok; ++kb) {
             const int s = kb % STAGES;
             if (kb >= STAGES) ok = mbar_wait(empty(s), ((kb / STAGES) - 1) & 1, &abort_s);
             if (!ok) break;
             unsigned char* at = smem + s * stage_bytes(NT);
-            const int m1 = kb * BK + c0 + 1;  // 1-based inputs m1, m1 + 1
-#pragma unroll 4
-            for (int rr = 0; rr < 32; ++rr) {
-                const int r = warp * 32 + rr;
-                const int row = mt * BM + r;
-                float f[2] = {0.f, 0.f};
-                if (row < a.rows) {
-                    const int mode = 1 + row / a.nj, j = a.jlo + row % a.nj;
-                    const float* x = a.x + mode * a.ls + (long long)j * a.pitch;  // x_m at x[m - 1]
+            for (int rb = 0; rb < ROWS; rb += RB) {
+                float xa[RB][2], xb[RB][2];
+#pragma unroll
+                for (int u = 0; u < RB; ++u) {
+                    const long long o = rowoff[warp * ROWS + rb + u];
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
-                        const int m = m1 + e;
-                        float v = 0.f;
-                        if (m < H) {
-                            const float xa = __ldg(x + m - 1), xb = __ldg(x + N - m - 1);
-                            v = par == 0 ? xa + xb : xa - xb;
-                        } else if (m == H && par == 0) {
-                            v = __ldg(x + m - 1);
-                        }
-                        f[e] = v;
+                        const int m = kb * BK + lane + 32 * e + 1;  // 1-based input index
+                        xa[u][e] = (o >= 0 && m <= H) ? __ldg(a.x + o + m - 1) : 0.f;
+                        xb[u][e] = (o >= 0 && m < H) ? __ldg(a.x + o + N - m - 1) : 0.f;
                     }
                 }
-                __nv_bfloat16 t[3][2];
-                split3(f[0], t[0][0], t[1][0], t[2][0]);
-                split3(f[1], t[0][1], t[1][1], t[2][1]);
-                const unsigned off = sw128(r, c0);
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    __nv_bfloat162 pr;
-                    pr.x = t[q][0];
-                    pr.y = t[q][1];
-                    *reinterpret_cast<__nv_bfloat162*>(at + q * a_tile_bytes() + off) = pr;
+                for (int u = 0; u < RB; ++u) {
+                    const int r = warp * ROWS + rb + u;
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        // u_m = x_m + x_{N-m} (u_{N/2} = x_{N/2}); v_m = x_m - x_{N-m} (v_{N/2} = 0)
+                        const int m = kb * BK + lane + 32 * e + 1;
+                        const float v = par == 0 ? xa[u][e] + xb[u][e] : (m < H ? xa[u][e] - xb[u][e] : 0.f);
+                        __nv_bfloat16 t1, t2, t3;
+                        split3(v, t1, t2, t3);
+                        const int c = lane + 32 * e;
+                        const unsigned off = (unsigned)(r * 128 + ((((c >> 3) ^ (r & 7)) & 7) << 4) + (c & 7) * 2);
+                        *reinterpret_cast<__nv_bfloat16*>(at + 0 * a_tile_bytes() + off) = t1;
+                        *reinterpret_cast<__nv_bfloat16*>(at + 1 * a_tile_bytes() + off) = t2;
+                        *reinterpret_cast<__nv_bfloat16*>(at + 2 * a_tile_bytes() + off) = t3;
+                    }
                 }
             }
             fence_async_smem();
             mbar_arrive(full_a(s));
         }
         if (!ok) abort_s = 1;
-    } else if (warp == 4) {
+    } else if (warp == LOADERS) {
         // ---- TMA producer of the B terms ----------------------------------
         if (lane == 0) {
             const int yb = par * 3 * H + n0;
@@ -320,30 +329,34 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
     // ---- epilogue: accumulator -> shared memory -> output rows -------------
     bool done_ok = true;
-    if (warp < 4) {
+    if (warp < LOADERS) {
         done_ok = mbar_wait(done_bar, 0, nullptr);
         tc_fence_after();
     }
     __syncthreads();  // every role has finished issuing; shared memory is reusable
     const bool good = done_ok && !abort_s;
-    if (warp < 4 && good) {
+    if (warp < LOADERS && good) {
+        // Warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (its lane
+        // quarter), columns [0, NT/2) for w < 4 and [NT/2, NT) above.
         float* stage = reinterpret_cast<float*>(smem);  // [128][NT + 1]
-        const int r = warp * 32 + lane;
+        const int r = (warp & 3) * 32 + lane;
+        constexpr int HALF = NT / 2 < 32 ? 32 : NT / 2;
+        const int c_begin = (warp < 4 || NT < 64) ? 0 : HALF;
+        const int c_end = NT < 64 ? (warp < 4 ? NT : 0) : c_begin + HALF;
 #pragma unroll 1
-        for (int c = 0; c < NT; c += 32) {
+        for (int c = c_begin; c < c_end; c += 32) {
             float v[32];
-            tmem_ld32(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c, v);
+            tmem_ld32(tmem + ((unsigned)((warp & 3) * 32) << 16) + (unsigned)c, v);
 #pragma unroll
             for (int q = 0; q < 32; ++q) stage[r * (NT + 1) + c + q] = v[q];
         }
         tc_fence_before();
-        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        asm volatile("bar.sync 1, %0;\n" ::"r"(32 * LOADERS) : "memory");
         // Output wavenumber k = 2q + 1 (odd) or 2q (even, q >= 1), stored at k - 1.
-        for (int rr = warp; rr < BM; rr += 4) {
-            const int row = mt * BM + rr;
-            if (row >= a.rows) break;
-            const int mode = 1 + row / a.nj, j = a.jlo + row % a.nj;
-            float* y = a.y + mode * a.ls + (long long)j * a.pitch;
+        for (int rr = warp; rr < BM; rr += LOADERS) {
+            const long long o = rowoff[rr];
+            if (o < 0) break;
+            float* y = a.y + o;
             for (int c = lane; c < NT; c += 32) {
                 const int q = n0 + c;
                 const int k = par == 0 ? 2 * q + 1 : 2 * q;
@@ -352,8 +365,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
     }
     if (!good && threadIdx.x == 0) atomicOr(a.status, (int)ST_MMA_TIMEOUT);
-    if (!done_ok && warp == 5 && lane == 0) {
-        // products may still be in flight: wait (bounded) before freeing
+    if (warp == LOADERS + 1 && lane == 0) {
+        // the products this thread issued have finished before the tensor
+        // memory is freed (immediate unless a wait ran out)
         mbar_wait(done_bar, 0, nullptr);
     }
     tc_fence_before();

@@ -903,9 +903,16 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                              "l"(g + (long long)t * pitch), "r"(nbytes)
                              : "memory");
         } else {
+            // Eight loads in flight per thread, then widened into the strip.
             const float* g = specf + go;
-#pragma unroll 4
-            for (int t = 0; t < Rq; ++t) sdst[t] = colok ? (double)g[(long long)t * pitch] : 0.0;
+            for (int t0 = 0; t0 < Rq; t0 += 8) {
+                float v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = (colok && t0 + u < Rq) ? g[(long long)(t0 + u) * pitch] : 0.f;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (t0 + u < Rq) sdst[t0 + u] = (double)v[u];
+            }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
