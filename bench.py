@@ -254,7 +254,7 @@ def bench_config(a, world):
             "parallelism": f"replicas{world}"}
 
 
-def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False, diag_every=0):
+def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False, diag_every=0, force_algo=None):
     """One run of cfg on this rank: device-timed steps (value), back-to-back
     graph replay, per-kernel event times and the e2e exchange through the C
     ABI.  Returns a dict of the measurements (max over ranks)."""
@@ -269,8 +269,13 @@ def measure_single(cfg, K, warmup, dev, dist, rank, world, seed, pdl=False, diag
     if pdl:
         m.set_tuning(pdl=1)
     # The autotuner picks the row-DST algorithm (butterfly or tensor-core
-    # DST for the mixed form's baroclinic modes) for this shape.
-    algo = m.autotune()
+    # DST for the mixed form's baroclinic modes) for this shape, unless one
+    # is forced.
+    if force_algo:
+        m.set_tuning(dst_algo=force_algo)
+        algo = force_algo
+    else:
+        algo = m.autotune()
     ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=seed, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
     m.init_perturb(ic)
     m.step(max(3, warmup))
@@ -434,6 +439,15 @@ def run_ours(a, rank, world, local_rank):
         cfg = make_config(a.size, a.layers, a.dt, precision=prec)
         res[name] = measure_single(cfg, K, a.warmup, dev, dist, rank, world, seed, pdl=a.pdl,
                                    diag_every=a.diag_every)
+    # The mixed form with the other row-DST algorithm than the autotuner's
+    # choice (the tensor-core DST when it chose the butterfly), reported
+    # beside it.
+    other = None
+    if "mixed" in res:
+        from pequod_b200 import DST_BUTTERFLY, DST_TENSOR
+        alt = DST_TENSOR if res["mixed"]["dst_algo"] == "butterfly" else DST_BUTTERFLY
+        cfg = make_config(a.size, a.layers, a.dt, precision=1)
+        other = measure_single(cfg, K, a.warmup, dev, dist, rank, world, seed, pdl=a.pdl, force_algo=alt)
     batched = {}
     if a.ensemble > 0:
         # The batched form: an ensemble of runs of the same configuration
@@ -481,6 +495,11 @@ def run_ours(a, rank, world, local_rank):
                          "note": "CUDA-graph replay, L2 not flushed"},
         "clocks": head["clocks"],
     }
+    if other is not None:
+        line["mixed_other_dst"] = {"dst_algo": other["dst_algo"], "value": other["value"],
+                                   "ms_per_step": other["ms_per_step"],
+                                   "kernel_ms": {k: v[0] / max(1, v[1]) for k, v in other["kt"].items()},
+                                   "note": "the same mixed run with the row-DST algorithm the autotuner did not pick"}
     if batched:
         line["batched"] = batched
         if "mixed" in batched and "fp64" in res:
