@@ -584,7 +584,7 @@ def run_batched(a, rank, world, local_rank):
     # others FP32): FP32 butterfly, tensor-core DST, and the per-class
     # autotuner's choice; accuracy against this FP64 solve (which equals the
     # oracle's helm to 1e-12, tests/test_gpu_batch.py).
-    ref = [b.get(k) for k in range(len(shapes))]
+    ref = [b.get(k) for k in range(len(shapes))]  # the e2e pass above solved the right-hand sides once
     variants = {}
     for vname, algo in (("fp32_butterfly", pq.DST_BUTTERFLY), ("bf16x3_tensor", pq.DST_TENSOR),
                         ("mixed_autotuned", 0)):
@@ -602,6 +602,12 @@ def run_batched(a, rank, world, local_rank):
             evv[k][1].record(sv)
         bv.sync()
         msv = float(sum(x.elapsed_time(y) for x, y in evv))
+        # helm works in place: solve the right-hand sides once more for the
+        # accuracy check (the timed solves re-solved their own outputs)
+        for k, sh in enumerate(shapes):
+            pq.lib().pq_batch_set_rhs(bv.ctx, k, dptr(rhs_of[sh]), pq.PTR_HOST)
+        bv.solve_async()
+        bv.sync()
         worst = 0.0
         for k in range(len(shapes)):
             o = bv.get(k)

@@ -10,8 +10,10 @@ g'_k = 1.5 * 2^-k cm s^-2.  The initial condition is the seeded white-noise
 vorticity smoothed by a 3-cell Gaussian (`make_ic`).
 
 `python -m pequod_b200.workloads --size 513 --steps 6` runs the
-initialisation and a few eagerly launched steps (one launch per kernel), the
-command the committed kernel profiles were taken with.
+initialisation and a few eagerly launched steps (one launch per kernel) and
+prints each kernel's event-timed microseconds, the command the committed
+kernel profiles were taken with; `--dst-algo 2` selects the tensor-core DST
+of the mixed form, `--inversions N` runs N pv_inversions instead.
 """
 from __future__ import annotations
 
@@ -110,9 +112,22 @@ def main(argv=None) -> None:
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--dst-lanes", type=int, default=0, help="lanes per row-DST unit, both directions (0: default)")
     ap.add_argument("--pdl", action="store_true", help="programmatic dependent launch of the step kernels")
+    ap.add_argument("--dst-algo", type=int, default=0,
+                    help="row-DST algorithm of the mixed form: 1 butterfly, 2 tensor-core DST (0: default)")
+    ap.add_argument("--inversions", type=int, default=0,
+                    help="instead of stepping: this many pv_inversions of a seeded random zeta")
     a = ap.parse_args(argv)
     cfg = double_gyre(a.size, a.layers, a.dt, pq.PREC_FP64 if a.precision == "fp64" else pq.PREC_MIXED)
     m = pq.Model(cfg)
+    if a.dst_algo:
+        m.set_tuning(dst_algo=a.dst_algo)
+    if a.inversions:
+        z = np.asfortranarray(np.random.default_rng(1).standard_normal((cfg.ii, cfg.jj, cfg.layers)))
+        for _ in range(a.inversions):
+            psi = m.pv_inversion(z)
+        print("pv_inversion x", a.inversions, "max |psi|", float(np.abs(psi).max()))
+        m.close()
+        return
     m.init_perturb(initial_condition(cfg))
     if a.dst_lanes:
         m.set_tuning(dst_lanes=a.dst_lanes, dst_lanes_inv=a.dst_lanes)
