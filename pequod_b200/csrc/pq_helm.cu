@@ -903,19 +903,24 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
                              "l"(g + (long long)t * pitch), "r"(nbytes)
                              : "memory");
         } else {
-            // Eight loads in flight per thread, then widened into the strip.
+            // FP32 rows: asynchronous 4-byte copies into the upper half of
+            // the chunk's slots (float t at float offset RS + t), widened in
+            // place below (double t covers floats 2t, 2t + 1 < RS + t for
+            // t < RS, so each float is read before it is overwritten).
             const float* g = specf + go;
-            for (int t0 = 0; t0 < Rq; t0 += 8) {
-                float v[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) v[u] = (colok && t0 + u < Rq) ? g[(long long)(t0 + u) * pitch] : 0.f;
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (t0 + u < Rq) sdst[t0 + u] = (double)v[u];
-            }
+            const unsigned fbase = (unsigned)__cvta_generic_to_shared(reinterpret_cast<float*>(sdst) + RS);
+            const int nbytes = colok ? 4 : 0;
+            for (int t = 0; t < Rq; ++t)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(fbase + 4u * t),
+                             "l"(g + (long long)t * pitch), "r"(nbytes)
+                             : "memory");
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        if (f32) {
+            const float* fsrc = reinterpret_cast<const float*>(sdst) + RS;
+            for (int t = 0; t < Rq; ++t) sdst[t] = (double)fsrc[t];
+        }
     }
     __syncthreads();
 
