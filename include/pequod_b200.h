@@ -513,7 +513,10 @@ PQ_API long pq_server_launches(const pq_server* s);
  * CUDA graphs, so that many small or medium runs fill the GPU.  A member's
  * results are the same as the run alone.  pq_ensemble_member gives a
  * member's context for pq_get_field / pq_energy / pq_write_checkpoint (call
- * pq_ensemble_sync first); do not step a member on its own.  The row-DST
+ * pq_ensemble_sync first); do not step a member on its own, nor change its
+ * settings (pq_set_tuning, pq_average) once the ensemble has stepped: the
+ * merged launches use the members' descriptors as they were at the first
+ * step.  The row-DST
  * algorithm (pq_ensemble_autotune / pq_ensemble_set_dst_algo, as pq_autotune
  * and pq_tuning.dst_algo) is chosen before the first step. */
 typedef struct pq_ensemble pq_ensemble;
