@@ -298,7 +298,7 @@ extern "C" {
 
 const char* pq_last_error(const pq_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-size_t pq_device_bytes(const pq_ctx* c) { return c ? c->arena_bytes : 0; }
+size_t pq_device_bytes(const pq_ctx* c) { return c ? c->arena_bytes + c->mma_bytes : 0; }
 
 void* pq_stream(pq_ctx* c) { return c ? (void*)c->stream : nullptr; }
 

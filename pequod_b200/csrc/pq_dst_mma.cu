@@ -466,12 +466,9 @@ template <int NT>
 static cudaError_t launch_nt(const DstMmaArgs& a, const CUtensorMap& map, cudaStream_t st) {
     const int H = a.N / 2;
     const size_t smem = smem_bytes(NT);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_dst_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    // per device and cheap: set on every launch, as the row-DST launches do
+    cudaError_t e = cudaFuncSetAttribute(k_dst_mma<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)((a.rows + BM - 1) / BM), (unsigned)(2 * (H / NT)));
     k_dst_mma<NT><<<grid, NTHREADS, smem, st>>>(a, map);
     return cudaGetLastError();
