@@ -102,7 +102,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const double cffbc = Mb.alpha / (Mb.alpha + 3.0);
     const bool lim = Mb.limiter != 0;
     const bool top = (l == 0), bottom = (l == L - 1);
-    double umax = 0.0;
+    T umax = 0;  // |u| is exact in T: widened once at the end
 
     auto ld = [&](int off, int row) -> double {
         if (EDGE) return (in_i && row >= 0 && row < jj) ? B[off + row * pitch] : 0.0;
@@ -116,10 +116,12 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         return (T)((double)z + s1 * (p - pm) + s2 * (p - pp));
     };
     // Limited upwind extrapolation (cabaret_extrapolator, interior branch).
+    // The upwind side only selects the inputs and the sign of the gradient
+    // term, so both directions evaluate one instance (no divergent branch).
     auto extrap = [&](T u1, T u2, T fi1, T fi2, T psi_n, T psi_o, bool pos) -> T {
         const T v0 = (u1 + u2) / (T)2;
-        const T d_f = pos ? -(psi_n - psi_o) * (T)2 - dt * v0 * (fi1 - fi2)
-                          : -(psi_n - psi_o) * (T)2 - dt * v0 * (fi2 - fi1);
+        const T dfi = pos ? fi1 - fi2 : fi2 - fi1;
+        const T d_f = -(psi_n - psi_o) * (T)2 - dt * v0 * dfi;
         T v = (T)2 * psi_n - fi2;
         if (lim) {
             const T fmx = fmax(fmax(fi1, fi2), psi_n) - d_f;
@@ -202,6 +204,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     T UIm2 = 0;            // ui row s-2 (face a = i)
     T zpb_prev = 0;
     double pm_prev = 0, pp_prev = 0, pe_prev = 0;
+    double up1_prev = shup(P2, 1);  // the lane above's psi at row j0 - 3 (P1 of the first iteration)
 
 #pragma unroll 1
     for (int r = j0; r < rend; ++r) {
@@ -295,8 +298,9 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         }
 
         // ---- corner psi and face velocities ------------------------------------
-        // pe_here: corner between nodes (i-1, i) x (s-1, s).
-        const double pe_here = 0.25 * (P2 + P1 + up1 + shup(P1, 1));
+        // pe_here: corner between nodes (i-1, i) x (s-1, s); the lane above's
+        // P1 is the previous row's up1.
+        const double pe_here = 0.25 * (P2 + P1 + up1 + up1_prev);
         const double pe_dn = shdn(pe_here, 1);
         T uj_s = 0, ujm_s = 0;  // face b = s, column i
         const bool fj_ok = !EDGE || (s >= 1 && s <= jj - 1 && i >= 1 && i <= ii - 2);
@@ -317,11 +321,13 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         const bool bfj_ok = !EDGE || (bf >= 1 && bf <= jj - 1 && i >= 1 && i <= ii - 2);
         if (bfj_ok) {
             const T u1 = UJm1;
-            if (u1 >= (T)0)
-                fjn = (!EDGE || bf > 1) ? extrap(u1, UJm2, FJm1, FJm2, ZFm2, ZOm2, true) : extrap_wall(FJm1, ZFm2, ZOm2);
+            const bool pos = u1 >= (T)0;
+            if (!EDGE)
+                fjn = extrap(u1, pos ? UJm2 : uj_s, FJm1, pos ? FJm2 : fj_s, pos ? ZFm2 : zf_1, pos ? ZOm2 : zo_1, pos);
+            else if (pos)
+                fjn = bf > 1 ? extrap(u1, UJm2, FJm1, FJm2, ZFm2, ZOm2, true) : extrap_wall(FJm1, ZFm2, ZOm2);
             else
-                fjn = (!EDGE || bf < jj - 1) ? extrap(u1, uj_s, FJm1, fj_s, zf_1, zo_1, false)
-                                              : extrap_wall(FJm1, zf_1, zo_1);
+                fjn = bf < jj - 1 ? extrap(u1, uj_s, FJm1, fj_s, zf_1, zo_1, false) : extrap_wall(FJm1, zf_1, zo_1);
         }
 
         // ---- extrapolator, i-faces on row s-1: face a = i ------------------------
@@ -331,12 +337,14 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         T fin = 0;
         if (fi_ok) {
             const T u1 = ui_1;
-            if (u1 >= (T)0)
-                fin = (!EDGE || i > 1) ? extrap(u1, ui_up, fio_1, fi_up, zf_up, zo_up, true)
-                                       : extrap_wall(fio_1, zf_up, zo_up);
+            const bool pos = u1 >= (T)0;
+            if (!EDGE)
+                fin = extrap(u1, pos ? ui_up : ui_dn, fio_1, pos ? fi_up : fi_dn, pos ? zf_up : zf_1, pos ? zo_up : zo_1,
+                             pos);
+            else if (pos)
+                fin = i > 1 ? extrap(u1, ui_up, fio_1, fi_up, zf_up, zo_up, true) : extrap_wall(fio_1, zf_up, zo_up);
             else
-                fin = (!EDGE || i < ii - 1) ? extrap(u1, ui_dn, fio_1, fi_dn, zf_1, zo_1, false)
-                                            : extrap_wall(fio_1, zf_1, zo_1);
+                fin = i < ii - 1 ? extrap(u1, ui_dn, fio_1, fi_dn, zf_1, zo_1, false) : extrap_wall(fio_1, zf_1, zo_1);
         }
         const T flj_1 = UJm1 * fjn;  // flux_j on face s-1
         const T fli_1 = ui_1 * fin;  // flux_i on row s-1, face i
@@ -372,12 +380,12 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
                 W[o_ui + s1r * pitch] = ui_1;
                 W[o_uimon + s1r * pitch] = uim_1;
                 W[o_fin + s1r * pitch] = fin;
-                umax = fmax(umax, (double)fabs(ui_1));
+                umax = fmax(umax, fabs(ui_1));
             }
             if (fj_ok && s >= j0 && s < j0 + SH) {
                 W[o_uj + s * pitch] = uj_s;
                 W[o_ujmon + s * pitch] = ujm_s;
-                umax = fmax(umax, (double)fabs(uj_s));
+                umax = fmax(umax, fabs(uj_s));
             }
             if (bfj_ok && bf >= j0 && bf < j0 + SH) W[o_fjn + bf * pitch] = fjn;
         }
@@ -397,8 +405,9 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         pm_prev = pm_s;
         pp_prev = pp_s;
         pe_prev = pe_here;
+        up1_prev = up1;
     }
-    return umax;
+    return (double)umax;
 }
 
 // Last CTA of a member: max |u| over the CTAs' partial maxima, the CFL
