@@ -382,11 +382,14 @@ PQ_API int pq_energy_noalloc(const double* psi, int ii, int jj, int layers, int 
 /* Tile parameters of the step kernels (defaults per grid size are set by
  * pq_create; results do not depend on them).
  *   cab_kernel CABARET step formulation: 0 one CTA per 28 x 16 tile and
- *              layer, 1 warp sweeps down bands of cab_band rows (default:
- *              tiles up to jj = 700, sweeps above)
- *   cab_band   output rows per warp of the sweep formulation, 4..128
- *              (default: 8, 32, 35 or 56 for up to 300, 700, 1500 rows
- *              and above)
+ *              layer; 1 warp sweeps down bands of cab_band rows of a
+ *              32-column strip, claimed from a queue by resident warps;
+ *              2 the same with two columns per lane (64-column strips; the
+ *              mixed form only).  Default: tiles up to jj = 700, then
+ *              sweeps; two-column sweeps in the mixed form above jj = 1500
+ *   cab_band   output rows per sweep, 4..128 (default: 8 up to 300 rows,
+ *              32 up to 700, then 24 (FP64) or 16 (mixed) up to 1500, and
+ *              40 (FP64) or 24 (mixed) above)
  *   dst_group  row groups per DST CTA: a CTA holds dst_group * layers
  *              warps (0: automatic, 1); layers * dst_group <= 8
  *   dst_lanes, dst_lanes_inv  lanes per (row, mode) unit of the forward

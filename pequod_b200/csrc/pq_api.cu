@@ -382,19 +382,20 @@ int pq::create_ctx(pq_ctx** out, const pq_model_desc* d, int device, bool helm_o
     const size_t lstride = (size_t)c->pitch * jj;
     c->field_bytes = lstride * L * sizeof(double);
     const int ntiles_tri = tri_ctas(n, jj, L);
-    // Default CABARET band height by grid size (measured on B200: shorter
-    // bands give small grids enough warps, taller ones cut halo rows on big
-    // ones; swept 32..128 at 1025 x 1025 x 3 (best 35) and 2049 x 2049 x 5
-    // (best 56)).
-    const int cab_sh = jj <= 300 ? 8 : jj <= 700 ? 32 : jj <= 1500 ? 35 : 56;
-    // CABARET formulation by grid size (measured on B200): tiles up to
-    // 700 rows, warp sweeps above (pq_tuning.cab_kernel overrides).
-    const int cab_kernel = jj <= 700 ? 0 : 1;
+    // CABARET formulation and band height by grid size (measured on B200,
+    // pq_tuning overrides): tiles up to 700 rows; above, persistent warp
+    // sweeps, two columns per lane in the mixed form beyond 1500 rows.  Bands
+    // (swept 8..48): short ones keep the end of the sweep queue short, tall
+    // ones cut halo rows -- 1025 x 1025 x 3: 24 (FP64), 16 (mixed);
+    // 2049 x 2049 x 5: 40 (FP64), 24 (mixed, two columns).
+    const bool mixed = d->precision == PQ_PREC_MIXED;
+    const int cab_kernel = jj <= 700 ? 0 : (mixed && jj > 1500) ? 2 : 1;
+    const int cab_sh = jj <= 300 ? 8 : jj <= 700 ? 32 : jj <= 1500 ? (mixed ? 16 : 24) : (mixed ? 24 : 40);
     const int ntiles_cab = d->periodic_j ? channel_ctas(ii, jj)
                            : cab_kernel == 0 ? cabaret_tile_ctas(ii, jj, L)
-                                             : cabaret_ctas(ii, jj, L, cab_sh);
+                                             : cabaret_ctas(ii, jj, L, cab_sh, cab_kernel, mixed);
     const int ntiles_cab_max =
-        std::max({cabaret_ctas(ii, jj, L, kMinBand), cabaret_tile_ctas(ii, jj, L), channel_ctas(ii, jj)});
+        std::max({cabaret_ctas_bound(ii, jj, L, kMinBand), cabaret_tile_ctas(ii, jj, L), channel_ctas(ii, jj)});
 
     // Tables.
     std::vector<double2> tw(M), wsplit(M);
@@ -1119,7 +1120,9 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     if (t->cab_band < kMinBand || t->cab_band > kMaxBand) return fail(c, PQ_ERR_ARG, "cab_band out of range");
     CK(cudaStreamSynchronize(c->stream));
     if (t->dst_group < 0 || c->L * t->dst_group > 8) return fail(c, PQ_ERR_ARG, "dst_group out of range");
-    if (t->cab_kernel < 0 || t->cab_kernel > 1) return fail(c, PQ_ERR_ARG, "cab_kernel out of range");
+    if (t->cab_kernel < 0 || t->cab_kernel > 2) return fail(c, PQ_ERR_ARG, "cab_kernel out of range");
+    if (t->cab_kernel == 2 && !c->mixed)
+        return fail(c, PQ_ERR_ARG, "cab_kernel 2 (two columns per lane) needs the mixed form's FP32 fields");
     if (t->pdl < 0 || t->pdl > 1) return fail(c, PQ_ERR_ARG, "pdl is 0 or 1");
     if (t->dst_algo < 0 || t->dst_algo > PQ_DST_TENSOR) return fail(c, PQ_ERR_ARG, "dst_algo is 0, 1 or 2");
     if (t->dst_algo) {
@@ -1140,7 +1143,7 @@ int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     for (int p = 0; p < 2; ++p) {
         c->hm[p].cab_sh = t->cab_band;
         c->hm[p].ntiles_cab = c->periodic   ? channel_ctas(c->ii, c->jj)
-                              : t->cab_kernel ? cabaret_ctas(c->ii, c->jj, c->L, t->cab_band)
+                              : t->cab_kernel ? cabaret_ctas(c->ii, c->jj, c->L, t->cab_band, t->cab_kernel, c->mixed)
                                               : cabaret_tile_ctas(c->ii, c->jj, c->L);
         c->ls[p].cab_kernel = t->cab_kernel;
         c->ls[p].ctas_cab = c->hm[p].ntiles_cab;

@@ -12,51 +12,154 @@
 // writing back only the fields the next step needs.  Halo values are
 // recomputed, never exchanged.  Fields read at nodes or faces owned by another
 // warp (zeta_old, uimo, ujmo, zeta_fi, zeta_fj) are ping-ponged.
+#include <algorithm>
+
 #include "pq_common.cuh"
 #include "pq_kernels.h"
 
 namespace pq {
 
-// Sweep decomposition: a warp owns one layer of a strip of 32 columns
-// (CAB_SW = 28 output columns plus 2 halo lanes on each side) and marches down
-// a band of Mb.cab_sh output rows (a tuning parameter).  Every per-lane quantity lives in registers as
-// a rolling window over rows; the i-neighbours come from warp shuffles.  At
-// iteration r (s = r - 2) the warp loads psi row s+2 and the inputs of rows
-// s, s-1, and produces
+// Sweep decomposition: a warp owns one layer of a strip of 32 NC columns --
+// NC consecutive columns per lane, cab_sw(NC) = 32 NC - 4 output columns plus
+// 2 halo columns on each side -- and marches down a band of Mb.cab_sh output
+// rows (a tuning parameter).  Every per-lane quantity lives in registers as
+// a rolling window over rows; the i-neighbours come from the lane's own
+// columns or, across a lane boundary, from warp shuffles.  At iteration r
+// (s = r - 2) the warp loads psi row s+2 and the inputs of rows s, s-1, and
+// produces
 //   rel(s), zeta after BC/forcing at row s-1, uj on face row s, ui on row s-1,
 //   zeta_fj on face row s-1, zeta_fi on row s-1, and res / zeta_old at row s-2,
 // so output row o is final at iteration o + 4.
+// NC = 2 (FP32 fields only, pq_tuning.cab_kernel = 2): each row access of a
+// field is one 8-byte vector per lane (16 bytes for psi) and one shuffle
+// serves two columns, 26 % fewer instructions per node than NC = 1; it needs
+// more registers (two CTAs per SM instead of three), so it pays on large
+// grids (2049^2 x 5) and not at 1025^2.
 constexpr int CAB_WARPS = 4;
-constexpr int CAB_SW = 28;  // output columns per warp
-constexpr int CAB_D = 4;    // depth of the per-warp cp.async row pipeline
+constexpr int CAB_D = 4;  // depth of the per-warp cp.async row pipeline
 // Streamed inputs of one iteration (rows relative to s = r - 2).
 enum { F_PSI2 = 0, F_ZPB, F_PSIM, F_PSIP, F_ZO, F_UIMO, F_UJMO, F_FIO, F_FJ, F_WIND, F_RB, CAB_NF };
-constexpr int CAB_RING = CAB_D * CAB_NF * 32;  // doubles per warp
+__host__ __device__ constexpr int cab_sw(int nc) { return 32 * nc - 4; }  // output columns per warp
+// Ring stage layout: each field a slot of the warp's 32 NC values at their
+// own width (FP64 for psi and the wind, T for the rest), in enum order.
+__host__ __device__ constexpr bool cab_f64_field(int f) {
+    return f == F_PSI2 || f == F_PSIM || f == F_PSIP || f == F_WIND;
+}
+template <typename T, int NC>
+__host__ __device__ constexpr int cab_slot(int f) {  // offset of field f in a stage, in doubles
+    int o = 0;
+    for (int k = 0; k < f; ++k) o += cab_f64_field(k) ? 32 * NC : 32 * NC * (int)sizeof(T) / 8;
+    return o;
+}
+template <typename T, int NC>
+__host__ __device__ constexpr int cab_ring() {  // doubles per warp
+    return CAB_D * cab_slot<T, NC>(CAB_NF);
+}
 
 __device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ float shup(float v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 __device__ __forceinline__ float shdn(float v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
 
+// Neighbours of a lane's NC columns: o[c] = v at column (c - 1), (c + 1),
+// (c - 2), (c + 2) of the lane's frame.  Every lane must call them (shuffles).
+template <int NC, typename V>
+__device__ __forceinline__ void col_up(const V (&v)[NC], V (&o)[NC]) {
+    const V t = shup(v[NC - 1], 1);
+#pragma unroll
+    for (int c = NC - 1; c > 0; --c) o[c] = v[c - 1];
+    o[0] = t;
+}
+template <int NC, typename V>
+__device__ __forceinline__ void col_dn(const V (&v)[NC], V (&o)[NC]) {
+    const V t = shdn(v[0], 1);
+#pragma unroll
+    for (int c = 0; c < NC - 1; ++c) o[c] = v[c + 1];
+    o[NC - 1] = t;
+}
+template <int NC, typename V>
+__device__ __forceinline__ void col_up2(const V (&v)[NC], V (&o)[NC]) {
+    if constexpr (NC == 1) {
+        o[0] = shup(v[0], 2);
+    } else {
+        const V t0 = shup(v[NC - 2], 1), t1 = shup(v[NC - 1], 1);
+#pragma unroll
+        for (int c = NC - 1; c > 1; --c) o[c] = v[c - 2];
+        o[0] = t0;
+        o[1] = t1;
+    }
+}
+template <int NC, typename V>
+__device__ __forceinline__ void col_dn2(const V (&v)[NC], V (&o)[NC]) {
+    if constexpr (NC == 1) {
+        o[0] = shdn(v[0], 2);
+    } else {
+        const V t0 = shdn(v[0], 1), t1 = shdn(v[1], 1);
+#pragma unroll
+        for (int c = 0; c < NC - 2; ++c) o[c] = v[c + 2];
+        o[NC - 2] = t0;
+        o[NC - 1] = t1;
+    }
+}
+// NC consecutive values: one vector access (shared or global memory).
+template <int NC, typename V>
+__device__ __forceinline__ void vld(const V* p, V (&v)[NC]) {
+    if constexpr (NC == 1) {
+        v[0] = p[0];
+    } else if constexpr (sizeof(V) == 8) {
+        const double2 t = *reinterpret_cast<const double2*>(p);
+        v[0] = t.x;
+        v[1] = t.y;
+    } else {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        v[0] = t.x;
+        v[1] = t.y;
+    }
+}
+template <int NC, typename V>
+__device__ __forceinline__ void vst(V* p, const V (&v)[NC]) {
+    if constexpr (NC == 1) {
+        p[0] = v[0];
+    } else if constexpr (sizeof(V) == 8) {
+        *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    } else {
+        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    }
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async_ca(unsigned dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src), "n"(BYTES), "r"(src_bytes)
+                 : "memory");
+}
+
 // One warp's sweep over layer l of the strip starting at column i0 and the
 // band starting at row j0.  EDGE = false is the specialisation for warps
-// whose whole footprint (columns i0-2 .. i0+29, rows j0-4 .. j0+sh+3) lies
-// at least two nodes inside the domain: no bounds checks, no boundary
-// branches.  PRED = true also applies the next step's cabaret_predictor and
-// cabaret_beta (fixed dt) to every interior node it finishes, writing the
-// next step's inversion input zeta_next and res_beta_other.  T is the type
-// of the CABARET fields (double, or float in the mixed form); psi is FP64
-// and everything computed from psi differences (the rel coupling, the
-// boundary rel, the corner streamfunction and the face velocities before
-// the time weighting) is evaluated in FP64.  Returns the largest |u| of the
-// faces it wrote.
-template <bool EDGE, bool PRED, typename T>
+// whose whole footprint (columns i0-2 .. i0+32NC-3, rows j0-4 .. j0+sh+3)
+// lies at least two nodes inside the domain: no bounds checks, no boundary
+// branches, vector loads and stores.  PRED = true also applies the next
+// step's cabaret_predictor and cabaret_beta (fixed dt) to every interior
+// node it finishes, writing the next step's inversion input zeta_next and
+// res_beta_other.  T is the type of the CABARET fields (double, or float in
+// the mixed form); psi is FP64 and everything computed from psi differences
+// (the rel coupling, the boundary rel, the corner streamfunction and the face
+// velocities before the time weighting) is evaluated in FP64.  Returns the
+// largest |u| of the faces it wrote.
+template <bool EDGE, bool PRED, typename T, int NC>
 __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int j0, int lane, double* ring) {
+    static_assert(NC == 1 || NC == 2, "one or two columns per lane");
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L, pitch = Mb.pitch;
     const long long ls = Mb.lstride;
-    const int i = i0 - 2 + lane;
-    const bool in_i = !EDGE || (i >= 0 && i < ii);
-    const bool out_i = (lane >= 2 && lane < 2 + CAB_SW && in_i);  // owner of node / i-face / j-face column i
+    const int ib = i0 - 2 + NC * lane;  // the lane's first column
+    int ic[NC];
+    bool in_i[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        ic[c] = ib + c;
+        in_i[c] = !EDGE || (ic[c] >= 0 && ic[c] < ii);
+    }
+    constexpr int HL = 2 / NC;  // halo lanes on each side
+    // Owner lanes of their columns' nodes, i-faces (a = i) and j-faces.
+    const bool out_lane = lane >= HL && lane < 32 - HL;
     const int cur = Mb.cur, nxt = cur ^ 1;
     const double dt64 = Mb.sc->dt;
     const T dt = (T)dt64, tu = (T)Mb.sc->tweight_u;
@@ -66,12 +169,15 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const int SH = Mb.cab_sh;
     // All fields of a member live in one allocation: address them by 32-bit
     // element offsets from one base (fewer live registers than 16 pointers);
-    // FP64 fields (psi, wind) from B, T fields from BT.
+    // FP64 fields (psi, wind) from B, T fields from BT.  Every field starts
+    // on a 256-byte boundary and rows are a multiple of 32 values apart, so
+    // the lane's NC values (from an even column when NC = 2) are aligned for
+    // one vector access.
     const double* B = Mb.psi;
     const T* BT = reinterpret_cast<const T*>(B);
     auto ofs = [&](const void* f) { return (int)(reinterpret_cast<const double*>(f) - B); };
     auto ofst = [&](const void* f) { return (int)(reinterpret_cast<const T*>(f) - BT); };
-    const int lo = (int)(l * ls) + i;  // layer and column part of every offset
+    const int lo = (int)(l * ls) + ib;  // layer and column part of every offset
     const int o_psil = lo;
     const int o_psim = (l > 0) ? lo - (int)ls : lo;
     const int o_psip = (l < L - 1) ? lo + (int)ls : lo;
@@ -94,7 +200,7 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const int o_zpn = PRED ? ofst(Mb.zeta_next) + lo : 0;
     const T ta = (T)Mb.sc->tweight_a, beta_l = (T)Mb.beta[l];
     const bool has_wind = (l == 0 && Mb.wind);
-    const int o_wind = has_wind ? ofs(Mb.wind) + i : 0;
+    const int o_wind = has_wind ? ofs(Mb.wind) + ib : 0;
     T* W = const_cast<T*>(BT);
     const T nu = (T)Mb.viscosity, vb = (T)Mb.visc_bot;
     const double s1 = Mb.s1[l], s2 = Mb.s2[l];
@@ -104,9 +210,9 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
     const bool top = (l == 0), bottom = (l == L - 1);
     T umax = 0;  // |u| is exact in T: widened once at the end
 
-    auto ld = [&](int off, int row) -> double {
-        if (EDGE) return (in_i && row >= 0 && row < jj) ? B[off + row * pitch] : 0.0;
-        return B[off + row * pitch];
+    auto ld = [&](int off, int row, int c) -> double {
+        if (EDGE) return (in_i[c] && row >= 0 && row < jj) ? B[off + c + row * pitch] : 0.0;
+        return B[off + c + row * pitch];
     };
     // rel_from_zeta_and_psi coupling for an interior node.
     auto rel_int = [&](T z, double p, double pm, double pp) -> T {
@@ -145,67 +251,93 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         return v;
     };
 
-    // Rolling windows.
-    // Row copies of iteration r into ring stage r % CAB_D (cp.async per lane;
-    // rows outside the domain, and zeta at non-interior nodes, are
-    // zero-filled by a source size of 0 with the source clamped in range).
-    // Every field has a slot of 32 doubles per stage; T fields use its start.
-    const int rend = j0 + SH + 4;
-    auto cp64 = [&](double* slot, int off, int row, bool ok) {
-        const int rr = ok ? row : 0;
-        const unsigned sa = (unsigned)__cvta_generic_to_shared(slot + lane);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(B + (off + rr * pitch)),
-                     "r"(ok ? 8 : 0)
-                     : "memory");
+    // Row copies of iteration r into ring stage r % CAB_D: per field one
+    // cp.async of the lane's NC values (interior warps), or one per value
+    // (edge warps: values outside the domain, and zeta at non-interior nodes,
+    // are zero-filled by a source size of 0, the source then the field base).
+    // Slots: cab_slot (each field at its own width).
+    constexpr int STAGE = cab_slot<T, NC>(CAB_NF);
+    constexpr int S_PSI2 = cab_slot<T, NC>(F_PSI2), S_ZPB = cab_slot<T, NC>(F_ZPB), S_PSIM = cab_slot<T, NC>(F_PSIM),
+                  S_PSIP = cab_slot<T, NC>(F_PSIP), S_ZO = cab_slot<T, NC>(F_ZO), S_UIMO = cab_slot<T, NC>(F_UIMO),
+                  S_UJMO = cab_slot<T, NC>(F_UJMO), S_FIO = cab_slot<T, NC>(F_FIO), S_FJ = cab_slot<T, NC>(F_FJ),
+                  S_WIND = cab_slot<T, NC>(F_WIND), S_RB = cab_slot<T, NC>(F_RB);
+    auto cp64 = [&](double* slot, int off, int row) {
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(slot + NC * lane);
+        if (!EDGE) {
+            cp_async_ca<8 * NC>(sa, B + (off + row * pitch), 8 * NC);
+        } else {
+            const bool rok = row >= 0 && row < jj;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const bool ok = rok && in_i[c];
+                cp_async_ca<8>(sa + 8u * c, ok ? B + (off + c + row * pitch) : B, ok ? 8 : 0);
+            }
+        }
     };
-    auto cpt = [&](double* slot, int off, int row, bool ok) {
-        const int rr = ok ? row : 0;
-        const unsigned sa = (unsigned)__cvta_generic_to_shared(reinterpret_cast<T*>(slot) + lane);
-        if (sizeof(T) == 8)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(BT + (off + rr * pitch)),
-                         "r"(ok ? 8 : 0)
-                         : "memory");
-        else
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(BT + (off + rr * pitch)),
-                         "r"(ok ? 4 : 0)
-                         : "memory");
+    auto cpt = [&](double* slot, int off, int row, bool node_int) {
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(reinterpret_cast<T*>(slot) + NC * lane);
+        if (!EDGE) {
+            cp_async_ca<(int)sizeof(T) * NC>(sa, BT + (off + row * pitch), (int)sizeof(T) * NC);
+        } else {
+            const bool rok = node_int ? (row > 0 && row < jj - 1) : (row >= 0 && row < jj);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const bool ok = rok && (node_int ? (ic[c] > 0 && ic[c] < ii - 1) : in_i[c]);
+                cp_async_ca<(int)sizeof(T)>(sa + (unsigned)sizeof(T) * c, ok ? BT + (off + c + row * pitch) : BT,
+                                            ok ? (int)sizeof(T) : 0);
+            }
+        }
     };
-    auto rowok = [&](int row) { return !EDGE || (in_i && row >= 0 && row < jj); };
     auto issue = [&](int rr) {
         const int ss = rr - 2;
-        double* d = ring + ((rr % CAB_D) * CAB_NF << 5);
-        cp64(d + (F_PSI2 << 5), o_psil, ss + 2, rowok(ss + 2));
-        const bool intn = !EDGE || (in_i && i > 0 && i < ii - 1 && ss > 0 && ss < jj - 1);
-        cpt(d + (F_ZPB << 5), o_zpb, ss, intn);
+        double* d = ring + (rr % CAB_D) * STAGE;
+        cp64(d + S_PSI2, o_psil, ss + 2);
+        cpt(d + S_ZPB, o_zpb, ss, true);
         if (L > 1) {
-            cp64(d + (F_PSIM << 5), o_psim, ss, rowok(ss));
-            cp64(d + (F_PSIP << 5), o_psip, ss, rowok(ss));
+            cp64(d + S_PSIM, o_psim, ss);
+            cp64(d + S_PSIP, o_psip, ss);
         }
-        cpt(d + (F_ZO << 5), o_zo, ss - 1, rowok(ss - 1));
-        cpt(d + (F_UIMO << 5), o_uimo, ss - 1, rowok(ss - 1));
-        cpt(d + (F_UJMO << 5), o_ujmo, ss, rowok(ss));
-        cpt(d + (F_FIO << 5), o_fio, ss - 1, rowok(ss - 1));
-        cpt(d + (F_FJ << 5), o_fjo, ss, rowok(ss));
-        if (has_wind) cp64(d + (F_WIND << 5), o_wind, ss - 1, rowok(ss - 1));
-        if (PRED) cpt(d + (F_RB << 5), o_rb, ss - 2, rowok(ss - 2));
+        cpt(d + S_ZO, o_zo, ss - 1, false);
+        cpt(d + S_UIMO, o_uimo, ss - 1, false);
+        cpt(d + S_UJMO, o_ujmo, ss, false);
+        cpt(d + S_FIO, o_fio, ss - 1, false);
+        cpt(d + S_FJ, o_fjo, ss, false);
+        if (has_wind) cp64(d + S_WIND, o_wind, ss - 1);
+        if (PRED) cpt(d + S_RB, o_rb, ss - 2, false);
     };
     for (int rr = j0; rr < j0 + CAB_D - 1; ++rr) {
         issue(rr);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    double P0 = 0, P1 = ld(o_psil, j0 - 4), P2 = ld(o_psil, j0 - 3), P3 = ld(o_psil, j0 - 2), P4 = ld(o_psil, j0 - 1);
-    T Rm2 = 0, Rm1 = 0;    // rel rows s-2, s-1
-    T ZFm2 = 0;            // zeta after forcing, row s-2
-    T ZOm2 = 0;            // zeta_old row s-2
-    T UJm2 = 0, UJm1 = 0;  // uj faces s-2, s-1
-    T FJm2 = 0, FJm1 = 0;  // zeta_fj (old) faces s-2, s-1
-    T FLJm2 = 0;           // flux_j face s-2
-    T FLI = 0;             // flux_i row s-2 (face a = i)
-    T UIm2 = 0;            // ui row s-2 (face a = i)
-    T zpb_prev = 0;
-    double pm_prev = 0, pp_prev = 0, pe_prev = 0;
-    double up1_prev = shup(P2, 1);  // the lane above's psi at row j0 - 3 (P1 of the first iteration)
+    // Rolling windows.
+    double P0[NC], P1[NC], P2[NC], P3[NC], P4[NC];
+    T Rm2[NC], Rm1[NC];    // rel rows s-2, s-1
+    T ZFm2[NC];            // zeta after forcing, row s-2
+    T ZOm2[NC];            // zeta_old row s-2
+    T UJm2[NC], UJm1[NC];  // uj faces s-2, s-1
+    T FJm2[NC], FJm1[NC];  // zeta_fj (old) faces s-2, s-1
+    T FLJm2[NC];           // flux_j face s-2
+    T FLI[NC];             // flux_i row s-2 (face a = i)
+    T UIm2[NC];            // ui row s-2 (face a = i)
+    T zpb_prev[NC];
+    double pm_prev[NC], pp_prev[NC], pe_prev[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        P0[c] = 0;
+        P1[c] = ld(o_psil, j0 - 4, c);
+        P2[c] = ld(o_psil, j0 - 3, c);
+        P3[c] = ld(o_psil, j0 - 2, c);
+        P4[c] = ld(o_psil, j0 - 1, c);
+        Rm2[c] = Rm1[c] = ZFm2[c] = ZOm2[c] = UJm2[c] = UJm1[c] = FJm2[c] = FJm1[c] = FLJm2[c] = FLI[c] = UIm2[c] =
+            zpb_prev[c] = 0;
+        pm_prev[c] = pp_prev[c] = pe_prev[c] = 0;
+    }
+    // The left neighbour of P1 (psi row s-1) is, for the lane's first column,
+    // the previous row's left neighbour of P2 (carried over, so the corner
+    // needs no second shuffle), for the others the lane's own column.
+    double up1_prev0 = shup(P2[NC - 1], 1);
 
+    const int rend = j0 + SH + 4;
 #pragma unroll 1
     for (int r = j0; r < rend; ++r) {
         const int s = r - 2;
@@ -214,198 +346,319 @@ __device__ __forceinline__ double cab_sweep(const Member& Mb, int l, int i0, int
         if (r + CAB_D - 1 < rend) issue(r + CAB_D - 1);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group %0;\n" ::"n"(CAB_D - 1) : "memory");
-        const double* st = ring + ((r % CAB_D) * CAB_NF << 5);
-        auto get64 = [&](int f) { return st[(f << 5) + lane]; };
-        auto gett = [&](int f) { return reinterpret_cast<const T*>(st + (f << 5))[lane]; };
-        P0 = P1;
-        P1 = P2;
-        P2 = P3;
-        P3 = P4;
-        P4 = get64(F_PSI2);
-        const bool node_s = !EDGE || (in_i && s >= 0 && s < jj);
-        const T zpb_s = gett(F_ZPB);
-        const double pm_s = (L > 1) ? get64(F_PSIM) : 0.0;
-        const double pp_s = (L > 1) ? get64(F_PSIP) : 0.0;
-        const T zo_1 = gett(F_ZO);
-        const T uimo_1 = gett(F_UIMO);
-        const T ujmo_s = gett(F_UJMO);
-        const T fio_1 = gett(F_FIO);
-        const T fj_s = gett(F_FJ);
-        const T w_1 = has_wind ? (T)get64(F_WIND) : (T)0;
-        const T rb_2 = PRED ? gett(F_RB) : (T)0;
+        const double* st = ring + (r % CAB_D) * STAGE;
+        auto get64 = [&](int so, double(&v)[NC]) { vld<NC>(st + so + NC * lane, v); };
+        auto gett = [&](int so, T(&v)[NC]) { vld<NC>(reinterpret_cast<const T*>(st + so) + NC * lane, v); };
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            P0[c] = P1[c];
+            P1[c] = P2[c];
+            P2[c] = P3[c];
+            P3[c] = P4[c];
+        }
+        get64(S_PSI2, P4);
+        T zpb_s[NC], zo_1[NC], uimo_1[NC], ujmo_s[NC], fio_1[NC], fj_s[NC], w_1[NC], rb_2[NC];
+        double pm_s[NC], pp_s[NC];
+        gett(S_ZPB, zpb_s);
+        if (L > 1) {
+            get64(S_PSIM, pm_s);
+            get64(S_PSIP, pp_s);
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) pm_s[c] = pp_s[c] = 0.0;
+        }
+        gett(S_ZO, zo_1);
+        gett(S_UIMO, uimo_1);
+        gett(S_UJMO, ujmo_s);
+        gett(S_FIO, fio_1);
+        gett(S_FJ, fj_s);
+        if (has_wind) {
+            double w[NC];
+            get64(S_WIND, w);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) w_1[c] = (T)w[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) w_1[c] = (T)0;
+        }
+        if (PRED) {
+            gett(S_RB, rb_2);
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) rb_2[c] = (T)0;
+        }
 
         // ---- rel(s): rel_from_zeta_and_psi + apply_rel_bc -------------------
-        double up1 = 0.0, up2 = 0.0, dn1 = 0.0, dn2 = 0.0;
+        double up1[NC], up2[NC], dn1[NC], dn2[NC];
+        col_up(P2, up1);
         if (EDGE) {
-            up1 = shup(P2, 1);
-            up2 = shup(P2, 2);
-            dn1 = shdn(P2, 1);
-            dn2 = shdn(P2, 2);
-        } else {
-            up1 = shup(P2, 1);
+            col_up2(P2, up2);
+            col_dn(P2, dn1);
+            col_dn2(P2, dn2);
         }
-        T rel_s = 0;
-        if (!EDGE) {
-            rel_s = rel_int(zpb_s, P2, pm_s, pp_s);
-        } else if (node_s) {
-            const bool bj = (s == 0 || s == jj - 1), bi = (i == 0 || i == ii - 1);
-            if (bj || bi) {
-                if (bc != 3) {
-                    double q1, q2;
-                    if (bj) {
-                        q1 = (s == 0) ? P3 : P1;
-                        q2 = (s == 0) ? P4 : P0;
-                    } else {
-                        q1 = (i == 0) ? dn1 : up1;
-                        q2 = (i == 0) ? dn2 : up2;
+        T rel_s[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            rel_s[c] = 0;
+            if (!EDGE) {
+                rel_s[c] = rel_int(zpb_s[c], P2[c], pm_s[c], pp_s[c]);
+            } else if (in_i[c] && s >= 0 && s < jj) {
+                const int i = ic[c];
+                const bool bj = (s == 0 || s == jj - 1), bi = (i == 0 || i == ii - 1);
+                if (bj || bi) {
+                    if (bc != 3) {
+                        double q1, q2;
+                        if (bj) {
+                            q1 = (s == 0) ? P3[c] : P1[c];
+                            q2 = (s == 0) ? P4[c] : P0[c];
+                        } else {
+                            q1 = (i == 0) ? dn1[c] : up1[c];
+                            q2 = (i == 0) ? dn2[c] : up2[c];
+                        }
+                        rel_s[c] = (T)((bc == 1) ? cffbc * (-3.5 * P2[c] + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - P2[c]));
                     }
-                    rel_s = (T)((bc == 1) ? cffbc * (-3.5 * P2 + 4.0 * q1 - 0.5 * q2) : 2.0 * (q1 - P2));
+                } else {
+                    rel_s[c] = rel_int(zpb_s[c], P2[c], pm_s[c], pp_s[c]);
                 }
-            } else {
-                rel_s = rel_int(zpb_s, P2, pm_s, pp_s);
             }
         }
 
         // ---- zeta at row s-1 after update_zeta_bc and cabaret_forcing -------
         const int s1r = s - 1;
-        const T rl_up = shup(Rm1, 1), rl_dn = shdn(Rm1, 1);
-        T zf_1 = 0;
-        const bool node_1 = !EDGE || (in_i && s1r >= 0 && s1r < jj);
-        if (node_1) {
-            const bool bnd = EDGE && (s1r == 0 || s1r == jj - 1 || i == 0 || i == ii - 1);
-            if (bnd) {
-                if (L == 1)
-                    zf_1 = Rm1;
-                else if (top)
-                    zf_1 = (T)((double)Rm1 - s2 * (P1 - pp_prev));
-                else if (bottom)
-                    zf_1 = (T)((double)Rm1 - s1 * (P1 - pm_prev));
-                else
-                    zf_1 = (T)((double)Rm1 - s1 * (P1 - pm_prev) - s2 * (P1 - pp_prev));
-            } else {
-                const T lap = (T)-4 * Rm1 + rl_up + rl_dn + Rm2 + rel_s;
-                T rv;
-                if (L == 1)
-                    rv = dt * (w_1 - vb * Rm1 + nu * lap);
-                else if (top)
-                    rv = dt * (w_1 + nu * lap);
-                else if (bottom)
-                    rv = dt * (-vb * Rm1 + nu * lap);
-                else
-                    rv = dt * nu * lap;
-                zf_1 = zpb_prev + rv;
+        T rl_up[NC], rl_dn[NC];
+        col_up(Rm1, rl_up);
+        col_dn(Rm1, rl_dn);
+        T zf_1[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            zf_1[c] = 0;
+            const int i = ic[c];
+            if (!EDGE || (in_i[c] && s1r >= 0 && s1r < jj)) {
+                const bool bnd = EDGE && (s1r == 0 || s1r == jj - 1 || i == 0 || i == ii - 1);
+                if (bnd) {
+                    if (L == 1)
+                        zf_1[c] = Rm1[c];
+                    else if (top)
+                        zf_1[c] = (T)((double)Rm1[c] - s2 * (P1[c] - pp_prev[c]));
+                    else if (bottom)
+                        zf_1[c] = (T)((double)Rm1[c] - s1 * (P1[c] - pm_prev[c]));
+                    else
+                        zf_1[c] = (T)((double)Rm1[c] - s1 * (P1[c] - pm_prev[c]) - s2 * (P1[c] - pp_prev[c]));
+                } else {
+                    const T lap = (T)-4 * Rm1[c] + rl_up[c] + rl_dn[c] + Rm2[c] + rel_s[c];
+                    T rv;
+                    if (L == 1)
+                        rv = dt * (w_1[c] - vb * Rm1[c] + nu * lap);
+                    else if (top)
+                        rv = dt * (w_1[c] + nu * lap);
+                    else if (bottom)
+                        rv = dt * (-vb * Rm1[c] + nu * lap);
+                    else
+                        rv = dt * nu * lap;
+                    zf_1[c] = zpb_prev[c] + rv;
+                }
             }
         }
 
         // ---- corner psi and face velocities ------------------------------------
-        // pe_here: corner between nodes (i-1, i) x (s-1, s); the lane above's
-        // P1 is the previous row's up1.
-        const double pe_here = 0.25 * (P2 + P1 + up1 + up1_prev);
-        const double pe_dn = shdn(pe_here, 1);
-        T uj_s = 0, ujm_s = 0;  // face b = s, column i
-        const bool fj_ok = !EDGE || (s >= 1 && s <= jj - 1 && i >= 1 && i <= ii - 2);
-        if (fj_ok) {
-            ujm_s = (T)(pe_dn - pe_here);
-            uj_s = ((T)1 + tu) * ujm_s - tu * ujmo_s;
-        }
-        T ui_1 = 0, uim_1 = 0;  // row s-1, face a = i
-        const bool fi_ok = !EDGE || (i >= 1 && i <= ii - 1 && s1r >= 1 && s1r <= jj - 2);
-        if (fi_ok) {
-            uim_1 = (T)(-pe_here + pe_prev);
-            ui_1 = ((T)1 + tu) * uim_1 - tu * uimo_1;
+        // pe_here: corner between nodes (i-1, i) x (s-1, s).
+        double left1[NC], pe_here[NC], pe_dn[NC];  // left1: psi row s-1, column i-1
+        left1[0] = up1_prev0;
+#pragma unroll
+        for (int c = 1; c < NC; ++c) left1[c] = P1[c - 1];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) pe_here[c] = 0.25 * (P2[c] + P1[c] + up1[c] + left1[c]);
+        col_dn(pe_here, pe_dn);
+        T uj_s[NC], ujm_s[NC], ui_1[NC], uim_1[NC];
+        bool fj_ok[NC], fi_ok[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int i = ic[c];
+            uj_s[c] = ujm_s[c] = 0;  // face b = s, column i
+            fj_ok[c] = !EDGE || (s >= 1 && s <= jj - 1 && i >= 1 && i <= ii - 2);
+            if (fj_ok[c]) {
+                ujm_s[c] = (T)(pe_dn[c] - pe_here[c]);
+                uj_s[c] = ((T)1 + tu) * ujm_s[c] - tu * ujmo_s[c];
+            }
+            ui_1[c] = uim_1[c] = 0;  // row s-1, face a = i
+            fi_ok[c] = !EDGE || (i >= 1 && i <= ii - 1 && s1r >= 1 && s1r <= jj - 2);
+            if (fi_ok[c]) {
+                uim_1[c] = (T)(-pe_here[c] + pe_prev[c]);
+                ui_1[c] = ((T)1 + tu) * uim_1[c] - tu * uimo_1[c];
+            }
         }
 
         // ---- extrapolator, j-faces: face b = s-1 -------------------------------
-        T fjn = 0;
+        T fjn[NC];
+        bool bfj_ok[NC];
         const int bf = s - 1;
-        const bool bfj_ok = !EDGE || (bf >= 1 && bf <= jj - 1 && i >= 1 && i <= ii - 2);
-        if (bfj_ok) {
-            const T u1 = UJm1;
-            const bool pos = u1 >= (T)0;
-            if (!EDGE)
-                fjn = extrap(u1, pos ? UJm2 : uj_s, FJm1, pos ? FJm2 : fj_s, pos ? ZFm2 : zf_1, pos ? ZOm2 : zo_1, pos);
-            else if (pos)
-                fjn = bf > 1 ? extrap(u1, UJm2, FJm1, FJm2, ZFm2, ZOm2, true) : extrap_wall(FJm1, ZFm2, ZOm2);
-            else
-                fjn = bf < jj - 1 ? extrap(u1, uj_s, FJm1, fj_s, zf_1, zo_1, false) : extrap_wall(FJm1, zf_1, zo_1);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            fjn[c] = 0;
+            bfj_ok[c] = !EDGE || (bf >= 1 && bf <= jj - 1 && ic[c] >= 1 && ic[c] <= ii - 2);
+            if (bfj_ok[c]) {
+                const T u1 = UJm1[c];
+                const bool pos = u1 >= (T)0;
+                if (!EDGE)
+                    fjn[c] = extrap(u1, pos ? UJm2[c] : uj_s[c], FJm1[c], pos ? FJm2[c] : fj_s[c],
+                                    pos ? ZFm2[c] : zf_1[c], pos ? ZOm2[c] : zo_1[c], pos);
+                else if (pos)
+                    fjn[c] = bf > 1 ? extrap(u1, UJm2[c], FJm1[c], FJm2[c], ZFm2[c], ZOm2[c], true)
+                                    : extrap_wall(FJm1[c], ZFm2[c], ZOm2[c]);
+                else
+                    fjn[c] = bf < jj - 1 ? extrap(u1, uj_s[c], FJm1[c], fj_s[c], zf_1[c], zo_1[c], false)
+                                         : extrap_wall(FJm1[c], zf_1[c], zo_1[c]);
+            }
         }
 
         // ---- extrapolator, i-faces on row s-1: face a = i ------------------------
-        const T ui_up = shup(ui_1, 1), ui_dn = shdn(ui_1, 1);
-        const T fi_up = shup(fio_1, 1), fi_dn = shdn(fio_1, 1);
-        const T zf_up = shup(zf_1, 1), zo_up = shup(zo_1, 1);
-        T fin = 0;
-        if (fi_ok) {
-            const T u1 = ui_1;
-            const bool pos = u1 >= (T)0;
-            if (!EDGE)
-                fin = extrap(u1, pos ? ui_up : ui_dn, fio_1, pos ? fi_up : fi_dn, pos ? zf_up : zf_1, pos ? zo_up : zo_1,
-                             pos);
-            else if (pos)
-                fin = i > 1 ? extrap(u1, ui_up, fio_1, fi_up, zf_up, zo_up, true) : extrap_wall(fio_1, zf_up, zo_up);
-            else
-                fin = i < ii - 1 ? extrap(u1, ui_dn, fio_1, fi_dn, zf_1, zo_1, false) : extrap_wall(fio_1, zf_1, zo_1);
+        T ui_up[NC], ui_dn[NC], fi_up[NC], fi_dn[NC], zf_up[NC], zo_up[NC];
+        col_up(ui_1, ui_up);
+        col_dn(ui_1, ui_dn);
+        col_up(fio_1, fi_up);
+        col_dn(fio_1, fi_dn);
+        col_up(zf_1, zf_up);
+        col_up(zo_1, zo_up);
+        T fin[NC], flj_1[NC], fli_1[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            fin[c] = 0;
+            if (fi_ok[c]) {
+                const int i = ic[c];
+                const T u1 = ui_1[c];
+                const bool pos = u1 >= (T)0;
+                if (!EDGE)
+                    fin[c] = extrap(u1, pos ? ui_up[c] : ui_dn[c], fio_1[c], pos ? fi_up[c] : fi_dn[c],
+                                    pos ? zf_up[c] : zf_1[c], pos ? zo_up[c] : zo_1[c], pos);
+                else if (pos)
+                    fin[c] = i > 1 ? extrap(u1, ui_up[c], fio_1[c], fi_up[c], zf_up[c], zo_up[c], true)
+                                   : extrap_wall(fio_1[c], zf_up[c], zo_up[c]);
+                else
+                    fin[c] = i < ii - 1 ? extrap(u1, ui_dn[c], fio_1[c], fi_dn[c], zf_1[c], zo_1[c], false)
+                                        : extrap_wall(fio_1[c], zf_1[c], zo_1[c]);
+            }
+            flj_1[c] = UJm1[c] * fjn[c];  // flux_j on face s-1
+            fli_1[c] = ui_1[c] * fin[c];  // flux_i on row s-1, face i
         }
-        const T flj_1 = UJm1 * fjn;  // flux_j on face s-1
-        const T fli_1 = ui_1 * fin;  // flux_i on row s-1, face i
 
         // ---- corrector at row o = s-2 -----------------------------------------
         const int o = s - 2;
-        const T fli_dn = shdn(FLI, 1);
-        const T ui_e = PRED ? shdn(UIm2, 1) : (T)0;  // ui on face a = i + 1, row o
-        const bool band_o = (o >= j0 && o < j0 + SH) && (!EDGE || (o >= 0 && o < jj));
-        if (out_i && band_o) {
-            const bool bnd = EDGE && (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
-            T z = ZFm2;
-            if (!bnd) {
-                const T rr = -(fli_dn - FLI + flj_1 - FLJm2);
-                W[o_res + o * pitch] = rr;
-                z = z + hdt * rr;
+        T fli_dn[NC], ui_e[NC];  // flux_i and (PRED) ui on face a = i + 1, row o
+        col_dn(FLI, fli_dn);
+        if (PRED) {
+            col_dn(UIm2, ui_e);
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) ui_e[c] = (T)0;
+        }
+        if ((o >= j0 && o < j0 + SH) && (!EDGE || (o >= 0 && o < jj))) {
+            T z[NC], rr[NC], zz[NC], rbn[NC];
+            bool bnd[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const int i = ic[c];
+                bnd[c] = EDGE && (o == 0 || o == jj - 1 || i == 0 || i == ii - 1);
+                rr[c] = -(fli_dn[c] - FLI[c] + flj_1[c] - FLJm2[c]);
+                z[c] = ZFm2[c];
+                if (!bnd[c]) z[c] = z[c] + hdt * rr[c];
+                zz[c] = rbn[c] = 0;
                 if (PRED) {
                     // Next step: cabaret_predictor (qg3p_aux.F90:1012-1018) and
                     // cabaret_beta (:1051-1059) with this step's ui.
-                    T zz = z + hdt * rr;
-                    const T rbn = dt * ((T)0.5 * (ui_e + UIm2) * beta_l);
-                    zz = zz + ((T)1 + ta) * rbn - ta * rb_2;
-                    W[o_rbn + o * pitch] = rbn;
-                    W[o_zpn + o * pitch] = zz;
+                    zz[c] = z[c] + hdt * rr[c];
+                    rbn[c] = dt * ((T)0.5 * (ui_e[c] + UIm2[c]) * beta_l);
+                    zz[c] = zz[c] + ((T)1 + ta) * rbn[c] - ta * rb_2[c];
                 }
             }
-            W[o_zn + o * pitch] = z;
-            if (avg) psi_av[o_psil + o * pitch] += dt64 * B[o_psil + o * pitch];
+            const int ro = o * pitch;
+            if (!EDGE) {
+                if (out_lane) {
+                    vst<NC>(W + (o_res + ro), rr);
+                    if (PRED) {
+                        vst<NC>(W + (o_rbn + ro), rbn);
+                        vst<NC>(W + (o_zpn + ro), zz);
+                    }
+                    vst<NC>(W + (o_zn + ro), z);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    if (out_lane && in_i[c]) {
+                        if (!bnd[c]) {
+                            W[o_res + c + ro] = rr[c];
+                            if (PRED) {
+                                W[o_rbn + c + ro] = rbn[c];
+                                W[o_zpn + c + ro] = zz[c];
+                            }
+                        }
+                        W[o_zn + c + ro] = z[c];
+                    }
+                }
+            }
+            if (avg && out_lane) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    if (in_i[c]) psi_av[o_psil + c + ro] += dt64 * B[o_psil + c + ro];
+            }
         }
         // ---- owned face writes ---------------------------------------------------
-        if (out_i) {
-            if (fi_ok && s1r >= j0 && s1r < j0 + SH) {
-                W[o_ui + s1r * pitch] = ui_1;
-                W[o_uimon + s1r * pitch] = uim_1;
-                W[o_fin + s1r * pitch] = fin;
-                umax = fmax(umax, fabs(ui_1));
+        const bool row_i = s1r >= j0 && s1r < j0 + SH, row_j = s >= j0 && s < j0 + SH, row_b = bf >= j0 && bf < j0 + SH;
+        if (!EDGE) {
+            if (out_lane) {
+                if (row_i) {
+                    vst<NC>(W + (o_ui + s1r * pitch), ui_1);
+                    vst<NC>(W + (o_uimon + s1r * pitch), uim_1);
+                    vst<NC>(W + (o_fin + s1r * pitch), fin);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) umax = fmax(umax, fabs(ui_1[c]));
+                }
+                if (row_j) {
+                    vst<NC>(W + (o_uj + s * pitch), uj_s);
+                    vst<NC>(W + (o_ujmon + s * pitch), ujm_s);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) umax = fmax(umax, fabs(uj_s[c]));
+                }
+                if (row_b) vst<NC>(W + (o_fjn + bf * pitch), fjn);
             }
-            if (fj_ok && s >= j0 && s < j0 + SH) {
-                W[o_uj + s * pitch] = uj_s;
-                W[o_ujmon + s * pitch] = ujm_s;
-                umax = fmax(umax, fabs(uj_s));
+        } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (out_lane && in_i[c]) {
+                    if (fi_ok[c] && row_i) {
+                        W[o_ui + c + s1r * pitch] = ui_1[c];
+                        W[o_uimon + c + s1r * pitch] = uim_1[c];
+                        W[o_fin + c + s1r * pitch] = fin[c];
+                        umax = fmax(umax, fabs(ui_1[c]));
+                    }
+                    if (fj_ok[c] && row_j) {
+                        W[o_uj + c + s * pitch] = uj_s[c];
+                        W[o_ujmon + c + s * pitch] = ujm_s[c];
+                        umax = fmax(umax, fabs(uj_s[c]));
+                    }
+                    if (bfj_ok[c] && row_b) W[o_fjn + c + bf * pitch] = fjn[c];
+                }
             }
-            if (bfj_ok && bf >= j0 && bf < j0 + SH) W[o_fjn + bf * pitch] = fjn;
         }
         // ---- shift the windows ---------------------------------------------------
-        Rm2 = Rm1;
-        Rm1 = rel_s;
-        ZFm2 = zf_1;
-        ZOm2 = zo_1;
-        UJm2 = UJm1;
-        UJm1 = uj_s;
-        FJm2 = FJm1;
-        FJm1 = fj_s;
-        FLJm2 = flj_1;
-        FLI = fli_1;
-        UIm2 = ui_1;
-        zpb_prev = zpb_s;
-        pm_prev = pm_s;
-        pp_prev = pp_s;
-        pe_prev = pe_here;
-        up1_prev = up1;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            Rm2[c] = Rm1[c];
+            Rm1[c] = rel_s[c];
+            ZFm2[c] = zf_1[c];
+            ZOm2[c] = zo_1[c];
+            UJm2[c] = UJm1[c];
+            UJm1[c] = uj_s[c];
+            FJm2[c] = FJm1[c];
+            FJm1[c] = fj_s[c];
+            FLJm2[c] = flj_1[c];
+            FLI[c] = fli_1[c];
+            UIm2[c] = ui_1[c];
+            zpb_prev[c] = zpb_s[c];
+            pm_prev[c] = pm_s[c];
+            pp_prev[c] = pp_s[c];
+            pe_prev[c] = pe_here[c];
+        }
+        up1_prev0 = up1[0];
     }
     return (double)umax;
 }
@@ -441,38 +694,57 @@ __device__ void finish_step(const Member& Mb, double* red) {
         if (ndt < 1.0e-6) atomicOr(Mb.status, (int)ST_SMALL_DT);
     }
     Mb.counters[1] = 0u;
+    Mb.counters[3] = 0u;  // the sweep queue of k_cabaret_fused
 }
 
-// Three CTAs per SM (at most 168 registers): measured 16 % faster than the
-// unconstrained allocation (two CTAs) at 1025 x 1025 x 3 FP64, 15 % at
-// 2049 x 2049 x 5; four CTAs spill heavily and are slower.
-template <bool PRED, typename T>
-__global__ void __launch_bounds__(CAB_WARPS * 32, 3) k_cabaret_fused(const Member* __restrict__ mems,
-                                                                    const int* __restrict__ prefix, int nmem,
-                                                                    const __grid_constant__ Member one, int use_one) {
+// Three CTAs per SM (at most 168 registers) with one column per lane:
+// measured 16 % faster than the unconstrained allocation (two CTAs) at
+// 1025 x 1025 x 3 FP64, 15 % at 2049 x 2049 x 5; four CTAs spill heavily
+// and are slower.  Two columns per lane: two CTAs per SM, no spills.
+//
+// Persistent: a member's CTAs (at most the resident ones, cabaret_ctas) share
+// its (layer, strip, band) sweeps through a counter (counters[3]); each warp
+// claims the next sweep when it finishes one, so warps run until the queue is
+// empty instead of idling in partly filled CTAs and waves.  The boundary
+// bands (bounds checks and boundary branches: slower) are claimed first, so
+// the last sweeps claimed are interior ones.  The last CTA resets the counter.
+template <bool PRED, typename T, int NC>
+__global__ void __launch_bounds__(CAB_WARPS * 32, NC == 2 ? 2 : 3)
+    k_cabaret_fused(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem,
+                    const __grid_constant__ Member one, int use_one) {
     __shared__ Member Mb;
     __shared__ double red[CAB_WARPS];
     __shared__ int is_last;
-    extern __shared__ __align__(16) double cab_ring[];  // [CAB_WARPS][CAB_RING]
+    extern __shared__ __align__(16) double cab_smem[];  // [CAB_WARPS][cab_ring<T, NC>()]
     pdl_wait();
     int local;
     cta_member(Mb, one, use_one, mems, prefix, nmem, blockIdx.x, &local);
     __syncthreads();
     const int ii = Mb.ii, jj = Mb.jj, L = Mb.L;
     const int SH = Mb.cab_sh;
-    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + SH - 1) / SH;
+    constexpr int SW = cab_sw(NC);
+    const int nstrips = (ii + SW - 1) / SW, nbands = (jj + SH - 1) / SH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int task = local * CAB_WARPS + warp;
+    const int ntasks = nstrips * nbands * L;
+    double* ring = cab_smem + warp * cab_ring<T, NC>();
     double umax = 0.0;
-    if (task < nstrips * nbands * L) {
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = (int)atomicAdd(&Mb.counters[3], 1u);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        if (task >= ntasks) break;
         const int l = task % L;
         const int sb = task / L;
-        const int strip = sb % nstrips, band = sb / nstrips;
-        const int i0 = strip * CAB_SW, j0 = band * SH;
-        const bool interior = (i0 - 2 >= 2) && (i0 + 29 <= ii - 3) && (j0 - 4 >= 2) && (j0 + SH + 3 <= jj - 3);
-        double* ring = cab_ring + warp * CAB_RING;
-        umax = interior ? cab_sweep<false, PRED, T>(Mb, l, i0, j0, lane, ring)
-                        : cab_sweep<true, PRED, T>(Mb, l, i0, j0, lane, ring);
+        const int strip = sb % nstrips, bq = sb / nstrips;
+        const int band = nbands < 3 ? bq : bq == 0 ? 0 : bq == 1 ? nbands - 1 : bq - 1;
+        const int i0 = strip * SW, j0 = band * SH;
+        // Footprint: columns i0-2 .. i0+32NC-3, rows j0-4 .. j0+SH+3.
+        const bool interior =
+            (i0 - 2 >= 2) && (i0 + 32 * NC - 3 <= ii - 3) && (j0 - 4 >= 2) && (j0 + SH + 3 <= jj - 3);
+        const double u = interior ? cab_sweep<false, PRED, T, NC>(Mb, l, i0, j0, lane, ring)
+                                  : cab_sweep<true, PRED, T, NC>(Mb, l, i0, j0, lane, ring);
+        umax = fmax(umax, u);
+        __syncwarp();  // the ring's last reads before the next sweep's copies
     }
     pdl_release();
 
@@ -976,13 +1248,53 @@ __global__ void __launch_bounds__(CT_THREADS, MINB) k_cabaret_tile(const Member*
     if (is_last) finish_step(Mb, red);
 }
 
-int cabaret_ctas(int ii, int jj, int L, int sh) {
-    const int nstrips = (ii + CAB_SW - 1) / CAB_SW, nbands = (jj + sh - 1) / sh;
+// CTAs of k_cabaret_fused resident on the current device at once (at least 1).
+template <typename T, int NC>
+static int cabaret_resident_t() {
+    const size_t bytes = (size_t)CAB_WARPS * cab_ring<T, NC>() * sizeof(double);
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(k_cabaret_fused<true, T, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cabaret_fused<true, T, NC>, CAB_WARPS * 32, bytes) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return std::max(1, per * sms);
+}
+
+int cabaret_ctas_bound(int ii, int jj, int L, int min_sh) {
+    const int sw = cab_sw(1), nstrips = (ii + sw - 1) / sw, nbands = (jj + min_sh - 1) / min_sh;
     return (nstrips * nbands * L + CAB_WARPS - 1) / CAB_WARPS;
+}
+
+int cabaret_ctas(int ii, int jj, int L, int sh, int nc, bool f32) {
+    const int sw = cab_sw(nc);
+    const int nstrips = (ii + sw - 1) / sw, nbands = (jj + sh - 1) / sh;
+    const int need = (nstrips * nbands * L + CAB_WARPS - 1) / CAB_WARPS;
+    const int resident = !f32 ? cabaret_resident_t<double, 1>()
+                         : nc == 2 ? cabaret_resident_t<float, 2>()
+                                   : cabaret_resident_t<float, 1>();
+    return std::min(need, resident);
 }
 
 int cabaret_tile_ctas(int ii, int jj, int L) {
     return ((ii + CT_X - 1) / CT_X) * ((jj + CT_Y - 1) / CT_Y) * L;
+}
+
+template <bool PRED, typename T, int NC>
+static cudaError_t launch_sweeps(const LaunchSet& ls, cudaStream_t st) {
+    const size_t bytes = (size_t)CAB_WARPS * cab_ring<T, NC>() * sizeof(double);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_cabaret_fused<PRED, T, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    cudaError_t le = launch_step_kernel(ls.pdl, k_cabaret_fused<PRED, T, NC>, dim3(ls.ctas_cab),
+                                        dim3(CAB_WARPS * 32), bytes, st, ls.members, ls.prefix_cab, ls.nmem,
+                                        member_arg(ls), member_arg_used(ls));
+    if (le != cudaSuccess) return le;
+    return cudaGetLastError();
 }
 
 template <bool PRED, typename T>
@@ -1003,15 +1315,10 @@ static cudaError_t launch_cab(const LaunchSet& ls, cudaStream_t st) {
         return launch_step_kernel(ls.pdl, kern, dim3(ls.ctas_cab), dim3(CT_THREADS), tb, st, ls.members,
                                   ls.prefix_cab, ls.nmem, member_arg(ls), member_arg_used(ls));
     }
-    const size_t bytes = (size_t)CAB_WARPS * CAB_RING * sizeof(double);
-    cudaError_t e =
-        cudaFuncSetAttribute(k_cabaret_fused<PRED, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return e;
-    cudaError_t le = launch_step_kernel(ls.pdl, k_cabaret_fused<PRED, T>, dim3(ls.ctas_cab), dim3(CAB_WARPS * 32),
-                                        bytes, st, ls.members, ls.prefix_cab, ls.nmem, member_arg(ls),
-                                        member_arg_used(ls));
-    if (le != cudaSuccess) return le;
-    return cudaGetLastError();
+    if constexpr (sizeof(T) == 4) {
+        if (ls.cab_kernel == 2) return launch_sweeps<PRED, T, 2>(ls, st);
+    }
+    return launch_sweeps<PRED, T, 1>(ls, st);
 }
 
 

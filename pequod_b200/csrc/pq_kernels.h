@@ -27,7 +27,7 @@ struct LaunchSet {
     int ctas_dst[2];                  //   (ceil(rows / dst_rows_per_cta) per member)
     int dst_group;                    // row groups per DST CTA (0: automatic)
     int dst_lanes[2];                 // lanes P per DST unit (values per lane M / P), forward [0] / inverse [1]
-    int cab_kernel;                   // CABARET formulation: 0 tiles, 1 warp sweeps
+    int cab_kernel;                   // CABARET formulation: 0 tiles, 1 warp sweeps, 2 two-column sweeps (FP32)
     int periodic;                     // channel periodic in j: every row is transformed
     int sm_count;                     // SMs of the device (persistent grids)
     int pdl;                          // launch the step kernels with programmatic dependent launch
@@ -84,7 +84,11 @@ cudaError_t launch_cabaret_channel(const LaunchSet& ls, int f32, cudaStream_t st
 int channel_ctas(int ii, int jj);
 // The quad eddy covariances of the step (before its CABARET kernel).
 cudaError_t launch_quad(const LaunchSet& ls, int f32, int lf, cudaStream_t st);
-int cabaret_ctas(int ii, int jj, int L, int sh);  // CTAs of the sweep kernel per member (band height sh)
+// CTAs of the (persistent) sweep kernel per member: band height sh, nc
+// columns per lane, FP32 fields when f32; at most the CTAs resident at once.
+int cabaret_ctas(int ii, int jj, int L, int sh, int nc, bool f32);
+// An upper bound of cabaret_ctas over every tuning with bands of at least min_sh rows.
+int cabaret_ctas_bound(int ii, int jj, int L, int min_sh);
 int cabaret_tile_ctas(int ii, int jj, int L);     // CTAs of the tile kernel per member
 cudaError_t launch_rel(const LaunchSet& ls, int f32, cudaStream_t st);
 cudaError_t launch_init_finish(const LaunchSet& ls, int f32, cudaStream_t st);

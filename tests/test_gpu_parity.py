@@ -356,7 +356,9 @@ def test_energy_kats_gpu():
 def test_tile_parameters_do_not_change_results(kernel, band, group, lanes):
     """The CABARET formulation (tiles or warp sweeps), the sweep's band height,
     the DST CTA width and the DST lanes per unit are tuning knobs: results
-    must match the oracle for any choice."""
+    must match the oracle for any choice.  At 129 x 129 the sweeps are
+    mostly boundary sweeps and, with 4-row bands, more than the resident
+    warps, so every warp claims several from the queue."""
     cfg = double_gyre(129, 3)
     g, o = start(cfg, seed=5)
     g.set_tuning(cab_kernel=kernel, cab_band=band, dst_group=group, dst_lanes=lanes, dst_lanes_inv=lanes)
@@ -366,6 +368,39 @@ def test_tile_parameters_do_not_change_results(kernel, band, group, lanes):
     g.step(3)
     o.step(3)
     compare(g, o, TOL_STEP * 10)
+
+
+@pytest.mark.parametrize("ii,kernel,band", [(129, 1, 4), (129, 2, 4), (257, 2, 16), (65, 2, 8), (1025, 1, 16),
+                                            (1025, 2, 32), (1025, 0, 16)])
+def test_mixed_cabaret_formulations_agree(ii, kernel, band):
+    """The mixed form's CABARET formulations -- tiles, sweeps with one and
+    with two columns per lane (interior sweeps with vector loads and stores;
+    boundary sweeps, whose last strip ends mid-lane-pair since ii is odd;
+    at 65 x 65 two strips, both boundary ones) -- give the same fields: psi
+    within 1e-6 of the FP64 oracle after 5 steps, and the state fields of
+    two formulations within 1e-6 of each other (they round FP32 sums in
+    different orders)."""
+    cfg = double_gyre(ii, 3, precision=pq.PREC_MIXED)
+    res = []
+    for k in (kernel, 1 if kernel != 1 else 0):
+        g, o = start(cfg, seed=8)
+        g.set_tuning(cab_kernel=k, cab_band=band)
+        assert g.get_tuning()["cab_kernel"] == k
+        g.step(5)
+        res.append({f: g.get(f) for f in ("psi", "zeta", "ui", "uj", "zeta_fi", "zeta_fj")})
+        if k == kernel:
+            o.step(5)
+            assert rel_l2(g.get("psi"), o.get("psi")) <= 1e-6
+        g.close()
+    for f in res[0]:
+        assert rel_l2(res[0][f], res[1][f]) <= 1e-6, f
+
+
+def test_two_column_sweeps_refused_in_fp64():
+    g = pq.Model(double_gyre(129, 3))
+    with pytest.raises(pq.PQError):
+        g.set_tuning(cab_kernel=2)
+    g.close()
 
 
 def test_state_writes_between_steps():
