@@ -41,7 +41,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -85,7 +84,14 @@ def make_config(ii, layers, dt, precision=0):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+
+    One `nvidia-smi -lms` process samples every 50 ms; it is started, and
+    its first sample awaited, before the timed region, so that no process
+    start and no Python thread competes with the host's launches inside the
+    region (a launch delayed there shows up as device time between the
+    events).  The samples kept are the last one before the region, those
+    during it and the first one after it."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -94,28 +100,48 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.samples = []
-        self._stop = threading.Event()
-        self._t = None
+        self._p = None
+        self._f = None
+        self._n0 = 0
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append(out.stdout.strip().splitlines()[0])
-            except Exception:
-                pass
-            self._stop.wait(0.1)
+    def _lines(self):
+        self._f.seek(0)
+        return [x for x in self._f.read().splitlines() if x.strip()]
+
+    def _wait_lines(self, n, timeout):
+        t = time.time() + timeout
+        while time.time() < t:
+            if len(self._lines()) >= n or (self._p and self._p.poll() is not None):
+                break
+            time.sleep(0.01)
+        return self._lines()
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        import tempfile
+
+        self._f = tempfile.TemporaryFile(mode="w+")
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits", "-lms", "50"], stdout=self._f,
+                                       stderr=subprocess.DEVNULL)
+        except OSError:
+            self._p = None
+            return self
+        self._n0 = len(self._wait_lines(1, 5.0))
         return self
 
     def __exit__(self, *exc):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is None:
+            return
+        lines = self._wait_lines(self._n0 + 1, 1.0)
+        self._p.terminate()
+        try:
+            self._p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self._p.kill()
+            self._p.wait()
+        self.samples = lines[max(0, self._n0 - 1):]
+        self._f.close()
 
     def summary(self):
         sm, mx, reasons = [], None, set()
