@@ -114,6 +114,9 @@ def main(argv=None) -> None:
     ap.add_argument("--pdl", action="store_true", help="programmatic dependent launch of the step kernels")
     ap.add_argument("--dst-algo", type=int, default=0,
                     help="row-DST algorithm of the mixed form: 1 butterfly, 2 tensor-core DST (0: default)")
+    ap.add_argument("--cab-kernel", type=int, default=-1,
+                    help="CABARET formulation: 0 tiles, 1 sweeps, 2 two-column sweeps (mixed; -1: default)")
+    ap.add_argument("--cab-band", type=int, default=0, help="rows per CABARET sweep (0: default)")
     ap.add_argument("--inversions", type=int, default=0,
                     help="instead of stepping: this many pv_inversions of a seeded random zeta")
     a = ap.parse_args(argv)
@@ -133,6 +136,10 @@ def main(argv=None) -> None:
         m.set_tuning(dst_lanes=a.dst_lanes, dst_lanes_inv=a.dst_lanes)
     if a.pdl:
         m.set_tuning(pdl=1)
+    if a.cab_kernel >= 0:
+        m.set_tuning(cab_kernel=a.cab_kernel)
+    if a.cab_band:
+        m.set_tuning(cab_band=a.cab_band)
     m.step(4)
     m.kernel_timing(True)  # eager: one launch per kernel
     for _ in range(a.steps):
