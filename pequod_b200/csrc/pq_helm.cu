@@ -807,11 +807,18 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
 //
 // The strip (Mr = jj - 2 rows x 8 wavenumbers) is staged in shared memory by
 // wavenumber, and within a wavenumber by chunk: row p (0-based) of chunk
-// q = p / R, t = p % R lives at c*CS + q*RS + t with RS = R | 1 and
-// CS = 32*RS + 1 both odd, so the 32 lanes of a warp (one chunk each) hit 32
-// distinct banks and the staging writes of 8 wavenumbers do too.  Lane q of
-// warp c runs the forward and backward Thomas recurrences of its chunk of
-// wavenumber c.
+// q = p / R, t = p % R lives at c*CS + q*RS + t with RS = R | 1 odd and CS
+// from tri_cs, so the 32 lanes of a warp (one chunk each) and the half-warps
+// of the staging and write-back phases hit distinct banks.  Lane q of warp c
+// runs the forward and backward Thomas recurrences of its chunk of
+// wavenumber c, on registers for chunks of 4, 8 or 16 rows (RR).
+// Column stride of the strip in doubles: NQ*RS plus a pad that makes the 16
+// threads of a half-warp of the staging and write-back phases -- KT columns
+// x 16/KT chunks each -- hit 16 distinct 8-byte bank pairs: NQ*RS is a
+// multiple of 16, so c*CS + q*RS = RS*(c*16/KT + q) (mod 16) with RS odd.
+// In the solve phase a warp's lanes (one column, 32 chunks) are RS apart.
+__host__ __device__ inline int tri_cs(int NQ, int RS, int KT) { return NQ * RS + (RS * (16 / KT)) % 16; }
+
 struct PivotRow {
     const double* piv;  // explicit reciprocal pivots, piv[p - 1] for p <= len
     int len;
@@ -833,7 +840,7 @@ struct PivotRow {
 // recurrences never wait on a global load; used whenever both strips fit.
 // The CTA also accumulates the domain mean of the solution in spectral space;
 // the last CTA of a member finishes psiC.
-template <typename S, bool GS>
+template <typename S, bool GS, int RR>
 __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restrict__ mems,
                                                           const int* __restrict__ prefix, int nmem, int do_mean,
                                                           const __grid_constant__ Member one, int use_one) {
@@ -856,7 +863,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     const int Mr = jj - 2;
     const int R = (Mr + NQ - 1) / NQ;
     const int RS = R | 1;
-    const int CS = NQ * RS + 1;
+    const int CS = tri_cs(NQ, RS, KT);
     const bool f32 = sizeof(S) == 4 && m > 0;  // this mode's rows are FP32
     double* spec = ((sizeof(S) == 4) ? Mb.spec64 : reinterpret_cast<double*>(Mb.spec)) + (long long)m * Mb.lstride;
     float* specf = reinterpret_cast<float*>(Mb.spec) + (long long)m * Mb.lstride;
@@ -921,6 +928,10 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
             const float* fsrc = reinterpret_cast<const float*>(sdst) + RS;
             for (int t = 0; t < Rq; ++t) sdst[t] = (double)fsrc[t];
         }
+        // Register sweeps: the rows past the column's end are zeros (after
+        // the widening above, whose staging area they overlap).
+        if (RR > 0 && R == RR)
+            for (int t = max(Rq, 0); t < R; ++t) sdst[t] = 0.0;
     }
     __syncthreads();
 
@@ -948,20 +959,61 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
             return g(p);
         }
     };
+    // Register sweeps (RR > 0 and R == RR: every chunk exactly RR rows, the
+    // column's end padded with rows whose value and pivot are 0) take the
+    // chunk into v[] and its pivots into gv[] (gv[u] = g(a + u - 1)) once,
+    // without the lambda, so that both arrays stay in registers: the loops
+    // below have constant trip counts and no guards (a guard on a chunk's row
+    // count turns a loop bound into a runtime one and the arrays into local
+    // memory).  A padded row's x is 0 (pivot 0), so it changes no real row,
+    // no chunk map that a real row uses, and no column sum.  Four sweeps on
+    // registers: two shared-memory accesses per row instead of eight.
+    const bool regs = RR > 0 && R == RR;
+    constexpr int RV = RR > 0 ? RR : 1;
+    double v[RV] = {}, gv[RV + 1] = {};
+    if constexpr (RR > 0) {
+        if (regs) {
+#pragma unroll
+            for (int u = 0; u <= RR; ++u) {
+                const int p = a + u - 1;
+                double gg;
+                if constexpr (GS)
+                    gg = u >= 1 ? gs[u - 1] : gstrip[c * CS + max(q - 1, 0) * RS + (R - 1)];
+                else
+                    gg = g(max(p, 1));
+                gv[u] = (active && p >= 1 && p <= Mr) ? gg : 0.0;
+            }
+#pragma unroll
+            for (int t = 0; t < RR; ++t) v[t] = s[t];
+        }
+    }
 
     // Forward elimination, local: y~_a = f_a, y~_p = f_p - g_{p-1} y~_{p-1};
     // y_p = y~_p + A_p y_{a-1}, A_a = -g_{a-1}, A_p = -g_{p-1} A_{p-1}.
     double A = 1.0, cend = 0.0;
     if (active && cnt > 0) {
-        double y = s[0];
-        A = (a > 1) ? -G(a - 1) : 0.0;
-        for (int t = 1; t < cnt; ++t) {
-            const double gp = G(a + t - 1);
-            y = s[t] - gp * y;
-            s[t] = y;
-            A = -gp * A;
+        if (regs) {
+            A = (a > 1) ? -gv[0] : 0.0;
+            double y = v[0];
+#pragma unroll
+            for (int t = 1; t < RV; ++t) {
+                const double gp = gv[t];
+                y = v[t] - gp * y;
+                v[t] = y;
+                A = -gp * A;
+            }
+            cend = y;
+        } else {
+            A = (a > 1) ? -G(a - 1) : 0.0;
+            double y = s[0];
+            for (int t = 1; t < cnt; ++t) {
+                const double gp = G(a + t - 1);
+                y = s[t] - gp * y;
+                s[t] = y;
+                A = -gp * A;
+            }
+            cend = y;
         }
-        cend = y;
     }
     // Inclusive scan of the affine chunk maps y_out = c + A y_in in the warp,
     // then the column's earlier warps' totals composed in order.
@@ -989,23 +1041,45 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     // B_b = -g_b, B_p = -g_p B_{p+1}.
     double B = 1.0, cstart = 0.0;
     if (active && cnt > 0) {
-        double Ap = (a > 1) ? -G(a - 1) : 0.0;
-        s[0] = s[0] + Ap * yin;
-        for (int t = 1; t < cnt; ++t) {
-            Ap = -G(a + t - 1) * Ap;
-            s[t] = s[t] + Ap * yin;
+        if (regs) {
+            double Ap = (a > 1) ? -gv[0] : 0.0;
+            v[0] = v[0] + Ap * yin;
+#pragma unroll
+            for (int t = 1; t < RV; ++t) {
+                Ap = -gv[t] * Ap;
+                v[t] = v[t] + Ap * yin;
+            }
+            const double gb = gv[RV];  // g(b)
+            double x = v[RV - 1] * gb;
+            v[RV - 1] = x;
+            B = -gb;
+#pragma unroll
+            for (int t = RV - 2; t >= 0; --t) {
+                const double gp = gv[t + 1];
+                x = (v[t] - x) * gp;
+                v[t] = x;
+                B = -gp * B;
+            }
+            cstart = x;
+        } else {
+            double Ap = (a > 1) ? -G(a - 1) : 0.0;
+            const double gb = G(b);
+            s[0] = s[0] + Ap * yin;
+            for (int t = 1; t < cnt; ++t) {
+                Ap = -G(a + t - 1) * Ap;
+                s[t] = s[t] + Ap * yin;
+            }
+            double x = s[cnt - 1] * gb;
+            s[cnt - 1] = x;
+            B = -gb;
+            for (int t = cnt - 2; t >= 0; --t) {
+                const double gp = G(a + t);
+                x = (s[t] - x) * gp;
+                s[t] = x;
+                B = -gp * B;
+            }
+            cstart = x;
         }
-        const double gb = G(b);
-        double x = s[cnt - 1] * gb;
-        s[cnt - 1] = x;
-        B = -gb;
-        for (int t = cnt - 2; t >= 0; --t) {
-            const double gp = G(a + t);
-            x = (s[t] - x) * gp;
-            s[t] = x;
-            B = -gp * B;
-        }
-        cstart = x;
     }
     // Reverse inclusive scan of x_start = c + B x_next, then the column's
     // later warps' totals composed in order.
@@ -1030,15 +1104,26 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
     const double xin = (lane == 31) ? x0 : nc + nB * x0;
     double lsum = 0.0;
     if (active && cnt > 0) {
-        double Bp = -G(b);
-        double v = s[cnt - 1] + Bp * xin;
-        s[cnt - 1] = v;
-        lsum += v;
-        for (int t = cnt - 2; t >= 0; --t) {
-            Bp = -G(a + t) * Bp;
-            v = s[t] + Bp * xin;
-            s[t] = v;
-            lsum += v;
+        if (regs) {
+            double Bp = -gv[RV];
+#pragma unroll
+            for (int t = RV - 1; t >= 0; --t) {
+                if (t < RV - 1) Bp = -gv[t + 1] * Bp;
+                const double u = v[t] + Bp * xin;
+                lsum += u;
+                s[t] = u;
+            }
+        } else {
+            double Bp = -G(b);
+            double u = s[cnt - 1] + Bp * xin;
+            s[cnt - 1] = u;
+            lsum += u;
+            for (int t = cnt - 2; t >= 0; --t) {
+                Bp = -G(a + t) * Bp;
+                u = s[t] + Bp * xin;
+                s[t] = u;
+                lsum += u;
+            }
         }
     }
     if (Mb.periodic) {
@@ -1180,7 +1265,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tridiag(const Member* __restric
 __host__ __device__ inline size_t tri_smem_bytes(int jj) {
     const int W = tri_warps(jj), KT = 8 / W, NQ = 32 * W;
     const int Mr = jj - 2, R = (Mr + NQ - 1) / NQ, RS = R | 1;
-    return (size_t)KT * (NQ * RS + 1) * sizeof(double);
+    return (size_t)KT * (NQ * RS + 16) * sizeof(double);  // tri_cs pads by at most 15
 }
 
 // ---------------------------------------------------------------------------
@@ -1255,29 +1340,31 @@ cudaError_t launch_dst_inverse(const LaunchSet& ls, int epilogue, int f32, cudaS
     return f32 ? launch_dst<float, PRO_PLAIN, EPI_PV>(ls, st) : launch_dst<double, PRO_PLAIN, EPI_PV>(ls, st);
 }
 
-template <typename S, bool GS>
+template <typename S, bool GS, int RR>
 static cudaError_t launch_tri(const LaunchSet& ls, int do_mean, size_t bytes, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_tridiag<S, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_tridiag<S, GS, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    cudaError_t le = launch_step_kernel(ls.pdl, k_tridiag<S, GS>, dim3(ls.ctas_tri), dim3(TRI_THREADS), bytes, st,
+    cudaError_t le = launch_step_kernel(ls.pdl, k_tridiag<S, GS, RR>, dim3(ls.ctas_tri), dim3(TRI_THREADS), bytes, st,
                                         ls.members, ls.prefix_tri, ls.nmem, do_mean, member_arg(ls),
                                         member_arg_used(ls));
     if (le != cudaSuccess) return le;
     return cudaGetLastError();
 }
 
-// Resident CTAs per SM of k_tridiag<S, GS> with `bytes` of shared memory
+// Resident CTAs per SM of k_tridiag<S, GS, RR> with `bytes` of shared memory
 // (cached per host thread for the last size asked: contexts may be driven
 // from several threads).
-template <typename S, bool GS>
+template <typename S, bool GS, int RR>
 static int tri_resident(size_t bytes) {
     thread_local size_t cached_bytes = 0;
     thread_local int cached = 0;
     if (cached_bytes != bytes) {
         int n = 0;
-        if (cudaFuncSetAttribute(k_tridiag<S, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+        if (cudaFuncSetAttribute(k_tridiag<S, GS, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
                 cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tridiag<S, GS>, TRI_THREADS, bytes) != cudaSuccess) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tridiag<S, GS, RR>, TRI_THREADS, bytes) !=
+                cudaSuccess) {
             cudaGetLastError();
             n = 0;
         }
@@ -1285,6 +1372,13 @@ static int tri_resident(size_t bytes) {
         cached = n;
     }
     return cached;
+}
+
+template <typename S, int RR>
+static cudaError_t launch_tri_gs(const LaunchSet& ls, int do_mean, size_t bytes, size_t gs_limit, cudaStream_t st) {
+    const bool gs =
+        2 * bytes <= gs_limit && tri_resident<S, true, RR>(2 * bytes) >= tri_resident<S, false, RR>(bytes);
+    return gs ? launch_tri<S, true, RR>(ls, do_mean, 2 * bytes, st) : launch_tri<S, false, RR>(ls, do_mean, bytes, st);
 }
 
 cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean_in, int f32, cudaStream_t st) {
@@ -1295,12 +1389,20 @@ cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean_in, int f32, cudaStr
     // the staging costs no resident CTA per SM: measured on B200, staging that
     // lowers occupancy is slower (1025 x 1025 x 3: -2 % FP64, -4 % mixed per
     // step; 2049 x 2049 x 5 FP64: -4 %).
+    // Chunks of 4, 8 or 16 rows are solved in registers (the instance for
+    // the largest member's chunk length; a member whose chunks differ takes
+    // the shared-memory sweeps inside it).
+    const int W = tri_warps(ls.maxJ), R = (ls.maxJ - 2 + 32 * W - 1) / (32 * W);
     if (f32) {
-        const bool gs = 2 * bytes <= 100 * 1024 && tri_resident<float, true>(2 * bytes) >= tri_resident<float, false>(bytes);
-        return gs ? launch_tri<float, true>(ls, do_mean, 2 * bytes, st) : launch_tri<float, false>(ls, do_mean, bytes, st);
+        if (R == 4) return launch_tri_gs<float, 4>(ls, do_mean, bytes, 100 * 1024, st);
+        if (R == 8) return launch_tri_gs<float, 8>(ls, do_mean, bytes, 100 * 1024, st);
+        if (R == 16) return launch_tri_gs<float, 16>(ls, do_mean, bytes, 100 * 1024, st);
+        return launch_tri_gs<float, 0>(ls, do_mean, bytes, 100 * 1024, st);
     }
-    const bool gs = 2 * bytes <= 160 * 1024 && tri_resident<double, true>(2 * bytes) >= tri_resident<double, false>(bytes);
-    return gs ? launch_tri<double, true>(ls, do_mean, 2 * bytes, st) : launch_tri<double, false>(ls, do_mean, bytes, st);
+    if (R == 4) return launch_tri_gs<double, 4>(ls, do_mean, bytes, 160 * 1024, st);
+    if (R == 8) return launch_tri_gs<double, 8>(ls, do_mean, bytes, 160 * 1024, st);
+    if (R == 16) return launch_tri_gs<double, 16>(ls, do_mean, bytes, 160 * 1024, st);
+    return launch_tri_gs<double, 0>(ls, do_mean, bytes, 160 * 1024, st);
 }
 
 }  // namespace pq
