@@ -270,15 +270,17 @@ __device__ __forceinline__ void dst_unit(T* buf, int p, int P, int uid, T* utot,
 // scalars per unit buffer.  Default P (measured per grid size on B200): one
 // warp per unit up to M = 256 (fewer values per lane, more warps in flight,
 // shorter dependent chains), two warps (a named barrier between passes) from
-// M = 512 for the forward and M = 1024 for the inverse transform (whose
-// back-projection epilogue favours one warp at M = 512), when a row's L units
-// fit the kernel's thread bound.
+// M = 512 in both directions (the inverse's 8-value units in a register-
+// capped instance, whose back-projection otherwise held it to two CTAs per
+// SM), when a row's L units fit the kernel's thread bound; dir is kept for
+// callers that ask per direction.
 // Threads a DST CTA may have: 320 for 16 values per lane (five layers of
 // two-warp units at M = 1024), else 256, the bound the others' register
 // use was tuned for.
 __host__ __device__ constexpr int dst_max_threads(int V) { return V == 16 ? 320 : 256; }
 __host__ __device__ inline int dst_lanes_default_hd(int M, int L, int dir) {
-    if (M <= 256 || (dir == 1 && M <= 512)) return M / 2 < 32 ? (M / 2 < 1 ? 1 : M / 2) : 32;
+    (void)dir;
+    if (M <= 256) return M / 2 < 32 ? (M / 2 < 1 ? 1 : M / 2) : 32;
     return L * 64 <= dst_max_threads(M / 64) ? 64 : 32;
 }
 __host__ __device__ inline int dst_rows_per_cta(int P, int c) {
@@ -326,10 +328,11 @@ __device__ __forceinline__ void cp4z(void* dst, const void* src, bool ok) {
 // mixed form: the layer fields and the baroclinic spectral rows are FP32 and
 // transformed in FP32, while the barotropic mode (m = 0) is kept in FP64
 // end to end (spec64), as are the projection, the back-projection and psi.
+// The row-DST kernel's body; k_dst and k_dst_capped below are its kernels.
 template <typename S, int V, int PRO, int EPI>
-__global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
-                                             int nmem, int row_offset, int c, int corr_smem, int psic_here,
-                                             const __grid_constant__ Member one, int use_one, int gemm_bc) {
+__device__ __forceinline__ void dst_body(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem,
+                                         int row_offset, int c, int corr_smem, int psic_here, const Member& one,
+                                         int use_one, int gemm_bc) {
     constexpr bool MX = sizeof(S) == 4;
     __shared__ Member Mb;
     __shared__ double psic_s[PQ_MAXL];                   // closed basin: psiC of the inverse
@@ -800,6 +803,25 @@ __global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __rest
                 }
             }
     }
+}
+
+template <typename S, int V, int PRO, int EPI>
+__global__ void __launch_bounds__(dst_max_threads(V)) k_dst(const Member* __restrict__ mems, const int* __restrict__ prefix,
+                                                             int nmem, int row_offset, int c, int corr_smem,
+                                                             int psic_here, const __grid_constant__ Member one,
+                                                             int use_one, int gemm_bc) {
+    dst_body<S, V, PRO, EPI>(mems, prefix, nmem, row_offset, c, corr_smem, psic_here, one, use_one, gemm_bc);
+}
+// The inverse with 64-lane units of 8 values: registers capped so that three
+// 256-thread CTAs fit (80), hence four of its 192-thread CTAs, where its
+// back-projection would otherwise take 166 registers and allow two; the
+// epilogue spills a little.  (An explicit bound on the other instances would
+// raise their register counts, so they keep the plain one.)
+template <typename S, int V, int PRO, int EPI>
+__global__ void __launch_bounds__(dst_max_threads(V), 3)
+    k_dst_capped(const Member* __restrict__ mems, const int* __restrict__ prefix, int nmem, int row_offset, int c,
+                 int corr_smem, int psic_here, const __grid_constant__ Member one, int use_one, int gemm_bc) {
+    dst_body<S, V, PRO, EPI>(mems, prefix, nmem, row_offset, c, corr_smem, psic_here, one, use_one, gemm_bc);
 }
 
 // ---------------------------------------------------------------------------
@@ -1301,11 +1323,16 @@ static cudaError_t launch_dst_v(const LaunchSet& ls, cudaStream_t st) {
     if (corr_smem) bytes += cbytes;
     if (sizeof(S) == 4 && EPI == EPI_SPEC && PRO != PRO_STEP)
         bytes += (size_t)R * L * ls.maxN * (PRO == PRO_PLAIN ? sizeof(double) : sizeof(float));
-    cudaError_t e =
-        cudaFuncSetAttribute(k_dst<S, V, PRO, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // The inverse with 64-lane units of 8 values takes the register-capped
+    // instance (1025^2 x 3: 41.1 -> 37.3 us mixed, 44.5 -> 41.7 us FP64).
+    void (*kern)(const Member*, const int*, int, int, int, int, int, Member, int, int) = k_dst<S, V, PRO, EPI>;
+    if constexpr (EPI == EPI_PV && V == 8) {
+        if (M / V == 64) kern = k_dst_capped<S, V, PRO, EPI>;
+    }
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     const int dir = (EPI == EPI_SPEC) ? 0 : 1;
-    return launch_step_kernel(ls.pdl, k_dst<S, V, PRO, EPI>, dim3(ls.ctas_dst[dir]), dim3(threads), bytes, st,
+    return launch_step_kernel(ls.pdl, kern, dim3(ls.ctas_dst[dir]), dim3(threads), bytes, st,
                               ls.members, ls.prefix_dst[dir], ls.nmem, (EPI == EPI_SPEC && !ls.periodic) ? 1 : 0,
                               ls.dst_group, corr_smem, (EPI == EPI_PV) ? psic_in_inverse(ls) : 0, member_arg(ls),
                               member_arg_used(ls), sizeof(S) == 4 ? ls.gemm_bc : 0);

@@ -371,35 +371,48 @@ def test_tile_parameters_do_not_change_results(kernel, band, group, lanes):
 
 
 @pytest.mark.parametrize("ii,kernel,band", [(129, 1, 4), (129, 2, 4), (257, 2, 16), (65, 2, 8), (1025, 1, 16),
-                                            (1025, 2, 32), (1025, 0, 16)])
+                                            (1025, 2, 32), (1025, 2, 16), (1025, 0, 16)])
 def test_mixed_cabaret_formulations_agree(ii, kernel, band):
     """The mixed form's CABARET formulations -- tiles, sweeps with one and
     with two columns per lane (interior sweeps with vector loads and stores;
     boundary sweeps, whose last strip ends mid-lane-pair since ii is odd;
-    at 65 x 65 two strips, both boundary ones) -- against the FP64 oracle
-    after 5 steps: psi within 1e-6, and every state field of the chosen
-    formulation no further from the oracle than twice the distance of a
-    second formulation's (plus 1e-7).  The formulations round FP32 sums in
-    different orders, and the face velocities, differences of neighbouring
-    psi, magnify those last-bit differences (3e-6 relative at 1025^2)."""
+    at 65 x 65 two strips, both boundary ones).
+
+    One step from the same state (the oracle's after 4 steps): every field
+    of the formulation under test within 1e-5 of its maximum of a second
+    formulation's (they differ only in how FP32 sums are rounded: 7e-7
+    measured at 1025^2; the velocities come from FP64 psi and agree bit for
+    bit).  Trajectories are compared with the oracle only through psi (5
+    steps, 1e-6): later steps amplify last-bit differences, and where a face
+    velocity is near zero its upwind face value flips, which the FP32
+    residual res shows as local jumps of 1e-3 of its maximum."""
     cfg = double_gyre(ii, 3, precision=pq.PREC_MIXED)
     fields = ("psi", "zeta", "ui", "uj", "zeta_fi", "zeta_fj", "res")
-    err = []
-    o_ref = None
+    ic = pq.make_ic(cfg.ii, cfg.jj, cfg.layers, seed=8, amplitude=1e-7 * cfg.t_scale, sigma=3.0)
+    o = O.Model(O.cfg_from(cfg))
+    o.init(ic)
+    o.step(4)
+    state = {f: o.get(f) for f in ["psi", "zeta", "zeta_old", "ui", "uj", "uimo", "ujmo", "zeta_fi", "zeta_fj",
+                                   "res", "res_beta", "rel"]}
+    o.step(1)
+    psi5 = o.get("psi")
+    out = []
     for k in (kernel, 1 if kernel != 1 else 0):
-        g, o = start(cfg, seed=8)
+        g = pq.Model(cfg)
+        g.init_perturb(ic)
         g.set_tuning(cab_kernel=k, cab_band=band)
         assert g.get_tuning()["cab_kernel"] == k
-        g.step(5)
-        if o_ref is None:
-            o.step(5)
-            o_ref = {f: o.get(f) for f in fields}
-        err.append({f: rel_l2(g.get(f), o_ref[f]) for f in fields})
+        if k == kernel:
+            g.step(5)
+            assert rel_l2(g.get("psi"), psi5) <= 1e-6
+        for f, v in state.items():
+            g.set(f, v)
+        g.step(1)
+        out.append({f: g.get(f) for f in fields})
         g.close()
-    for e in err:
-        assert e["psi"] <= 1e-6, e
     for f in fields:
-        assert err[0][f] <= 2.0 * err[1][f] + 1e-7, (f, err)
+        d = np.abs(out[0][f] - out[1][f]).max()
+        assert d <= 1e-5 * np.abs(out[1][f]).max(), (f, d)
 
 
 def test_two_column_sweeps_refused_in_fp64():
