@@ -1118,6 +1118,7 @@ int pq_step_async(pq_ctx* c, int nsteps) {
 int pq_set_tuning(pq_ctx* c, const pq_tuning* t) {
     if (!c || !t) return PQ_ERR_ARG;
     if (t->cab_band < kMinBand || t->cab_band > kMaxBand) return fail(c, PQ_ERR_ARG, "cab_band out of range");
+    CK(cudaSetDevice(c->device));  // the CTA counts below query this device's occupancy
     CK(cudaStreamSynchronize(c->stream));
     if (t->dst_group < 0 || c->L * t->dst_group > 8) return fail(c, PQ_ERR_ARG, "dst_group out of range");
     if (t->cab_kernel < 0 || t->cab_kernel > 2) return fail(c, PQ_ERR_ARG, "cab_kernel out of range");
