@@ -1401,11 +1401,20 @@ static int tri_resident(size_t bytes) {
     return cached;
 }
 
+// Register sweeps read each pivot once per row, from the pivot table: staging
+// the pivots beside the strip measured slower for them (1025^2 x 3: 33.4 us
+// without, 36.5 with, mixed; 31.8 / 35.2 FP64), so only the shared-memory
+// sweeps stage them.
 template <typename S, int RR>
 static cudaError_t launch_tri_gs(const LaunchSet& ls, int do_mean, size_t bytes, size_t gs_limit, cudaStream_t st) {
-    const bool gs =
-        2 * bytes <= gs_limit && tri_resident<S, true, RR>(2 * bytes) >= tri_resident<S, false, RR>(bytes);
-    return gs ? launch_tri<S, true, RR>(ls, do_mean, 2 * bytes, st) : launch_tri<S, false, RR>(ls, do_mean, bytes, st);
+    if constexpr (RR > 0) {
+        return launch_tri<S, false, RR>(ls, do_mean, bytes, st);
+    } else {
+        const bool gs =
+            2 * bytes <= gs_limit && tri_resident<S, true, RR>(2 * bytes) >= tri_resident<S, false, RR>(bytes);
+        return gs ? launch_tri<S, true, RR>(ls, do_mean, 2 * bytes, st)
+                  : launch_tri<S, false, RR>(ls, do_mean, bytes, st);
+    }
 }
 
 cudaError_t launch_tridiag(const LaunchSet& ls, int do_mean_in, int f32, cudaStream_t st) {
