@@ -67,3 +67,31 @@ def test_ensemble_rules():
     bad = double_gyre(65, 3, 900.0, adapt_dt=1)
     with pytest.raises(pq.PQError):
         pq.Ensemble(bad, 2)
+
+
+@pytest.mark.parametrize("prec,kernel", [(pq.PREC_FP64, 1), (pq.PREC_MIXED, 1), (pq.PREC_MIXED, 2)])
+def test_ensemble_persistent_sweeps_equal_runs_alone(prec, kernel):
+    """The CABARET step as persistent warp sweeps inside the merged launch
+    (one and two columns per lane; 8-row bands at 257 x 257 give more
+    sweeps than there are resident warps): each member's CTAs claim only
+    that member's sweeps, from its own queue, so every member still steps
+    exactly as it does alone."""
+    cfg = double_gyre(257, 3, 900.0, precision=prec)
+    n = 3
+    ens = pq.Ensemble(cfg, n)
+    for k in range(n):
+        ens.members[k].set_tuning(cab_kernel=kernel, cab_band=8)
+        ens.init(k, ic(cfg, 60 + k))
+    ens.step(1)
+    ens.step(4)
+    for k in range(n):
+        assert ens.members[k].get_tuning()["cab_kernel"] == kernel
+        m = pq.Model(cfg)
+        m.set_tuning(cab_kernel=kernel, cab_band=8)
+        m.init_perturb(ic(cfg, 60 + k))
+        m.step(5)
+        for f in ("psi", "zeta", "res", "ui", "uj", "zeta_fi"):
+            a, b = ens.members[k].get(f), m.get(f)
+            assert rel_l2(a, b) <= (1e-13 if prec == pq.PREC_FP64 else 1e-12), (k, f, rel_l2(a, b))
+        m.close()
+    ens.close()
