@@ -53,6 +53,25 @@ def test_server_mix_equals_alone():
     srv.close()
 
 
+def test_server_persistent_sweeps_equal_alone():
+    """Runs above 700 rows take the persistent CABARET sweeps: in the server's
+    merged launch each run's CTAs claim only that run's sweeps, so every
+    result is still bit-identical to the run alone (two 1025 x 1025 runs
+    of each form, different step counts)."""
+    srv = pq.Server(16 << 30)
+    ids = []
+    for prec, seed, n in ((pq.PREC_MIXED, 21, 3), (pq.PREC_MIXED, 22, 5), (pq.PREC_FP64, 23, 4),
+                          (pq.PREC_FP64, 24, 2)):
+        cfg = cfg_of(1025, 3, prec)
+        ids.append((srv.submit(cfg, ic_of(cfg, seed), n), cfg, seed, n))
+    srv.run_until_done(max_steps=2)
+    for rid, cfg, seed, n in ids:
+        assert srv.status(rid) == 2
+        psi, _ = srv.collect(rid)
+        assert np.array_equal(psi, alone(cfg, ic_of(cfg, seed), n)), (cfg.ii, n)
+    srv.close()
+
+
 def test_server_budget_staging_and_pool():
     cfg = cfg_of(65, 3)
     probe = pq.Model(cfg)
